@@ -1,0 +1,150 @@
+/*
+ * rtpg.h -- C ABI of rtlib_b200, a B200-native (sm_100a) implementation of RTLib's
+ * path-guiding hot path.
+ *
+ * Conventions (the reference has no C ABI; these replace its C++ template API):
+ *   - every function returns int: 0 (RTPG_OK) on success, a negative RTPG_E* code on error;
+ *     rtpg_last_error() returns a message for the calling thread's last error;
+ *   - handles are opaque; all array arguments are DEVICE pointers unless the parameter name
+ *     starts with "host_"; sizes are element counts;
+ *   - "stream" is a cudaStream_t passed as void* (NULL = legacy default stream); calls are
+ *     asynchronous on that stream unless documented otherwise;
+ *   - a handle is not thread-safe: one host thread (or external synchronisation) per handle;
+ *   - device-side failures (capacity exhausted, fixed-point saturation) never trap: they set
+ *     bits in the handle's device status word, which rtpg_*_status() reads (synchronising).
+ */
+#ifndef RTPG_H
+#define RTPG_H
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- errors */
+#define RTPG_OK 0
+#define RTPG_EINVAL -1   /* bad argument */
+#define RTPG_ENOMEM -2   /* device allocation failed */
+#define RTPG_ECUDA -3    /* CUDA runtime error */
+#define RTPG_ECAPACITY -4 /* a fixed capacity would be exceeded */
+#define RTPG_ESTATE -5   /* call not valid in the current state */
+
+/* device status bits (rtpg_sdtree_status / rtpg_mqt_status / ...) */
+#define RTPG_STATUS_FX_SATURATED 0x1u      /* a fixed-point value or sum saturated */
+#define RTPG_STATUS_DTREE_NODE_CAP 0x2u    /* a quadtree reset hit the per-tree node cap */
+#define RTPG_STATUS_STREE_CAPACITY 0x4u    /* spatial refine skipped: STree/DTree capacity */
+#define RTPG_STATUS_DNODE_CAPACITY 0x8u    /* quadtree pool capacity exhausted */
+#define RTPG_STATUS_HASH_FULL 0x10u        /* a hash bucket was full (slot = UINT32_MAX) */
+#define RTPG_STATUS_QUEUE_OVERFLOW 0x20u   /* a wavefront queue overflowed */
+
+const char* rtpg_last_error(void);
+/* Library version as MAJOR*10000 + MINOR*100 + PATCH. */
+int rtpg_version(void);
+/* Fixed limits compiled into the library: per-quadtree node cap, maximum quadtree depth,
+ * hash bucket size. */
+int rtpg_query_limits(uint32_t* host_dtree_node_cap, uint32_t* host_max_dtree_depth, uint32_t* host_hash_block);
+
+/* ================================================================ SD-tree
+ * Replaces RTSTreeWrapperT / STreeT / DTreeWrapperT of RTLib
+ * (RTLib/Src/Ext/OPX7/Include/RTLib/Ext/OPX7/Utils/OPX7UtilsPathGuiding.h, "PG.h" below).
+ * The whole tree lives on the GPU: there is no Upload/Download round trip
+ * (PG.h:1353-1615); build, refine and reset run as kernels. */
+typedef struct rtpg_sdtree rtpg_sdtree;
+
+typedef struct rtpg_sdtree_caps {
+    uint32_t max_stree_nodes;       /* default 1<<20 */
+    uint32_t max_dtrees;            /* default 1<<19 */
+    uint32_t max_dtree_nodes_total; /* quadtree node pool (building and sampling), default 1<<23 */
+    int32_t fixed_point_bits;       /* sums are int64(value * 2^bits); default 24 */
+} rtpg_sdtree_caps;
+
+/* RTSTreeWrapperT(ctx, aabbMin, aabbMax, maxDTreeDepth = 20, fraction = 0.3), PG.h:1352.
+ * The AABB is cubified to its largest extent (RTSTreeT ctor, PG.h:1211-1217).  caps may be
+ * NULL for the defaults.  The new tree is one leaf with a one-node quadtree (PG.h:880-887). */
+int rtpg_sdtree_create(const float host_aabb_min[3], const float host_aabb_max[3], uint32_t max_dtree_depth,
+                       float fraction, const rtpg_sdtree_caps* caps, rtpg_sdtree** out);
+/* RTSTreeWrapperT::Destroy, PG.h:1616-1633 (also frees the handle). */
+int rtpg_sdtree_destroy(rtpg_sdtree* h);
+/* RTSTreeWrapperT::Clear, PG.h:1634-1636: back to a single leaf with an empty quadtree. */
+int rtpg_sdtree_clear(rtpg_sdtree* h, void* stream);
+
+/* Batch of radiance records: STreeT::GetDTreeWrapper (PG.h:639-648) + DTreeWrapperT::Record
+ * (PG.h:514-520) + DTreeT::Impl<DirectionalFilterNearest>::RecordIrradiance (PG.h:417-428) +
+ * DTreeNodeT::Record (PG.h:113-125), i.e. what TraceVertexT::Commit<Nearest,Nearest> records
+ * (PG.h:830-866).  pos: n x float3; dir: n x float2 canonical (dir_is_canonical = 1) or
+ * n x float3 unit vectors; radiance: n floats (the channel-averaged local radiance); wo_pdf,
+ * stat_weight, is_delta: optional (NULL = 1, 1, 0).  Sums accumulate as int64 fixed point
+ * with 64-bit integer atomics, so the result does not depend on record order. */
+int rtpg_sdtree_record(rtpg_sdtree* h, int64_t n, const float* pos, const float* dir, int dir_is_canonical,
+                       const float* radiance, const float* wo_pdf, const float* stat_weight,
+                       const uint8_t* is_delta, void* stream);
+/* RTSTreeWrapperT::Build, PG.h:1657-1663 -> RTDTreeWrapperT::Build, PG.h:1086-1090:
+ * bottom-up sums, area and root sum of every building quadtree, then sampling = building. */
+int rtpg_sdtree_build(rtpg_sdtree* h, void* stream);
+/* RTSTreeT::Refine(spatial_threshold, max_mb) (PG.h:1275-1311) followed by
+ * RTDTreeWrapperT::Reset(max_dtree_depth, dtree_subdiv_th) on every leaf (PG.h:1091-1094,
+ * 888-947).  max_mb < 0 disables the memory-footprint guard. */
+int rtpg_sdtree_refine(rtpg_sdtree* h, uint64_t spatial_threshold, int32_t max_mb, float dtree_subdiv_th,
+                       void* stream);
+/* RTSTreeWrapperT::Reset(iter, samplesPerPass), PG.h:1645-1656: no-op for iter <= 0, else
+ * threshold = size_t(sqrt(2^iter * spp / 4) * 4000), refine with 2000 MB, subdiv 0.01. */
+int rtpg_sdtree_reset(rtpg_sdtree* h, int32_t iteration, int32_t samples_per_pass, void* stream);
+/* Guided sample + pdf for a batch of points, as the closest-hit program uses the guide
+ * (SimpleGuide.cu:322-369): leaf = STreeT::GetDTreeWrapper(pos); uv = DTreeT::Sample(rng)
+ * (PG.h:478-484, 229-277); pdf_uv = DTreeT::Pdf(uv) (PG.h:485-490).  One Xorshift32 per
+ * query seeded with seeds[i] (or, seeds == NULL, with pcg1d(seed_base + i) | 1).
+ * Optional outputs (NULL = not written): out_uv n x float2, out_pdf_uv n, out_dir n x float3
+ * = normalize(canonical_to_dir(uv)), out_pdf_dir n = DTreeWrapperT::Pdf(out_dir). */
+int rtpg_sdtree_sample_pdf(rtpg_sdtree* h, int64_t n, const float* pos, const uint32_t* seeds, uint32_t seed_base,
+                           float* out_uv, float* out_pdf_uv, float* out_dir, float* out_pdf_dir, void* stream);
+/* DTreeT::Pdf (PG.h:485-490) at given canonical points (dir_is_canonical = 1) or
+ * directions (DTreeWrapperT::Pdf, PG.h:529-531). */
+int rtpg_sdtree_pdf(rtpg_sdtree* h, int64_t n, const float* pos, const float* dir, int dir_is_canonical,
+                    float* out_pdf, void* stream);
+/* Sizes of the current tree (synchronises the stream). */
+int rtpg_sdtree_stats(rtpg_sdtree* h, uint32_t* host_stree_nodes, uint32_t* host_dtrees,
+                      uint32_t* host_dtree_nodes, void* stream);
+/* RTSTreeWrapperT::GetMemoryFootPrint (PG.h:1729-1748) analogue: bytes in use on the device. */
+int rtpg_sdtree_memory_footprint(rtpg_sdtree* h, uint64_t* host_bytes);
+/* Device status word (RTPG_STATUS_* bits), synchronising; clear = 1 resets it. */
+int rtpg_sdtree_status(rtpg_sdtree* h, uint32_t* host_status, int clear, void* stream);
+/* Canonical export (download for inspection, like RTSTreeWrapperT::Dump, PG.h:1749-1756).
+ * Pre-order streams: stree_mask (1 interior / 0 leaf, child 0 first); per leaf 4 floats
+ * {building stat-weight, sampling sum, sampling area, sampling stat-weight} and the node
+ * count of its quadtree; per quadtree node (pre-order, quadrant 0..3) a child mask byte and
+ * 4 float sums.  sampling = 1 exports the sampling trees, 0 the building trees.
+ * Call with NULL buffers to get the sizes (host_sizes[3] = {stree nodes, leaves,
+ * quadtree nodes}), then with buffers of those sizes.  Synchronises the stream. */
+int rtpg_sdtree_export(rtpg_sdtree* h, int sampling, int64_t* host_sizes, uint8_t* host_stree_mask,
+                       float* host_leaf_scalars, int64_t* host_leaf_counts, uint8_t* host_dnode_mask,
+                       float* host_dnode_sums, void* stream);
+
+/* ---------------------------------------------------------------- pass controller
+ * RTSTreeControllerT (PG.h:1769-1920): the doubling pass schedule.  Host-side state only;
+ * begin/end call rtpg_sdtree_reset / rtpg_sdtree_build on the tree at the right moments. */
+typedef struct rtpg_controller rtpg_controller;
+#define RTPG_TRACE_RECORD 0
+#define RTPG_TRACE_RECORD_AND_SAMPLE 1
+#define RTPG_TRACE_SAMPLE 2
+int rtpg_controller_create(rtpg_sdtree* tree, uint32_t sample_for_budget, uint32_t iteration_for_built,
+                           float ratio_for_budget, uint32_t samples_per_launch, rtpg_controller** out);
+int rtpg_controller_destroy(rtpg_controller* c);
+int rtpg_controller_start(rtpg_controller* c);
+int rtpg_controller_begin(rtpg_controller* c, void* stream);
+int rtpg_controller_end(rtpg_controller* c, void* stream);
+/* state (RTPG_TRACE_*), current iteration, samples done in this pass, whether tracing is
+ * still executing. */
+int rtpg_controller_get(rtpg_controller* c, int32_t* host_state, uint32_t* host_iteration,
+                        uint32_t* host_samples_in_pass, int32_t* host_executing);
+
+#ifdef __cplusplus
+}
+#endif
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+#endif /* RTPG_H */

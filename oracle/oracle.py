@@ -1,0 +1,372 @@
+"""ctypes bindings to the two CPU checkers.  TEST INFRASTRUCTURE ONLY.
+
+* ``Oracle``    -- oracle/_build/liboracle.so, this project's C restatement (rtpg_oracle.c);
+* ``Reference`` -- oracle/_ref/libref_rtlib.so, RTLib's own guiding code built on the host
+                   (oracle/ref), available where the reference tree was present at build
+                   time or where the prebuilt library travelled with the repository.
+
+Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg may import this.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "_build", "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libref_rtlib.so")
+
+_f = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+_u32 = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
+_u64 = np.ctypeslib.ndpointer(dtype=np.uint64, flags="C_CONTIGUOUS")
+_i64 = np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")
+_u8 = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
+P = C.c_void_p
+
+
+def build_oracle() -> None:
+    subprocess.check_call(["make", "-s", "-C", HERE], stdout=subprocess.DEVNULL)
+
+
+def build_reference() -> bool:
+    """Build oracle/_ref from the reference tree when it is present.  Returns whether the
+    library exists afterwards."""
+    ref = os.environ.get("RTLIB_REFERENCE", "/root/reference")
+    if os.path.isdir(ref):
+        subprocess.check_call(["make", "-s", "-C", os.path.join(HERE, "ref"), f"REF={ref}"],
+                              stdout=subprocess.DEVNULL)
+    return os.path.exists(REF_SO)
+
+
+def _opt(a, dtype):
+    if a is None:
+        return None
+    return np.ascontiguousarray(a, dtype=dtype).ctypes.data_as(P)
+
+
+class _Export:
+    def __init__(self, smask, scalars, counts, dmask, dsums):
+        self.smask, self.scalars, self.counts, self.dmask, self.dsums = smask, scalars, counts, dmask, dsums
+
+    @property
+    def topology(self):
+        return (self.smask.tobytes(), self.counts.tobytes(), self.dmask.tobytes())
+
+
+class Oracle:
+    """SD-tree / hash grid / Morton quadtree restated in C (rtpg_oracle.c)."""
+
+    def __init__(self):
+        if not os.path.exists(ORACLE_SO):
+            build_oracle()
+        L = self.L = C.CDLL(ORACLE_SO)
+        L.or_sdtree_new.restype = P
+        L.or_sdtree_new.argtypes = [_f, _f, C.c_int, C.c_float, C.c_int, C.c_uint32]
+        L.or_sdtree_free.argtypes = [P]
+        L.or_sdtree_status.argtypes = [P]
+        L.or_sdtree_status.restype = C.c_uint32
+        L.or_sdtree_record.argtypes = [P, C.c_int64, _f, _f, _f, P, P, P]
+        L.or_sdtree_build.argtypes = [P]
+        L.or_sdtree_refine.argtypes = [P, C.c_uint64, C.c_int]
+        L.or_sdtree_export.argtypes = [P, C.c_int, _i64]
+        L.or_sdtree_export_copy.argtypes = [_u8, _f, _i64, _u8, _f]
+        L.or_sdtree_sample_pdf.argtypes = [P, C.c_int64, _f, _u32, P, P, P, P]
+        L.or_sdtree_pdf.argtypes = [P, C.c_int64, _f, _f, _f]
+        L.or_sdtree_num_stree_nodes.argtypes = [P]
+        L.or_sdtree_num_stree_nodes.restype = C.c_uint32
+        L.or_sdtree_num_dtrees.argtypes = [P]
+        L.or_sdtree_num_dtrees.restype = C.c_uint32
+        L.or_pcg1d.argtypes = [C.c_uint32]
+        L.or_pcg1d.restype = C.c_uint32
+        L.or_dir_to_canonical.argtypes = [C.c_int64, _f, _f]
+        L.or_hashgrid_insert.argtypes = [C.c_int64, _f, _f, _f, _u32, C.c_uint32, _u32, _u32]
+        L.or_hashgrid_lookup.argtypes = [C.c_int64, _f, _f, _f, _u32, C.c_uint32, _u32, _u32]
+        L.or_mhash_insert.argtypes = [C.c_int64, _f, _f, _f, _u32, C.c_uint32, _u64, _u32, P]
+        L.or_mhash_lookup.argtypes = [C.c_int64, _f, _f, _f, _u32, C.c_uint32, _u64, _u32]
+        L.or_morton3.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32]
+        L.or_morton3.restype = C.c_uint64
+        L.or_morton2.argtypes = [C.c_uint32, C.c_uint32]
+        L.or_morton2.restype = C.c_uint32
+        L.or_mqt_record.argtypes = [C.c_int64, C.c_uint32, C.c_int, _i64, _u32, _f, _f, P]
+        L.or_mqt_build.argtypes = [C.c_uint32, C.c_uint32, C.c_int, _i64, _f]
+        L.or_mqt_sample_pdf.argtypes = [C.c_int64, C.c_uint32, _f, _u32, _u32, _f, _f, P]
+
+    # ---- SD-tree
+    def sdtree(self, aabb_min, aabb_max, max_dtree_depth=20, subdiv_th=0.01, frac_bits=24, node_cap=65535):
+        return OracleSDTree(self, aabb_min, aabb_max, max_dtree_depth, subdiv_th, frac_bits, node_cap)
+
+    def dir_to_canonical(self, d):
+        d = np.ascontiguousarray(d, dtype=np.float32)
+        out = np.empty((d.shape[0], 2), np.float32)
+        self.L.or_dir_to_canonical(d.shape[0], d, out)
+        return out
+
+    # ---- hash grid (reference keying)
+    def hashgrid_insert(self, pos, off, size, bounds, nslots, cur):
+        pos = np.ascontiguousarray(pos, np.float32)
+        out = np.empty(pos.shape[0], np.uint32)
+        self.L.or_hashgrid_insert(pos.shape[0], pos, np.asarray(off, np.float32), np.asarray(size, np.float32),
+                                  np.asarray(bounds, np.uint32), nslots, cur, out)
+        return out
+
+    def hashgrid_lookup(self, pos, off, size, bounds, nslots, prv):
+        pos = np.ascontiguousarray(pos, np.float32)
+        out = np.empty(pos.shape[0], np.uint32)
+        self.L.or_hashgrid_lookup(pos.shape[0], pos, np.asarray(off, np.float32), np.asarray(size, np.float32),
+                                  np.asarray(bounds, np.uint32), nslots, prv, out)
+        return out
+
+    def mhash_insert(self, pos, off, size, bounds, nslots, cur):
+        pos = np.ascontiguousarray(pos, np.float32)
+        out = np.empty(pos.shape[0], np.uint32)
+        keys = np.empty(pos.shape[0], np.uint64)
+        self.L.or_mhash_insert(pos.shape[0], pos, np.asarray(off, np.float32), np.asarray(size, np.float32),
+                               np.asarray(bounds, np.uint32), nslots, cur, out, keys.ctypes.data_as(P))
+        return out, keys
+
+    def mhash_lookup(self, pos, off, size, bounds, nslots, prv):
+        pos = np.ascontiguousarray(pos, np.float32)
+        out = np.empty(pos.shape[0], np.uint32)
+        self.L.or_mhash_lookup(pos.shape[0], pos, np.asarray(off, np.float32), np.asarray(size, np.float32),
+                               np.asarray(bounds, np.uint32), nslots, prv, out)
+        return out
+
+    # ---- Morton quadtree
+    def mqt_record(self, level, frac_bits, leaves, cell, uv, value):
+        st = np.zeros(1, np.uint32)
+        self.L.or_mqt_record(cell.shape[0], level, frac_bits, leaves, np.ascontiguousarray(cell, np.uint32),
+                             np.ascontiguousarray(uv, np.float32), np.ascontiguousarray(value, np.float32),
+                             st.ctypes.data_as(P))
+        return int(st[0])
+
+    def mqt_build(self, ncells, level, frac_bits, leaves):
+        per = ((1 << (2 * (level + 1))) - 1) // 3
+        pyr = np.empty(ncells * per, np.float32)
+        self.L.or_mqt_build(ncells, level, frac_bits, leaves, pyr)
+        return pyr
+
+    def mqt_sample_pdf(self, level, pyramid, cell, seeds):
+        n = cell.shape[0]
+        uv = np.empty((n, 2), np.float32)
+        pdf = np.empty(n, np.float32)
+        pe = np.empty(n, np.float32)
+        self.L.or_mqt_sample_pdf(n, level, pyramid, np.ascontiguousarray(cell, np.uint32),
+                                 np.ascontiguousarray(seeds, np.uint32), uv, pdf, pe.ctypes.data_as(P))
+        return uv, pdf, pe
+
+
+class OracleSDTree:
+    def __init__(self, o, mn, mx, max_depth, th, bits, cap):
+        self.o, self.L = o, o.L
+        self.h = self.L.or_sdtree_new(np.asarray(mn, np.float32), np.asarray(mx, np.float32), max_depth, th, bits, cap)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.L.or_sdtree_free(self.h)
+            self.h = None
+
+    def record(self, pos, uv, radiance, wo_pdf=None, stat_w=None, is_delta=None):
+        pos = np.ascontiguousarray(pos, np.float32)
+        self.L.or_sdtree_record(self.h, pos.shape[0], pos, np.ascontiguousarray(uv, np.float32),
+                                np.ascontiguousarray(radiance, np.float32), _opt(wo_pdf, np.float32),
+                                _opt(stat_w, np.float32), _opt(is_delta, np.uint8))
+
+    def build(self):
+        self.L.or_sdtree_build(self.h)
+
+    def refine(self, spatial_th, max_mb=2000):
+        self.L.or_sdtree_refine(self.h, int(spatial_th), int(max_mb))
+
+    @property
+    def status(self):
+        return int(self.L.or_sdtree_status(self.h))
+
+    def num_stree_nodes(self):
+        return int(self.L.or_sdtree_num_stree_nodes(self.h))
+
+    def num_dtrees(self):
+        return int(self.L.or_sdtree_num_dtrees(self.h))
+
+    def export(self, sampling=True):
+        sz = np.zeros(5, np.int64)
+        self.L.or_sdtree_export(self.h, int(sampling), sz)
+        e = _Export(np.empty(sz[0], np.uint8), np.empty(sz[1] * 4, np.float32), np.empty(sz[1], np.int64),
+                    np.empty(sz[2], np.uint8), np.empty(sz[2] * 4, np.float32))
+        self.L.or_sdtree_export_copy(e.smask, e.scalars, e.counts, e.dmask, e.dsums)
+        return e
+
+    def sample_pdf(self, pos, seeds, with_dir=False):
+        pos = np.ascontiguousarray(pos, np.float32)
+        n = pos.shape[0]
+        uv = np.empty((n, 2), np.float32)
+        pdf = np.empty(n, np.float32)
+        d = np.empty((n, 3), np.float32) if with_dir else None
+        pd = np.empty(n, np.float32) if with_dir else None
+        self.L.or_sdtree_sample_pdf(self.h, n, pos, np.ascontiguousarray(seeds, np.uint32), uv.ctypes.data_as(P),
+                                    pdf.ctypes.data_as(P), _opt(d, np.float32) if with_dir else None,
+                                    pd.ctypes.data_as(P) if with_dir else None)
+        if with_dir:
+            # _opt copies; use the buffers directly instead
+            d2 = np.empty((n, 3), np.float32)
+            pd2 = np.empty(n, np.float32)
+            self.L.or_sdtree_sample_pdf(self.h, n, pos, np.ascontiguousarray(seeds, np.uint32), None, None,
+                                        d2.ctypes.data_as(P), pd2.ctypes.data_as(P))
+            return uv, pdf, d2, pd2
+        return uv, pdf
+
+    def pdf(self, pos, uv):
+        pos = np.ascontiguousarray(pos, np.float32)
+        out = np.empty(pos.shape[0], np.float32)
+        self.L.or_sdtree_pdf(self.h, pos.shape[0], pos, np.ascontiguousarray(uv, np.float32), out)
+        return out
+
+
+class Reference:
+    """RTLib's own guiding code (oracle/_ref/libref_rtlib.so)."""
+
+    def __init__(self):
+        if not os.path.exists(REF_SO) and not build_reference():
+            raise FileNotFoundError(REF_SO)
+        L = self.L = C.CDLL(REF_SO)
+        L.ref_sdtree_new.restype = P
+        L.ref_sdtree_new.argtypes = [_f, _f]
+        L.ref_sdtree_free.argtypes = [P]
+        L.ref_sdtree_record.argtypes = [P, C.c_int64, _f, P, P, _f, P, P, P]
+        L.ref_sdtree_build.argtypes = [P]
+        L.ref_sdtree_refine.argtypes = [P, C.c_uint64, C.c_int, C.c_int, C.c_float]
+        L.ref_sdtree_threshold.argtypes = [C.c_int, C.c_int]
+        L.ref_sdtree_threshold.restype = C.c_uint64
+        L.ref_sdtree_num_stree_nodes.argtypes = [P]
+        L.ref_sdtree_num_stree_nodes.restype = C.c_int64
+        L.ref_sdtree_export.argtypes = [P, C.c_int, _i64]
+        L.ref_sdtree_export_copy.argtypes = [_u8, _f, _i64, _u8, _f]
+        L.ref_sdtree_sample_pdf.argtypes = [P, C.c_int64, _f, _u32, P, P, P, P, C.c_int]
+        L.ref_sdtree_pdf.argtypes = [P, C.c_int64, _f, _f, _f]
+        L.ref_pcg1d.argtypes = [C.c_uint32]
+        L.ref_pcg1d.restype = C.c_uint32
+        L.ref_xxhash.argtypes = [C.c_uint32]
+        L.ref_xxhash.restype = C.c_uint32
+        L.ref_xorshift32_floats.argtypes = [C.c_uint32, C.c_int, _f, _u32]
+        L.ref_dir_to_canonical.argtypes = [C.c_int64, _f, _f]
+        L.ref_canonical_to_dir.argtypes = [C.c_int64, _f, _f]
+        L.ref_hashgrid_insert.argtypes = [C.c_int64, _f, _f, _f, _u32, C.c_uint32, _u32, _u32]
+        L.ref_hashgrid_lookup.argtypes = [C.c_int64, _f, _f, _f, _u32, C.c_uint32, _u32, _u32]
+        L.ref_mqt_record.argtypes = [C.c_int64, C.c_uint32, C.c_uint32, _f, _u32, _f, _f]
+        L.ref_mqt_build.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, _f]
+        L.ref_mqt_sample_pdf.argtypes = [C.c_int64, C.c_uint32, C.c_uint32, _f, _u32, _u32, _f, _f, P]
+        L.ref_morton2_code.argtypes = [C.c_uint32, C.c_uint32]
+        L.ref_morton2_code.restype = C.c_uint32
+
+    def sdtree(self, mn, mx):
+        return RefSDTree(self, mn, mx)
+
+    def xorshift32_floats(self, seed, n):
+        out = np.empty(n, np.float32)
+        st = np.zeros(1, np.uint32)
+        self.L.ref_xorshift32_floats(seed, n, out, st)
+        return out, int(st[0])
+
+    def dir_to_canonical(self, d):
+        d = np.ascontiguousarray(d, dtype=np.float32)
+        out = np.empty((d.shape[0], 2), np.float32)
+        self.L.ref_dir_to_canonical(d.shape[0], d, out)
+        return out
+
+    def hashgrid_insert(self, pos, off, size, bounds, nslots, cur):
+        pos = np.ascontiguousarray(pos, np.float32)
+        out = np.empty(pos.shape[0], np.uint32)
+        self.L.ref_hashgrid_insert(pos.shape[0], pos, np.asarray(off, np.float32), np.asarray(size, np.float32),
+                                   np.asarray(bounds, np.uint32), nslots, cur, out)
+        return out
+
+    def hashgrid_lookup(self, pos, off, size, bounds, nslots, prv):
+        pos = np.ascontiguousarray(pos, np.float32)
+        out = np.empty(pos.shape[0], np.uint32)
+        self.L.ref_hashgrid_lookup(pos.shape[0], pos, np.asarray(off, np.float32), np.asarray(size, np.float32),
+                                   np.asarray(bounds, np.uint32), nslots, prv, out)
+        return out
+
+    def mqt_record(self, level, weights, cell, uv, value):
+        per = ((1 << (2 * (6 + 1))) - 1) // 3
+        self.L.ref_mqt_record(cell.shape[0], level, per, weights, np.ascontiguousarray(cell, np.uint32),
+                              np.ascontiguousarray(uv, np.float32), np.ascontiguousarray(value, np.float32))
+
+    def mqt_build(self, ncells, level, weights):
+        per = ((1 << (2 * (6 + 1))) - 1) // 3
+        self.L.ref_mqt_build(ncells, level, per, weights)
+
+    def mqt_sample_pdf(self, level, weights, cell, seeds):
+        per = ((1 << (2 * (6 + 1))) - 1) // 3
+        n = cell.shape[0]
+        uv = np.empty((n, 2), np.float32)
+        pdf = np.empty(n, np.float32)
+        pe = np.empty(n, np.float32)
+        self.L.ref_mqt_sample_pdf(n, level, per, weights, np.ascontiguousarray(cell, np.uint32),
+                                  np.ascontiguousarray(seeds, np.uint32), uv, pdf, pe.ctypes.data_as(P))
+        return uv, pdf, pe
+
+
+class RefSDTree:
+    def __init__(self, r, mn, mx):
+        self.L = r.L
+        self.h = self.L.ref_sdtree_new(np.asarray(mn, np.float32), np.asarray(mx, np.float32))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.L.ref_sdtree_free(self.h)
+            self.h = None
+
+    def record(self, pos, uv=None, radiance=None, wo_pdf=None, stat_w=None, is_delta=None, dir_xyz=None):
+        pos = np.ascontiguousarray(pos, np.float32)
+        uvp = np.ascontiguousarray(uv, np.float32) if uv is not None else None
+        dp = np.ascontiguousarray(dir_xyz, np.float32) if dir_xyz is not None else None
+        wo = np.ascontiguousarray(wo_pdf, np.float32) if wo_pdf is not None else None
+        sw = np.ascontiguousarray(stat_w, np.float32) if stat_w is not None else None
+        dl = np.ascontiguousarray(is_delta, np.uint8) if is_delta is not None else None
+        self.L.ref_sdtree_record(self.h, pos.shape[0], pos,
+                                 uvp.ctypes.data_as(P) if uvp is not None else None,
+                                 dp.ctypes.data_as(P) if dp is not None else None,
+                                 np.ascontiguousarray(radiance, np.float32),
+                                 wo.ctypes.data_as(P) if wo is not None else None,
+                                 sw.ctypes.data_as(P) if sw is not None else None,
+                                 dl.ctypes.data_as(P) if dl is not None else None)
+
+    def build(self):
+        self.L.ref_sdtree_build(self.h)
+
+    def refine(self, spatial_th, max_mb=2000, max_dtree_depth=20, subdiv_th=0.01):
+        self.L.ref_sdtree_refine(self.h, int(spatial_th), int(max_mb), int(max_dtree_depth), float(subdiv_th))
+
+    def num_stree_nodes(self):
+        return int(self.L.ref_sdtree_num_stree_nodes(self.h))
+
+    def export(self, sampling=True):
+        sz = np.zeros(5, np.int64)
+        self.L.ref_sdtree_export(self.h, int(sampling), sz)
+        e = _Export(np.empty(sz[0], np.uint8), np.empty(sz[1] * 4, np.float32), np.empty(sz[1], np.int64),
+                    np.empty(sz[2], np.uint8), np.empty(sz[2] * 4, np.float32))
+        self.L.ref_sdtree_export_copy(e.smask, e.scalars, e.counts, e.dmask, e.dsums)
+        return e
+
+    def sample_pdf(self, pos, seeds, threads=1, with_dir=False):
+        pos = np.ascontiguousarray(pos, np.float32)
+        n = pos.shape[0]
+        uv = np.empty((n, 2), np.float32)
+        pdf = np.empty(n, np.float32)
+        d = np.empty((n, 3), np.float32)
+        pd = np.empty(n, np.float32)
+        self.L.ref_sdtree_sample_pdf(self.h, n, pos, np.ascontiguousarray(seeds, np.uint32), uv.ctypes.data_as(P),
+                                     pdf.ctypes.data_as(P), d.ctypes.data_as(P) if with_dir else None,
+                                     pd.ctypes.data_as(P) if with_dir else None, int(threads))
+        if with_dir:
+            return uv, pdf, d, pd
+        return uv, pdf
+
+    def pdf(self, pos, uv):
+        pos = np.ascontiguousarray(pos, np.float32)
+        out = np.empty(pos.shape[0], np.float32)
+        self.L.ref_sdtree_pdf(self.h, pos.shape[0], pos, np.ascontiguousarray(uv, np.float32), out)
+        return out

@@ -1,0 +1,743 @@
+/*
+ * rtpg_oracle.c -- CPU restatement of RTLib's path-guiding hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This is the checker for the CUDA kernels of rtlib_b200: only
+ * tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg load it.  The product
+ * never calls it and has no CPU fallback.
+ *
+ * Parity is pinned: tests/test_oracle_vs_reference.py checks this restatement against
+ * RTLib's OWN code compiled on the host (oracle/ref, built into oracle/_ref) on identical
+ * seeded inputs -- topology bit-exact, sums and pdfs within float-rounding tolerance
+ * (RTLib sums in float, this restatement in 64-bit fixed point).
+ *
+ * It restates, with the same float expression order as the reference:
+ *   SD-tree      OPX7UtilsPathGuiding.h (PG.h below)
+ *     spatial descent   STreeT::GetDTreeWrapper / STreeNodeT::GetChildIdx   PG.h:639-648,546-569
+ *     record            DTreeWrapperT::Record -> DTreeT::Impl<Nearest>::RecordIrradiance
+ *                       -> DTreeNodeT::Record                                PG.h:514-520,417-428,113-125
+ *     build             RTDTreeT::Build / DTreeNodeT::Build,GetArea          PG.h:948-957,356-369,342-355
+ *     spatial refine    RTSTreeT::Refine / SubDivide / ShallSplit            PG.h:1275-1311,1231-1247,1270-1274
+ *     quadtree reset    RTDTreeT::Reset                                      PG.h:888-947
+ *     sample / pdf      DTreeT::Sample,Pdf,GetMean / DTreeNodeT::Sample,Pdf  PG.h:478-490,447-451,229-320
+ *   math / rng   Xorshift32 (Random.h:37-51), to_uniform_float (Math.h:682-694),
+ *                dir_to_canonical / canonical_to_dir (VectorFunction.h:5698-5720), pcg1d (Hash.h:13-18)
+ *   hash grid    DoubleBufferedHashGrid3T FindFromCur / FindFromPrv           OPX7UtilsGrid.h:157-353
+ *   Morton tree  MortonQuadTreeT Record / SampleAndPdf / Pdf, Morton2Utils    OPX7UtilsMorton.h:39-449
+ *                mortonBuildKernel pyramid                                    OPX7UtilsMortonBuild.cu:2-16
+ *
+ * The two deliberate differences from the reference are the ones the CUDA path makes:
+ *   1. sums are accumulated as int64 fixed point (value * 2^frac_bits, round to nearest)
+ *      so that they do not depend on record order; they become float when a tree is built;
+ *   2. quadtree nodes are numbered breadth first (the reference numbers them depth first,
+ *      last child first); export_* write a canonical pre-order stream so topologies compare
+ *      independently of numbering.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define O_INV_2PI ((float)0.15915494309189533576888376337251436203445964574046)
+#define O_2PI ((float)6.283185307179586476925286766559)
+
+/* ------------------------------------------------------------------ rng / math */
+static inline uint32_t xs32_next(uint32_t* s) {
+    uint32_t y = *s;
+    y = y ^ (y << 13);
+    y = y ^ (y >> 17);
+    return *s = y ^ (y << 5);
+}
+static inline float to_uniform_float(uint32_t v) {
+    uint32_t b = (v >> 9) | (0x7Fu << 23);
+    float f;
+    memcpy(&f, &b, 4);
+    return f - 1.0f;
+}
+static inline float rnd1(uint32_t* s) { return to_uniform_float(xs32_next(s)); }
+
+uint32_t or_pcg1d(uint32_t input) {
+    uint32_t state = input * 747796405u + 2891336453u;
+    uint32_t word = ((state >> ((state >> 28u) + 4u)) ^ state) * 277803737u;
+    return (word >> 22u) ^ word;
+}
+
+void or_dir_to_canonical(int64_t n, const float* d, float* uv) {
+    for (int64_t i = 0; i < n; ++i) {
+        float x = d[3 * i], y = d[3 * i + 1], z = d[3 * i + 2];
+        if (!isfinite(x) || !isfinite(y) || !isfinite(z)) { uv[2 * i] = 0.0f; uv[2 * i + 1] = 0.0f; continue; }
+        z = z < -1.0f ? -1.0f : (z > 1.0f ? 1.0f : z);
+        float phi = atan2f(y, x);
+        while (phi < 0.0f) phi += O_2PI;
+        uv[2 * i] = (z + 1.0f) / 2.0f;
+        uv[2 * i + 1] = phi * O_INV_2PI;
+    }
+}
+static void canonical_to_dir(float u, float v, float* out) {
+    const float cosTheta = 2.0f * u - 1.0f;
+    const float sinTheta = sqrtf(1.0f - cosTheta * cosTheta);
+    const float phi = O_2PI * v;
+    out[0] = sinTheta * cosf(phi);
+    out[1] = sinTheta * sinf(phi);
+    out[2] = cosTheta;
+}
+static void normalize3(float* v) {
+    float l = sqrtf((v[0] * v[0]) + (v[1] * v[1]) + (v[2] * v[2]));
+    v[0] /= l; v[1] /= l; v[2] /= l;
+}
+
+/* fixed point: round-to-nearest of v * 2^bits, saturated */
+static inline int64_t to_fx(float v, int bits, uint32_t* status) {
+    float s = ldexpf(v, bits);
+    if (!(s < 9.2233720368547758e18f)) { *status |= 1u; return INT64_MAX; }
+    return llrintf(s);
+}
+static inline float fx_to_float(int64_t x, int bits) { return ldexpf((float)x, -bits); }
+
+/* ------------------------------------------------------------------ SD-tree */
+typedef struct { uint32_t c[4]; } OChild; /* local child index, 0 = leaf */
+
+typedef struct {
+    /* building tree */
+    uint32_t nb;
+    OChild* bch;
+    int64_t* bsum; /* 4 per node */
+    int64_t bstatw;
+    float bstatw_f; /* building stat-weight as the reference would hold it during Refine */
+    /* sampling tree */
+    uint32_t ns;
+    OChild* sch;
+    float* ssum;
+    float s_sum, s_area, s_statw;
+    int max_depth_seen;
+} ODTree;
+
+typedef struct {
+    int32_t child0; /* first child (children are child0, child0+1); -1 for a leaf */
+    int32_t dtree;  /* leaf: dtree index */
+} OSNode;
+
+typedef struct {
+    float mn[3], mx[3];
+    int frac_bits;
+    int max_dtree_depth;
+    float subdiv_th;
+    uint32_t node_cap;
+    OSNode* st;
+    uint32_t nst, capst;
+    ODTree* dt;
+    uint32_t ndt, capdt;
+    uint32_t status;
+} OSDTree;
+
+static void dtree_init_single(ODTree* d) {
+    memset(d, 0, sizeof(*d));
+    d->nb = 1;
+    d->bch = (OChild*)calloc(1, sizeof(OChild));
+    d->bsum = (int64_t*)calloc(4, sizeof(int64_t));
+    d->ns = 1;
+    d->sch = (OChild*)calloc(1, sizeof(OChild));
+    d->ssum = (float*)calloc(4, sizeof(float));
+}
+static void dtree_free(ODTree* d) { free(d->bch); free(d->bsum); free(d->sch); free(d->ssum); }
+
+static uint32_t add_dtree(OSDTree* t) {
+    if (t->ndt == t->capdt) {
+        t->capdt = t->capdt ? 2 * t->capdt : 64;
+        t->dt = (ODTree*)realloc(t->dt, sizeof(ODTree) * t->capdt);
+    }
+    return t->ndt++;
+}
+static uint32_t add_snodes(OSDTree* t, uint32_t k) {
+    while (t->nst + k > t->capst) {
+        t->capst = t->capst ? 2 * t->capst : 256;
+        t->st = (OSNode*)realloc(t->st, sizeof(OSNode) * t->capst);
+    }
+    uint32_t r = t->nst;
+    t->nst += k;
+    return r;
+}
+
+/* RTSTreeT constructor (PG.h:1211-1217): the AABB is cubified to its largest extent. */
+void* or_sdtree_new(const float* mn, const float* mx, int max_dtree_depth, float subdiv_th, int frac_bits,
+                    uint32_t node_cap) {
+    OSDTree* t = (OSDTree*)calloc(1, sizeof(OSDTree));
+    float size[3] = {mx[0] - mn[0], mx[1] - mn[1], mx[2] - mn[2]};
+    float m = size[0] > size[1] ? size[0] : size[1];
+    m = m > size[2] ? m : size[2];
+    for (int k = 0; k < 3; ++k) { t->mn[k] = mn[k]; t->mx[k] = mn[k] + m; }
+    t->frac_bits = frac_bits;
+    t->max_dtree_depth = max_dtree_depth;
+    t->subdiv_th = subdiv_th;
+    t->node_cap = node_cap;
+    uint32_t r = add_snodes(t, 1);
+    uint32_t d = add_dtree(t);
+    dtree_init_single(&t->dt[d]);
+    t->st[r].child0 = -1;
+    t->st[r].dtree = (int32_t)d;
+    return t;
+}
+void or_sdtree_free(void* h) {
+    OSDTree* t = (OSDTree*)h;
+    for (uint32_t i = 0; i < t->ndt; ++i) dtree_free(&t->dt[i]);
+    free(t->dt); free(t->st); free(t);
+}
+uint32_t or_sdtree_status(void* h) { return ((OSDTree*)h)->status; }
+
+/* STreeT::GetDTreeWrapper (PG.h:639-648) + STreeNodeT::GetChildIdx (PG.h:546-552).
+ * The axis of a node is its depth mod 3 (root 0, SubDivide gives children (axis+1)%3,
+ * PG.h:1240).  The child index int(2p) is clamped to [0,1] so that p == 1 or positions
+ * outside the AABB stay in bounds (the reference would index out of range there). */
+static int32_t leaf_dtree(const OSDTree* t, const float* pos) {
+    float size[3] = {t->mx[0] - t->mn[0], t->mx[1] - t->mn[1], t->mx[2] - t->mn[2]};
+    float p[3];
+    for (int k = 0; k < 3; ++k) p[k] = (pos[k] - t->mn[k]) / size[k];
+    uint32_t n = 0;
+    int axis = 0;
+    while (t->st[n].child0 >= 0) {
+        float v = p[axis] * 2.0f;
+        int idx = (int)v;
+        idx = idx < 0 ? 0 : (idx > 1 ? 1 : idx);
+        p[axis] = v - (float)idx;
+        n = (uint32_t)t->st[n].child0 + (uint32_t)idx;
+        axis = axis == 2 ? 0 : axis + 1;
+    }
+    return t->st[n].dtree;
+}
+
+/* DTreeNodeT::GetChildIdx (PG.h:69-82). */
+static inline int quad_child(float* p) {
+    int r = 0;
+    for (int i = 0; i < 2; ++i) {
+        if (p[i] < 0.5f) p[i] *= 2.0f;
+        else { p[i] = 2.0f * p[i] - 1.0f; r |= 1 << i; }
+    }
+    return r;
+}
+
+/* DTreeWrapperT::Record (PG.h:514-520) -> Impl<Nearest>::RecordIrradiance (PG.h:417-428)
+ * -> DTreeNodeT::Record (PG.h:113-125), with fixed-point accumulation. */
+void or_sdtree_record(void* h, int64_t n, const float* pos, const float* uv, const float* radiance,
+                      const float* wo_pdf, const float* stat_w, const uint8_t* is_delta) {
+    OSDTree* t = (OSDTree*)h;
+    for (int64_t i = 0; i < n; ++i) {
+        if (is_delta && is_delta[i]) continue;
+        const float wo = wo_pdf ? wo_pdf[i] : 1.0f;
+        const float sw = stat_w ? stat_w[i] : 1.0f;
+        const float irr = radiance[i] / wo;
+        ODTree* d = &t->dt[leaf_dtree(t, pos + 3 * i)];
+        if (!(isfinite(sw) && sw > 0.0f)) continue;
+        d->bstatw += to_fx(sw, t->frac_bits, &t->status);
+        if (!(isfinite(irr) && irr > 0.0f)) continue;
+        const float v = irr * sw;
+        float p[2] = {uv[2 * i], uv[2 * i + 1]};
+        uint32_t cur = 0;
+        int idx = quad_child(p);
+        while (d->bch[cur].c[idx] != 0) {
+            cur = d->bch[cur].c[idx];
+            idx = quad_child(p);
+        }
+        d->bsum[4 * cur + idx] += to_fx(v, t->frac_bits, &t->status);
+    }
+}
+
+/* RTDTreeT::Build (PG.h:948-957): bottom-up sums (nodes are breadth-first, so every child
+ * has a larger index than its parent), area (DTreeNodeT::GetArea, PG.h:342-355) in the same
+ * float order, root sum, then RTDTreeWrapperT::Build's "sampling = building" (PG.h:1086-1090). */
+static void dtree_build(ODTree* d, int bits) {
+    for (int64_t n = (int64_t)d->nb - 1; n >= 0; --n) {
+        for (int i = 0; i < 4; ++i) {
+            uint32_t c = d->bch[n].c[i];
+            if (c) d->bsum[4 * n + i] = d->bsum[4 * c] + d->bsum[4 * c + 1] + d->bsum[4 * c + 2] + d->bsum[4 * c + 3];
+        }
+    }
+    free(d->sch); free(d->ssum);
+    d->ns = d->nb;
+    d->sch = (OChild*)malloc(sizeof(OChild) * d->nb);
+    d->ssum = (float*)malloc(sizeof(float) * 4 * d->nb);
+    memcpy(d->sch, d->bch, sizeof(OChild) * d->nb);
+    for (uint32_t k = 0; k < 4 * d->nb; ++k) d->ssum[k] = fx_to_float(d->bsum[k], bits);
+    float* area = (float*)malloc(sizeof(float) * d->nb);
+    for (int64_t n = (int64_t)d->nb - 1; n >= 0; --n) {
+        float a = 0.0f;
+        for (int i = 0; i < 4; ++i) {
+            if (d->ssum[4 * n + i] > 0.0f) {
+                uint32_t c = d->sch[n].c[i];
+                if (!c) a += 1.0f / 4.0f;
+                else a += area[c] / 4.0f;
+            }
+        }
+        area[n] = a;
+    }
+    d->s_area = area[0];
+    free(area);
+    float s = 0.0f;
+    for (int i = 0; i < 4; ++i) s += d->ssum[i];
+    d->s_sum = s;
+    d->s_statw = fx_to_float(d->bstatw, bits);
+    d->bstatw_f = d->s_statw;
+}
+void or_sdtree_build(void* h) {
+    OSDTree* t = (OSDTree*)h;
+    for (uint32_t i = 0; i < t->ndt; ++i) dtree_build(&t->dt[i], t->frac_bits);
+}
+
+/* RTDTreeT::Reset (PG.h:888-947), breadth first.  A node either mirrors a node of the
+ * previous (sampling) tree, or -- below a previous leaf quadrant -- is a "copy of itself"
+ * whose four sums are the parent quadrant's sum / 4 (PG.h:926-933). */
+typedef struct { uint32_t src; float vsum; int depth; } OSrc; /* src == UINT32_MAX: virtual */
+
+static void dtree_reset(ODTree* d, int max_depth, float th, uint32_t cap, uint32_t* status) {
+    const float total = d->s_sum;
+    uint32_t capn = 64, nn = 1;
+    OChild* ch = (OChild*)calloc(capn, sizeof(OChild));
+    OSrc* src = (OSrc*)malloc(sizeof(OSrc) * capn);
+    src[0].src = 0; src[0].vsum = 0.0f; src[0].depth = 1;
+    int maxd = 0;
+    int full = 0;
+    for (uint32_t n = 0; n < nn && !full; ++n) {
+        const OSrc s = src[n];
+        if (s.depth > maxd) maxd = s.depth;
+        for (int i = 0; i < 4; ++i) {
+            const float si = s.src != UINT32_MAX ? d->ssum[4 * s.src + i] : s.vsum;
+            const float fraction = total > 0.0f ? si / total : powf(0.25f, (float)s.depth);
+            if (s.depth < max_depth && fraction > th) {
+                if (nn == cap) { *status |= 2u; full = 1; break; }
+                if (nn == capn) {
+                    capn *= 2;
+                    ch = (OChild*)realloc(ch, sizeof(OChild) * capn);
+                    src = (OSrc*)realloc(src, sizeof(OSrc) * capn);
+                }
+                memset(&ch[nn], 0, sizeof(OChild));
+                if (s.src != UINT32_MAX && d->sch[s.src].c[i] != 0) { src[nn].src = d->sch[s.src].c[i]; src[nn].vsum = 0.0f; }
+                else { src[nn].src = UINT32_MAX; src[nn].vsum = si / 4.0f; }
+                src[nn].depth = s.depth + 1;
+                ch[n].c[i] = nn;
+                ++nn;
+            }
+        }
+    }
+    free(src);
+    free(d->bch); free(d->bsum);
+    d->nb = nn;
+    d->bch = ch;
+    d->bsum = (int64_t*)calloc(4 * (size_t)nn, sizeof(int64_t));
+    d->bstatw = 0;
+    d->bstatw_f = 0.0f;
+    d->max_depth_seen = maxd;
+}
+
+/* RTSTreeT::Refine (PG.h:1275-1311): the memory-footprint guard, then every leaf whose
+ * building stat-weight exceeds the threshold splits; SubDivide (PG.h:1231-1247) gives both
+ * children a copy of the DTree wrapper and half the stat-weight, so the split cascades into a
+ * complete subtree of depth k = number of halvings while w > th.  Then every leaf runs
+ * RTDTreeWrapperT::Reset(maxDepth, subdivTh) (PG.h:1091-1094, RTSTreeWrapperT::Reset
+ * PG.h:1650-1655).  The footprint counts 24-byte DTree nodes and 24-byte DTree headers for
+ * the building and sampling tree of every STree node, as GetApproxMemoryFootPrint does
+ * (PG.h:970-972,1052-1054); interior nodes hold default one-node trees. */
+void or_sdtree_refine(void* h, uint64_t spatial_th, int max_mb) {
+    OSDTree* t = (OSDTree*)h;
+    int do_spatial = 1;
+    if (max_mb >= 0) {
+        uint64_t fp = 0;
+        for (uint32_t i = 0; i < t->nst; ++i) {
+            if (t->st[i].child0 >= 0) fp += 96;
+            else { const ODTree* d = &t->dt[t->st[i].dtree]; fp += 24ull * (d->nb + d->ns) + 48; }
+        }
+        if (fp / 1000000 >= (uint64_t)max_mb) do_spatial = 0;
+    }
+    const float thf = (float)spatial_th;
+    if (do_spatial) {
+        /* pre-order walk with an explicit stack so that new children are visited too */
+        uint32_t cap = 64, top = 0;
+        uint32_t* stack = (uint32_t*)malloc(sizeof(uint32_t) * cap);
+        stack[top++] = 0;
+        while (top) {
+            uint32_t n = stack[--top];
+            if (t->st[n].child0 < 0) {
+                ODTree* d = &t->dt[t->st[n].dtree];
+                if (d->bstatw_f > thf) {
+                    const uint32_t c = add_snodes(t, 2);
+                    const int32_t dold = t->st[n].dtree;
+                    const uint32_t dnew = add_dtree(t);
+                    d = &t->dt[dold];
+                    ODTree* e = &t->dt[dnew];
+                    *e = *d;
+                    e->bch = (OChild*)malloc(sizeof(OChild) * d->nb); memcpy(e->bch, d->bch, sizeof(OChild) * d->nb);
+                    e->bsum = (int64_t*)malloc(sizeof(int64_t) * 4 * d->nb); memcpy(e->bsum, d->bsum, sizeof(int64_t) * 4 * d->nb);
+                    e->sch = (OChild*)malloc(sizeof(OChild) * d->ns); memcpy(e->sch, d->sch, sizeof(OChild) * d->ns);
+                    e->ssum = (float*)malloc(sizeof(float) * 4 * d->ns); memcpy(e->ssum, d->ssum, sizeof(float) * 4 * d->ns);
+                    d->bstatw_f = d->bstatw_f / 2.0f;
+                    e->bstatw_f = d->bstatw_f;
+                    t->st[n].child0 = (int32_t)c;
+                    t->st[n].dtree = -1;
+                    t->st[c].child0 = -1; t->st[c].dtree = dold;
+                    t->st[c + 1].child0 = -1; t->st[c + 1].dtree = (int32_t)dnew;
+                }
+            }
+            if (t->st[n].child0 >= 0) {
+                if (top + 2 > cap) { cap *= 2; stack = (uint32_t*)realloc(stack, sizeof(uint32_t) * cap); }
+                stack[top++] = (uint32_t)t->st[n].child0;
+                stack[top++] = (uint32_t)t->st[n].child0 + 1;
+            }
+        }
+        free(stack);
+    }
+    for (uint32_t i = 0; i < t->ndt; ++i)
+        dtree_reset(&t->dt[i], t->max_dtree_depth, t->subdiv_th, t->node_cap, &t->status);
+}
+
+/* canonical export, same stream format as the product's rtpg_sdtree_export */
+typedef struct { uint8_t* smask; float* scalars; int64_t* counts; uint8_t* dmask; float* dsums;
+                 int64_t ns, nl, nd, cs, cl, cd; } OExp;
+static void grow(void** p, int64_t* cap, int64_t need, size_t el) {
+    if (need <= *cap) return;
+    while (*cap < need) *cap = *cap ? 2 * *cap : 1024;
+    *p = realloc(*p, (size_t)*cap * el);
+}
+static void exp_dtree(OExp* e, const OChild* ch, const float* sums_f, const int64_t* sums_i, int bits, uint32_t n) {
+    grow((void**)&e->dmask, &e->cd, e->nd + 1, 1);
+    int64_t cd4 = e->cd;  /* dsums sized 4 * cd */
+    e->dsums = (float*)realloc(e->dsums, (size_t)cd4 * 4 * sizeof(float));
+    uint8_t m = 0;
+    for (int i = 0; i < 4; ++i) if (ch[n].c[i]) m |= (uint8_t)(1u << i);
+    e->dmask[e->nd] = m;
+    for (int i = 0; i < 4; ++i) e->dsums[4 * e->nd + i] = sums_f ? sums_f[4 * n + i] : fx_to_float(sums_i[4 * n + i], bits);
+    e->nd++;
+    for (int i = 0; i < 4; ++i) if (ch[n].c[i]) exp_dtree(e, ch, sums_f, sums_i, bits, ch[n].c[i]);
+}
+static void exp_stree(OExp* e, const OSDTree* t, uint32_t n, int sampling) {
+    grow((void**)&e->smask, &e->cs, e->ns + 1, 1);
+    const OSNode s = t->st[n];
+    e->smask[e->ns++] = s.child0 >= 0 ? 1 : 0;
+    if (s.child0 < 0) {
+        const ODTree* d = &t->dt[s.dtree];
+        grow((void**)&e->counts, &e->cl, e->nl + 1, sizeof(int64_t));
+        e->scalars = (float*)realloc(e->scalars, (size_t)e->cl * 4 * sizeof(float));
+        e->scalars[4 * e->nl + 0] = fx_to_float(d->bstatw, t->frac_bits);
+        e->scalars[4 * e->nl + 1] = d->s_sum;
+        e->scalars[4 * e->nl + 2] = d->s_area;
+        e->scalars[4 * e->nl + 3] = d->s_statw;
+        const int64_t before = e->nd;
+        if (sampling) exp_dtree(e, d->sch, d->ssum, NULL, t->frac_bits, 0);
+        else exp_dtree(e, d->bch, NULL, d->bsum, t->frac_bits, 0);
+        e->counts[e->nl++] = e->nd - before;
+        return;
+    }
+    exp_stree(e, t, (uint32_t)s.child0, sampling);
+    exp_stree(e, t, (uint32_t)s.child0 + 1, sampling);
+}
+static OExp g_exp;
+void or_sdtree_export(void* h, int sampling, int64_t* sizes) {
+    free(g_exp.smask); free(g_exp.scalars); free(g_exp.counts); free(g_exp.dmask); free(g_exp.dsums);
+    memset(&g_exp, 0, sizeof(g_exp));
+    exp_stree(&g_exp, (OSDTree*)h, 0, sampling);
+    sizes[0] = g_exp.ns; sizes[1] = g_exp.nl; sizes[2] = g_exp.nd;
+}
+void or_sdtree_export_copy(uint8_t* smask, float* scalars, int64_t* counts, uint8_t* dmask, float* dsums) {
+    memcpy(smask, g_exp.smask, (size_t)g_exp.ns);
+    memcpy(scalars, g_exp.scalars, (size_t)g_exp.nl * 4 * sizeof(float));
+    memcpy(counts, g_exp.counts, (size_t)g_exp.nl * sizeof(int64_t));
+    memcpy(dmask, g_exp.dmask, (size_t)g_exp.nd);
+    memcpy(dsums, g_exp.dsums, (size_t)g_exp.nd * 4 * sizeof(float));
+}
+
+/* DTreeT::GetMean (PG.h:447-451) */
+static inline float dtree_mean(const ODTree* d) {
+    if (d->s_statw <= 0.0f) return 0.0f;
+    const float factor = O_INV_2PI / (2.0f * d->s_statw);
+    return factor * d->s_sum;
+}
+/* DTreeNodeT::Sample (PG.h:229-277) + DTreeT::Sample (PG.h:478-484) */
+static void dtree_sample(const ODTree* d, uint32_t* rng, float* out) {
+    if (dtree_mean(d) <= 0.0f) { out[0] = rnd1(rng); out[1] = rnd1(rng); return; }
+    uint32_t cur = 0;
+    float rx = 0.0f, ry = 0.0f, size = 1.0f;
+    for (;;) {
+        const float* s = d->ssum + 4 * cur;
+        int idx = 0;
+        float topLeft = s[0], topRight = s[1];
+        float partial = s[0] + s[2];
+        float total = s[0] + s[1] + s[2] + s[3];
+        float boundary = partial / total;
+        float ox = 0.0f, oy = 0.0f;
+        float sample = rnd1(rng);
+        if (sample < boundary) { sample = sample / boundary; boundary = topLeft / partial; }
+        else {
+            partial = total - partial; ox = 0.5f;
+            sample = (sample - boundary) / (1.0f - boundary);
+            boundary = topRight / partial; idx |= 1;
+        }
+        if (sample >= boundary) { oy = 0.5f; idx |= 2; }
+        rx += size * ox; ry += size * oy;
+        size *= 0.5f;
+        if (d->sch[cur].c[idx] == 0 || s[idx] <= 0.0f) {
+            const float a = rnd1(rng), b = rnd1(rng);
+            rx += size * a; ry += size * b;
+            break;
+        }
+        cur = d->sch[cur].c[idx];
+    }
+    out[0] = rx < 0.0f ? 0.0f : (rx > 1.0f ? 1.0f : rx);
+    out[1] = ry < 0.0f ? 0.0f : (ry > 1.0f ? 1.0f : ry);
+}
+/* DTreeNodeT::Pdf (PG.h:279-320) + DTreeT::Pdf (PG.h:485-490) */
+static float dtree_pdf(const ODTree* d, float u, float v) {
+    if (dtree_mean(d) <= 0.0f) return 1.0f * O_INV_2PI / 2.0f;
+    float p[2] = {u, v};
+    float result = 1.0f;
+    uint32_t cur = 0;
+    int idx = quad_child(p);
+    for (;;) {
+        const float* s = d->ssum + 4 * cur;
+        float total = s[0] + s[1] + s[2] + s[3];
+        if (s[idx] <= 0.0f) { result = 0.0f; break; }
+        const float factor = 4.0f * s[idx] / total;
+        result *= factor;
+        if (d->sch[cur].c[idx] == 0) break;
+        cur = d->sch[cur].c[idx];
+        idx = quad_child(p);
+    }
+    return result * O_INV_2PI / 2.0f;
+}
+/* guided sample + pdf as SimpleGuide.cu:359-369 uses them */
+void or_sdtree_sample_pdf(void* h, int64_t n, const float* pos, const uint32_t* seeds, float* out_uv,
+                          float* out_pdf_uv, float* out_dir, float* out_pdf_dir) {
+    OSDTree* t = (OSDTree*)h;
+    for (int64_t i = 0; i < n; ++i) {
+        const ODTree* d = &t->dt[leaf_dtree(t, pos + 3 * i)];
+        uint32_t rng = seeds[i];
+        float uv[2];
+        dtree_sample(d, &rng, uv);
+        if (out_uv) { out_uv[2 * i] = uv[0]; out_uv[2 * i + 1] = uv[1]; }
+        if (out_pdf_uv) out_pdf_uv[i] = dtree_pdf(d, uv[0], uv[1]);
+        if (out_dir || out_pdf_dir) {
+            float dir[3];
+            canonical_to_dir(uv[0], uv[1], dir);
+            normalize3(dir);
+            if (out_dir) { out_dir[3 * i] = dir[0]; out_dir[3 * i + 1] = dir[1]; out_dir[3 * i + 2] = dir[2]; }
+            if (out_pdf_dir) {
+                float c[2];
+                or_dir_to_canonical(1, dir, c);
+                out_pdf_dir[i] = dtree_pdf(d, c[0], c[1]);
+            }
+        }
+    }
+}
+void or_sdtree_pdf(void* h, int64_t n, const float* pos, const float* uv, float* out) {
+    OSDTree* t = (OSDTree*)h;
+    for (int64_t i = 0; i < n; ++i) out[i] = dtree_pdf(&t->dt[leaf_dtree(t, pos + 3 * i)], uv[2 * i], uv[2 * i + 1]);
+}
+uint32_t or_sdtree_num_stree_nodes(void* h) { return ((OSDTree*)h)->nst; }
+uint32_t or_sdtree_num_dtrees(void* h) { return ((OSDTree*)h)->ndt; }
+
+/* ------------------------------------------------------------------ hash grid */
+/* Cell coordinates as DoubleBufferedHashGrid3T::FindFromCur/Prv compute them
+ * (OPX7UtilsGrid.h:189-199): uint(bounds * (p - off) / size), clamped to bounds-1; negative
+ * products clamp to 0 (the device conversion semantics). */
+static void grid_cell(const float* p, const float* off, const float* size, const uint32_t* b, uint32_t* ijk) {
+    for (int k = 0; k < 3; ++k) {
+        float f = (p[k] - off[k]) / size[k];
+        float s = (float)b[k] * f;
+        uint32_t v = s <= 0.0f ? 0u : (s >= 4294967040.0f ? 0xFFFFFFFFu : (uint32_t)s);
+        ijk[k] = v > b[k] - 1 ? b[k] - 1 : v;
+    }
+}
+/* DoubleBufferedHashGrid3T::Hash1 / GetCurCellIndex / GetPrvCellIndex (OPX7UtilsGrid.h:241-300) */
+void or_hashgrid_insert(int64_t n, const float* pos, const float* off, const float* size, const uint32_t* b,
+                        uint32_t nslots, uint32_t* cur, uint32_t* out_slot) {
+    const uint32_t nb = nslots / 32;
+    for (int64_t i = 0; i < n; ++i) {
+        uint32_t c[3];
+        grid_cell(pos + 3 * i, off, size, b, c);
+        const uint32_t bucket = or_pcg1d(nslots + c[2] + or_pcg1d(c[1] + or_pcg1d(c[0]))) % nb;
+        const uint32_t cs = 1u + b[0] * b[1] * c[2] + b[0] * c[1] + c[0];
+        uint32_t r = UINT32_MAX;
+        for (uint32_t k = 0; k < 32; ++k) {
+            uint32_t* s = &cur[32 * bucket + k];
+            if (*s == 0) { *s = cs; r = 32 * bucket + k; break; }
+            if (*s == cs) { r = 32 * bucket + k; break; }
+        }
+        out_slot[i] = r;
+    }
+}
+void or_hashgrid_lookup(int64_t n, const float* pos, const float* off, const float* size, const uint32_t* b,
+                        uint32_t nslots, const uint32_t* prv, uint32_t* out_slot) {
+    const uint32_t nb = nslots / 32;
+    for (int64_t i = 0; i < n; ++i) {
+        uint32_t c[3];
+        grid_cell(pos + 3 * i, off, size, b, c);
+        const uint32_t bucket = or_pcg1d(nslots + c[2] + or_pcg1d(c[1] + or_pcg1d(c[0]))) % nb;
+        const uint32_t cs = 1u + b[0] * b[1] * c[2] + b[0] * c[1] + c[0];
+        uint32_t r = UINT32_MAX;
+        for (uint32_t k = 0; k < 32; ++k) {
+            const uint32_t s = prv[32 * bucket + k];
+            if (s == 0) break;
+            if (s == cs) { r = 32 * bucket + k; break; }
+        }
+        out_slot[i] = r;
+    }
+}
+/* Morton keying (this library's own mode): 21 bits per axis interleaved into 63 bits,
+ * key = morton + 1 so that 0 marks an empty slot; bucket = 64-bit mix of the key. */
+static uint64_t part1by2_21(uint64_t x) {
+    x &= 0x1fffffull;
+    x = (x | x << 32) & 0x1f00000000ffffull;
+    x = (x | x << 16) & 0x1f0000ff0000ffull;
+    x = (x | x << 8) & 0x100f00f00f00f00full;
+    x = (x | x << 4) & 0x10c30c30c30c30c3ull;
+    x = (x | x << 2) & 0x1249249249249249ull;
+    return x;
+}
+uint64_t or_morton3(uint32_t x, uint32_t y, uint32_t z) { return part1by2_21(x) | (part1by2_21(y) << 1) | (part1by2_21(z) << 2); }
+static uint64_t mix64(uint64_t z) {
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    return z ^ (z >> 31);
+}
+void or_mhash_insert(int64_t n, const float* pos, const float* off, const float* size, const uint32_t* b,
+                     uint32_t nslots, uint64_t* cur, uint32_t* out_slot, uint64_t* out_key) {
+    const uint32_t nb = nslots / 32;
+    for (int64_t i = 0; i < n; ++i) {
+        uint32_t c[3];
+        grid_cell(pos + 3 * i, off, size, b, c);
+        const uint64_t key = or_morton3(c[0], c[1], c[2]) + 1ull;
+        const uint32_t bucket = (uint32_t)(mix64(key) % nb);
+        uint32_t r = UINT32_MAX;
+        for (uint32_t k = 0; k < 32; ++k) {
+            uint64_t* s = &cur[32 * (uint64_t)bucket + k];
+            if (*s == 0) { *s = key; r = 32 * bucket + k; break; }
+            if (*s == key) { r = 32 * bucket + k; break; }
+        }
+        out_slot[i] = r;
+        if (out_key) out_key[i] = key;
+    }
+}
+void or_mhash_lookup(int64_t n, const float* pos, const float* off, const float* size, const uint32_t* b,
+                     uint32_t nslots, const uint64_t* prv, uint32_t* out_slot) {
+    const uint32_t nb = nslots / 32;
+    for (int64_t i = 0; i < n; ++i) {
+        uint32_t c[3];
+        grid_cell(pos + 3 * i, off, size, b, c);
+        const uint64_t key = or_morton3(c[0], c[1], c[2]) + 1ull;
+        const uint32_t bucket = (uint32_t)(mix64(key) % nb);
+        uint32_t r = UINT32_MAX;
+        for (uint32_t k = 0; k < 32; ++k) {
+            const uint64_t s = prv[32 * (uint64_t)bucket + k];
+            if (s == 0) break;
+            if (s == key) { r = 32 * bucket + k; break; }
+        }
+        out_slot[i] = r;
+    }
+}
+
+/* ------------------------------------------------------------------ Morton quadtree */
+/* MortonUtils::Part1By1_16 (OPX7UtilsMorton.h:41-64); code = (part(y) << 1) + part(x)
+ * (Morton2Utils::GetCodeFromPosIdx, :165-167). */
+static uint32_t part1by1(uint32_t x) {
+    x &= 0x0000FFFF;
+    x = (x ^ (x << 8)) & 0x00FF00FF;
+    x = (x ^ (x << 4)) & 0x0F0F0F0F;
+    x = (x ^ (x << 2)) & 0x33333333;
+    x = (x ^ (x << 1)) & 0x55555555;
+    return x;
+}
+static uint32_t compact1by1(uint32_t x) {
+    x &= 0x55555555;
+    x = (x ^ (x >> 1)) & 0x33333333;
+    x = (x ^ (x >> 2)) & 0x0F0F0F0F;
+    x = (x ^ (x >> 4)) & 0x00FF00FF;
+    x = (x ^ (x >> 8)) & 0x0000FFFF;
+    return x;
+}
+uint32_t or_morton2(uint32_t x, uint32_t y) { return (part1by1(y) << 1) + part1by1(x); }
+static inline uint32_t mqt_off(uint32_t level) { return ((1u << (2 * level)) - 1u) / 3u; }
+/* MortonQuadTreeT::Record (OPX7UtilsMorton.h:262-285, leaf only): pos = uint(uv * 2^L),
+ * clamped to 2^L - 1 (uv == 1 would address past the level).  Leaves accumulate in fixed
+ * point: leaves[cell * 4^L + code]. */
+void or_mqt_record(int64_t n, uint32_t level, int bits, int64_t* leaves, const uint32_t* cell, const float* uv,
+                   const float* value, uint32_t* status) {
+    const float numNodes = ldexpf(1.0f, (int)level);
+    const uint32_t maxi = (1u << level) - 1u;
+    for (int64_t i = 0; i < n; ++i) {
+        if (cell[i] == UINT32_MAX) continue;
+        const float v = value[i];
+        if (!(isfinite(v) && v > 0.0f)) continue;
+        uint32_t px = (uint32_t)(uv[2 * i] * numNodes), py = (uint32_t)(uv[2 * i + 1] * numNodes);
+        px = px > maxi ? maxi : px;
+        py = py > maxi ? maxi : py;
+        leaves[((uint64_t)cell[i] << (2 * level)) + or_morton2(px, py)] += to_fx(v, bits, status);
+    }
+}
+/* mortonBuildKernel (OPX7UtilsMortonBuild.cu:2-16): the pyramid of a cell; here from exact
+ * integer leaf sums, each level converted to float once. */
+void or_mqt_build(uint32_t ncells, uint32_t level, int bits, const int64_t* leaves, float* pyramid) {
+    const uint32_t per = mqt_off(level + 1), nl = 1u << (2 * level);
+    int64_t* tmp = (int64_t*)malloc(sizeof(int64_t) * per);
+    for (uint32_t c = 0; c < ncells; ++c) {
+        const int64_t* lf = leaves + (uint64_t)c * nl;
+        memcpy(tmp + mqt_off(level), lf, sizeof(int64_t) * nl);
+        for (int l = (int)level - 1; l >= 0; --l) {
+            const uint32_t o = mqt_off((uint32_t)l), oc = mqt_off((uint32_t)l + 1), cnt = 1u << (2 * l);
+            for (uint32_t k = 0; k < cnt; ++k)
+                tmp[o + k] = tmp[oc + 4 * k] + tmp[oc + 4 * k + 1] + tmp[oc + 4 * k + 2] + tmp[oc + 4 * k + 3];
+        }
+        float* w = pyramid + (uint64_t)c * per;
+        for (uint32_t k = 0; k < per; ++k) w[k] = fx_to_float(tmp[k], bits);
+    }
+    free(tmp);
+}
+/* MortonQuadTreeT::SampleAndPdf (OPX7UtilsMorton.h:286-344) and ::Pdf (:401-414). */
+void or_mqt_sample_pdf(int64_t n, uint32_t level, const float* pyramid, const uint32_t* cell, const uint32_t* seeds,
+                       float* out_uv, float* out_pdf, float* out_pdf_eval) {
+    const uint32_t per = mqt_off(level + 1);
+    for (int64_t i = 0; i < n; ++i) {
+        const float* w = pyramid + (uint64_t)cell[i] * per;
+        uint32_t rng = seeds[i];
+        float ux, uy, pdf;
+        float total = w[0];
+        if (total <= 0.0f) {
+            ux = rnd1(&rng); uy = rnd1(&rng); pdf = 1.0f;
+        } else {
+            uint32_t size = 4, offset = 1, code = 0;
+            for (uint32_t l = 0; l < level; ++l) {
+                const float* q = w + offset + (code << 2);
+                uint32_t cl = 0;
+                float partial = q[0] + q[2];
+                float boundary = partial / total;
+                float sample = rnd1(&rng);
+                if (sample < boundary) { sample /= boundary; boundary = q[0] / partial; }
+                else {
+                    partial = q[1] + q[3];
+                    sample = (sample - boundary) / (1.0f - boundary);
+                    boundary = q[1] / partial;
+                    cl |= 1;
+                }
+                if (sample >= boundary) cl |= 2;
+                total = q[cl];
+                code = (code << 2) + cl;
+                offset += size;
+                size *= 4;
+            }
+            const float nn = ldexpf(1.0f, (int)level);
+            const uint32_t xi = compact1by1(code), yi = compact1by1(code >> 1);
+            ux = ((float)xi + rnd1(&rng)) / nn;
+            uy = ((float)yi + rnd1(&rng)) / nn;
+            pdf = total / w[0] * ldexpf(1.0f, (int)(2 * level));
+        }
+        out_uv[2 * i] = ux; out_uv[2 * i + 1] = uy;
+        out_pdf[i] = pdf;
+        if (out_pdf_eval) {
+            float pe;
+            if (w[0] <= 0.0f) pe = 1.0f;
+            else {
+                const float nn = ldexpf(1.0f, (int)level);
+                const uint32_t maxi = (1u << level) - 1u;
+                uint32_t px = (uint32_t)(ux * nn), py = (uint32_t)(uy * nn);
+                px = px > maxi ? maxi : px;
+                py = py > maxi ? maxi : py;
+                pe = w[mqt_off(level) + or_morton2(px, py)] / w[0] * nn * nn;
+            }
+            out_pdf_eval[i] = pe;
+        }
+    }
+}

@@ -1,0 +1,887 @@
+// SD-tree on the GPU: record, build, spatial refine + quadtree reset, guided sample / pdf,
+// plus the C ABI (rtpg_sdtree_*) and the pass controller (rtpg_controller_*).
+//
+// RTLib keeps the tree on the host and round-trips it through PCIe every pass
+// (RTSTreeWrapperT::Download / Build / Reset / Upload, OPX7UtilsPathGuiding.h:1353-1728,
+// driven by RTSTreeControllerT::BegTrace/EndTrace :1808-1887).  Here every step is a kernel
+// on device-resident arrays; counts stay in device memory so a whole pass can be captured
+// in a CUDA graph.
+#include <math.h>
+#include <vector>
+#include <algorithm>
+#include <new>
+
+#include "common.cuh"
+#include "sdtree_dev.cuh"
+
+namespace rtpg {
+
+constexpr int kRecordBlock = 256;
+constexpr int kTreeBlock = 256;
+constexpr uint32_t kVirtual = 0xffffffffu;
+constexpr uint32_t kStageSTree = 8192;  // STree nodes staged in shared memory by the queries
+
+// ------------------------------------------------------------------ clear
+__global__ void k_clear(SDTreeDev t) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        t.counts[0] = 1;
+        t.counts[1] = 1;
+        t.counts[2] = 1;
+        t.snode[0] = kLeafBit | 0u;
+        t.b_off[0] = 0; t.b_cnt[0] = 1; t.s_off[0] = 0; t.s_cnt[0] = 1;
+        t.b_statw[0] = 0ull;
+        t.s_sum[0] = 0.0f; t.s_area[0] = 0.0f; t.s_statw[0] = 0.0f;
+        t.b_lvl[0] = 0; t.b_lvl[1] = 1; t.b_nlvl[0] = 1;
+        for (int q = 0; q < 4; ++q) t.b_sums[q] = 0ull;
+        t.b_child[0] = make_ushort4(0, 0, 0, 0);
+        SNode z;
+        z.sums = make_float4(0.f, 0.f, 0.f, 0.f);
+        z.child = make_ushort4(0, 0, 0, 0);
+        z.pad0 = z.pad1 = 0;
+        t.s_nodes[0] = z;
+    }
+}
+
+// ------------------------------------------------------------------ record
+// One thread per record (grid-stride, warp-uniform trip count so that the warp-aggregated
+// atomics run converged).  Two 64-bit atomics per record: the DTree's stat-weight and the
+// leaf quadrant sum (RecordIrradiance, PG.h:417-428).
+template <bool CANON>
+__global__ void __launch_bounds__(kRecordBlock) k_record(SDTreeDev t, int64_t n, const float* __restrict__ pos,
+                                                         const float* __restrict__ dir, const float* __restrict__ radiance,
+                                                         const float* __restrict__ wo_pdf,
+                                                         const float* __restrict__ stat_w,
+                                                         const uint8_t* __restrict__ is_delta) {
+    __shared__ uint32_t s_st[kStageSTree];
+    const uint32_t nst = t.counts[0];
+    const bool staged = nst <= kStageSTree;
+    if (staged)
+        for (uint32_t i = threadIdx.x; i < nst; i += blockDim.x) s_st[i] = t.snode[i];
+    __syncthreads();
+    const uint32_t* st = staged ? s_st : t.snode;
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    for (int64_t base = int64_t(blockIdx.x) * blockDim.x; base < n; base += stride) {
+        const int64_t i = base + threadIdx.x;
+        unsigned long long k_w = ~0ull, k_s = ~0ull, v_w = 0, v_s = 0;
+        if (i < n && !(is_delta && is_delta[i])) {
+            const float wo = wo_pdf ? wo_pdf[i] : 1.0f;
+            const float sw = stat_w ? stat_w[i] : 1.0f;
+            const float irr = __fdiv_rn(radiance[i], wo);
+            if (isfinite(sw) && sw > 0.0f) {
+                const uint32_t d = stree_lookup(st, t.mn, t.mx, pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]);
+                k_w = d;
+                v_w = to_fx(sw, t.fx, t.status);
+                if (isfinite(irr) && irr > 0.0f) {
+                    float u, v;
+                    if (CANON) {
+                        const float2 c = reinterpret_cast<const float2*>(dir)[i];
+                        u = c.x; v = c.y;
+                    } else {
+                        const float2 c = dir_to_canonical(dir[3 * i], dir[3 * i + 1], dir[3 * i + 2]);
+                        u = c.x; v = c.y;
+                    }
+                    k_s = dtree_record_slot(t.b_child, t.b_off[d], u, v);
+                    v_s = to_fx(__fmul_rn(irr, sw), t.fx, t.status);
+                }
+            }
+        }
+        warp_add_u64(k_w, v_w, t.b_statw);
+        warp_add_u64(k_s, v_s, t.b_sums);
+    }
+}
+
+// ------------------------------------------------------------------ build
+// One CTA per DTree (grid-stride over trees).  Levels of the breadth-first building tree are
+// processed deepest first: an interior quadrant's fixed-point sum is the exact sum of its
+// child's four quadrants (DTreeNodeT::Build, PG.h:356-369).  Then the float sums, the area
+// (DTreeNodeT::GetArea, PG.h:342-355, same float order), the root sum (RTDTreeT::Build,
+// PG.h:948-957) and the sampling copy (RTDTreeWrapperT::Build, PG.h:1086-1090).
+__global__ void __launch_bounds__(kTreeBlock) k_build(SDTreeDev t) {
+    const uint32_t ndt = t.counts[1];
+    for (uint32_t d = blockIdx.x; d < ndt; d += gridDim.x) {
+        const uint32_t off = t.b_off[d];
+        const uint32_t cnt = t.b_cnt[d];
+        const int nl = t.b_nlvl[d];
+        const uint16_t* lv = t.b_lvl + size_t(d) * (kMaxLevels + 1);
+        for (int l = nl - 2; l >= 0; --l) {
+            const uint32_t a = lv[l], b = lv[l + 1];
+            for (uint32_t j = a + threadIdx.x; j < b; j += blockDim.x) {
+                const ushort4 c = t.b_child[off + j];
+                const uint32_t cc[4] = {c.x, c.y, c.z, c.w};
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    if (cc[q]) {
+                        const unsigned long long* s = t.b_sums + size_t(off + cc[q]) * 4;
+                        t.b_sums[size_t(off + j) * 4 + q] = s[0] + s[1] + s[2] + s[3];
+                    }
+                }
+            }
+            __syncthreads();
+        }
+        // area bottom-up, writes sampling nodes
+        for (int l = nl - 1; l >= 0; --l) {
+            const uint32_t a = lv[l], b = lv[l + 1];
+            for (uint32_t j = a + threadIdx.x; j < b; j += blockDim.x) {
+                const ushort4 c = t.b_child[off + j];
+                const uint32_t cc[4] = {c.x, c.y, c.z, c.w};
+                const unsigned long long* s = t.b_sums + size_t(off + j) * 4;
+                float f[4];
+                float area = 0.0f;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    f[q] = fx_to_float(s[q], t.fx);
+                    if (f[q] > 0.0f) {
+                        if (!cc[q]) area = __fadd_rn(area, 0.25f);
+                        else area = __fadd_rn(area, __fdiv_rn(t.b_area[off + cc[q]], 4.0f));
+                    }
+                }
+                t.b_area[off + j] = area;
+                SNode nd;
+                nd.sums = make_float4(f[0], f[1], f[2], f[3]);
+                nd.child = c;
+                nd.pad0 = nd.pad1 = 0;
+                t.s_nodes[off + j] = nd;
+            }
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) {
+            const float4 r = t.s_nodes[off].sums;
+            t.s_sum[d] = __fadd_rn(__fadd_rn(__fadd_rn(r.x, r.y), r.z), r.w);
+            t.s_area[d] = t.b_area[off];
+            t.s_statw[d] = fx_to_float(t.b_statw[d], t.fx);
+            t.s_off[d] = off;
+            t.s_cnt[d] = cnt;
+        }
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------------ spatial refine
+// Footprint guard of RTSTreeT::Refine (PG.h:1276-1285): 24-byte nodes and 24-byte headers
+// of the building and sampling tree of every STree node; interior nodes hold default
+// one-node trees (SubDivide resets the parent's wrapper, PG.h:1246).
+__global__ void k_footprint(SDTreeDev t, unsigned long long* fp) {
+    const uint32_t n = t.counts[0];
+    unsigned long long s = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t c = t.snode[i];
+        if (c & kLeafBit) {
+            const uint32_t d = c & ~kLeafBit;
+            s += 24ull * (t.b_cnt[d] + t.s_cnt[d]) + 48ull;
+        } else {
+            s += 96ull;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0 && s) atomicAdd(fp, s);
+}
+
+// Per STree node: how many halvings of the building stat-weight stay above the threshold
+// (ShallSplit, PG.h:1270-1274, cascading through SubDivide's w/2, PG.h:1243).  A leaf that
+// splits k times becomes a complete subtree with 2^(k+1)-2 new nodes and 2^k leaves.
+// tot64[1] / tot64[2] receive the 64-bit totals of new STree nodes / DTrees, which the apply
+// step checks against the capacities (the 32-bit scan totals could wrap).
+__global__ void k_refine_count(SDTreeDev t, float thf, int32_t max_mb, uint32_t kmax, unsigned long long* tot64,
+                               uint32_t* cnt_s, uint32_t* cnt_d, uint32_t* ksplit) {
+    const uint32_t n = t.counts[0];
+    const bool allowed = max_mb < 0 || (tot64[0] / 1000000ull) < (unsigned long long)max_mb;
+    unsigned long long ss = 0, sd = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t c = t.snode[i];
+        uint32_t k = 0;
+        if (allowed && (c & kLeafBit)) {
+            float w = fx_to_float(t.b_statw[c & ~kLeafBit], t.fx);
+            while (w > thf && k < kmax) {
+                w = __fdiv_rn(w, 2.0f);
+                ++k;
+            }
+        }
+        ksplit[i] = k;
+        cnt_s[i] = k ? (2u << k) - 2u : 0u;
+        cnt_d[i] = k ? (1u << k) - 1u : 0u;
+        ss += cnt_s[i];
+        sd += cnt_d[i];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        ss += __shfl_down_sync(0xffffffffu, ss, o);
+        sd += __shfl_down_sync(0xffffffffu, sd, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (ss) atomicAdd(tot64 + 1, ss);
+        if (sd) atomicAdd(tot64 + 2, sd);
+    }
+}
+
+// Writes the complete subtrees.  New STree nodes are numbered level by level inside each
+// leaf's block; leaf j of the subtree gets the old DTree (j == 0) or a new one, which shares
+// the parent's sampling quadtree (read-only until the next build) -- SubDivide copies the
+// whole wrapper into both children (PG.h:1236-1244).
+__global__ void k_refine_apply(SDTreeDev t, const uint32_t* ksplit, const uint32_t* off_s, const uint32_t* off_d,
+                               const unsigned long long* tot64) {
+    const uint32_t n = t.counts[0], ndt = t.counts[1];
+    if (n + tot64[1] > t.cap_snodes || ndt + tot64[2] > t.cap_dtrees) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(t.status, RTPG_STATUS_STREE_CAPACITY);
+        return;
+    }
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t k = ksplit[i];
+        if (!k) continue;
+        const uint32_t dold = t.snode[i] & ~kLeafBit;
+        const uint32_t B = n + off_s[i];
+        const uint32_t D = ndt + off_d[i];
+        t.snode[i] = B;
+        for (uint32_t l = 1; l <= k; ++l) {
+            const uint32_t w = 1u << l;
+            for (uint32_t j = 0; j < w; ++j) {
+                const uint32_t idx = B + (w - 2) + j;
+                if (l < k) {
+                    t.snode[idx] = B + (2 * w - 2) + 2 * j;
+                } else {
+                    const uint32_t d = j == 0 ? dold : D + j - 1;
+                    t.snode[idx] = kLeafBit | d;
+                    if (j) {
+                        // building fields alias the parent's tree until the quadtree reset
+                        // writes the new one; they only stay if the reset hits a capacity
+                        // limit (RTPG_STATUS_DNODE_CAPACITY), which keeps records in bounds
+                        t.b_off[d] = t.b_off[dold];
+                        t.b_cnt[d] = t.b_cnt[dold];
+                        t.b_nlvl[d] = t.b_nlvl[dold];
+                        t.b_statw[d] = 0ull;
+                        for (uint32_t q = 0; q <= kMaxLevels; ++q)
+                            t.b_lvl[size_t(d) * (kMaxLevels + 1) + q] = t.b_lvl[size_t(dold) * (kMaxLevels + 1) + q];
+                        t.s_off[d] = t.s_off[dold];
+                        t.s_cnt[d] = t.s_cnt[dold];
+                        t.s_sum[d] = t.s_sum[dold];
+                        t.s_area[d] = t.s_area[dold];
+                        t.s_statw[d] = t.s_statw[dold];
+                    }
+                }
+            }
+        }
+    }
+}
+__global__ void k_refine_commit(SDTreeDev t, const unsigned long long* tot64) {
+    const uint32_t n = t.counts[0], ndt = t.counts[1];
+    if (n + tot64[1] > t.cap_snodes || ndt + tot64[2] > t.cap_dtrees) return;
+    t.counts[0] = n + (uint32_t)tot64[1];
+    t.counts[1] = ndt + (uint32_t)tot64[2];
+}
+
+// ------------------------------------------------------------------ quadtree reset
+// RTDTreeT::Reset (PG.h:888-947) breadth first, one CTA per tree.  New node j either mirrors
+// node src[j] of the tree's sampling quadtree or -- under a sampling leaf quadrant -- is a
+// "copy of itself" whose four sums are vsum[j] = parent quadrant / 4 (PG.h:926-933).
+// Quadrant i of a node at depth `depth` gets a child iff depth < maxDepth and
+// sum_i / total > th (total = sampling root sum; 0.25^depth when total <= 0).  Children are
+// numbered in (node, quadrant) order via a block scan, level by level; the same pass runs
+// twice, first to count, then to write at the scanned offset.
+template <bool WRITE>
+__global__ void __launch_bounds__(kTreeBlock) k_reset(SDTreeDev t, float th, uint32_t* node_count,
+                                                      const uint32_t* node_off, unsigned long long* node_total) {
+    extern __shared__ uint32_t sm[];
+    uint32_t* src = sm;                                              // kDTreeNodeCap
+    float* vsum = reinterpret_cast<float*>(sm + kDTreeNodeCap);      // kDTreeNodeCap
+    __shared__ uint32_t warp_tot[kTreeBlock / 32];
+    __shared__ uint32_t s_ntotal;
+    if (WRITE && *node_total > t.cap_nodes) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(t.status, RTPG_STATUS_DNODE_CAPACITY);
+        return;
+    }
+    const uint32_t ndt = t.counts[1];
+    for (uint32_t d = blockIdx.x; d < ndt; d += gridDim.x) {
+        const float total = t.s_sum[d];
+        const uint32_t soff = t.s_off[d];
+        const uint32_t boff = WRITE ? node_off[d] : 0;
+        uint16_t* lv = t.b_lvl + size_t(d) * (kMaxLevels + 1);
+        if (threadIdx.x == 0) {
+            src[0] = 0;
+            vsum[0] = 0.0f;
+            s_ntotal = 1;
+            if (WRITE) lv[0] = 0;
+        }
+        __syncthreads();
+        uint32_t lvl_start = 0, lvl_end = 1, nlev = 0;
+        int depth = 1;
+        while (lvl_start < lvl_end) {
+            const float frac_empty = ldexpf(1.0f, -2 * depth);
+            for (uint32_t chunk = lvl_start; chunk < lvl_end; chunk += blockDim.x) {
+                const uint32_t j = chunk + threadIdx.x;
+                uint32_t mask = 0;
+                float si[4] = {0.f, 0.f, 0.f, 0.f};
+                ushort4 sc = make_ushort4(0, 0, 0, 0);
+                uint32_t s = kVirtual;
+                if (j < lvl_end) {
+                    s = src[j];
+                    if (s != kVirtual) {
+                        const SNode nd = t.s_nodes[soff + s];
+                        si[0] = nd.sums.x; si[1] = nd.sums.y; si[2] = nd.sums.z; si[3] = nd.sums.w;
+                        sc = nd.child;
+                    } else {
+                        si[0] = si[1] = si[2] = si[3] = vsum[j];
+                    }
+                    if (depth < (int)t.max_depth) {
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+                            const float f = total > 0.0f ? __fdiv_rn(si[q], total) : frac_empty;
+                            if (f > th) mask |= 1u << q;
+                        }
+                    }
+                }
+                const uint32_t base = s_ntotal;
+                uint32_t tot;
+                uint32_t next = base + block_exclusive_scan<kTreeBlock>(__popc(mask), warp_tot, tot);
+                ushort4 out = make_ushort4(0, 0, 0, 0);
+                if (j < lvl_end) {
+                    const uint32_t scc[4] = {sc.x, sc.y, sc.z, sc.w};
+                    uint32_t oc[4] = {0, 0, 0, 0};
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        if (mask & (1u << q)) {
+                            const uint32_t idx = next++;
+                            if (idx < kDTreeNodeCap) {
+                                if (s != kVirtual && scc[q]) { src[idx] = scc[q]; vsum[idx] = 0.0f; }
+                                else { src[idx] = kVirtual; vsum[idx] = __fdiv_rn(si[q], 4.0f); }
+                                oc[q] = idx;
+                            }
+                        }
+                    }
+                    out = make_ushort4(oc[0], oc[1], oc[2], oc[3]);
+                    if (WRITE) t.b_child[boff + j] = out;
+                }
+                __syncthreads();
+                if (threadIdx.x == 0) {
+                    uint32_t nt = base + tot;
+                    if (nt > kDTreeNodeCap) {
+                        nt = kDTreeNodeCap;
+                        atomicOr(t.status, RTPG_STATUS_DTREE_NODE_CAP);
+                    }
+                    s_ntotal = nt;
+                }
+                __syncthreads();
+            }
+            lvl_start = lvl_end;
+            lvl_end = s_ntotal;
+            ++nlev;
+            ++depth;
+            if (WRITE && threadIdx.x == 0) lv[nlev] = (uint16_t)lvl_start;
+        }
+        const uint32_t cnt = s_ntotal;
+        if (!WRITE) {
+            if (threadIdx.x == 0) {
+                node_count[d] = cnt;
+                atomicAdd(node_total, (unsigned long long)cnt);
+            }
+        } else {
+            for (uint32_t j = threadIdx.x; j < 4 * cnt; j += blockDim.x) t.b_sums[size_t(boff) * 4 + j] = 0ull;
+            if (threadIdx.x == 0) {
+                t.b_off[d] = boff;
+                t.b_cnt[d] = cnt;
+                t.b_statw[d] = 0ull;
+                t.b_nlvl[d] = (uint8_t)nlev;
+            }
+        }
+        __syncthreads();
+    }
+}
+__global__ void k_reset_commit(SDTreeDev t, const unsigned long long* node_total) {
+    if (*node_total <= t.cap_nodes) t.counts[2] = (uint32_t)*node_total;
+}
+
+// ------------------------------------------------------------------ sample / pdf
+__global__ void __launch_bounds__(256) k_sample_pdf(SDTreeDev t, int64_t n, const float* __restrict__ pos,
+                                                    const uint32_t* __restrict__ seeds, uint32_t seed_base,
+                                                    float* __restrict__ out_uv, float* __restrict__ out_pdf_uv,
+                                                    float* __restrict__ out_dir, float* __restrict__ out_pdf_dir) {
+    __shared__ uint32_t s_st[kStageSTree];
+    const uint32_t nst = t.counts[0];
+    const bool staged = nst <= kStageSTree;
+    if (staged)
+        for (uint32_t i = threadIdx.x; i < nst; i += blockDim.x) s_st[i] = t.snode[i];
+    __syncthreads();
+    const uint32_t* st = staged ? s_st : t.snode;
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const uint32_t d = stree_lookup(st, t.mn, t.mx, pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]);
+        uint32_t rng = seeds ? seeds[i] : (pcg1d(seed_base + (uint32_t)i) | 1u);
+        const uint32_t off = t.s_off[d];
+        const float statw = t.s_statw[d], sum = t.s_sum[d];
+        const float2 uv = dtree_sample(t.s_nodes, off, statw, sum, rng);
+        if (out_uv) reinterpret_cast<float2*>(out_uv)[i] = uv;
+        if (out_pdf_uv) out_pdf_uv[i] = dtree_pdf(t.s_nodes, off, statw, sum, uv.x, uv.y);
+        if (out_dir || out_pdf_dir) {
+            const float3 dv = normalize3(canonical_to_dir(uv.x, uv.y));
+            if (out_dir) {
+                out_dir[3 * i] = dv.x;
+                out_dir[3 * i + 1] = dv.y;
+                out_dir[3 * i + 2] = dv.z;
+            }
+            if (out_pdf_dir) {
+                const float2 c = dir_to_canonical(dv.x, dv.y, dv.z);
+                out_pdf_dir[i] = dtree_pdf(t.s_nodes, off, statw, sum, c.x, c.y);
+            }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) k_pdf(SDTreeDev t, int64_t n, const float* __restrict__ pos,
+                                             const float* __restrict__ dir, int canonical, float* __restrict__ out) {
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const uint32_t d = stree_lookup(t.snode, t.mn, t.mx, pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]);
+        float2 c;
+        if (canonical) c = reinterpret_cast<const float2*>(dir)[i];
+        else c = dir_to_canonical(dir[3 * i], dir[3 * i + 1], dir[3 * i + 2]);
+        out[i] = dtree_pdf(t.s_nodes, t.s_off[d], t.s_statw[d], t.s_sum[d], c.x, c.y);
+    }
+}
+
+}  // namespace rtpg
+
+using namespace rtpg;
+
+// ================================================================== host object
+struct rtpg_sdtree {
+    SDTreeDev dev{};
+    float mn[3], mx[3];
+    uint32_t max_depth = 20;
+    float fraction = 0.3f;
+    int bits = 24;
+    std::vector<void*> allocs;
+    // refine scratch
+    uint32_t *cnt_s = nullptr, *off_s = nullptr, *cnt_d = nullptr, *off_d = nullptr, *ksplit = nullptr;
+    uint32_t *partials = nullptr, *totals = nullptr, *node_cnt = nullptr, *node_off = nullptr;
+    unsigned long long* fp = nullptr;
+    size_t bytes = 0;
+
+    template <class T>
+    int alloc(T** p, size_t count) {
+        void* q = nullptr;
+        cudaError_t e = cudaMalloc(&q, count * sizeof(T));
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return fail(RTPG_ENOMEM, "cudaMalloc(%zu bytes) failed: %s", count * sizeof(T), cudaGetErrorString(e));
+        }
+        allocs.push_back(q);
+        bytes += count * sizeof(T);
+        *p = static_cast<T*>(q);
+        return RTPG_OK;
+    }
+    ~rtpg_sdtree() {
+        for (void* p : allocs) cudaFree(p);
+    }
+};
+
+static int sdtree_clear(rtpg_sdtree* h, cudaStream_t st) {
+    RTPG_CUDA(cudaMemsetAsync(h->dev.status, 0, sizeof(unsigned), st));
+    k_clear<<<1, 32, 0, st>>>(h->dev);
+    RTPG_LAUNCH_CHECK();
+    return RTPG_OK;
+}
+
+static int reset_smem() { return int(kDTreeNodeCap * 8); }
+
+extern "C" {
+
+int rtpg_sdtree_create(const float* aabb_min, const float* aabb_max, uint32_t max_dtree_depth, float fraction,
+                       const rtpg_sdtree_caps* caps, rtpg_sdtree** out) {
+    if (!aabb_min || !aabb_max || !out) return fail(RTPG_EINVAL, "rtpg_sdtree_create: null argument");
+    if (max_dtree_depth < 1 || max_dtree_depth > kMaxDTreeDepth)
+        return fail(RTPG_EINVAL, "rtpg_sdtree_create: max_dtree_depth must be in [1, %u]", kMaxDTreeDepth);
+    rtpg_sdtree_caps c{1u << 20, 1u << 19, 1u << 23, 24};
+    if (caps) {
+        if (caps->max_stree_nodes) c.max_stree_nodes = caps->max_stree_nodes;
+        if (caps->max_dtrees) c.max_dtrees = caps->max_dtrees;
+        if (caps->max_dtree_nodes_total) c.max_dtree_nodes_total = caps->max_dtree_nodes_total;
+        if (caps->fixed_point_bits) c.fixed_point_bits = caps->fixed_point_bits;
+    }
+    if (c.fixed_point_bits < 0 || c.fixed_point_bits > 40)
+        return fail(RTPG_EINVAL, "rtpg_sdtree_create: fixed_point_bits must be in [0, 40]");
+    if (c.max_stree_nodes >= kLeafBit || c.max_dtrees >= kLeafBit || c.max_dtree_nodes_total >= (1u << 31))
+        return fail(RTPG_EINVAL, "rtpg_sdtree_create: capacities must be below 2^31");
+    for (int k = 0; k < 3; ++k)
+        if (!(aabb_max[k] >= aabb_min[k]) || !isfinite(aabb_min[k]) || !isfinite(aabb_max[k]))
+            return fail(RTPG_EINVAL, "rtpg_sdtree_create: invalid AABB");
+    auto* h = new (std::nothrow) rtpg_sdtree();
+    if (!h) return fail(RTPG_ENOMEM, "rtpg_sdtree_create: out of host memory");
+    // RTSTreeT ctor (PG.h:1211-1217): cubify to the largest extent
+    const float sx = aabb_max[0] - aabb_min[0], sy = aabb_max[1] - aabb_min[1], sz = aabb_max[2] - aabb_min[2];
+    const float m = std::max(std::max(sx, sy), sz);
+    for (int k = 0; k < 3; ++k) {
+        h->mn[k] = aabb_min[k];
+        h->mx[k] = aabb_min[k] + m;
+    }
+    h->max_depth = max_dtree_depth;
+    h->fraction = fraction;
+    h->bits = c.fixed_point_bits;
+    SDTreeDev& t = h->dev;
+    t.mn = make_float3(h->mn[0], h->mn[1], h->mn[2]);
+    t.mx = make_float3(h->mx[0], h->mx[1], h->mx[2]);
+    t.fx.scale = ldexpf(1.0f, c.fixed_point_bits);
+    t.fx.inv_scale = ldexpf(1.0f, -c.fixed_point_bits);
+    t.cap_snodes = c.max_stree_nodes;
+    t.cap_dtrees = c.max_dtrees;
+    t.cap_nodes = c.max_dtree_nodes_total;
+    t.max_depth = max_dtree_depth;
+    t.fraction = fraction;
+    int r = RTPG_OK;
+    const size_t nd = c.max_dtrees, nn = c.max_dtree_nodes_total, ns = c.max_stree_nodes;
+    if ((r = h->alloc(&t.status, 1)) || (r = h->alloc(&t.counts, 4)) || (r = h->alloc(&t.snode, ns)) ||
+        (r = h->alloc(&t.b_off, nd)) || (r = h->alloc(&t.b_cnt, nd)) || (r = h->alloc(&t.s_off, nd)) ||
+        (r = h->alloc(&t.s_cnt, nd)) || (r = h->alloc(&t.b_statw, nd)) || (r = h->alloc(&t.s_sum, nd)) ||
+        (r = h->alloc(&t.s_area, nd)) || (r = h->alloc(&t.s_statw, nd)) ||
+        (r = h->alloc(&t.b_lvl, nd * (kMaxLevels + 1))) || (r = h->alloc(&t.b_nlvl, nd)) ||
+        (r = h->alloc(&t.b_sums, nn * 4)) || (r = h->alloc(&t.b_child, nn)) || (r = h->alloc(&t.b_area, nn)) ||
+        (r = h->alloc(&t.s_nodes, nn)) || (r = h->alloc(&h->cnt_s, ns)) || (r = h->alloc(&h->off_s, ns)) ||
+        (r = h->alloc(&h->cnt_d, ns)) || (r = h->alloc(&h->off_d, ns)) || (r = h->alloc(&h->ksplit, ns)) ||
+        (r = h->alloc(&h->node_cnt, nd)) || (r = h->alloc(&h->node_off, nd)) ||
+        (r = h->alloc(&h->partials, scan_partials_words(std::max(c.max_stree_nodes, c.max_dtrees)))) ||
+        (r = h->alloc(&h->totals, 4)) || (r = h->alloc(&h->fp, 4))) {
+        delete h;
+        return r;
+    }
+    cudaError_t e = cudaFuncSetAttribute(k_reset<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, reset_smem());
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_reset<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, reset_smem());
+    if (e != cudaSuccess) {
+        delete h;
+        return fail(RTPG_ECUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
+    }
+    if ((r = sdtree_clear(h, 0))) {
+        delete h;
+        return r;
+    }
+    e = cudaStreamSynchronize(0);
+    if (e != cudaSuccess) {
+        delete h;
+        return fail(RTPG_ECUDA, "rtpg_sdtree_create: %s", cudaGetErrorString(e));
+    }
+    *out = h;
+    return RTPG_OK;
+}
+
+int rtpg_sdtree_destroy(rtpg_sdtree* h) {
+    if (!h) return fail(RTPG_EINVAL, "rtpg_sdtree_destroy: null handle");
+    delete h;
+    return RTPG_OK;
+}
+
+int rtpg_sdtree_clear(rtpg_sdtree* h, void* stream) {
+    if (!h) return fail(RTPG_EINVAL, "rtpg_sdtree_clear: null handle");
+    return sdtree_clear(h, as_stream(stream));
+}
+
+int rtpg_sdtree_record(rtpg_sdtree* h, int64_t n, const float* pos, const float* dir, int dir_is_canonical,
+                       const float* radiance, const float* wo_pdf, const float* stat_weight, const uint8_t* is_delta,
+                       void* stream) {
+    if (!h) return fail(RTPG_EINVAL, "rtpg_sdtree_record: null handle");
+    if (n < 0) return fail(RTPG_EINVAL, "rtpg_sdtree_record: n < 0");
+    if (n == 0) return RTPG_OK;
+    if (!pos || !dir || !radiance) return fail(RTPG_EINVAL, "rtpg_sdtree_record: pos, dir and radiance are required");
+    const int g = grid_for(n, kRecordBlock, 8);
+    if (dir_is_canonical)
+        k_record<true><<<g, kRecordBlock, 0, as_stream(stream)>>>(h->dev, n, pos, dir, radiance, wo_pdf, stat_weight, is_delta);
+    else
+        k_record<false><<<g, kRecordBlock, 0, as_stream(stream)>>>(h->dev, n, pos, dir, radiance, wo_pdf, stat_weight, is_delta);
+    RTPG_LAUNCH_CHECK();
+    return RTPG_OK;
+}
+
+int rtpg_sdtree_build(rtpg_sdtree* h, void* stream) {
+    if (!h) return fail(RTPG_EINVAL, "rtpg_sdtree_build: null handle");
+    k_build<<<kSMs * 4, kTreeBlock, 0, as_stream(stream)>>>(h->dev);
+    RTPG_LAUNCH_CHECK();
+    return RTPG_OK;
+}
+
+int rtpg_sdtree_refine(rtpg_sdtree* h, uint64_t spatial_threshold, int32_t max_mb, float dtree_subdiv_th, void* stream) {
+    if (!h) return fail(RTPG_EINVAL, "rtpg_sdtree_refine: null handle");
+    cudaStream_t st = as_stream(stream);
+    SDTreeDev& t = h->dev;
+    // spatial part; fp[0] footprint, fp[1..2] new STree nodes / DTrees, fp[3] quadtree nodes
+    RTPG_CUDA(cudaMemsetAsync(h->fp, 0, 4 * sizeof(unsigned long long), st));
+    if (max_mb >= 0) {
+        k_footprint<<<kSMs * 2, 256, 0, st>>>(t, h->fp);
+        RTPG_LAUNCH_CHECK();
+    }
+    const float thf = (float)spatial_threshold;  // the size_t threshold as the float compare sees it
+    uint32_t kmax = 0;
+    while (kmax < 24 && (2ull << (kmax + 1)) <= t.cap_snodes) ++kmax;
+    k_refine_count<<<grid_for(t.cap_snodes, 256, 8), 256, 0, st>>>(t, thf, max_mb, kmax, h->fp, h->cnt_s, h->cnt_d,
+                                                                   h->ksplit);
+    RTPG_LAUNCH_CHECK();
+    int r;
+    if ((r = scan_exclusive_u32(h->cnt_s, h->off_s, t.counts + 0, t.cap_snodes, h->partials, h->totals + 0, st))) return r;
+    if ((r = scan_exclusive_u32(h->cnt_d, h->off_d, t.counts + 0, t.cap_snodes, h->partials, h->totals + 1, st))) return r;
+    k_refine_apply<<<grid_for(t.cap_snodes, 128, 8), 128, 0, st>>>(t, h->ksplit, h->off_s, h->off_d, h->fp);
+    k_refine_commit<<<1, 1, 0, st>>>(t, h->fp);
+    RTPG_LAUNCH_CHECK();
+    // quadtree reset of every leaf
+    k_reset<false><<<kSMs, kTreeBlock, reset_smem(), st>>>(t, dtree_subdiv_th, h->node_cnt, nullptr, h->fp + 3);
+    RTPG_LAUNCH_CHECK();
+    if ((r = scan_exclusive_u32(h->node_cnt, h->node_off, t.counts + 1, t.cap_dtrees, h->partials, h->totals + 2, st)))
+        return r;
+    k_reset<true><<<kSMs, kTreeBlock, reset_smem(), st>>>(t, dtree_subdiv_th, nullptr, h->node_off, h->fp + 3);
+    k_reset_commit<<<1, 1, 0, st>>>(t, h->fp + 3);
+    RTPG_LAUNCH_CHECK();
+    return RTPG_OK;
+}
+
+int rtpg_sdtree_reset(rtpg_sdtree* h, int32_t iteration, int32_t samples_per_pass, void* stream) {
+    if (!h) return fail(RTPG_EINVAL, "rtpg_sdtree_reset: null handle");
+    if (iteration <= 0) return RTPG_OK;
+    // size_t sTreeTh = std::sqrt(std::pow(2.0, iter) * samplePerPasses / 4.0f) * 4000 (PG.h:1649)
+    const uint64_t th = (uint64_t)(std::sqrt(std::pow(2.0, iteration) * samples_per_pass / 4.0f) * 4000);
+    return rtpg_sdtree_refine(h, th, 2000, 0.01f, stream);
+}
+
+int rtpg_sdtree_sample_pdf(rtpg_sdtree* h, int64_t n, const float* pos, const uint32_t* seeds, uint32_t seed_base,
+                           float* out_uv, float* out_pdf_uv, float* out_dir, float* out_pdf_dir, void* stream) {
+    if (!h) return fail(RTPG_EINVAL, "rtpg_sdtree_sample_pdf: null handle");
+    if (n < 0 || (n > 0 && !pos)) return fail(RTPG_EINVAL, "rtpg_sdtree_sample_pdf: bad arguments");
+    if (n == 0) return RTPG_OK;
+    k_sample_pdf<<<grid_for(n, 256, 8), 256, 0, as_stream(stream)>>>(h->dev, n, pos, seeds, seed_base, out_uv,
+                                                                     out_pdf_uv, out_dir, out_pdf_dir);
+    RTPG_LAUNCH_CHECK();
+    return RTPG_OK;
+}
+
+int rtpg_sdtree_pdf(rtpg_sdtree* h, int64_t n, const float* pos, const float* dir, int dir_is_canonical,
+                    float* out_pdf, void* stream) {
+    if (!h) return fail(RTPG_EINVAL, "rtpg_sdtree_pdf: null handle");
+    if (n < 0 || (n > 0 && (!pos || !dir || !out_pdf))) return fail(RTPG_EINVAL, "rtpg_sdtree_pdf: bad arguments");
+    if (n == 0) return RTPG_OK;
+    k_pdf<<<grid_for(n, 256, 8), 256, 0, as_stream(stream)>>>(h->dev, n, pos, dir, dir_is_canonical, out_pdf);
+    RTPG_LAUNCH_CHECK();
+    return RTPG_OK;
+}
+
+int rtpg_sdtree_stats(rtpg_sdtree* h, uint32_t* stree_nodes, uint32_t* dtrees, uint32_t* dtree_nodes, void* stream) {
+    if (!h) return fail(RTPG_EINVAL, "rtpg_sdtree_stats: null handle");
+    uint32_t c[4];
+    RTPG_CUDA(cudaMemcpyAsync(c, h->dev.counts, sizeof(c), cudaMemcpyDeviceToHost, as_stream(stream)));
+    RTPG_CUDA(cudaStreamSynchronize(as_stream(stream)));
+    if (stree_nodes) *stree_nodes = c[0];
+    if (dtrees) *dtrees = c[1];
+    if (dtree_nodes) *dtree_nodes = c[2];
+    return RTPG_OK;
+}
+
+int rtpg_sdtree_memory_footprint(rtpg_sdtree* h, uint64_t* bytes) {
+    if (!h || !bytes) return fail(RTPG_EINVAL, "rtpg_sdtree_memory_footprint: null argument");
+    *bytes = h->bytes;
+    return RTPG_OK;
+}
+
+int rtpg_sdtree_status(rtpg_sdtree* h, uint32_t* status, int clear, void* stream) {
+    if (!h || !status) return fail(RTPG_EINVAL, "rtpg_sdtree_status: null argument");
+    cudaStream_t st = as_stream(stream);
+    RTPG_CUDA(cudaMemcpyAsync(status, h->dev.status, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    if (clear) RTPG_CUDA(cudaMemsetAsync(h->dev.status, 0, sizeof(uint32_t), st));
+    RTPG_CUDA(cudaStreamSynchronize(st));
+    return RTPG_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------ export (host side)
+namespace {
+struct HostTree {
+    std::vector<uint32_t> snode, b_off, b_cnt, s_off, s_cnt;
+    std::vector<unsigned long long> b_statw, b_sums;
+    std::vector<float> s_sum, s_area, s_statw;
+    std::vector<ushort4> b_child;
+    std::vector<SNode> s_nodes;
+    float inv_scale;
+};
+struct ExportOut {
+    std::vector<uint8_t> smask, dmask;
+    std::vector<float> scalars, dsums;
+    std::vector<int64_t> counts;
+};
+void exp_dtree(const HostTree& h, bool sampling, uint32_t off, uint32_t n, ExportOut& e) {
+    uint32_t c[4];
+    float s[4];
+    if (sampling) {
+        const SNode& nd = h.s_nodes[off + n];
+        c[0] = nd.child.x; c[1] = nd.child.y; c[2] = nd.child.z; c[3] = nd.child.w;
+        s[0] = nd.sums.x; s[1] = nd.sums.y; s[2] = nd.sums.z; s[3] = nd.sums.w;
+    } else {
+        const ushort4 ch = h.b_child[off + n];
+        c[0] = ch.x; c[1] = ch.y; c[2] = ch.z; c[3] = ch.w;
+        for (int q = 0; q < 4; ++q) s[q] = (float)(long long)h.b_sums[size_t(off + n) * 4 + q] * h.inv_scale;
+    }
+    uint8_t m = 0;
+    for (int q = 0; q < 4; ++q)
+        if (c[q]) m |= uint8_t(1u << q);
+    e.dmask.push_back(m);
+    for (int q = 0; q < 4; ++q) e.dsums.push_back(s[q]);
+    for (int q = 0; q < 4; ++q)
+        if (c[q]) exp_dtree(h, sampling, off, c[q], e);
+}
+void exp_stree(const HostTree& h, bool sampling, uint32_t i, ExportOut& e) {
+    const uint32_t code = h.snode[i];
+    const bool leaf = (code & kLeafBit) != 0;
+    e.smask.push_back(leaf ? 0 : 1);
+    if (leaf) {
+        const uint32_t d = code & ~kLeafBit;
+        e.scalars.push_back((float)(long long)h.b_statw[d] * h.inv_scale);
+        e.scalars.push_back(h.s_sum[d]);
+        e.scalars.push_back(h.s_area[d]);
+        e.scalars.push_back(h.s_statw[d]);
+        const size_t before = e.dmask.size();
+        exp_dtree(h, sampling, sampling ? h.s_off[d] : h.b_off[d], 0, e);
+        e.counts.push_back(int64_t(e.dmask.size() - before));
+        return;
+    }
+    exp_stree(h, sampling, code, e);
+    exp_stree(h, sampling, code + 1, e);
+}
+template <class T>
+cudaError_t dl(std::vector<T>& v, const T* p, size_t n, cudaStream_t st) {
+    v.resize(n);
+    if (!n) return cudaSuccess;
+    return cudaMemcpyAsync(v.data(), p, n * sizeof(T), cudaMemcpyDeviceToHost, st);
+}
+}  // namespace
+
+extern "C" int rtpg_sdtree_export(rtpg_sdtree* h, int sampling, int64_t* sizes, uint8_t* smask, float* scalars,
+                                  int64_t* counts, uint8_t* dmask, float* dsums, void* stream) {
+    if (!h || !sizes) return fail(RTPG_EINVAL, "rtpg_sdtree_export: null argument");
+    cudaStream_t st = as_stream(stream);
+    uint32_t c[4];
+    RTPG_CUDA(cudaMemcpyAsync(c, h->dev.counts, sizeof(c), cudaMemcpyDeviceToHost, st));
+    RTPG_CUDA(cudaStreamSynchronize(st));
+    HostTree ht;
+    const SDTreeDev& t = h->dev;
+    ht.inv_scale = t.fx.inv_scale;
+    const uint32_t ns = c[0], nd = c[1];
+    RTPG_CUDA(dl(ht.snode, t.snode, ns, st));
+    RTPG_CUDA(dl(ht.b_off, t.b_off, nd, st));
+    RTPG_CUDA(dl(ht.b_cnt, t.b_cnt, nd, st));
+    RTPG_CUDA(dl(ht.s_off, t.s_off, nd, st));
+    RTPG_CUDA(dl(ht.s_cnt, t.s_cnt, nd, st));
+    RTPG_CUDA(dl(ht.b_statw, t.b_statw, nd, st));
+    RTPG_CUDA(dl(ht.s_sum, t.s_sum, nd, st));
+    RTPG_CUDA(dl(ht.s_area, t.s_area, nd, st));
+    RTPG_CUDA(dl(ht.s_statw, t.s_statw, nd, st));
+    RTPG_CUDA(cudaStreamSynchronize(st));
+    uint32_t bmax = 0, smax = 0;
+    for (uint32_t d = 0; d < nd; ++d) {
+        bmax = std::max(bmax, ht.b_off[d] + ht.b_cnt[d]);
+        smax = std::max(smax, ht.s_off[d] + ht.s_cnt[d]);
+    }
+    RTPG_CUDA(dl(ht.b_child, t.b_child, bmax, st));
+    RTPG_CUDA(dl(ht.b_sums, t.b_sums, size_t(bmax) * 4, st));
+    RTPG_CUDA(dl(ht.s_nodes, t.s_nodes, smax, st));
+    RTPG_CUDA(cudaStreamSynchronize(st));
+    ExportOut e;
+    exp_stree(ht, sampling != 0, 0, e);
+    sizes[0] = (int64_t)e.smask.size();
+    sizes[1] = (int64_t)e.counts.size();
+    sizes[2] = (int64_t)e.dmask.size();
+    if (smask) memcpy(smask, e.smask.data(), e.smask.size());
+    if (scalars) memcpy(scalars, e.scalars.data(), e.scalars.size() * sizeof(float));
+    if (counts) memcpy(counts, e.counts.data(), e.counts.size() * sizeof(int64_t));
+    if (dmask) memcpy(dmask, e.dmask.data(), e.dmask.size());
+    if (dsums) memcpy(dsums, e.dsums.data(), e.dsums.size() * sizeof(float));
+    return RTPG_OK;
+}
+
+// ================================================================== pass controller
+// RTSTreeControllerT (PG.h:1769-1920), host logic unchanged; the Download/Upload pairs
+// around Reset and Build disappear because the tree never leaves the GPU.
+struct rtpg_controller {
+    rtpg_sdtree* tree;
+    uint32_t sample_for_budget, samples_per_launch, iteration_for_built;
+    float ratio_for_budget;
+    bool start = false, executing = false;
+    uint32_t per_all = 0, per_tmp = 0, remain = 0, pass = 0, iteration = 0;
+    int32_t state = RTPG_TRACE_RECORD;
+};
+
+extern "C" {
+
+int rtpg_controller_create(rtpg_sdtree* tree, uint32_t sample_for_budget, uint32_t iteration_for_built,
+                           float ratio_for_budget, uint32_t samples_per_launch, rtpg_controller** out) {
+    if (!tree || !out || samples_per_launch == 0) return fail(RTPG_EINVAL, "rtpg_controller_create: bad arguments");
+    auto* c = new (std::nothrow) rtpg_controller();
+    if (!c) return fail(RTPG_ENOMEM, "rtpg_controller_create: out of host memory");
+    c->tree = tree;
+    c->sample_for_budget = sample_for_budget;
+    c->samples_per_launch = samples_per_launch;
+    c->iteration_for_built = iteration_for_built;
+    c->ratio_for_budget = ratio_for_budget;
+    *out = c;
+    return RTPG_OK;
+}
+int rtpg_controller_destroy(rtpg_controller* c) {
+    delete c;
+    return RTPG_OK;
+}
+int rtpg_controller_start(rtpg_controller* c) {
+    if (!c) return fail(RTPG_EINVAL, "rtpg_controller_start: null handle");
+    c->start = true;  // RTSTreeControllerT::Start, PG.h:1804-1806
+    return RTPG_OK;
+}
+// RTSTreeControllerT::BegTrace (PG.h:1808-1865)
+int rtpg_controller_begin(rtpg_controller* c, void* stream) {
+    if (!c) return fail(RTPG_EINVAL, "rtpg_controller_begin: null handle");
+    int r;
+    if (c->start) {
+        c->per_all = 0;
+        c->per_tmp = 0;
+        c->iteration = 0;
+        c->start = false;
+        c->executing = true;
+        c->remain = ((c->sample_for_budget - 1 + c->samples_per_launch) / c->samples_per_launch) * c->samples_per_launch;
+        c->pass = 0;
+        c->state = RTPG_TRACE_RECORD;
+        if ((r = rtpg_sdtree_clear(c->tree, stream))) return r;
+    }
+    if (!c->executing) return RTPG_OK;
+    if (c->per_tmp == 0) {
+        c->remain -= c->pass;
+        c->pass = std::min<uint32_t>(c->remain, (1u << c->iteration) * c->samples_per_launch);
+        if ((c->remain - c->pass < 2 * c->pass) ||
+            (c->per_all >= c->ratio_for_budget * static_cast<float>(c->sample_for_budget)))
+            c->pass = c->remain;
+        if (c->remain > c->pass)
+            if ((r = rtpg_sdtree_reset(c->tree, (int32_t)c->iteration, (int32_t)c->pass, stream))) return r;
+    }
+    if (c->iteration > c->iteration_for_built)
+        c->state = c->remain > c->pass ? RTPG_TRACE_RECORD_AND_SAMPLE : RTPG_TRACE_SAMPLE;
+    else
+        c->state = RTPG_TRACE_RECORD;
+    return RTPG_OK;
+}
+// RTSTreeControllerT::EndTrace (PG.h:1867-1887)
+int rtpg_controller_end(rtpg_controller* c, void* stream) {
+    if (!c) return fail(RTPG_EINVAL, "rtpg_controller_end: null handle");
+    if (!c->executing) return RTPG_OK;
+    c->per_all += c->samples_per_launch;
+    c->per_tmp += c->samples_per_launch;
+    if (c->per_tmp >= c->pass) {
+        int r = rtpg_sdtree_build(c->tree, stream);
+        if (r) return r;
+        c->iteration++;
+        c->per_tmp = 0;
+    }
+    if (c->per_all > c->sample_for_budget) {
+        c->executing = false;
+        c->per_all = 0;
+    }
+    return RTPG_OK;
+}
+int rtpg_controller_get(rtpg_controller* c, int32_t* state, uint32_t* iteration, uint32_t* samples_in_pass,
+                        int32_t* executing) {
+    if (!c) return fail(RTPG_EINVAL, "rtpg_controller_get: null handle");
+    if (state) *state = c->state;
+    if (iteration) *iteration = c->iteration;
+    if (samples_in_pass) *samples_in_pass = c->per_tmp;
+    if (executing) *executing = c->executing ? 1 : 0;
+    return RTPG_OK;
+}
+
+}  // extern "C"

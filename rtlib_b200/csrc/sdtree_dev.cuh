@@ -1,0 +1,226 @@
+// Device-side SD-tree layout and per-query routines (record descent, guided sample, pdf).
+//
+// Layout in HBM (all capacities fixed at creation, counts live in device memory):
+//   STree   snode[i] (u32): leaf -> kLeafBit | dtree index, interior -> index of child 0
+//           (child 1 = child 0 + 1).  The split axis of a node is its depth mod 3, as
+//           RTLib's SubDivide assigns it (OPX7UtilsPathGuiding.h:1240).
+//   DTrees  per tree d: building range b_off/b_cnt, sampling range s_off/s_cnt, building
+//           stat-weight (int64 fixed point), sampling sum / area / stat-weight (float),
+//           level starts of the breadth-first building tree.
+//   pools   building nodes: 4 x u64 fixed-point sums (32 B) + ushort4 local children;
+//           sampling nodes: SNode, 32 B = one DRAM sector: float4 sums + ushort4 children.
+#pragma once
+#include "common.cuh"
+#include "limits.cuh"
+
+namespace rtpg {
+
+constexpr uint32_t kLeafBit = 0x80000000u;
+constexpr uint32_t kMaxLevels = kMaxDTreeDepth + 1;  // level-start entries per tree
+
+struct __align__(32) SNode {
+    float4 sums;
+    ushort4 child;  // local index of the child quadtree node, 0 = leaf quadrant
+    uint32_t pad0, pad1;
+};
+
+struct SDTreeDev {
+    float3 mn, mx;  // cubified AABB
+    FixedPoint fx;
+    unsigned* status;
+    uint32_t* counts;  // [0] STree nodes, [1] DTrees, [2] building nodes in use
+    uint32_t* snode;
+    uint32_t* b_off;
+    uint32_t* b_cnt;
+    uint32_t* s_off;
+    uint32_t* s_cnt;
+    unsigned long long* b_statw;
+    float* s_sum;
+    float* s_area;
+    float* s_statw;
+    uint16_t* b_lvl;  // kMaxLevels + 1 per tree
+    uint8_t* b_nlvl;
+    unsigned long long* b_sums;  // 4 per building node
+    ushort4* b_child;
+    float* b_area;  // per building node, scratch of the build
+    SNode* s_nodes;
+    uint32_t cap_snodes, cap_dtrees, cap_nodes;
+    uint32_t max_depth;
+    float fraction;
+};
+
+// STreeT::GetDTreeWrapper (PG.h:639-648) with STreeNodeT::GetChildIdx (PG.h:546-552):
+// p = (pos - min) / (max - min); at each interior node p[axis] *= 2, idx = int(p[axis]),
+// p[axis] -= idx.  idx is clamped to [0,1] so that p == 1 or points outside the box stay
+// in bounds.  Also returns the voxel size (the reference halves size[axis] per level).
+__device__ __forceinline__ uint32_t stree_lookup(const uint32_t* __restrict__ snode, float3 mn, float3 mx, float px,
+                                                 float py, float pz) {
+    const float sx = __fsub_rn(mx.x, mn.x), sy = __fsub_rn(mx.y, mn.y), sz = __fsub_rn(mx.z, mn.z);
+    float p[3] = {__fdiv_rn(__fsub_rn(px, mn.x), sx), __fdiv_rn(__fsub_rn(py, mn.y), sy),
+                  __fdiv_rn(__fsub_rn(pz, mn.z), sz)};
+    uint32_t code = snode[0];
+    int axis = 0;
+    while (!(code & kLeafBit)) {
+        const float v = __fmul_rn(p[axis], 2.0f);
+        int idx = __float2int_rz(v);
+        idx = idx < 0 ? 0 : (idx > 1 ? 1 : idx);
+        p[axis] = __fsub_rn(v, (float)idx);
+        code = snode[code + (uint32_t)idx];
+        axis = axis == 2 ? 0 : axis + 1;
+    }
+    return code & ~kLeafBit;
+}
+__device__ __forceinline__ uint32_t stree_lookup_voxel(const uint32_t* __restrict__ snode, float3 mn, float3 mx,
+                                                       float px, float py, float pz, float3& voxel) {
+    const float sx = __fsub_rn(mx.x, mn.x), sy = __fsub_rn(mx.y, mn.y), sz = __fsub_rn(mx.z, mn.z);
+    float p[3] = {__fdiv_rn(__fsub_rn(px, mn.x), sx), __fdiv_rn(__fsub_rn(py, mn.y), sy),
+                  __fdiv_rn(__fsub_rn(pz, mn.z), sz)};
+    float s[3] = {sx, sy, sz};
+    uint32_t code = snode[0];
+    int axis = 0;
+    while (!(code & kLeafBit)) {
+        const float v = __fmul_rn(p[axis], 2.0f);
+        int idx = __float2int_rz(v);
+        idx = idx < 0 ? 0 : (idx > 1 ? 1 : idx);
+        p[axis] = __fsub_rn(v, (float)idx);
+        s[axis] = s[axis] / 2.0f;
+        code = snode[code + (uint32_t)idx];
+        axis = axis == 2 ? 0 : axis + 1;
+    }
+    voxel = make_float3(s[0], s[1], s[2]);
+    return code & ~kLeafBit;
+}
+
+// DTreeNodeT::GetChildIdx (PG.h:69-82)
+__device__ __forceinline__ int quad_child(float& u, float& v) {
+    int r = 0;
+    if (u < 0.5f) u = __fmul_rn(u, 2.0f);
+    else { u = __fsub_rn(__fmul_rn(2.0f, u), 1.0f); r |= 1; }
+    if (v < 0.5f) v = __fmul_rn(v, 2.0f);
+    else { v = __fsub_rn(__fmul_rn(2.0f, v), 1.0f); r |= 2; }
+    return r;
+}
+
+// Building-tree descent of DTreeNodeT::Record (PG.h:113-125): returns the global index of the
+// quadrant sum (node * 4 + quadrant) the record lands in.
+__device__ __forceinline__ uint32_t dtree_record_slot(const ushort4* __restrict__ b_child, uint32_t off, float u,
+                                                      float v) {
+    uint32_t cur = 0;
+    int idx = quad_child(u, v);
+    for (;;) {
+        const ushort4 c = b_child[off + cur];
+        const uint32_t nxt = idx == 0 ? c.x : (idx == 1 ? c.y : (idx == 2 ? c.z : c.w));
+        if (!nxt) break;
+        cur = nxt;
+        idx = quad_child(u, v);
+    }
+    return (off + cur) * 4u + (uint32_t)idx;
+}
+
+__device__ __forceinline__ float sel4(const float4& s, int i) { return i == 0 ? s.x : (i == 1 ? s.y : (i == 2 ? s.z : s.w)); }
+__device__ __forceinline__ uint32_t sel4(const ushort4& s, int i) { return i == 0 ? s.x : (i == 1 ? s.y : (i == 2 ? s.z : s.w)); }
+
+// DTreeT::GetMean (PG.h:447-451)
+__device__ __forceinline__ float dtree_mean(float statw, float sum) {
+    if (statw <= 0.0f) return 0.0f;
+    const float factor = __fdiv_rn(kInv2Pi, __fmul_rn(2.0f, statw));
+    return __fmul_rn(factor, sum);
+}
+
+// DTreeT::Sample (PG.h:478-484) -> DTreeNodeT::Sample (PG.h:229-277), float order as written.
+__device__ __forceinline__ float2 dtree_sample(const SNode* __restrict__ nodes, uint32_t off, float statw, float sum,
+                                               uint32_t& rng) {
+    if (dtree_mean(statw, sum) <= 0.0f) {
+        const float a = rnd1(rng);
+        const float b = rnd1(rng);
+        return make_float2(a, b);
+    }
+    uint32_t cur = 0;
+    float rx = 0.0f, ry = 0.0f, size = 1.0f;
+    for (;;) {
+        const SNode nd = nodes[off + cur];
+        const float4 s = nd.sums;
+        int idx = 0;
+        const float topLeft = s.x, topRight = s.y;
+        float partial = __fadd_rn(s.x, s.z);
+        const float total = __fadd_rn(__fadd_rn(__fadd_rn(s.x, s.y), s.z), s.w);
+        float boundary = __fdiv_rn(partial, total);
+        float ox = 0.0f, oy = 0.0f;
+        float sample = rnd1(rng);
+        if (sample < boundary) {
+            sample = __fdiv_rn(sample, boundary);
+            boundary = __fdiv_rn(topLeft, partial);
+        } else {
+            partial = __fsub_rn(total, partial);
+            ox = 0.5f;
+            sample = __fdiv_rn(__fsub_rn(sample, boundary), __fsub_rn(1.0f, boundary));
+            boundary = __fdiv_rn(topRight, partial);
+            idx |= 1;
+        }
+        if (sample >= boundary) {
+            oy = 0.5f;
+            idx |= 2;
+        }
+        rx = __fadd_rn(rx, __fmul_rn(size, ox));
+        ry = __fadd_rn(ry, __fmul_rn(size, oy));
+        size = __fmul_rn(size, 0.5f);
+        const uint32_t c = sel4(nd.child, idx);
+        if (c == 0 || sel4(s, idx) <= 0.0f) {
+            const float a = rnd1(rng);
+            const float b = rnd1(rng);
+            rx = __fadd_rn(rx, __fmul_rn(size, a));
+            ry = __fadd_rn(ry, __fmul_rn(size, b));
+            break;
+        }
+        cur = c;
+    }
+    return make_float2(fminf(fmaxf(rx, 0.0f), 1.0f), fminf(fmaxf(ry, 0.0f), 1.0f));
+}
+
+// DTreeT::Pdf (PG.h:485-490) -> DTreeNodeT::Pdf (PG.h:279-320)
+__device__ __forceinline__ float dtree_pdf(const SNode* __restrict__ nodes, uint32_t off, float statw, float sum,
+                                           float u, float v) {
+    if (dtree_mean(statw, sum) <= 0.0f) return __fdiv_rn(__fmul_rn(1.0f, kInv2Pi), 2.0f);
+    float result = 1.0f;
+    uint32_t cur = 0;
+    int idx = quad_child(u, v);
+    for (;;) {
+        const SNode nd = nodes[off + cur];
+        const float4 s = nd.sums;
+        const float total = __fadd_rn(__fadd_rn(__fadd_rn(s.x, s.y), s.z), s.w);
+        const float si = sel4(s, idx);
+        if (si <= 0.0f) {
+            result = 0.0f;
+            break;
+        }
+        result = __fmul_rn(result, __fdiv_rn(__fmul_rn(4.0f, si), total));
+        const uint32_t c = sel4(nd.child, idx);
+        if (!c) break;
+        cur = c;
+        idx = quad_child(u, v);
+    }
+    return __fdiv_rn(__fmul_rn(result, kInv2Pi), 2.0f);
+}
+
+// canonical_to_dir / dir_to_canonical (VectorFunction.h:5698-5720)
+__device__ __forceinline__ float3 canonical_to_dir(float u, float v) {
+    const float cosTheta = 2.0f * u - 1.0f;
+    const float sinTheta = sqrtf(1.0f - cosTheta * cosTheta);
+    const float phi = k2Pi * v;
+    float sp, cp;
+    sincosf(phi, &sp, &cp);
+    return make_float3(sinTheta * cp, sinTheta * sp, cosTheta);
+}
+__device__ __forceinline__ float2 dir_to_canonical(float x, float y, float z) {
+    if (!isfinite(x) || !isfinite(y) || !isfinite(z)) return make_float2(0.0f, 0.0f);
+    z = fminf(fmaxf(z, -1.0f), 1.0f);
+    float phi = atan2f(y, x);
+    while (phi < 0.0f) phi += k2Pi;
+    return make_float2((z + 1.0f) / 2.0f, phi * kInv2Pi);
+}
+__device__ __forceinline__ float3 normalize3(float3 v) {
+    const float l = sqrtf(v.x * v.x + v.y * v.y + v.z * v.z);
+    return make_float3(v.x / l, v.y / l, v.z / l);
+}
+
+}  // namespace rtpg
