@@ -36,7 +36,7 @@ N_Q = 1 << 22
 # algorithmic bytes of one sample+pdf query: position in (12 B), direction (12 B) and pdf
 # (4 B) out; the Xorshift32 seed is derived from the query index
 Q_BYTES = 28
-LAUNCHES_PER_STEP = 20  # clear 1, record 1, build 1, refine 16, sample 1
+LAUNCHES_PER_STEP = 21  # clear 1, record 1, build 1, refine 17, sample 1
 
 
 def _env_int(k, d):
@@ -47,50 +47,54 @@ def _env_int(k, d):
 
 
 class ClockSampler:
-    """nvidia-smi samples every 200 ms while the timed region runs."""
+    """SM clock and throttle reasons sampled through NVML every ~2 ms while the timed region
+    runs (reading only; no setting of the GPU is touched)."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40,
+               "hw_power_brake_slowdown": 0x80, "sw_power_cap": 0x4}
 
     def __init__(self, gpu_index):
         self.gpu = gpu_index
-        self.proc = None
-        self.path = None
+        self.samples = []
+        self.run = False
+        self.th = None
+        self.nv = None
 
     def start(self):
-        fd, self.path = tempfile.mkstemp(suffix=".csv")
-        os.close(fd)
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
-                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
-        except OSError:
-            self.proc = None
+            import pynvml as nv
+            nv.nvmlInit()
+            self.nv = nv
+            self.h = nv.nvmlDeviceGetHandleByIndex(self.gpu)
+            self.max_mhz = nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM)
+        except Exception as e:  # noqa: BLE001
+            self.err = str(e)
+            return
+        self.run = True
+
+        def loop():
+            while self.run:
+                try:
+                    self.samples.append((self.nv.nvmlDeviceGetClockInfo(self.h, self.nv.NVML_CLOCK_SM),
+                                         self.nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)))
+                except Exception:  # noqa: BLE001
+                    pass
+                time.sleep(0.002)
+
+        self.th = threading.Thread(target=loop, daemon=True)
+        self.th.start()
 
     def stop(self):
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-        rows = []
-        with open(self.path) as f:
-            for line in f:
-                p = [x.strip() for x in line.split(",")]
-                if len(p) >= 9:
-                    rows.append(p)
-        os.unlink(self.path)
-        if not rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(rows)}
+        if self.nv is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [f"nvml unavailable: {getattr(self, 'err', '')}"]}
+        self.run = False
+        self.th.join()
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["no samples"]}
+        mhz = [m for m, _ in self.samples]
+        reasons = sorted({k for _, r in self.samples for k, bit in self.REASONS.items() if r & bit})
+        return {"sm_mhz": statistics.median(mhz), "sm_max_mhz": self.max_mhz, "reasons": reasons,
+                "samples": len(self.samples), "source": "nvml, ~2 ms period"}
 
 
 def _peaks():
@@ -110,6 +114,15 @@ def _sdtree_inputs():
     return rec, q, W.spatial_threshold(1)
 
 
+def _traffic(kernel):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary, or None."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f).get(kernel)
+    return None
+
+
 def bench_sdtree_ours(args, rank, world):
     import torch
     from rtlib_b200.sdtree import SDTree
@@ -124,20 +137,39 @@ def bench_sdtree_ours(args, rank, world):
     out_pdf = torch.empty(N_Q, dtype=torch.float32, device=dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     tree = SDTree((0, 0, 0), (1, 1, 1))
-    stream = torch.cuda.current_stream()
 
-    def step(p, u, r, qp):
+    def build_part(p, u, r):
         tree.clear()
         tree.record(p, u, r)
         tree.build()
         tree.refine(th)
-        tree.sample_pdf(qp, None, seed_base=0, out_dir=out_dir, out_pdf_dir=out_pdf)
 
-    for _ in range(args.warmup):
-        step(pos, uv, rad, qpos)
+    def sample_part(qp):
+        # guided direction + pdf of the sampled point (DTreeT::Sample + DTreeT::Pdf)
+        tree.sample_pdf(qp, None, seed_base=0, out_dir=out_dir, out_pdf_uv=out_pdf)
+
+    # one CUDA graph per half of the step (the split lets the sample kernel be timed alone)
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):
+        for _ in range(2):
+            build_part(pos, uv, rad)
+            sample_part(qpos)
+    torch.cuda.current_stream().wait_stream(side)
+    g_build, g_sample = torch.cuda.CUDAGraph(), torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g_build):
+        build_part(pos, uv, rad)
+    with torch.cuda.graph(g_sample):
+        sample_part(qpos)
+    stream = torch.cuda.current_stream()
+    t0 = time.perf_counter()
+    k = 0
+    while k < args.warmup or time.perf_counter() - t0 < 0.5:  # also lets the clocks ramp up
+        g_build.replay()
+        g_sample.replay()
+        k += 1
     torch.cuda.synchronize()
 
-    # device-resident timed steps, with the sample kernel timed on its own as well
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
            torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     clocks = ClockSampler(dev.index)
@@ -148,12 +180,9 @@ def bench_sdtree_ours(args, rank, world):
         flush.fill_(k & 0xff)
         a, b, c = ev[k]
         a.record(stream)
-        tree.clear()
-        tree.record(pos, uv, rad)
-        tree.build()
-        tree.refine(th)
+        g_build.replay()
         b.record(stream)
-        tree.sample_pdf(qpos, None, seed_base=0, out_dir=out_dir, out_pdf_dir=out_pdf)
+        g_sample.replay()
         c.record(stream)
     torch.cuda.synchronize()
     _barrier(world)
@@ -162,8 +191,10 @@ def bench_sdtree_ours(args, rank, world):
     sample_ms = [b.elapsed_time(c) for a, b, c in ev]
     ms = sum(step_ms) / len(step_ms)
     ms = _max_over_ranks(ms, world, dev)
+    st = tree.stats()
+    assert tree.status() == 0
 
-    # e2e: pinned host buffers through the same calls, copies inside the timed region
+    # e2e: pinned host buffers through the same C-ABI calls, copies inside the timed region
     hp = {k: torch.from_numpy(v).pin_memory() for k, v in (("pos", rec["pos"]), ("uv", rec["uv"]),
                                                           ("rad", rec["radiance"]), ("qpos", q["pos"]))}
     h_dir = torch.empty((N_Q, 3), dtype=torch.float32).pin_memory()
@@ -180,7 +211,8 @@ def bench_sdtree_ours(args, rank, world):
         duv.copy_(hp["uv"], non_blocking=True)
         drad.copy_(hp["rad"], non_blocking=True)
         dq.copy_(hp["qpos"], non_blocking=True)
-        step(dpos, duv, drad, dq)
+        build_part(dpos, duv, drad)
+        sample_part(dq)
         h_dir.copy_(out_dir, non_blocking=True)
         h_pdf.copy_(out_pdf, non_blocking=True)
         c.record(stream)
@@ -200,11 +232,12 @@ def bench_sdtree_ours(args, rank, world):
         "e2e": {"value": ops / (e2e * 1e-3) / 1e6, "unit": "Mops/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "roofline": {"kernel": "k_sample_pdf", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
-                     "algorithmic_bytes_per_launch": Q_BYTES * N_Q, "launch_ms": s_ms},
+                     "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs (burst copy)",
+                     "traffic": _traffic("k_sample_pdf"), "algorithmic_bytes_per_launch": Q_BYTES * N_Q,
+                     "launch_ms": s_ms},
         "clocks": clk,
         "gpu_launches": LAUNCHES_PER_STEP * args.steps,
-        "sdtree": tree.stats(),
+        "sdtree": st,
     }
 
 

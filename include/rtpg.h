@@ -141,6 +141,72 @@ int rtpg_controller_end(rtpg_controller* c, void* stream);
 int rtpg_controller_get(rtpg_controller* c, int32_t* host_state, uint32_t* host_iteration,
                         uint32_t* host_samples_in_pass, int32_t* host_executing);
 
+/* ================================================================ hash grid
+ * Replaces DoubleBufferedHashGrid3T (RTLib/Src/Ext/OPX7/Include/RTLib/Ext/OPX7/Utils/
+ * OPX7UtilsGrid.h:157-353, "GR.h") and its host buffer DoubleBufferedHashGrid3Buffer
+ * (RTLib/Src/Ext/OPX7/Test/Include/RTLibExtOPX7Test.h:1472-1570, "T.h"). */
+typedef struct rtpg_hashgrid rtpg_hashgrid;
+#define RTPG_HASH_KEY_REFERENCE 0 /* RTLib's bucket hash (pcg1d chain) and uint32 checksum */
+#define RTPG_HASH_KEY_MORTON 1    /* 63-bit Morton code of the cell (21 bits per axis) */
+/* DoubleBufferedHashGrid3Buffer::Alloc(gridSize, cellSize) + GetHandle (T.h:1503-1507,
+ * 1561-1568): grid `bounds` over [aabb_min, aabb_max], num_slots slots (a multiple of 32,
+ * buckets of 32).  max_batch bounds the scratch of one insert chunk (0 = 1<<22). */
+int rtpg_hashgrid_create(const float host_aabb_min[3], const float host_aabb_max[3], const uint32_t host_bounds[3],
+                         uint32_t num_slots, int32_t keying, uint32_t max_batch, rtpg_hashgrid** out);
+int rtpg_hashgrid_destroy(rtpg_hashgrid* h);
+/* DoubleBufferedHashGrid3Buffer::Clear (T.h:1529-1543): empty both tables. */
+int rtpg_hashgrid_clear(rtpg_hashgrid* h, void* stream);
+/* DoubleBufferedHashGrid3Buffer::Update (T.h:1544-1559): previous := current. */
+int rtpg_hashgrid_swap(rtpg_hashgrid* h, void* stream);
+/* DoubleBufferedHashGrid3T::FindFromCur (GR.h:189-216, 246-277) for a batch of points:
+ * out_slot[i] = slot of the point's cell in the current table (inserted if absent), or
+ * UINT32_MAX when the bucket is full.  Slots are those of inserting the points one by one
+ * in index order.  out_key (optional) receives each point's key. */
+int rtpg_hashgrid_insert(rtpg_hashgrid* h, int64_t n, const float* pos, uint32_t* out_slot, uint64_t* out_key,
+                         void* stream);
+/* DoubleBufferedHashGrid3T::FindFromPrv (GR.h:217-237, 278-300): slot in the previous table
+ * or UINT32_MAX. */
+int rtpg_hashgrid_lookup(rtpg_hashgrid* h, int64_t n, const float* pos, uint32_t* out_slot, void* stream);
+/* Cell coordinates (n x uint3) and keys of points (either output optional). */
+int rtpg_hashgrid_cells(rtpg_hashgrid* h, int64_t n, const float* pos, uint32_t* out_cell_xyz, uint64_t* out_key,
+                        void* stream);
+/* Copy the current (previous = 0) or previous (1) table (num_slots keys, 0 = empty). */
+int rtpg_hashgrid_export(rtpg_hashgrid* h, int previous, uint64_t* host_table, void* stream);
+int rtpg_hashgrid_status(rtpg_hashgrid* h, uint32_t* host_status, int clear, void* stream);
+/* Device pointers of the two tables (uint64 keys), for kernels that probe them directly. */
+int rtpg_hashgrid_device_view(rtpg_hashgrid* h, void** dev_current, void** dev_previous);
+
+/* ================================================================ Morton quadtrees
+ * Replaces MortonQuadTreeT / MortonQuadTreeWrapperT / RTMortonQuadTreeWrapperT
+ * (RTLib/Src/Ext/OPX7/Include/RTLib/Ext/OPX7/Utils/OPX7UtilsMorton.h, "MO.h") and
+ * mortonBuildKernel (OPX7UtilsMortonBuild.cu:2-16): one complete quadtree of `level`
+ * levels per hash-grid cell. */
+typedef struct rtpg_mqt rtpg_mqt;
+/* RTMortonQuadTreeWrapperT(ctx, maxHashSize, maxTreeLevel, fraction) + Allocate
+ * (MO.h:597-638); leaves accumulate as int64(value * 2^fixed_point_bits) (0 = 24). */
+int rtpg_mqt_create(uint32_t num_cells, uint32_t level, float fraction, int32_t fixed_point_bits, rtpg_mqt** out);
+int rtpg_mqt_destroy(rtpg_mqt* h);
+/* zero the building leaves and the sampling pyramid (Allocate on a live wrapper, MO.h:618-637) */
+int rtpg_mqt_clear(rtpg_mqt* h, void* stream);
+/* MortonQuadTreeWrapperT::Record (MO.h:477-484) -> MortonQuadTreeT::Record (MO.h:262-285):
+ * leaf-only accumulation; cell UINT32_MAX, non-finite and non-positive values are skipped. */
+int rtpg_mqt_record(rtpg_mqt* h, int64_t n, const uint32_t* cell, const float* dir, int dir_is_canonical,
+                    const float* value, void* stream);
+/* RTMortonQuadTreeWrapperT::Update + mortonBuildKernel (MO.h:640-651, 916-941): the sampling
+ * pyramid is rebuilt from the building leaves, which are then zeroed. */
+int rtpg_mqt_update(rtpg_mqt* h, void* stream);
+/* MortonQuadTreeWrapperT::SampleAndPdf (MO.h:486-500): out_pdf includes 1/(4 pi);
+ * out_pdf_tree is the tree-level pdf of MortonQuadTreeT::SampleAndPdf (MO.h:286-344). */
+int rtpg_mqt_sample_pdf(rtpg_mqt* h, int64_t n, const uint32_t* cell, const uint32_t* seeds, uint32_t seed_base,
+                        float* out_uv, float* out_pdf, float* out_dir, float* out_pdf_tree, void* stream);
+/* MortonQuadTreeWrapperT::Pdf (MO.h:515-524), or MortonQuadTreeT::Pdf (MO.h:401-414) when
+ * tree_level = 1. */
+int rtpg_mqt_pdf(rtpg_mqt* h, int64_t n, const uint32_t* cell, const float* dir, int dir_is_canonical, float* out,
+                 int tree_level, void* stream);
+/* Copy the building leaves (int64) and / or the sampling pyramid (float); NULL skips. */
+int rtpg_mqt_export(rtpg_mqt* h, int64_t* host_leaves, float* host_pyramid, void* stream);
+int rtpg_mqt_status(rtpg_mqt* h, uint32_t* host_status, int clear, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -47,6 +47,25 @@ _SIGS = {
     "rtpg_controller_begin": [P, P],
     "rtpg_controller_end": [P, P],
     "rtpg_controller_get": [P, P, P, P, P],
+    "rtpg_hashgrid_create": [P, P, P, U32, I32, U32, P],
+    "rtpg_hashgrid_destroy": [P],
+    "rtpg_hashgrid_clear": [P, P],
+    "rtpg_hashgrid_swap": [P, P],
+    "rtpg_hashgrid_insert": [P, I64, P, P, P, P],
+    "rtpg_hashgrid_lookup": [P, I64, P, P, P],
+    "rtpg_hashgrid_cells": [P, I64, P, P, P, P],
+    "rtpg_hashgrid_export": [P, C.c_int, P, P],
+    "rtpg_hashgrid_status": [P, P, C.c_int, P],
+    "rtpg_hashgrid_device_view": [P, P, P],
+    "rtpg_mqt_create": [U32, U32, F32, I32, P],
+    "rtpg_mqt_destroy": [P],
+    "rtpg_mqt_clear": [P, P],
+    "rtpg_mqt_record": [P, I64, P, P, C.c_int, P, P],
+    "rtpg_mqt_update": [P, P],
+    "rtpg_mqt_sample_pdf": [P, I64, P, P, U32, P, P, P, P, P],
+    "rtpg_mqt_pdf": [P, I64, P, P, C.c_int, P, C.c_int, P],
+    "rtpg_mqt_export": [P, P, P, P],
+    "rtpg_mqt_status": [P, P, C.c_int, P],
 }
 _RESTYPE = {"rtpg_last_error": C.c_char_p}
 

@@ -1,0 +1,259 @@
+// Morton-indexed directional quadtrees, one complete tree per hash-grid cell (RTLib's "HashTree"
+// guide: MortonQuadTreeT / MortonQuadTreeWrapperT, OPX7UtilsMorton.h:253-531, host wrapper
+// RTMortonQuadTreeWrapperT :590-764, pyramid build mortonBuildKernel,
+// OPX7UtilsMortonBuild.cu:2-16).
+//
+// Layout in HBM: building leaves, int64 fixed point, cell-major: leaves[cell * 4^L + code]
+// (the reference records only the leaf level too, OPX7UtilsMorton.h:282-283); sampling
+// pyramid, float, per cell (4^(L+1)-1)/3 entries, level l at offset (4^l-1)/3, Morton order
+// inside a level (code = part1by1(y) << 1 | part1by1(x)).
+//
+// Update (RTMortonQuadTreeWrapperT::Update + LaunchBuildKernel, :640-651, :916-941) is one
+// kernel: a CTA per cell reads the cell's leaves, reduces the pyramid in shared memory with
+// exact integer sums, writes it as float to the sampling buffer and zeroes the leaves
+// (RTLib launches 1024x more blocks than cells and loops serially per cell).
+#include <new>
+#include <vector>
+
+#include "common.cuh"
+#include "limits.cuh"
+#include "mqt_dev.cuh"
+
+namespace rtpg {
+
+constexpr int kMqtBuildBlock = 256;
+
+__global__ void __launch_bounds__(256) k_mqt_record(MqtDev t, int64_t n, const uint32_t* __restrict__ cell,
+                                                    const float* __restrict__ dir, int canonical,
+                                                    const float* __restrict__ value) {
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    for (int64_t base = int64_t(blockIdx.x) * blockDim.x; base < n; base += stride) {
+        const int64_t i = base + threadIdx.x;
+        unsigned long long key = ~0ull, v = 0;
+        if (i < n) {
+            const uint32_t c = cell[i];
+            const float x = value[i];
+            if (c != 0xffffffffu && c < t.ncells && isfinite(x) && x > 0.0f) {
+                float2 uv;
+                if (canonical) uv = reinterpret_cast<const float2*>(dir)[i];
+                else uv = dir_to_canonical_mqt(dir[3 * i], dir[3 * i + 1], dir[3 * i + 2]);
+                key = ((unsigned long long)c << (2 * t.level)) + mqt_leaf_code(t.level, uv.x, uv.y);
+                v = to_fx(x, t.fx, t.status);
+            }
+        }
+        warp_add_u64(key, v, t.leaves);
+    }
+}
+
+// One CTA per cell: leaves -> exact pyramid in shared memory -> float sampling pyramid.
+__global__ void __launch_bounds__(kMqtBuildBlock) k_mqt_build(MqtDev t) {
+    extern __shared__ unsigned long long sp[];  // (4^(L+1)-1)/3 entries
+    const uint32_t L = t.level;
+    const uint32_t nleaf = 1u << (2 * L);
+    const uint32_t off_leaf = mqt_level_offset(L);
+    const uint32_t per = mqt_level_offset(L + 1);
+    for (uint32_t c = blockIdx.x; c < t.ncells; c += gridDim.x) {
+        unsigned long long* lf = t.leaves + (size_t)c * nleaf;
+        for (uint32_t k = threadIdx.x; k < nleaf; k += blockDim.x) {
+            sp[off_leaf + k] = lf[k];
+            lf[k] = 0ull;
+        }
+        __syncthreads();
+        for (int l = (int)L - 1; l >= 0; --l) {
+            const uint32_t o = mqt_level_offset(l), oc = mqt_level_offset(l + 1), cnt = 1u << (2 * l);
+            for (uint32_t k = threadIdx.x; k < cnt; k += blockDim.x)
+                sp[o + k] = sp[oc + 4 * k] + sp[oc + 4 * k + 1] + sp[oc + 4 * k + 2] + sp[oc + 4 * k + 3];
+            __syncthreads();
+        }
+        float* w = t.pyramid + (size_t)c * per;
+        for (uint32_t k = threadIdx.x; k < per; k += blockDim.x) w[k] = fx_to_float(sp[k], t.fx);
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(256) k_mqt_sample(MqtDev t, int64_t n, const uint32_t* __restrict__ cell,
+                                                    const uint32_t* __restrict__ seeds, uint32_t seed_base,
+                                                    float* __restrict__ out_uv, float* __restrict__ out_pdf,
+                                                    float* __restrict__ out_dir, float* __restrict__ out_pdf_tree) {
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const uint32_t c = cell[i];
+        uint32_t rng = seeds ? seeds[i] : (pcg1d(seed_base + (uint32_t)i) | 1u);
+        float pdf;
+        const float2 uv = mqt_sample_and_pdf(t, c, rng, pdf);
+        if (out_uv) reinterpret_cast<float2*>(out_uv)[i] = uv;
+        if (out_pdf_tree) out_pdf_tree[i] = pdf;
+        // MortonQuadTreeWrapperT::SampleAndPdf (OPX7UtilsMorton.h:486-500):
+        // pdf *= (0.25f * RTLIB_M_INV_PI), evaluated in double as written
+        if (out_pdf) out_pdf[i] = (float)((double)pdf * (0.25 * kInvPiD));
+        if (out_dir) {
+            const float3 d = canonical_to_dir_mqt(uv.x, uv.y);
+            out_dir[3 * i] = d.x;
+            out_dir[3 * i + 1] = d.y;
+            out_dir[3 * i + 2] = d.z;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) k_mqt_pdf(MqtDev t, int64_t n, const uint32_t* __restrict__ cell,
+                                                 const float* __restrict__ dir, int canonical, float* __restrict__ out,
+                                                 int tree_level) {
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
+        float2 uv;
+        if (canonical) uv = reinterpret_cast<const float2*>(dir)[i];
+        else uv = dir_to_canonical_mqt(dir[3 * i], dir[3 * i + 1], dir[3 * i + 2]);
+        const float p = mqt_pdf(t, cell[i], uv.x, uv.y);
+        // MortonQuadTreeWrapperT::Pdf (:515-524): tree.Pdf(dir2) * 0.25f * RTLIB_M_INV_PI
+        out[i] = tree_level ? p : (float)((double)(p * 0.25f) * kInvPiD);
+    }
+}
+
+}  // namespace rtpg
+
+using namespace rtpg;
+
+struct rtpg_mqt {
+    MqtDev dev{};
+    std::vector<void*> allocs;
+    size_t bytes = 0;
+    template <class T>
+    int alloc(T** p, size_t count) {
+        void* q = nullptr;
+        cudaError_t e = cudaMalloc(&q, count * sizeof(T));
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return fail(RTPG_ENOMEM, "cudaMalloc(%zu bytes) failed: %s", count * sizeof(T), cudaGetErrorString(e));
+        }
+        allocs.push_back(q);
+        bytes += count * sizeof(T);
+        *p = static_cast<T*>(q);
+        return RTPG_OK;
+    }
+    ~rtpg_mqt() {
+        for (void* p : allocs) cudaFree(p);
+    }
+};
+
+static int mqt_smem(uint32_t level) { return int(mqt_level_offset(level + 1) * sizeof(unsigned long long)); }
+
+extern "C" {
+
+// RTMortonQuadTreeWrapperT(ctx, maxHashSize, maxTreeLevel, fraction) + Allocate (MO.h:597-638)
+int rtpg_mqt_create(uint32_t num_cells, uint32_t level, float fraction, int32_t fixed_point_bits, rtpg_mqt** out) {
+    if (!out || num_cells == 0) return fail(RTPG_EINVAL, "rtpg_mqt_create: bad arguments");
+    if (level < 1 || level > kMqtMaxLevel) return fail(RTPG_EINVAL, "rtpg_mqt_create: level must be in [1, %u]", kMqtMaxLevel);
+    if (fixed_point_bits == 0) fixed_point_bits = 24;
+    if (fixed_point_bits < 0 || fixed_point_bits > 40) return fail(RTPG_EINVAL, "rtpg_mqt_create: fixed_point_bits in [0,40]");
+    auto* h = new (std::nothrow) rtpg_mqt();
+    if (!h) return fail(RTPG_ENOMEM, "rtpg_mqt_create: out of host memory");
+    MqtDev& t = h->dev;
+    t.ncells = num_cells;
+    t.level = level;
+    t.fraction = fraction;
+    t.fx.scale = ldexpf(1.0f, fixed_point_bits);
+    t.fx.inv_scale = ldexpf(1.0f, -fixed_point_bits);
+    const size_t nleaf = (size_t)num_cells << (2 * level), npyr = (size_t)num_cells * mqt_level_offset(level + 1);
+    int r;
+    if ((r = h->alloc(&t.leaves, nleaf)) || (r = h->alloc(&t.pyramid, npyr)) || (r = h->alloc(&t.status, 1))) {
+        delete h;
+        return r;
+    }
+    if (cudaMemset(t.leaves, 0, nleaf * 8) != cudaSuccess || cudaMemset(t.pyramid, 0, npyr * 4) != cudaSuccess ||
+        cudaMemset(t.status, 0, 4) != cudaSuccess) {
+        delete h;
+        return fail(RTPG_ECUDA, "rtpg_mqt_create: memset failed");
+    }
+    cudaError_t e = cudaFuncSetAttribute(k_mqt_build, cudaFuncAttributeMaxDynamicSharedMemorySize, mqt_smem(kMqtMaxLevel));
+    if (e != cudaSuccess) {
+        delete h;
+        return fail(RTPG_ECUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
+    }
+    *out = h;
+    return RTPG_OK;
+}
+
+int rtpg_mqt_destroy(rtpg_mqt* h) {
+    if (!h) return fail(RTPG_EINVAL, "rtpg_mqt_destroy: null handle");
+    delete h;
+    return RTPG_OK;
+}
+
+// RTMortonQuadTreeWrapperT::Allocate on an existing wrapper: zero both buffers (MO.h:618-637)
+int rtpg_mqt_clear(rtpg_mqt* h, void* stream) {
+    if (!h) return fail(RTPG_EINVAL, "rtpg_mqt_clear: null handle");
+    cudaStream_t st = as_stream(stream);
+    const MqtDev& t = h->dev;
+    RTPG_CUDA(cudaMemsetAsync(t.leaves, 0, ((size_t)t.ncells << (2 * t.level)) * 8, st));
+    RTPG_CUDA(cudaMemsetAsync(t.pyramid, 0, (size_t)t.ncells * mqt_level_offset(t.level + 1) * 4, st));
+    RTPG_CUDA(cudaMemsetAsync(t.status, 0, 4, st));
+    return RTPG_OK;
+}
+
+// MortonQuadTreeWrapperT::Record (MO.h:477-484): cell UINT32_MAX is skipped.
+int rtpg_mqt_record(rtpg_mqt* h, int64_t n, const uint32_t* cell, const float* dir, int dir_is_canonical,
+                    const float* value, void* stream) {
+    if (!h) return fail(RTPG_EINVAL, "rtpg_mqt_record: null handle");
+    if (n < 0 || (n > 0 && (!cell || !dir || !value))) return fail(RTPG_EINVAL, "rtpg_mqt_record: bad arguments");
+    if (n == 0) return RTPG_OK;
+    k_mqt_record<<<grid_for(n, 256, 8), 256, 0, as_stream(stream)>>>(h->dev, n, cell, dir, dir_is_canonical, value);
+    RTPG_LAUNCH_CHECK();
+    return RTPG_OK;
+}
+
+// Update + mortonBuildKernel: building leaves -> sampling pyramid, building cleared.
+int rtpg_mqt_update(rtpg_mqt* h, void* stream) {
+    if (!h) return fail(RTPG_EINVAL, "rtpg_mqt_update: null handle");
+    const int g = (int)std::min<uint32_t>(h->dev.ncells, kSMs * 8);
+    k_mqt_build<<<g, kMqtBuildBlock, mqt_smem(h->dev.level), as_stream(stream)>>>(h->dev);
+    RTPG_LAUNCH_CHECK();
+    return RTPG_OK;
+}
+
+// MortonQuadTreeWrapperT::SampleAndPdf (MO.h:486-500); out_pdf includes the 1/(4 pi) factor,
+// out_pdf_tree is MortonQuadTreeT::SampleAndPdf's pdf (MO.h:286-344).
+int rtpg_mqt_sample_pdf(rtpg_mqt* h, int64_t n, const uint32_t* cell, const uint32_t* seeds, uint32_t seed_base,
+                        float* out_uv, float* out_pdf, float* out_dir, float* out_pdf_tree, void* stream) {
+    if (!h) return fail(RTPG_EINVAL, "rtpg_mqt_sample_pdf: null handle");
+    if (n < 0 || (n > 0 && !cell)) return fail(RTPG_EINVAL, "rtpg_mqt_sample_pdf: bad arguments");
+    if (n == 0) return RTPG_OK;
+    k_mqt_sample<<<grid_for(n, 256, 8), 256, 0, as_stream(stream)>>>(h->dev, n, cell, seeds, seed_base, out_uv, out_pdf,
+                                                                     out_dir, out_pdf_tree);
+    RTPG_LAUNCH_CHECK();
+    return RTPG_OK;
+}
+
+// MortonQuadTreeWrapperT::Pdf (MO.h:515-524) or, tree_level = 1, MortonQuadTreeT::Pdf (:401-414).
+int rtpg_mqt_pdf(rtpg_mqt* h, int64_t n, const uint32_t* cell, const float* dir, int dir_is_canonical, float* out,
+                 int tree_level, void* stream) {
+    if (!h) return fail(RTPG_EINVAL, "rtpg_mqt_pdf: null handle");
+    if (n < 0 || (n > 0 && (!cell || !dir || !out))) return fail(RTPG_EINVAL, "rtpg_mqt_pdf: bad arguments");
+    if (n == 0) return RTPG_OK;
+    k_mqt_pdf<<<grid_for(n, 256, 8), 256, 0, as_stream(stream)>>>(h->dev, n, cell, dir, dir_is_canonical, out, tree_level);
+    RTPG_LAUNCH_CHECK();
+    return RTPG_OK;
+}
+
+int rtpg_mqt_export(rtpg_mqt* h, int64_t* host_leaves, float* host_pyramid, void* stream) {
+    if (!h) return fail(RTPG_EINVAL, "rtpg_mqt_export: null handle");
+    cudaStream_t st = as_stream(stream);
+    const MqtDev& t = h->dev;
+    if (host_leaves)
+        RTPG_CUDA(cudaMemcpyAsync(host_leaves, t.leaves, ((size_t)t.ncells << (2 * t.level)) * 8, cudaMemcpyDeviceToHost, st));
+    if (host_pyramid)
+        RTPG_CUDA(cudaMemcpyAsync(host_pyramid, t.pyramid, (size_t)t.ncells * mqt_level_offset(t.level + 1) * 4,
+                                  cudaMemcpyDeviceToHost, st));
+    RTPG_CUDA(cudaStreamSynchronize(st));
+    return RTPG_OK;
+}
+
+int rtpg_mqt_status(rtpg_mqt* h, uint32_t* host_status, int clear, void* stream) {
+    if (!h || !host_status) return fail(RTPG_EINVAL, "rtpg_mqt_status: null argument");
+    cudaStream_t st = as_stream(stream);
+    RTPG_CUDA(cudaMemcpyAsync(host_status, h->dev.status, 4, cudaMemcpyDeviceToHost, st));
+    if (clear) RTPG_CUDA(cudaMemsetAsync(h->dev.status, 0, 4, st));
+    RTPG_CUDA(cudaStreamSynchronize(st));
+    return RTPG_OK;
+}
+
+}  // extern "C"

@@ -44,21 +44,36 @@ __global__ void k_clear(SDTreeDev t) {
 
 // ------------------------------------------------------------------ record
 // One thread per record (grid-stride, warp-uniform trip count so that the warp-aggregated
-// atomics run converged).  Two 64-bit atomics per record: the DTree's stat-weight and the
-// leaf quadrant sum (RecordIrradiance, PG.h:417-428).
+// atomics run converged).  Two 64-bit fixed-point atomics per record: the DTree's stat-weight
+// and the leaf quadrant sum (RecordIrradiance, PG.h:417-428).  When the whole tree is small
+// (at most kPrivQuads quadrants and kPrivTrees DTrees) every CTA accumulates in shared memory
+// and flushes once, which removes the same-address contention of a freshly cleared tree.
+constexpr uint32_t kPrivQuads = 2048;
+constexpr uint32_t kPrivTrees = 512;
+constexpr uint32_t kStageSTreeRecord = 4096;  // 16 KB + 16 KB + 4 KB of static shared memory
 template <bool CANON>
 __global__ void __launch_bounds__(kRecordBlock) k_record(SDTreeDev t, int64_t n, const float* __restrict__ pos,
                                                          const float* __restrict__ dir, const float* __restrict__ radiance,
                                                          const float* __restrict__ wo_pdf,
                                                          const float* __restrict__ stat_w,
                                                          const uint8_t* __restrict__ is_delta) {
-    __shared__ uint32_t s_st[kStageSTree];
+    __shared__ uint32_t s_st[kStageSTreeRecord];
+    __shared__ unsigned long long s_q[kPrivQuads];
+    __shared__ unsigned long long s_w[kPrivTrees];
     const uint32_t nst = t.counts[0];
-    const bool staged = nst <= kStageSTree;
+    const uint32_t nq = t.counts[2] * 4u, ndt = t.counts[1];
+    const bool staged = nst <= kStageSTreeRecord;
+    const bool priv = nq <= kPrivQuads && ndt <= kPrivTrees;
     if (staged)
         for (uint32_t i = threadIdx.x; i < nst; i += blockDim.x) s_st[i] = t.snode[i];
+    if (priv) {
+        for (uint32_t i = threadIdx.x; i < nq; i += blockDim.x) s_q[i] = 0ull;
+        for (uint32_t i = threadIdx.x; i < ndt; i += blockDim.x) s_w[i] = 0ull;
+    }
     __syncthreads();
     const uint32_t* st = staged ? s_st : t.snode;
+    unsigned long long* acc_w = priv ? s_w : t.b_statw;
+    unsigned long long* acc_q = priv ? s_q : t.b_sums;
     const int64_t stride = int64_t(gridDim.x) * blockDim.x;
     for (int64_t base = int64_t(blockIdx.x) * blockDim.x; base < n; base += stride) {
         const int64_t i = base + threadIdx.x;
@@ -85,8 +100,15 @@ __global__ void __launch_bounds__(kRecordBlock) k_record(SDTreeDev t, int64_t n,
                 }
             }
         }
-        warp_add_u64(k_w, v_w, t.b_statw);
-        warp_add_u64(k_s, v_s, t.b_sums);
+        warp_add_u64(k_w, v_w, acc_w);
+        warp_add_u64(k_s, v_s, acc_q);
+    }
+    if (priv) {
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < nq; i += blockDim.x)
+            if (s_q[i]) atomicAdd(t.b_sums + i, s_q[i]);
+        for (uint32_t i = threadIdx.x; i < ndt; i += blockDim.x)
+            if (s_w[i]) atomicAdd(t.b_statw + i, s_w[i]);
     }
 }
 
@@ -196,6 +218,7 @@ __global__ void k_refine_count(SDTreeDev t, float thf, int32_t max_mb, uint32_t 
                 w = __fdiv_rn(w, 2.0f);
                 ++k;
             }
+            if (w > thf) atomicOr(t.status, RTPG_STATUS_STREE_CAPACITY);  // depth capped by capacity
         }
         ksplit[i] = k;
         cnt_s[i] = k ? (2u << k) - 2u : 0u;
@@ -214,53 +237,71 @@ __global__ void k_refine_count(SDTreeDev t, float thf, int32_t max_mb, uint32_t 
     }
 }
 
-// Writes the complete subtrees.  New STree nodes are numbered level by level inside each
-// leaf's block; leaf j of the subtree gets the old DTree (j == 0) or a new one, which shares
-// the parent's sampling quadtree (read-only until the next build) -- SubDivide copies the
-// whole wrapper into both children (PG.h:1236-1244).
-__global__ void k_refine_apply(SDTreeDev t, const uint32_t* ksplit, const uint32_t* off_s, const uint32_t* off_d,
-                               const unsigned long long* tot64) {
+// Writes the complete subtrees, one thread per new STree node and one per new DTree (the
+// owning leaf is found by binary search in the scanned offsets).  New nodes are numbered level
+// by level inside each leaf's block; leaf j of a subtree gets the old DTree (j == 0) or a new
+// one that shares the parent's sampling quadtree (read-only until the next build) --
+// SubDivide copies the whole wrapper into both children (PG.h:1236-1244).
+__device__ __forceinline__ uint32_t owner_of(const uint32_t* off, const uint32_t* cnt, uint32_t n, uint32_t q) {
+    uint32_t lo = 0, hi = n;  // last i with off[i] <= q and cnt[i] > 0
+    while (hi - lo > 1) {
+        const uint32_t m = (lo + hi) >> 1;
+        if (off[m] <= q) lo = m;
+        else hi = m;
+    }
+    while (cnt[lo] == 0 || off[lo] > q) --lo;  // skip empty entries sharing the same offset
+    return lo;
+}
+__global__ void k_refine_apply(SDTreeDev t, const uint32_t* ksplit, const uint32_t* off_s, const uint32_t* cnt_s,
+                               const uint32_t* off_d, const uint32_t* cnt_d, const unsigned long long* tot64) {
     const uint32_t n = t.counts[0], ndt = t.counts[1];
     if (n + tot64[1] > t.cap_snodes || ndt + tot64[2] > t.cap_dtrees) {
         if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(t.status, RTPG_STATUS_STREE_CAPACITY);
         return;
     }
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint32_t tot_s = (uint32_t)tot64[1], tot_d = (uint32_t)tot64[2];
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < tot_s; q += stride) {
+        const uint32_t i = owner_of(off_s, cnt_s, n, q);
         const uint32_t k = ksplit[i];
-        if (!k) continue;
-        const uint32_t dold = t.snode[i] & ~kLeafBit;
         const uint32_t B = n + off_s[i];
-        const uint32_t D = ndt + off_d[i];
-        t.snode[i] = B;
-        for (uint32_t l = 1; l <= k; ++l) {
-            const uint32_t w = 1u << l;
-            for (uint32_t j = 0; j < w; ++j) {
-                const uint32_t idx = B + (w - 2) + j;
-                if (l < k) {
-                    t.snode[idx] = B + (2 * w - 2) + 2 * j;
-                } else {
-                    const uint32_t d = j == 0 ? dold : D + j - 1;
-                    t.snode[idx] = kLeafBit | d;
-                    if (j) {
-                        // building fields alias the parent's tree until the quadtree reset
-                        // writes the new one; they only stay if the reset hits a capacity
-                        // limit (RTPG_STATUS_DNODE_CAPACITY), which keeps records in bounds
-                        t.b_off[d] = t.b_off[dold];
-                        t.b_cnt[d] = t.b_cnt[dold];
-                        t.b_nlvl[d] = t.b_nlvl[dold];
-                        t.b_statw[d] = 0ull;
-                        for (uint32_t q = 0; q <= kMaxLevels; ++q)
-                            t.b_lvl[size_t(d) * (kMaxLevels + 1) + q] = t.b_lvl[size_t(dold) * (kMaxLevels + 1) + q];
-                        t.s_off[d] = t.s_off[dold];
-                        t.s_cnt[d] = t.s_cnt[dold];
-                        t.s_sum[d] = t.s_sum[dold];
-                        t.s_area[d] = t.s_area[dold];
-                        t.s_statw[d] = t.s_statw[dold];
-                    }
-                }
-            }
+        const uint32_t r = q - off_s[i];  // position in the block: level l holds [2^l - 2, 2^(l+1) - 2)
+        const uint32_t l = 31 - __clz(r + 2);
+        const uint32_t j = r + 2 - (1u << l);
+        if (l < k) {
+            t.snode[B + r] = B + (2u << l) - 2 + 2 * j;
+        } else {
+            const uint32_t dold = t.snode[i] & ~kLeafBit;
+            t.snode[B + r] = kLeafBit | (j == 0 ? dold : ndt + off_d[i] + j - 1);
         }
     }
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < tot_d; q += stride) {
+        const uint32_t i = owner_of(off_d, cnt_d, n, q);
+        const uint32_t dold = t.snode[i] & ~kLeafBit;
+        const uint32_t d = ndt + q;
+        // building fields alias the parent's tree until the quadtree reset writes the new one;
+        // they only remain if the reset hits a capacity limit (RTPG_STATUS_DNODE_CAPACITY),
+        // which keeps later records in bounds
+        t.b_off[d] = t.b_off[dold];
+        t.b_cnt[d] = t.b_cnt[dold];
+        t.b_nlvl[d] = t.b_nlvl[dold];
+        t.b_statw[d] = 0ull;
+        for (uint32_t x = 0; x <= kMaxLevels; ++x)
+            t.b_lvl[size_t(d) * (kMaxLevels + 1) + x] = t.b_lvl[size_t(dold) * (kMaxLevels + 1) + x];
+        t.s_off[d] = t.s_off[dold];
+        t.s_cnt[d] = t.s_cnt[dold];
+        t.s_sum[d] = t.s_sum[dold];
+        t.s_area[d] = t.s_area[dold];
+        t.s_statw[d] = t.s_statw[dold];
+    }
+}
+// the split leaves become interior nodes; runs after k_refine_apply read snode[i]
+__global__ void k_refine_link(SDTreeDev t, const uint32_t* ksplit, const uint32_t* off_s,
+                              const unsigned long long* tot64) {
+    const uint32_t n = t.counts[0], ndt = t.counts[1];
+    if (n + tot64[1] > t.cap_snodes || ndt + tot64[2] > t.cap_dtrees) return;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        if (ksplit[i]) t.snode[i] = n + off_s[i];
 }
 __global__ void k_refine_commit(SDTreeDev t, const unsigned long long* tot64) {
     const uint32_t n = t.counts[0], ndt = t.counts[1];
@@ -390,6 +431,10 @@ __global__ void k_reset_commit(SDTreeDev t, const unsigned long long* node_total
 }
 
 // ------------------------------------------------------------------ sample / pdf
+// One query per thread: STree descent (tree staged in shared memory when it fits), the
+// DTree's GetMean test once, the guided sample, the pdf of the sampled canonical point
+// (DTreeT::Pdf) and optionally the direction and the pdf of that direction after the
+// dir -> canonical round trip the closest-hit program performs (SimpleGuide.cu:361-368).
 __global__ void __launch_bounds__(256) k_sample_pdf(SDTreeDev t, int64_t n, const float* __restrict__ pos,
                                                     const uint32_t* __restrict__ seeds, uint32_t seed_base,
                                                     float* __restrict__ out_uv, float* __restrict__ out_pdf_uv,
@@ -406,10 +451,10 @@ __global__ void __launch_bounds__(256) k_sample_pdf(SDTreeDev t, int64_t n, cons
         const uint32_t d = stree_lookup(st, t.mn, t.mx, pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]);
         uint32_t rng = seeds ? seeds[i] : (pcg1d(seed_base + (uint32_t)i) | 1u);
         const uint32_t off = t.s_off[d];
-        const float statw = t.s_statw[d], sum = t.s_sum[d];
-        const float2 uv = dtree_sample(t.s_nodes, off, statw, sum, rng);
+        const bool guided = dtree_mean(t.s_statw[d], t.s_sum[d]) > 0.0f;
+        const float2 uv = dtree_sample_g(t.s_nodes, off, guided, rng);
         if (out_uv) reinterpret_cast<float2*>(out_uv)[i] = uv;
-        if (out_pdf_uv) out_pdf_uv[i] = dtree_pdf(t.s_nodes, off, statw, sum, uv.x, uv.y);
+        if (out_pdf_uv) out_pdf_uv[i] = dtree_pdf_g(t.s_nodes, off, guided, uv.x, uv.y);
         if (out_dir || out_pdf_dir) {
             const float3 dv = normalize3(canonical_to_dir(uv.x, uv.y));
             if (out_dir) {
@@ -419,7 +464,7 @@ __global__ void __launch_bounds__(256) k_sample_pdf(SDTreeDev t, int64_t n, cons
             }
             if (out_pdf_dir) {
                 const float2 c = dir_to_canonical(dv.x, dv.y, dv.z);
-                out_pdf_dir[i] = dtree_pdf(t.s_nodes, off, statw, sum, c.x, c.y);
+                out_pdf_dir[i] = dtree_pdf_g(t.s_nodes, off, guided, c.x, c.y);
             }
         }
     }
@@ -614,7 +659,8 @@ int rtpg_sdtree_refine(rtpg_sdtree* h, uint64_t spatial_threshold, int32_t max_m
     int r;
     if ((r = scan_exclusive_u32(h->cnt_s, h->off_s, t.counts + 0, t.cap_snodes, h->partials, h->totals + 0, st))) return r;
     if ((r = scan_exclusive_u32(h->cnt_d, h->off_d, t.counts + 0, t.cap_snodes, h->partials, h->totals + 1, st))) return r;
-    k_refine_apply<<<grid_for(t.cap_snodes, 128, 8), 128, 0, st>>>(t, h->ksplit, h->off_s, h->off_d, h->fp);
+    k_refine_apply<<<kSMs * 4, 256, 0, st>>>(t, h->ksplit, h->off_s, h->cnt_s, h->off_d, h->cnt_d, h->fp);
+    k_refine_link<<<grid_for(t.cap_snodes, 256, 4), 256, 0, st>>>(t, h->ksplit, h->off_s, h->fp);
     k_refine_commit<<<1, 1, 0, st>>>(t, h->fp);
     RTPG_LAUNCH_CHECK();
     // quadtree reset of every leaf

@@ -12,6 +12,7 @@
 #pragma once
 #include "common.cuh"
 #include "limits.cuh"
+#include "canonical.cuh"
 
 namespace rtpg {
 
@@ -51,43 +52,50 @@ struct SDTreeDev {
 
 // STreeT::GetDTreeWrapper (PG.h:639-648) with STreeNodeT::GetChildIdx (PG.h:546-552):
 // p = (pos - min) / (max - min); at each interior node p[axis] *= 2, idx = int(p[axis]),
-// p[axis] -= idx.  idx is clamped to [0,1] so that p == 1 or points outside the box stay
-// in bounds.  Also returns the voxel size (the reference halves size[axis] per level).
+// p[axis] -= idx, the axis cycling x, y, z with depth.  idx is clamped to [0,1] so that
+// p == 1 or points outside the box stay in bounds.  The voxel variant also halves the voxel
+// size along the split axis per level, as GetDTreeWrapper(p, size) does.
+__device__ __forceinline__ bool stree_step(const uint32_t* __restrict__ snode, uint32_t& code, float& p) {
+    const float v = __fmul_rn(p, 2.0f);
+    int idx = __float2int_rz(v);
+    idx = idx < 0 ? 0 : (idx > 1 ? 1 : idx);
+    p = __fsub_rn(v, (float)idx);
+    code = snode[code + (uint32_t)idx];
+    return (code & kLeafBit) != 0;
+}
 __device__ __forceinline__ uint32_t stree_lookup(const uint32_t* __restrict__ snode, float3 mn, float3 mx, float px,
                                                  float py, float pz) {
-    const float sx = __fsub_rn(mx.x, mn.x), sy = __fsub_rn(mx.y, mn.y), sz = __fsub_rn(mx.z, mn.z);
-    float p[3] = {__fdiv_rn(__fsub_rn(px, mn.x), sx), __fdiv_rn(__fsub_rn(py, mn.y), sy),
-                  __fdiv_rn(__fsub_rn(pz, mn.z), sz)};
+    float x = __fdiv_rn(__fsub_rn(px, mn.x), __fsub_rn(mx.x, mn.x));
+    float y = __fdiv_rn(__fsub_rn(py, mn.y), __fsub_rn(mx.y, mn.y));
+    float z = __fdiv_rn(__fsub_rn(pz, mn.z), __fsub_rn(mx.z, mn.z));
     uint32_t code = snode[0];
-    int axis = 0;
-    while (!(code & kLeafBit)) {
-        const float v = __fmul_rn(p[axis], 2.0f);
-        int idx = __float2int_rz(v);
-        idx = idx < 0 ? 0 : (idx > 1 ? 1 : idx);
-        p[axis] = __fsub_rn(v, (float)idx);
-        code = snode[code + (uint32_t)idx];
-        axis = axis == 2 ? 0 : axis + 1;
+    if (!(code & kLeafBit)) {
+        for (;;) {
+            if (stree_step(snode, code, x)) break;
+            if (stree_step(snode, code, y)) break;
+            if (stree_step(snode, code, z)) break;
+        }
     }
     return code & ~kLeafBit;
 }
 __device__ __forceinline__ uint32_t stree_lookup_voxel(const uint32_t* __restrict__ snode, float3 mn, float3 mx,
                                                        float px, float py, float pz, float3& voxel) {
-    const float sx = __fsub_rn(mx.x, mn.x), sy = __fsub_rn(mx.y, mn.y), sz = __fsub_rn(mx.z, mn.z);
-    float p[3] = {__fdiv_rn(__fsub_rn(px, mn.x), sx), __fdiv_rn(__fsub_rn(py, mn.y), sy),
-                  __fdiv_rn(__fsub_rn(pz, mn.z), sz)};
-    float s[3] = {sx, sy, sz};
+    float sx = __fsub_rn(mx.x, mn.x), sy = __fsub_rn(mx.y, mn.y), sz = __fsub_rn(mx.z, mn.z);
+    float x = __fdiv_rn(__fsub_rn(px, mn.x), sx);
+    float y = __fdiv_rn(__fsub_rn(py, mn.y), sy);
+    float z = __fdiv_rn(__fsub_rn(pz, mn.z), sz);
     uint32_t code = snode[0];
-    int axis = 0;
-    while (!(code & kLeafBit)) {
-        const float v = __fmul_rn(p[axis], 2.0f);
-        int idx = __float2int_rz(v);
-        idx = idx < 0 ? 0 : (idx > 1 ? 1 : idx);
-        p[axis] = __fsub_rn(v, (float)idx);
-        s[axis] = s[axis] / 2.0f;
-        code = snode[code + (uint32_t)idx];
-        axis = axis == 2 ? 0 : axis + 1;
+    if (!(code & kLeafBit)) {
+        for (;;) {
+            sx *= 0.5f;
+            if (stree_step(snode, code, x)) break;
+            sy *= 0.5f;
+            if (stree_step(snode, code, y)) break;
+            sz *= 0.5f;
+            if (stree_step(snode, code, z)) break;
+        }
     }
-    voxel = make_float3(s[0], s[1], s[2]);
+    voxel = make_float3(sx, sy, sz);
     return code & ~kLeafBit;
 }
 
@@ -128,9 +136,10 @@ __device__ __forceinline__ float dtree_mean(float statw, float sum) {
 }
 
 // DTreeT::Sample (PG.h:478-484) -> DTreeNodeT::Sample (PG.h:229-277), float order as written.
-__device__ __forceinline__ float2 dtree_sample(const SNode* __restrict__ nodes, uint32_t off, float statw, float sum,
-                                               uint32_t& rng) {
-    if (dtree_mean(statw, sum) <= 0.0f) {
+// `guided` is DTreeT::GetMean() > 0 (uniform sampling of the square otherwise).
+__device__ __forceinline__ float2 dtree_sample_g(const SNode* __restrict__ nodes, uint32_t off, bool guided,
+                                                 uint32_t& rng) {
+    if (!guided) {
         const float a = rnd1(rng);
         const float b = rnd1(rng);
         return make_float2(a, b);
@@ -176,11 +185,15 @@ __device__ __forceinline__ float2 dtree_sample(const SNode* __restrict__ nodes, 
     }
     return make_float2(fminf(fmaxf(rx, 0.0f), 1.0f), fminf(fmaxf(ry, 0.0f), 1.0f));
 }
+__device__ __forceinline__ float2 dtree_sample(const SNode* __restrict__ nodes, uint32_t off, float statw, float sum,
+                                               uint32_t& rng) {
+    return dtree_sample_g(nodes, off, dtree_mean(statw, sum) > 0.0f, rng);
+}
 
 // DTreeT::Pdf (PG.h:485-490) -> DTreeNodeT::Pdf (PG.h:279-320)
-__device__ __forceinline__ float dtree_pdf(const SNode* __restrict__ nodes, uint32_t off, float statw, float sum,
-                                           float u, float v) {
-    if (dtree_mean(statw, sum) <= 0.0f) return __fdiv_rn(__fmul_rn(1.0f, kInv2Pi), 2.0f);
+__device__ __forceinline__ float dtree_pdf_g(const SNode* __restrict__ nodes, uint32_t off, bool guided, float u,
+                                             float v) {
+    if (!guided) return __fdiv_rn(__fmul_rn(1.0f, kInv2Pi), 2.0f);
     float result = 1.0f;
     uint32_t cur = 0;
     int idx = quad_child(u, v);
@@ -201,26 +214,9 @@ __device__ __forceinline__ float dtree_pdf(const SNode* __restrict__ nodes, uint
     }
     return __fdiv_rn(__fmul_rn(result, kInv2Pi), 2.0f);
 }
-
-// canonical_to_dir / dir_to_canonical (VectorFunction.h:5698-5720)
-__device__ __forceinline__ float3 canonical_to_dir(float u, float v) {
-    const float cosTheta = 2.0f * u - 1.0f;
-    const float sinTheta = sqrtf(1.0f - cosTheta * cosTheta);
-    const float phi = k2Pi * v;
-    float sp, cp;
-    sincosf(phi, &sp, &cp);
-    return make_float3(sinTheta * cp, sinTheta * sp, cosTheta);
-}
-__device__ __forceinline__ float2 dir_to_canonical(float x, float y, float z) {
-    if (!isfinite(x) || !isfinite(y) || !isfinite(z)) return make_float2(0.0f, 0.0f);
-    z = fminf(fmaxf(z, -1.0f), 1.0f);
-    float phi = atan2f(y, x);
-    while (phi < 0.0f) phi += k2Pi;
-    return make_float2((z + 1.0f) / 2.0f, phi * kInv2Pi);
-}
-__device__ __forceinline__ float3 normalize3(float3 v) {
-    const float l = sqrtf(v.x * v.x + v.y * v.y + v.z * v.z);
-    return make_float3(v.x / l, v.y / l, v.z / l);
+__device__ __forceinline__ float dtree_pdf(const SNode* __restrict__ nodes, uint32_t off, float statw, float sum,
+                                           float u, float v) {
+    return dtree_pdf_g(nodes, off, dtree_mean(statw, sum) > 0.0f, u, v);
 }
 
 }  // namespace rtpg

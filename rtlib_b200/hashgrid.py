@@ -1,0 +1,110 @@
+"""Host-side mirrors of RTLib's hash grid and Morton quadtree over the C ABI.
+
+``HashGrid`` stands for DoubleBufferedHashGrid3Buffer (RTLibExtOPX7Test.h:1472-1570) with the
+device routines DoubleBufferedHashGrid3T::FindFromCur / FindFromPrv batched;
+``MortonQuadTrees`` for RTMortonQuadTreeWrapperT (OPX7UtilsMorton.h:590-764) with
+MortonQuadTreeWrapperT::Record / SampleAndPdf / Pdf batched and the pyramid build.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from ._lib import call, ptr, stream_ptr
+
+KEY_REFERENCE, KEY_MORTON = 0, 1
+
+
+class HashGrid:
+    def __init__(self, aabb_min, aabb_max, bounds, num_slots, keying=KEY_REFERENCE, max_batch=0):
+        mn = (C.c_float * 3)(*[float(v) for v in aabb_min])
+        mx = (C.c_float * 3)(*[float(v) for v in aabb_max])
+        b = (C.c_uint32 * 3)(*[int(v) for v in bounds])
+        h = C.c_void_p()
+        call("rtpg_hashgrid_create", mn, mx, b, int(num_slots), int(keying), int(max_batch), C.byref(h))
+        self.h = h
+        self.num_slots = int(num_slots)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            call("rtpg_hashgrid_destroy", self.h)
+            self.h = None
+
+    def clear(self, stream=None):
+        call("rtpg_hashgrid_clear", self.h, stream_ptr(stream))
+
+    def swap(self, stream=None):
+        call("rtpg_hashgrid_swap", self.h, stream_ptr(stream))
+
+    def insert(self, pos, out_slot, out_key=None, stream=None):
+        call("rtpg_hashgrid_insert", self.h, int(pos.shape[0]), ptr(pos), ptr(out_slot), ptr(out_key),
+             stream_ptr(stream))
+
+    def lookup(self, pos, out_slot, stream=None):
+        call("rtpg_hashgrid_lookup", self.h, int(pos.shape[0]), ptr(pos), ptr(out_slot), stream_ptr(stream))
+
+    def cells(self, pos, out_cell=None, out_key=None, stream=None):
+        call("rtpg_hashgrid_cells", self.h, int(pos.shape[0]), ptr(pos), ptr(out_cell), ptr(out_key),
+             stream_ptr(stream))
+
+    def export(self, previous=False, stream=None):
+        t = np.empty(self.num_slots, np.uint64)
+        call("rtpg_hashgrid_export", self.h, int(previous), t.ctypes.data, stream_ptr(stream))
+        return t
+
+    def status(self, clear=False, stream=None):
+        s = C.c_uint32()
+        call("rtpg_hashgrid_status", self.h, C.byref(s), int(clear), stream_ptr(stream))
+        return s.value
+
+
+class MortonQuadTrees:
+    def __init__(self, num_cells, level=6, fraction=0.3, fixed_point_bits=0):
+        h = C.c_void_p()
+        call("rtpg_mqt_create", int(num_cells), int(level), float(fraction), int(fixed_point_bits), C.byref(h))
+        self.h = h
+        self.num_cells, self.level = int(num_cells), int(level)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            call("rtpg_mqt_destroy", self.h)
+            self.h = None
+
+    @property
+    def per_cell(self):
+        return ((1 << (2 * (self.level + 1))) - 1) // 3
+
+    def clear(self, stream=None):
+        call("rtpg_mqt_clear", self.h, stream_ptr(stream))
+
+    def record(self, cell, dir, value, canonical=None, stream=None):
+        if canonical is None:
+            canonical = dir.shape[-1] == 2
+        call("rtpg_mqt_record", self.h, int(cell.shape[0]), ptr(cell), ptr(dir), int(bool(canonical)), ptr(value),
+             stream_ptr(stream))
+
+    def update(self, stream=None):
+        call("rtpg_mqt_update", self.h, stream_ptr(stream))
+
+    def sample_pdf(self, cell, seeds=None, seed_base=0, out_uv=None, out_pdf=None, out_dir=None, out_pdf_tree=None,
+                   stream=None):
+        call("rtpg_mqt_sample_pdf", self.h, int(cell.shape[0]), ptr(cell), ptr(seeds), int(seed_base), ptr(out_uv),
+             ptr(out_pdf), ptr(out_dir), ptr(out_pdf_tree), stream_ptr(stream))
+
+    def pdf(self, cell, dir, out, canonical=None, tree_level=False, stream=None):
+        if canonical is None:
+            canonical = dir.shape[-1] == 2
+        call("rtpg_mqt_pdf", self.h, int(cell.shape[0]), ptr(cell), ptr(dir), int(bool(canonical)), ptr(out),
+             int(bool(tree_level)), stream_ptr(stream))
+
+    def export(self, stream=None):
+        leaves = np.empty(self.num_cells << (2 * self.level), np.int64)
+        pyr = np.empty(self.num_cells * self.per_cell, np.float32)
+        call("rtpg_mqt_export", self.h, leaves.ctypes.data, pyr.ctypes.data, stream_ptr(stream))
+        return leaves, pyr
+
+    def status(self, clear=False, stream=None):
+        s = C.c_uint32()
+        call("rtpg_mqt_status", self.h, C.byref(s), int(clear), stream_ptr(stream))
+        return s.value

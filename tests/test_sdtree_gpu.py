@@ -162,12 +162,20 @@ def test_memory_guard_and_capacity(cuda, oracle):
     g.refine(100, max_mb=0); o.refine(100, max_mb=0)
     _same_export(g.export(sampling=False), o.export(sampling=False))
     assert g.stats()["stree_nodes"] == 1
+    # 16 STree nodes allow three levels of splits (2^(k+1) <= 16); the cut is reported
     small = SDTree((0, 0, 0), (1, 1, 1), max_stree_nodes=16)
     small.record(_t(rec["pos"], cuda), _t(rec["uv"], cuda), _t(rec["radiance"], cuda))
     small.build()
     small.refine(100)
     assert small.status() & 0x4
-    assert small.stats()["stree_nodes"] == 1
+    assert small.stats()["stree_nodes"] == 15
+    # a second refine that would need more nodes than remain is skipped as a whole
+    small.record(_t(rec["pos"], cuda), _t(rec["uv"], cuda), _t(rec["radiance"], cuda))
+    small.build()
+    small.status(clear=True)
+    small.refine(100)
+    assert small.status() & 0x4
+    assert small.stats()["stree_nodes"] == 15
 
 
 def _schedule(budget, built, ratio, spl):
