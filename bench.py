@@ -2,17 +2,25 @@
 
 python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
 
+Workload "cornell" (default; the guided path-tracing configuration): the procedural
+Cornell-style box (5 walls, 2 boxes rotated -18/+18 degrees, 0.25 x 0.25 light of radiance
+(17,12,4)) at 512 x 512, max depth 8, NEE, SD-tree guiding with 50% BSDF/guide mixing, passes
+doubling from 1 to 1024 spp (2047 spp in total) under the pass controller, with record ->
+build -> refine between passes.  One step = one complete guided render.  Metric: Mpaths/s
+(camera paths = pixels x spp).  "e2e" repeats the step through the C ABI from host arrays:
+the scene goes host->device, the image comes back device->host, both inside the timed region.
+
 Workload "sdtree" (SD-tree standalone): 2^20 seeded radiance records (uniform positions,
 4-lobe vMF directions kappa 50, lognormal(0,1) radiance) are recorded, the trees are built and
-refined at 12000*sqrt(2), then 2^22 guided sample+pdf queries run at uniform positions.  One
-step = clear + record + build + refine + sample/pdf.  Inputs are resident in HBM when the
-timed region starts (value); "e2e" repeats the step through the C ABI from pinned host
-buffers with the host<->device copies inside the timed region.  L2 is flushed (a 256 MiB
+refined at 12000*sqrt(2), then 2^22 guided sample+pdf queries run at uniform positions.
+
+Inputs are resident in HBM when the timed region starts (value).  L2 is flushed (a 256 MiB
 write) before every timed step.  N GPUs run independent replicas (no collective): value is
 the work of all ranks over the slowest rank's time.
 
---impl reference runs RTLib's own SD-tree code (oracle/_ref, built from the reference sources)
-on this machine's host cores with the same workload and metric.
+--impl reference runs the CPU implementation of the same workload on this machine's host
+cores: RTLib's own SD-tree code (oracle/_ref) for "sdtree"; for "cornell", where RTLib's
+integrator exists only as OptiX programs, the CPU restatement of that integrator (oracle/).
 """
 from __future__ import annotations
 
@@ -284,6 +292,150 @@ def cpu_baseline_sdtree():
             "seconds_per_pass": s}
 
 
+# ---------------------------------------------------------------------------- Cornell workload
+C_W = C_H = 512
+C_BUDGET = 2047          # passes of 1, 2, 4, ..., 512, 1024 spp
+C_MAX_DEPTH = 8
+C_FRACTION = 0.5
+C_AABB = ((-0.005,) * 3, (1.005,) * 3)  # world AABB padded by 0.005 as the application does
+# compulsory SoA bytes of one extend visit (one path-bounce): reads queue index, origin,
+# direction, throughput, depth, flags, rng (52 B); writes pending flag, bounce radiance,
+# origin, direction, throughput, flags, rng (60 B) and the NEE shadow ray (28 B).  Scene,
+# material and tree reads are L2-resident and not counted; trace-vertex writes are excluded.
+EXTEND_BYTES = 140
+
+
+def bench_cornell_ours(args, rank, world):
+    import torch
+    from rtlib_b200 import scenes
+    from rtlib_b200.sdtree import SDTree, SDTreeController
+    from rtlib_b200.tracer import FLAG_NEE, Tracer
+
+    dev = torch.device("cuda", rank % max(1, torch.cuda.device_count()))
+    torch.cuda.set_device(dev)
+    sc = scenes.cornell_box(C_W, C_H)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    tr = Tracer(sc, dev, max_depth=C_MAX_DEPTH, seed=1)
+    tree = SDTree(*C_AABB, fraction=C_FRACTION)
+    ctrl = SDTreeController(tree, C_BUDGET, iteration_for_built=0, ratio_for_budget=1.0, samples_per_launch=1)
+    img = torch.empty((C_H, C_W, 3), dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream()
+
+    def step():
+        tr.clear()
+        ctrl.start()
+        tr.render_guided(tree, ctrl, FLAG_NEE, samples_per_launch=1)
+        tr.image(img)
+
+    t0 = time.perf_counter()
+    k = 0
+    while k < args.warmup or time.perf_counter() - t0 < 0.5:
+        step()
+        k += 1
+    torch.cuda.synchronize()
+    paths_per_step = C_W * C_H * (C_BUDGET + 1)  # the controller runs one extra launch after the last pass
+    clocks = ClockSampler(dev.index)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    _barrier(world)
+    torch.cuda.synchronize()
+    clocks.start()
+    for k in range(args.steps):
+        flush.fill_(k & 0xff)
+        a, c = ev[k]
+        a.record(stream)
+        step()
+        c.record(stream)
+    torch.cuda.synchronize()
+    _barrier(world)
+    clk = clocks.stop()
+    ms = sum(a.elapsed_time(c) for a, c in ev) / len(ev)
+    ms = _max_over_ranks(ms, world, dev)
+    cnt = tr.counters()
+    st = tree.stats()
+    assert tree.status() == 0
+    assert tr.stats()["samples"] == C_BUDGET + 1
+
+    # kernel times: one more step in measurement mode (events around every kernel, no graph)
+    tr.set_timing(True)
+    torch.cuda.synchronize()
+    step()
+    torch.cuda.synchronize()
+    tk = tr.timings()
+    tr.set_timing(False)
+    ext_ms = tk["extend"][0]
+    peak, peak_kind = _peaks()
+    achieved = cnt["path_bounces"] * EXTEND_BYTES / (ext_ms * 1e-3) / 1e9
+
+    # e2e: scene from host memory through the C ABI, image back to host
+    e2e_ms = []
+    h_img = torch.empty((C_H, C_W, 3), dtype=torch.float32).pin_memory()
+    h2d = sum(np.asarray(sc[k]).nbytes for k in ("tri_v", "tri_mat", "tri_uv", "light_tris"))
+    for k in range(max(1, args.steps // 2)):
+        flush.fill_(k & 0xff)
+        torch.cuda.synchronize()
+        a, c = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        tr2 = Tracer(sc, dev, max_depth=C_MAX_DEPTH, seed=1)
+        tree2 = SDTree(*C_AABB, fraction=C_FRACTION)
+        ctrl2 = SDTreeController(tree2, C_BUDGET, iteration_for_built=0, ratio_for_budget=1.0, samples_per_launch=1)
+        ctrl2.start()
+        tr2.render_guided(tree2, ctrl2, FLAG_NEE, samples_per_launch=1)
+        h_img.copy_(tr2.image(), non_blocking=True)
+        c.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms.append(a.elapsed_time(c))
+        del tr2, tree2, ctrl2
+    e2e = _max_over_ranks(sum(e2e_ms) / len(e2e_ms), world, dev)
+    paths = paths_per_step * world
+    return {
+        "metric": "Mpaths/s",
+        "value": paths / (ms * 1e-3) / 1e6,
+        "unit": "Mpaths/s",
+        "ms_per_step": ms,
+        "e2e": {"value": paths / (e2e * 1e-3) / 1e6, "unit": "Mpaths/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(h_img.numel() * 4)},
+        "roofline": {"kernel": "k_extend", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs (burst copy)",
+                     "traffic": _traffic("k_extend"), "algorithmic_bytes_per_path_bounce": EXTEND_BYTES,
+                     "path_bounces_per_step": cnt["path_bounces"],
+                     "launch_ms": ext_ms / max(1, tk["extend"][1]),
+                     "kernel_ms_per_step": {kk: v[0] for kk, v in tk.items()},
+                     "note": "extend = BVH closest hit + shading; its bound is instruction and latency, "
+                             "the HBM figure is the SoA state traffic"},
+        "clocks": clk,
+        "gpu_launches": (1 + 2 * C_MAX_DEPTH + 1) * (C_BUDGET + 1) * args.steps,
+        "counters_per_step": cnt,
+        "sdtree": st,
+    }
+
+
+def _cornell_cpu(threads, seconds, scene_px=32):
+    """Independent replicas of the guided render at scene_px^2 pixels with the same pass
+    schedule on the CPU restatement of the integrator, one per thread."""
+    import concurrent.futures as cf
+
+    from oracle.oracle import Oracle, OracleRenderer
+    from rtlib_b200 import scenes
+    o = Oracle()
+    sc = scenes.cornell_box(scene_px, scene_px)
+
+    def one(_):
+        t = o.sdtree(*C_AABB)
+        r = OracleRenderer(o, sc, max_depth=C_MAX_DEPTH, fraction=C_FRACTION, width=scene_px, height=scene_px)
+        r.render_guided(t, C_BUDGET, ratio_for_budget=1.0)
+        return r.samples * scene_px * scene_px
+
+    paths = 0
+    t0 = time.perf_counter()
+    with cf.ThreadPoolExecutor(threads) as ex:
+        while True:
+            paths += sum(ex.map(one, range(threads)))
+            if time.perf_counter() - t0 >= seconds:
+                break
+    dt = time.perf_counter() - t0
+    return paths / dt / 1e6, dt, paths
+
+
 # ---------------------------------------------------------------------------- plumbing
 def _barrier(world):
     if world > 1:
@@ -307,32 +459,53 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="sdtree", choices=["sdtree"])
+    ap.add_argument("--workload", default="cornell", choices=["cornell", "sdtree"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--budget", type=int, default=C_BUDGET,
+                    help="cornell: total spp of the pass schedule (2047 = passes 1..1024); smaller values "
+                         "give the short case used for profiling")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = _env_int("RANK", 0)
     world = _env_int("WORLD_SIZE", 1)
+    cornell = args.workload == "cornell"
+    global C_BUDGET
+    C_BUDGET = args.budget
+    if cornell:
+        cfg = {"workload": f"cornell-guided: 512x512, {C_BUDGET} spp budget in doubling passes, max depth 8, NEE, "
+                           "SD-tree guiding fraction 0.5", "width": C_W, "height": C_H, "spp": C_BUDGET + 1,
+               "max_depth": C_MAX_DEPTH}
+        metric, unit = "Mpaths/s", "Mpaths/s"
+    else:
+        cfg = {"workload": "sdtree-standalone: 2^20 records, refine at 12000*sqrt(2), 2^22 sample+pdf",
+               "records": N_REC, "queries": N_Q}
+        metric, unit = "SD-tree record+refine+sample throughput (config 1)", "Mops/s"
 
     if args.impl == "reference":
         if rank != 0:
             return 0
-        kind = _ref_kind()
         cores = os.cpu_count() or 1
-        threads = cores if kind == "reference" else 1
-        _ref_workload(kind, threads, reps=args.warmup)
-        times = _ref_workload(kind, threads, reps=args.steps)
-        s = sum(times) / len(times)
-        v = (N_REC + N_Q) / s / 1e6
-        line = {"impl": "reference", "metric": "SD-tree record+refine+sample throughput (config 1)", "value": v,
-                "unit": "Mops/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-                "ms_per_step": s * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "dtype": "f32", "data": "synthetic",
-                "config": {"workload": "sdtree-standalone: 2^20 records, refine at 12000*sqrt(2), 2^22 sample+pdf",
-                           "records": N_REC, "queries": N_Q},
-                "cpu_baseline": {"value": v, "unit": "Mops/s", "cores": threads, "kind": kind,
-                                 "sample": "full config-1 passes on the host"},
-                "e2e": {"value": v, "unit": "Mops/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        if cornell:
+            _cornell_cpu(cores, 0.0, scene_px=16)  # warm-up (builds the oracle, pages in)
+            v, dt, paths = _cornell_cpu(cores, 20.0)
+            kind, threads = "port", cores
+            sample = (f"{cores} independent replicas of the guided render at 32x32 px with the same 2048-launch "
+                      f"pass schedule on the CPU restatement of RTLib's integrator; {paths} paths in {dt:.1f} s")
+            ms = dt * 1e3
+        else:
+            kind = _ref_kind()
+            threads = cores if kind == "reference" else 1
+            _ref_workload(kind, threads, reps=args.warmup)
+            times = _ref_workload(kind, threads, reps=args.steps)
+            sec = sum(times) / len(times)
+            v = (N_REC + N_Q) / sec / 1e6
+            ms = sec * 1e3
+            sample = "full config-1 passes on the host"
+        line = {"impl": "reference", "metric": metric, "value": v, "unit": unit, "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": cfg,
+                "cpu_baseline": {"value": v, "unit": unit, "cores": threads, "kind": kind, "sample": sample},
+                "e2e": {"value": v, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
         return 0
 
@@ -342,18 +515,26 @@ def main():
         from datetime import timedelta
         torch.cuda.set_device(_env_int("LOCAL_RANK", rank))
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
-    res = bench_sdtree_ours(args, rank, world)
+    res = (bench_cornell_ours if cornell else bench_sdtree_ours)(args, rank, world)
+    cfg["l2"] = "flushed (256 MiB write) before every timed step"
+    cfg["parallelism"] = f"replicas x{world}"
     line = {"metric": res["metric"], "value": res["value"], "unit": res["unit"], "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["ms_per_step"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic",
-            "config": {"workload": "sdtree-standalone: 2^20 records, refine at 12000*sqrt(2), 2^22 sample+pdf",
-                       "records": N_REC, "queries": N_Q, "l2": "flushed (256 MiB write) before every timed step",
-                       "parallelism": f"replicas x{world}"},
-            "e2e": res["e2e"], "roofline": res["roofline"], "clocks": res["clocks"],
-            "gpu_launches": res["gpu_launches"], "sdtree": res["sdtree"]}
+            "data": "synthetic", "config": cfg, "e2e": res["e2e"], "roofline": res["roofline"],
+            "clocks": res["clocks"], "gpu_launches": res["gpu_launches"]}
+    for k in ("sdtree", "counters_per_step"):
+        if k in res:
+            line[k] = res[k]
     if rank == 0 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline_sdtree()
+        if cornell:
+            cores = os.cpu_count() or 1
+            v, dt, paths = _cornell_cpu(cores, 10.0)
+            line["cpu_baseline"] = {"value": v, "unit": "Mpaths/s", "cores": cores, "kind": "port",
+                                    "sample": f"{cores} replicas of the guided render at 32x32 px, full pass "
+                                              f"schedule, CPU restatement of the integrator; {paths} paths in {dt:.1f} s"}
+        else:
+            line["cpu_baseline"] = cpu_baseline_sdtree()
     if world > 1:
         import torch.distributed as dist
         dist.barrier()

@@ -207,6 +207,93 @@ int rtpg_mqt_pdf(rtpg_mqt* h, int64_t n, const uint32_t* cell, const float* dir,
 int rtpg_mqt_export(rtpg_mqt* h, int64_t* host_leaves, float* host_pyramid, void* stream);
 int rtpg_mqt_status(rtpg_mqt* h, uint32_t* host_status, int clear, void* stream);
 
+/* ================================================================ scene / hit queries
+ * The integrator's closest-hit and any-hit queries (RTLib: optixTrace inside TraceRadiance /
+ * TraceOccluded, RTLib/Src/Ext/OPX7/Test/cuda/SimpleKernel.h:347-366, "SK.h") answered by a
+ * linear BVH built on the GPU.  vertices: num_vertices x float3; indices: num_triangles x
+ * uint3 (device).  Creation synchronises the stream. */
+typedef struct rtpg_scene rtpg_scene;
+int rtpg_scene_create(const float* vertices, uint32_t num_vertices, const uint32_t* indices, uint32_t num_triangles,
+                      void* stream, rtpg_scene** out);
+int rtpg_scene_destroy(rtpg_scene* s);
+/* Batched queries: ray n has origin org[3n..], direction dir[3n..], interval (tmin, tmax)
+ * (NULL = 0 / 1e20).  any_hit = 0: closest hit (TraceRadiance), 1: any hit (TraceOccluded).
+ * out_t = -1 and out_prim = UINT32_MAX on a miss; out_uv: barycentrics (u, v) of vertices
+ * 1 and 2 (float2).  Outputs optional. */
+int rtpg_scene_intersect(rtpg_scene* s, int64_t n, const float* org, const float* dir, const float* tmin,
+                         const float* tmax, int any_hit, float* out_t, uint32_t* out_prim, float* out_uv, void* stream);
+
+/* ================================================================ path tracer
+ * The guided integrator of RTLib's OptiX programs (SimpleGuide.cu / SimpleTrace.cu, "SG.cu" /
+ * "ST.cu", with SK.h) as a wavefront of CUDA kernels. */
+typedef struct rtpg_tracer rtpg_tracer;
+/* HitgroupType (SK.h:232-239) */
+#define RTPG_MAT_PHONG 0
+#define RTPG_MAT_GLASS 1
+#define RTPG_MAT_NEE_LIGHT 2 /* emitter that NEE samples (emission counted only after delta bounces / camera rays) */
+#define RTPG_MAT_DEF_LIGHT 3 /* emitter outside the NEE list (emission always counted) */
+typedef struct rtpg_material {
+    float diffuse[3];
+    float specular[3];
+    float emission[3];
+    float shininess;
+    float ref_index;
+    int32_t type;            /* RTPG_MAT_* */
+    int32_t diffuse_texture; /* -1 = none, else index given to rtpg_tracer_set_texture */
+} rtpg_material;
+/* RayGenData (SK.h:191-199): direction = normalize(x * u + y * v + w), x, y in [-1, 1] */
+typedef struct rtpg_camera {
+    float eye[3], u[3], v[3], w[3];
+} rtpg_camera;
+typedef struct rtpg_tracer_desc {
+    uint32_t width, height;
+    uint32_t max_depth;          /* Params::maxDepth */
+    uint32_t num_candidates;     /* RIS candidates (Ris.NumCandidates, default 32) */
+    float background[3];         /* MissData::bgColor */
+    uint32_t seed;               /* per-pixel Xorshift32 streams are derived from it */
+    const float* light_emission; /* host, 3 floats per light mesh (MeshLight::emission) */
+} rtpg_tracer_desc;
+/* Params::flags (SK.h:145-154) */
+#define RTPG_TRACE_FLAG_NEE 1u
+#define RTPG_TRACE_FLAG_RIS 2u
+#define RTPG_TRACE_FLAG_USE_TREE 8u
+#define RTPG_TRACE_FLAG_BUILD 16u
+#define RTPG_TRACE_FLAG_FINAL 32u
+/* tri_vertices: num_triangles x 9 floats (v0, v1, v2 of triangle i, the scene's order);
+ * tri_material: uint32 per triangle; tri_uv: 6 floats per triangle or NULL; light_tris:
+ * triangle ids of the emitters, light mesh i = light_tris[first[i] .. first[i] + count[i])
+ * (MeshLightList, SK.h:107-122).  Device arrays are referenced, not copied. */
+int rtpg_tracer_create(rtpg_scene* scene, const float* tri_vertices, const uint32_t* tri_material, const float* tri_uv,
+                       const rtpg_material* host_materials, uint32_t num_materials, const uint32_t* light_tris,
+                       const uint32_t* host_light_mesh_first, const uint32_t* host_light_mesh_count,
+                       uint32_t num_light_meshes, const rtpg_camera* host_camera, const rtpg_tracer_desc* host_desc,
+                       rtpg_tracer** out);
+int rtpg_tracer_destroy(rtpg_tracer* h);
+/* diffuse texture `index`: width x height RGB floats (device, referenced), nearest texel, wrap */
+int rtpg_tracer_set_texture(rtpg_tracer* h, uint32_t index, uint32_t width, uint32_t height, const float* rgb);
+int rtpg_tracer_set_seed(rtpg_tracer* h, uint32_t seed);
+/* zero the FP64 accumulation and reseed the per-pixel streams */
+int rtpg_tracer_clear(rtpg_tracer* h, void* stream);
+/* `spp` samples per pixel with RTPG_TRACE_FLAG_* (tree required with USE_TREE) */
+int rtpg_tracer_render(rtpg_tracer* h, uint32_t spp, uint32_t flags, rtpg_sdtree* tree, void* stream);
+/* TracePipeline's loop for the guided tracers: controller begin / render / end, at most
+ * max_launches launches of samples_per_launch samples, flags from the controller state. */
+int rtpg_tracer_render_guided(rtpg_tracer* h, rtpg_sdtree* tree, rtpg_controller* ctrl, uint32_t base_flags,
+                              uint32_t samples_per_launch, uint32_t max_launches, void* stream);
+/* mean radiance per pixel, width x height x RGB float (device) */
+int rtpg_tracer_image(rtpg_tracer* h, float* out_rgb, void* stream);
+int rtpg_tracer_accumulation(rtpg_tracer* h, const double** dev_accum, uint64_t* host_samples);
+int rtpg_tracer_stats(rtpg_tracer* h, uint64_t* host_samples, uint64_t* host_paths);
+/* Device counters since the last clear: path-bounces shaded (extend visits) and shadow rays
+ * traced.  Synchronises the stream. */
+int rtpg_tracer_counters(rtpg_tracer* h, uint64_t* host_path_bounces, uint64_t* host_shadow_rays, void* stream);
+/* Measurement mode: enable = 1 makes rtpg_tracer_render launch waves without the CUDA graph,
+ * bracket every kernel with CUDA events on the stream and synchronise per wave; the summed
+ * device milliseconds of raygen / extend / connect / finish (and their launch counts) are
+ * read with rtpg_tracer_timings.  Enabling or disabling resets the sums. */
+int rtpg_tracer_set_timing(rtpg_tracer* h, int enable);
+int rtpg_tracer_timings(rtpg_tracer* h, double* host_ms4, uint64_t* host_launches4);
+
 #ifdef __cplusplus
 }
 #endif

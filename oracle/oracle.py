@@ -370,3 +370,106 @@ class RefSDTree:
         out = np.empty(pos.shape[0], np.float32)
         self.L.ref_sdtree_pdf(self.h, pos.shape[0], pos, np.ascontiguousarray(uv, np.float32), out)
         return out
+
+
+# ------------------------------------------------------------------ integrator oracle
+class _OMat(C.Structure):
+    _fields_ = [("diffuse", C.c_float * 3), ("tex", C.c_int32), ("specular", C.c_float * 3), ("shininess", C.c_float),
+                ("emission", C.c_float * 3), ("ref_index", C.c_float), ("type", C.c_int32), ("pad", C.c_int32 * 3)]
+
+
+class _OScene(C.Structure):
+    _fields_ = [("tri_v", P), ("tri_mat", P), ("tri_uv", P), ("ntris", C.c_uint32), ("mats", P), ("light_tris", P),
+                ("light_first", P), ("light_count", P), ("light_emit", P), ("nlights", C.c_uint32), ("tex", P),
+                ("tex_w", C.c_uint32), ("tex_h", C.c_uint32), ("eye", C.c_float * 3), ("cu", C.c_float * 3),
+                ("cv", C.c_float * 3), ("cw", C.c_float * 3), ("bg", C.c_float * 3), ("width", C.c_uint32),
+                ("height", C.c_uint32), ("max_depth", C.c_uint32), ("num_candidates", C.c_uint32),
+                ("fraction", C.c_float)]
+
+
+def tracer_seeds(width, height, seed):
+    """The per-pixel Xorshift32 seeds rtpg_tracer_clear derives: pcg1d(pcg1d(p) ^ seed*0x9E3779B9) | 1."""
+    def pcg(x):
+        state = (x * np.uint64(747796405) + np.uint64(2891336453)) & np.uint64(0xFFFFFFFF)
+        word = (((state >> ((state >> np.uint64(28)) + np.uint64(4))) ^ state) * np.uint64(277803737)) & np.uint64(0xFFFFFFFF)
+        return ((word >> np.uint64(22)) ^ word) & np.uint64(0xFFFFFFFF)
+    p = np.arange(width * height, dtype=np.uint64)
+    s = np.uint64((seed * 0x9E3779B9) & 0xFFFFFFFF)
+    return (pcg(pcg(p) ^ s) | np.uint64(1)).astype(np.uint32)
+
+
+class OracleRenderer:
+    """CPU restatement of the guided integrator (rtpg_oracle.c, or_render) for small scenes."""
+
+    def __init__(self, oracle, scene, max_depth=8, num_candidates=32, seed=1, fraction=0.3, width=None, height=None,
+                 texture=None, background=(0.0, 0.0, 0.0)):
+        L = self.L = oracle.L
+        L.or_render.argtypes = [P, C.c_uint32, P, C.c_uint32, C.c_uint32, _u32, np.ctypeslib.ndpointer(np.float64)]
+        L.or_render.restype = C.c_int64
+        s = scene
+        self.keep = {k: np.ascontiguousarray(s[k]) for k in ("tri_v", "tri_mat", "tri_uv", "light_tris", "light_first",
+                                                             "light_count", "light_emission")}
+        mats = (_OMat * len(s["materials"]))()
+        for i, m in enumerate(s["materials"]):
+            mats[i].diffuse[:] = m["diffuse"]
+            mats[i].specular[:] = m["specular"]
+            mats[i].emission[:] = m["emission"]
+            mats[i].shininess = m["shininess"]
+            mats[i].ref_index = m["ref_index"]
+            mats[i].type = m["type"]
+            mats[i].tex = m["texture"]
+        self.mats = mats
+        o = self.sc = _OScene()
+        k = self.keep
+        o.tri_v, o.tri_mat, o.tri_uv = k["tri_v"].ctypes.data, k["tri_mat"].ctypes.data, k["tri_uv"].ctypes.data
+        o.ntris = k["tri_v"].shape[0]
+        o.mats = C.cast(mats, P)
+        o.light_tris, o.light_first = k["light_tris"].ctypes.data, k["light_first"].ctypes.data
+        o.light_count, o.light_emit = k["light_count"].ctypes.data, k["light_emission"].ctypes.data
+        o.nlights = k["light_first"].shape[0]
+        if texture is not None:
+            self.tex = np.ascontiguousarray(texture, np.float32)
+            o.tex, o.tex_h, o.tex_w = self.tex.ctypes.data, self.tex.shape[0], self.tex.shape[1]
+        cam = s["camera"]
+        o.eye[:], o.cu[:], o.cv[:], o.cw[:] = (list(map(float, cam[x])) for x in ("eye", "u", "v", "w"))
+        o.bg[:] = list(background)
+        o.width, o.height = int(width or s["width"]), int(height or s["height"])
+        o.max_depth, o.num_candidates, o.fraction = max_depth, num_candidates, fraction
+        self.width, self.height = o.width, o.height
+        self.seeds = tracer_seeds(o.width, o.height, seed)
+        self.accum = np.zeros(3 * o.width * o.height, np.float64)
+        self.samples = 0
+
+    def render(self, spp, flags, tree=None):
+        for _ in range(spp):
+            self.L.or_render(C.byref(self.sc), int(flags), tree.h if tree is not None else None, 0,
+                             self.width * self.height, self.seeds, self.accum)
+        self.samples += spp
+
+    def image(self):
+        return (self.accum / max(self.samples, 1)).reshape(self.height, self.width, 3).astype(np.float32)
+
+    def render_guided(self, tree, budget, ratio_for_budget=1.0, iteration_for_built=0, base_flags=1):
+        """RTSTreeControllerT::BegTrace / EndTrace (OPX7UtilsPathGuiding.h:1808-1887) with one
+        sample per launch, flags by state as the application sets them."""
+        remain, pas, per_all, per_tmp, it = budget, 0, 0, 0, 0
+        while True:
+            if per_tmp == 0:
+                remain -= pas
+                pas = min(remain, 1 << it)
+                if remain - pas < 2 * pas or per_all >= ratio_for_budget * budget:
+                    pas = remain
+                if remain > pas and it > 0:
+                    tree.refine(int(np.sqrt(2.0 ** it * pas / 4.0) * 4000), 2000)
+            flags = (base_flags & 3) | 8
+            if it > iteration_for_built:
+                flags |= 16 if remain > pas else 16 | 32
+            self.render(1, flags, tree)
+            per_all += 1
+            per_tmp += 1
+            if per_tmp >= pas:
+                tree.build()
+                it += 1
+                per_tmp = 0
+            if per_all > budget:
+                break

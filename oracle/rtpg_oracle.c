@@ -741,3 +741,335 @@ void or_mqt_sample_pdf(int64_t n, uint32_t level, const float* pyramid, const ui
         }
     }
 }
+
+/* ------------------------------------------------------------------ integrator
+ * CPU restatement of RTLib's guided path tracer for small scenes (brute-force intersection):
+ *   raygen       SimpleGuide.cu:48-156 (jitter, bounce loop, trace vertices, commit)
+ *   closest hit  SimpleGuide.cu:287-520 (Phong/Lambert BSDF, guide mixture, NEE, RIS, glass,
+ *                emission rule), miss SimpleGuide.cu:202-219
+ *   lights       MeshLightList::Sample / MeshLight::Sample (SimpleKernel.h:81-122)
+ *   reservoir    Reservoir::Update (SimpleKernel.h:124-143)
+ *   commit       TraceVertexT::Commit (OPX7UtilsPathGuiding.h:830-866)
+ * The random numbers are drawn in the order the device code draws them (argument lists
+ * evaluated left to right), so a CPU path and a GPU path with the same seed follow the same
+ * decisions until float differences in transcendental functions separate them. */
+typedef struct { float x, y, z; } V3;
+static inline V3 v3(float x, float y, float z) { V3 r = {x, y, z}; return r; }
+static inline V3 vadd(V3 a, V3 b) { return v3(a.x + b.x, a.y + b.y, a.z + b.z); }
+static inline V3 vsub(V3 a, V3 b) { return v3(a.x - b.x, a.y - b.y, a.z - b.z); }
+static inline V3 vmul(V3 a, V3 b) { return v3(a.x * b.x, a.y * b.y, a.z * b.z); }
+static inline V3 vs(float s, V3 a) { return v3(s * a.x, s * a.y, s * a.z); }
+static inline V3 vdivs(V3 a, float s) { return v3(a.x / s, a.y / s, a.z / s); }
+static inline float vdot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+static inline V3 vcross(V3 a, V3 b) { return v3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x); }
+static inline float vlen(V3 a) { return sqrtf(vdot(a, a)); }
+static inline V3 vunit(V3 a) { return vdivs(a, vlen(a)); }
+static inline float vavg(V3 a) { return (a.x + a.y + a.z) / 3.0f; }
+static inline int vnan(V3 a) { return isnan(a.x) || isnan(a.y) || isnan(a.z); }
+static inline float sinpi_f(float x) { return (float)sin(3.14159265358979323846 * (double)x); }
+static inline float cospi_f(float x) { return (float)cos(3.14159265358979323846 * (double)x); }
+
+typedef struct {
+    float diffuse[3]; int32_t tex; float specular[3]; float shininess; float emission[3]; float ref_index;
+    int32_t type; int32_t pad[3];
+} OMat;
+typedef struct {
+    const float* tri_v; const uint32_t* tri_mat; const float* tri_uv; uint32_t ntris;
+    const OMat* mats; const uint32_t* light_tris; const uint32_t* light_first; const uint32_t* light_count;
+    const float* light_emit; uint32_t nlights;
+    const float* tex; uint32_t tex_w, tex_h;
+    float eye[3], cu[3], cv[3], cw[3], bg[3];
+    uint32_t width, height, max_depth, num_candidates;
+    float fraction; /* guide/BSDF mixing fraction of the SD-tree (STreeT::fraction) */
+} OScene;
+
+static V3 tri_vert(const OScene* s, uint32_t t, int k) {
+    const float* p = s->tri_v + 9 * (size_t)t + 3 * k;
+    return v3(p[0], p[1], p[2]);
+}
+/* Moller-Trumbore, the same operation order as the device test */
+static int o_trace(const OScene* s, V3 o, V3 d, float tmin, float tmax, int any, float* th, uint32_t* prim, float* hu,
+                   float* hv) {
+    int hit = 0;
+    float best = tmax;
+    for (uint32_t t = 0; t < s->ntris; ++t) {
+        V3 v0 = tri_vert(s, t, 0), e1 = vsub(tri_vert(s, t, 1), v0), e2 = vsub(tri_vert(s, t, 2), v0);
+        float px = d.y * e2.z - d.z * e2.y, py = d.z * e2.x - d.x * e2.z, pz = d.x * e2.y - d.y * e2.x;
+        float det = e1.x * px + e1.y * py + e1.z * pz;
+        if (fabsf(det) < 1e-20f) continue;
+        float inv = 1.0f / det;
+        float sx = o.x - v0.x, sy = o.y - v0.y, sz = o.z - v0.z;
+        float u = (sx * px + sy * py + sz * pz) * inv;
+        if (u < 0.0f || u > 1.0f) continue;
+        float qx = sy * e1.z - sz * e1.y, qy = sz * e1.x - sx * e1.z, qz = sx * e1.y - sy * e1.x;
+        float v = (d.x * qx + d.y * qy + d.z * qz) * inv;
+        if (v < 0.0f || u + v > 1.0f) continue;
+        float tt = (e2.x * qx + e2.y * qy + e2.z * qz) * inv;
+        if (tt > tmin && tt < best) {
+            best = tt; hit = 1;
+            if (th) *th = tt;
+            if (prim) *prim = t;
+            if (hu) *hu = u;
+            if (hv) *hv = v;
+            if (any) return 1;
+        }
+    }
+    return hit;
+}
+typedef struct { V3 t, b, n; } OOnb;
+static OOnb onb(V3 normal) {
+    OOnb r;
+    r.n = vunit(normal);
+    if (fabsf(r.n.x) > fabsf(r.n.z)) r.b = v3(-r.n.y, r.n.x, 0.0f);
+    else r.b = v3(0.0f, -r.n.z, r.n.y);
+    r.b = vunit(r.b);
+    r.t = vunit(vcross(r.n, r.b));
+    return r;
+}
+static V3 onb_local(OOnb o, V3 d) { return vadd(vadd(vs(d.x, o.t), vs(d.y, o.b)), vs(d.z, o.n)); }
+static float phong_pdf_o(V3 d, V3 refl, float s) {
+    float c = vdot(refl, d);
+    c = c > 0.0f ? c : 0.0f;
+    return (s + 1.0f) * powf(c, s) * O_INV_2PI;
+}
+static V3 reflect_o(V3 d, V3 n) { return vsub(d, vs(2.0f * vdot(d, n), n)); }
+static V3 phong_bsdf_o(V3 kd, V3 ks, float s, V3 d, V3 refl) {
+    return vadd(vs((float)0.318309886183790691216444201927515678107738494873046875, kd),
+                vs(phong_pdf_o(d, refl, s), vs((s + 2.0f) / (s + 1.0f), ks)));
+}
+typedef struct { V3 dir, normal, emission; float dist, inv_pdf; } OLight;
+static OLight o_sample_light(const OScene* s, V3 p_in, uint32_t* rng) {
+    uint32_t mi = xs32_next(rng) % s->nlights;
+    uint32_t ti = s->light_tris[s->light_first[mi] + xs32_next(rng) % s->light_count[mi]];
+    V3 v0 = tri_vert(s, ti, 0), v1 = tri_vert(s, ti, 1), v2 = tri_vert(s, ti, 2);
+    V3 nf = vcross(vsub(v1, v0), vsub(v2, v0));
+    float r0 = rnd1(rng), r1 = rnd1(rng);
+    float a = fminf(r0, r1), b = fmaxf(r0, r1);
+    V3 p = vadd(vadd(vs(a, v0), vs(1.0f - b, v1)), vs(b - a, v2));
+    V3 d = vsub(p, p_in);
+    OLight l;
+    l.dist = vlen(d);
+    l.dir = vunit(d);
+    l.emission = v3(s->light_emit[3 * mi], s->light_emit[3 * mi + 1], s->light_emit[3 * mi + 2]);
+    l.normal = vunit(nf);
+    l.inv_pdf = vlen(nf) / 2.0f * (float)s->light_count[mi] * (float)s->nlights;
+    return l;
+}
+#define O_NEE 1u
+#define O_RIS 2u
+#define O_TREE 8u
+#define O_BUILD 16u
+#define O_FINAL 32u
+#define O_KTV 10
+typedef struct { V3 pos, dir, thr, rad, bsdf; float wopdf, cosine; int valid, delta; } OVert;
+
+static void commit_vertex(OSDTree* t, const OVert* v) {
+    if (!v->valid || v->delta) return;
+    V3 r = v->rad, b = v->bsdf;
+    int okr = isfinite(r.x) && r.x >= 0.f && isfinite(r.y) && r.y >= 0.f && isfinite(r.z) && r.z >= 0.f;
+    int okb = isfinite(b.x) && b.x >= 0.f && isfinite(b.y) && b.y >= 0.f && isfinite(b.z) && b.z >= 0.f;
+    if (v->wopdf <= 0.0f || !okr || !okb) return;
+    V3 lr = v3(0, 0, 0);
+    if (v->thr.x * v->wopdf > 1e-4f) lr.x = r.x / v->thr.x;
+    if (v->thr.y * v->wopdf > 1e-4f) lr.y = r.y / v->thr.y;
+    if (v->thr.z * v->wopdf > 1e-4f) lr.z = r.z / v->thr.z;
+    lr = vs(fabsf(v->cosine), lr);
+    float lavg = (lr.x + lr.y + lr.z) / 3.0f;
+    float pos[3] = {v->pos.x, v->pos.y, v->pos.z}, d[3] = {v->dir.x, v->dir.y, v->dir.z}, uv[2];
+    or_dir_to_canonical(1, d, uv);
+    float one = 1.0f;
+    or_sdtree_record(t, 1, pos, uv, &lavg, &v->wopdf, &one, NULL);
+}
+
+/* One sample per pixel for pixels [p0, p1) of the frame; accum += color (double), seeds
+ * updated.  tree: an or_sdtree handle or NULL.  Returns the number of paths traced. */
+int64_t or_render(const OScene* s, uint32_t flags, void* tree_h, uint32_t p0, uint32_t p1, uint32_t* seeds,
+                  double* accum) {
+    OSDTree* tree = (OSDTree*)tree_h;
+    const int use_tree = (flags & O_TREE) != 0, build = (flags & O_BUILD) != 0;
+    const int recording = use_tree && !(flags & O_FINAL);
+    const float inv_pi = (float)0.318309886183790691216444201927515678107738494873046875;
+    for (uint32_t p = p0; p < p1; ++p) {
+        uint32_t x = p % s->width, y = p / s->width;
+        uint32_t rng = seeds[p];
+        float jx = rnd1(&rng), jy = rnd1(&rng);
+        float dx = (2.0f * ((float)x + jx) / (float)s->width) - 1.0f;
+        float dy = (2.0f * ((float)y + jy) / (float)s->height) - 1.0f;
+        V3 cu = v3(s->cu[0], s->cu[1], s->cu[2]), cv = v3(s->cv[0], s->cv[1], s->cv[2]), cw = v3(s->cw[0], s->cw[1], s->cw[2]);
+        V3 org = v3(s->eye[0], s->eye[1], s->eye[2]);
+        V3 dir = vunit(vadd(vadd(vs(dx, cu), vs(dy, cv)), cw));
+        V3 thr = v3(1, 1, 1), col = v3(0, 0, 0);
+        uint32_t pflags = 8u /* COUNT_EMITTED */, depth = 0;
+        OVert verts[O_KTV];
+        for (;;) {
+            uint32_t tvd = depth < O_KTV ? depth : O_KTV;
+            float t = 0, hu = 0, hv = 0;
+            uint32_t prim = 0;
+            V3 L = v3(0, 0, 0), cur_thr = thr, direction = v3(0, 0, 0), bsdf_val = v3(0, 0, 0);
+            float cosine = 0.0f, wo_pdf = 0.0f;
+            uint32_t hflags = 0;
+            V3 position = org;
+            int hit = o_trace(s, org, dir, 0.0001f, 1.0e20f, 0, &t, &prim, &hu, &hv);
+            if (!hit) {
+                L = vmul(thr, v3(s->bg[0], s->bg[1], s->bg[2]));
+                hflags = 16u;
+                if (recording && depth < O_KTV) verts[depth].valid = 0;
+            } else {
+                V3 v0 = tri_vert(s, prim, 0), v1 = tri_vert(s, prim, 1), v2 = tri_vert(s, prim, 2);
+                V3 fn = vunit(vcross(vsub(v1, v0), vsub(v2, v0)));
+                position = vadd(org, vs(t, dir));
+                const OMat* m = &s->mats[s->tri_mat[prim]];
+                V3 diffuse = v3(m->diffuse[0], m->diffuse[1], m->diffuse[2]);
+                V3 spec = v3(m->specular[0], m->specular[1], m->specular[2]);
+                V3 emis = v3(m->emission[0], m->emission[1], m->emission[2]);
+                if (m->tex >= 0 && s->tex && s->tri_uv) {
+                    const float* uv = s->tri_uv + 6 * (size_t)prim;
+                    float w0 = 1.0f - hu - hv;
+                    float tu = w0 * uv[0] + hu * uv[2] + hv * uv[4], tv = w0 * uv[1] + hu * uv[3] + hv * uv[5];
+                    float fu = tu - floorf(tu), fv = tv - floorf(tv);
+                    uint32_t ix = (uint32_t)(fu * s->tex_w), iy = (uint32_t)(fv * s->tex_h);
+                    if (ix > s->tex_w - 1) ix = s->tex_w - 1;
+                    if (iy > s->tex_h - 1) iy = s->tex_h - 1;
+                    const float* px = s->tex + 3 * ((size_t)iy * s->tex_w + ix);
+                    diffuse = vmul(diffuse, v3(px[0], px[1], px[2]));
+                }
+                int count_emitted = (pflags & 8u) || m->type == 3;
+                uint32_t dt = 0;
+                if (use_tree) dt = (uint32_t)leaf_dtree(tree, &position.x);
+                if (m->type == 0) {
+                    V3 refl = vunit(reflect_o(dir, fn));
+                    float a = rnd1(&rng), c = rnd1(&rng);
+                    float r = sqrtf(a), z = sqrtf(1.0f - a);
+                    V3 d0 = onb_local(onb(fn), v3(r * cospi_f(2.0f * c), r * sinpi_f(2.0f * c), z));
+                    float cosT = powf(rnd1(&rng), 1.0f / (m->shininess + 1.0f));
+                    float sinT = sqrtf(fmaxf(1.0f - cosT * cosT, 0.0f));
+                    float phi = O_2PI * rnd1(&rng);
+                    V3 d1 = onb_local(onb(refl), v3(sinT * cosf(phi), sinT * sinf(phi), cosT));
+                    float c0 = vdot(d0, fn), c1 = vdot(d1, fn);
+                    float cp0 = fmaxf(c0 * inv_pi, 0.0f), cp1 = fmaxf(c1 * inv_pi, 0.0f);
+                    float pp0 = phong_pdf_o(d0, refl, m->shininess), pp1 = phong_pdf_o(d1, refl, m->shininess);
+                    float ad = 1.0e-10f + vavg(diffuse), as = 1.0e-10f + vavg(spec);
+                    float sel = ad / (ad + as);
+                    float sf = (m->shininess + 2.0f) / (m->shininess + 1.0f);
+                    float bsdf_pdf;
+                    if (rnd1(&rng) < sel) {
+                        direction = d0; cosine = c0;
+                        bsdf_val = vadd(vs(inv_pi, diffuse), vs(pp0, vs(sf, spec)));
+                        bsdf_pdf = sel * cp0 + (1.0f - sel) * pp0;
+                    } else {
+                        direction = d1; cosine = c1;
+                        bsdf_val = vadd(vs(inv_pi, diffuse), vs(pp1, vs(sf, spec)));
+                        bsdf_pdf = sel * cp1 + (1.0f - sel) * pp1;
+                    }
+                    if (use_tree && build) {
+                        const ODTree* dd = &tree->dt[dt];
+                        if (rnd1(&rng) < s->fraction) {
+                            float uv[2];
+                            dtree_sample(dd, &rng, uv);
+                            float dv[3];
+                            const float cosTheta = 2.0f * uv[0] - 1.0f;
+                            const float sinTheta = sqrtf(fmaxf(1.0f - cosTheta * cosTheta, 0.0f));
+                            dv[0] = sinTheta * cospi_f(2.0f * uv[1]);
+                            dv[1] = sinTheta * sinpi_f(2.0f * uv[1]);
+                            dv[2] = cosTheta;
+                            float l = 1.0f / sqrtf(dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2]);
+                            direction = v3(dv[0] * l, dv[1] * l, dv[2] * l);
+                            cosine = vdot(direction, fn);
+                            float cp2 = fmaxf(cosine * inv_pi, 0.0f);
+                            float pp2 = phong_pdf_o(direction, refl, m->shininess);
+                            bsdf_val = vadd(vs(inv_pi, diffuse), vs(pp2, vs(sf, spec)));
+                            bsdf_pdf = sel * cp2 + (1.0f - sel) * pp2;
+                        }
+                        float dd3[3] = {direction.x, direction.y, direction.z}, c2[2];
+                        or_dir_to_canonical(1, dd3, c2);
+                        float dpdf = fmaxf(dtree_pdf(dd, c2[0], c2[1]), 0.0f);
+                        wo_pdf = (1.0f - s->fraction) * bsdf_pdf + s->fraction * dpdf;
+                    } else {
+                        wo_pdf = bsdf_pdf;
+                    }
+                    cur_thr = wo_pdf > 0.0f ? vmul(thr, vdivs(vs(fmaxf(cosine, 0.0f), bsdf_val), wo_pdf)) : v3(0, 0, 0);
+                    if (flags & O_NEE) {
+                        if (depth < s->max_depth - 1 && s->nlights > 0) {
+                            if (flags & O_RIS) {
+                                float w_sum = 0.0f, fay = 0.0f, disty = 0.0f;
+                                uint32_t mc = 0;
+                                V3 fy = v3(0, 0, 0), ldy = v3(0, 0, 0);
+                                for (uint32_t k = 0; k < s->num_candidates; ++k) {
+                                    OLight l = o_sample_light(s, position, &rng);
+                                    float ndl = vdot(l.dir, fn), lndl = -vdot(l.dir, l.normal);
+                                    V3 b = phong_bsdf_o(diffuse, spec, m->shininess, l.dir, refl);
+                                    float g = fmaxf(ndl, 0.0f) * fmaxf(lndl, 0.0f) / (l.dist * l.dist);
+                                    V3 f = vmul(vmul(b, l.emission), v3(g, g, g));
+                                    float fa = vavg(f), wi = fa * l.inv_pdf;
+                                    w_sum += wi;
+                                    ++mc;
+                                    if ((wi / w_sum) >= rnd1(&rng)) { fy = f; fay = fa; ldy = l.dir; disty = l.dist; }
+                                }
+                                if (w_sum > 0.0f && fay > 0.0f &&
+                                    !o_trace(s, position, ldy, 0.0001f, disty - 0.0001f, 1, 0, 0, 0, 0))
+                                    L = vadd(L, vs(w_sum / (fay * (float)mc), vmul(thr, fy)));
+                            } else {
+                                OLight l = o_sample_light(s, position, &rng);
+                                V3 b = phong_bsdf_o(diffuse, spec, m->shininess, l.dir, refl);
+                                float g = fmaxf(-vdot(l.dir, l.normal), 0.0f) * fabsf(vdot(l.dir, fn)) / (l.dist * l.dist);
+                                if (!o_trace(s, position, l.dir, 0.0001f, l.dist - 0.0001f, 1, 0, 0, 0, 0))
+                                    L = vadd(L, vs(l.inv_pdf, vs(g, vmul(vmul(thr, b), l.emission))));
+                            }
+                        }
+                    } else {
+                        hflags |= 8u;
+                    }
+                } else if (m->type == 1) {
+                    V3 rn;
+                    float rri, ci = vdot(fn, dir);
+                    if (ci < 0.0f) { rn = fn; rri = 1.0f / m->ref_index; ci = -ci; }
+                    else { rn = v3(-fn.x, -fn.y, -fn.z); rri = m->ref_index; }
+                    float so2 = (1.0f - ci * ci) * (rri * rri);
+                    float f0 = ((1.0f - rri) / (1.0f + rri)) * ((1.0f - rri) / (1.0f + rri));
+                    float om = 1.0f - ci;
+                    float fres = f0 + (1.0f - f0) * (om * om * om * om * om);
+                    V3 rd = vunit(reflect_o(dir, rn));
+                    if (rnd1(&rng) < fres || so2 > 1.0f) {
+                        position = vadd(position, vs(0.0001f, rn));
+                        direction = rd; cosine = fabsf(ci); bsdf_val = spec; cur_thr = vmul(thr, spec);
+                    } else {
+                        position = vsub(position, vs(0.0001f, rn));
+                        float si2 = fmaxf(1.0f - ci * ci, 0.0f), co = sqrtf(1.0f - so2);
+                        V3 rf;
+                        if (si2 > 0.0f) rf = vunit(vsub(vs(sqrtf(so2), vdivs(vadd(dir, vs(ci, rn)), sqrtf(si2))), vs(co, rn)));
+                        else rf = dir;
+                        direction = rf; cosine = fabsf(vdot(rf, rn)); bsdf_val = v3(1, 1, 1); cur_thr = thr;
+                    }
+                    wo_pdf = fabsf(cosine);
+                    hflags |= 8u | 2u;
+                }
+                if (vdot(dir, fn) < 0.0f && count_emitted) L = vadd(L, vmul(thr, emis));
+                if (emis.x + emis.y + emis.z > 0.0f) hflags |= 16u;
+                if (recording && depth < O_KTV) {
+                    OVert* v = &verts[depth];
+                    v->pos = position; v->dir = direction; v->thr = cur_thr; v->rad = v3(0, 0, 0);
+                    v->bsdf = bsdf_val; v->wopdf = wo_pdf; v->cosine = cosine; v->valid = 1; v->delta = (hflags & 2u) != 0;
+                }
+            }
+            if (recording)
+                for (uint32_t i = 0; i < tvd; ++i) verts[i].rad = vadd(verts[i].rad, L);
+            col = vadd(col, L);
+            org = position;
+            dir = direction;
+            thr = cur_thr;
+            pflags = hflags;
+            if (vnan(dir) || vnan(thr) || vnan(L)) break;
+            if ((hflags & 16u) || depth >= s->max_depth - 1) break;
+            ++depth;
+        }
+        if (recording) {
+            uint32_t nv = depth < O_KTV ? depth : O_KTV;
+            for (uint32_t i = 0; i < nv; ++i) commit_vertex(tree, &verts[i]);
+        }
+        accum[3 * (size_t)p] += col.x;
+        accum[3 * (size_t)p + 1] += col.y;
+        accum[3 * (size_t)p + 2] += col.z;
+        seeds[p] = rng;
+    }
+    return (int64_t)(p1 - p0);
+}

@@ -66,6 +66,22 @@ _SIGS = {
     "rtpg_mqt_pdf": [P, I64, P, P, C.c_int, P, C.c_int, P],
     "rtpg_mqt_export": [P, P, P, P],
     "rtpg_mqt_status": [P, P, C.c_int, P],
+    "rtpg_scene_create": [P, U32, P, U32, P, P],
+    "rtpg_scene_destroy": [P],
+    "rtpg_scene_intersect": [P, I64, P, P, P, P, C.c_int, P, P, P, P],
+    "rtpg_tracer_create": [P, P, P, P, P, U32, P, P, P, U32, P, P, P],
+    "rtpg_tracer_destroy": [P],
+    "rtpg_tracer_set_texture": [P, U32, U32, U32, P],
+    "rtpg_tracer_set_seed": [P, U32],
+    "rtpg_tracer_clear": [P, P],
+    "rtpg_tracer_render": [P, U32, U32, P, P],
+    "rtpg_tracer_render_guided": [P, P, P, U32, U32, U32, P],
+    "rtpg_tracer_image": [P, P, P],
+    "rtpg_tracer_accumulation": [P, P, P],
+    "rtpg_tracer_stats": [P, P, P],
+    "rtpg_tracer_set_timing": [P, C.c_int],
+    "rtpg_tracer_counters": [P, P, P, P],
+    "rtpg_tracer_timings": [P, P, P],
 }
 _RESTYPE = {"rtpg_last_error": C.c_char_p}
 

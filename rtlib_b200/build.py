@@ -1,9 +1,9 @@
 """Build recipe of the rtlib_b200 native library (nvcc, sm_100a only).
 
 Produces rtlib_b200/librtpg.so in-tree.  Every .cu file under csrc/ is compiled for
-``-gencode arch=compute_100a,code=sm_100a``.  The guiding kernels are compiled with
-``-fmad=false`` so every float operation rounds exactly as written (their results are
-checked bit for bit against the oracle); the tracer files keep FMA contraction.
+``-gencode arch=compute_100a,code=sm_100a``.  The guiding, hash-grid, BVH and tracer
+kernels are compiled with ``-fmad=false`` so every float operation rounds exactly as written
+(their results are checked against the CPU oracle, bit for bit where the arithmetic allows).
 """
 from __future__ import annotations
 
@@ -20,7 +20,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
           "-Xcompiler", "-Wall", "--expt-relaxed-constexpr", "-DRTPG_BUILD"]
 # files whose float arithmetic must round as written (bit-exact parity with the oracle)
-EXACT = {"sdtree.cu", "common.cu", "hashgrid.cu", "mqt.cu", "noalloc.cu"}
+EXACT = {"sdtree.cu", "common.cu", "hashgrid.cu", "mqt.cu", "tracer.cu", "bvh.cu"}
 
 
 def sources():

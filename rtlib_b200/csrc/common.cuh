@@ -27,6 +27,10 @@ int fail(int code, const char* fmt, ...);
 
 inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
+// float2 arrays are read and written as 8-byte vectors: their base must be 8-byte aligned
+inline bool aligned8(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 7u) == 0; }
+inline bool aligned4(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 3u) == 0; }
+
 constexpr int kSMs = 148;  // B200: 148 SMs on two dies
 
 inline int grid_for(int64_t n, int block, int per_sm = 8) {

@@ -195,6 +195,7 @@ int rtpg_mqt_record(rtpg_mqt* h, int64_t n, const uint32_t* cell, const float* d
                     const float* value, void* stream) {
     if (!h) return fail(RTPG_EINVAL, "rtpg_mqt_record: null handle");
     if (n < 0 || (n > 0 && (!cell || !dir || !value))) return fail(RTPG_EINVAL, "rtpg_mqt_record: bad arguments");
+    if (dir_is_canonical && !aligned8(dir)) return fail(RTPG_EINVAL, "rtpg_mqt_record: misaligned float2 array");
     if (n == 0) return RTPG_OK;
     k_mqt_record<<<grid_for(n, 256, 8), 256, 0, as_stream(stream)>>>(h->dev, n, cell, dir, dir_is_canonical, value);
     RTPG_LAUNCH_CHECK();
@@ -216,6 +217,7 @@ int rtpg_mqt_sample_pdf(rtpg_mqt* h, int64_t n, const uint32_t* cell, const uint
                         float* out_uv, float* out_pdf, float* out_dir, float* out_pdf_tree, void* stream) {
     if (!h) return fail(RTPG_EINVAL, "rtpg_mqt_sample_pdf: null handle");
     if (n < 0 || (n > 0 && !cell)) return fail(RTPG_EINVAL, "rtpg_mqt_sample_pdf: bad arguments");
+    if (!aligned8(out_uv)) return fail(RTPG_EINVAL, "rtpg_mqt_sample_pdf: misaligned float2 array");
     if (n == 0) return RTPG_OK;
     k_mqt_sample<<<grid_for(n, 256, 8), 256, 0, as_stream(stream)>>>(h->dev, n, cell, seeds, seed_base, out_uv, out_pdf,
                                                                      out_dir, out_pdf_tree);
@@ -228,6 +230,7 @@ int rtpg_mqt_pdf(rtpg_mqt* h, int64_t n, const uint32_t* cell, const float* dir,
                  int tree_level, void* stream) {
     if (!h) return fail(RTPG_EINVAL, "rtpg_mqt_pdf: null handle");
     if (n < 0 || (n > 0 && (!cell || !dir || !out))) return fail(RTPG_EINVAL, "rtpg_mqt_pdf: bad arguments");
+    if (dir_is_canonical && !aligned8(dir)) return fail(RTPG_EINVAL, "rtpg_mqt_pdf: misaligned float2 array");
     if (n == 0) return RTPG_OK;
     k_mqt_pdf<<<grid_for(n, 256, 8), 256, 0, as_stream(stream)>>>(h->dev, n, cell, dir, dir_is_canonical, out, tree_level);
     RTPG_LAUNCH_CHECK();

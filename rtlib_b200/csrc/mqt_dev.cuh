@@ -55,9 +55,11 @@ __device__ __forceinline__ float2 dir_to_canonical_mqt(float x, float y, float z
 __device__ __forceinline__ float3 canonical_to_dir_mqt(float u, float v) { return canonical_to_dir(u, v); }
 
 // MortonQuadTreeT::SampleAndPdf (:286-344), float order as written
+// A cell outside [0, ncells) (UINT32_MAX marks a hash-grid miss) samples like an empty
+// tree: uniform with pdf 1 (RTLib reads out of bounds there).
 __device__ __forceinline__ float2 mqt_sample_and_pdf(const MqtDev& t, uint32_t cell, uint32_t& rng, float& pdf) {
-    const float* w = t.pyramid + (size_t)cell * mqt_level_offset(t.level + 1);
-    float total = w[0];
+    const float* w = t.pyramid + (size_t)(cell < t.ncells ? cell : 0u) * mqt_level_offset(t.level + 1);
+    float total = cell < t.ncells ? w[0] : 0.0f;
     if (total <= 0.0f) {
         const float a = rnd1(rng);
         const float b = rnd1(rng);
@@ -66,7 +68,9 @@ __device__ __forceinline__ float2 mqt_sample_and_pdf(const MqtDev& t, uint32_t c
     }
     uint32_t size = 4, offset = 1, code = 0;
     for (uint32_t l = 0; l < t.level; ++l) {
-        const float4 q = *reinterpret_cast<const float4*>(w + offset + (code << 2));
+        // level offsets (4^l-1)/3 are odd, so the four children are read one by one
+        const float* qp = w + offset + (code << 2);
+        const float4 q = make_float4(qp[0], qp[1], qp[2], qp[3]);
         uint32_t cl = 0;
         float partial = __fadd_rn(q.x, q.z);
         float boundary = __fdiv_rn(partial, total);
@@ -98,6 +102,7 @@ __device__ __forceinline__ float2 mqt_sample_and_pdf(const MqtDev& t, uint32_t c
 
 // MortonQuadTreeT::Pdf (:401-414)
 __device__ __forceinline__ float mqt_pdf(const MqtDev& t, uint32_t cell, float u, float v) {
+    if (cell >= t.ncells) return 1.0f;
     const float* w = t.pyramid + (size_t)cell * mqt_level_offset(t.level + 1);
     if (w[0] <= 0.0f) return 1.0f;
     const float nn = (float)(1u << t.level);

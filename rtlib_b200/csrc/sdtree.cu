@@ -518,6 +518,10 @@ struct rtpg_sdtree {
     }
 };
 
+namespace rtpg {
+SDTreeDev sdtree_device_view(const rtpg_sdtree* t) { return t->dev; }
+}
+
 static int sdtree_clear(rtpg_sdtree* h, cudaStream_t st) {
     RTPG_CUDA(cudaMemsetAsync(h->dev.status, 0, sizeof(unsigned), st));
     k_clear<<<1, 32, 0, st>>>(h->dev);
@@ -624,6 +628,8 @@ int rtpg_sdtree_record(rtpg_sdtree* h, int64_t n, const float* pos, const float*
     if (n < 0) return fail(RTPG_EINVAL, "rtpg_sdtree_record: n < 0");
     if (n == 0) return RTPG_OK;
     if (!pos || !dir || !radiance) return fail(RTPG_EINVAL, "rtpg_sdtree_record: pos, dir and radiance are required");
+    if ((dir_is_canonical && !aligned8(dir)) || !aligned4(pos) || !aligned4(radiance))
+        return fail(RTPG_EINVAL, "rtpg_sdtree_record: misaligned array (float2 arrays need 8-byte alignment)");
     const int g = grid_for(n, kRecordBlock, 8);
     if (dir_is_canonical)
         k_record<true><<<g, kRecordBlock, 0, as_stream(stream)>>>(h->dev, n, pos, dir, radiance, wo_pdf, stat_weight, is_delta);
@@ -686,6 +692,7 @@ int rtpg_sdtree_sample_pdf(rtpg_sdtree* h, int64_t n, const float* pos, const ui
                            float* out_uv, float* out_pdf_uv, float* out_dir, float* out_pdf_dir, void* stream) {
     if (!h) return fail(RTPG_EINVAL, "rtpg_sdtree_sample_pdf: null handle");
     if (n < 0 || (n > 0 && !pos)) return fail(RTPG_EINVAL, "rtpg_sdtree_sample_pdf: bad arguments");
+    if (!aligned8(out_uv) || !aligned4(pos)) return fail(RTPG_EINVAL, "rtpg_sdtree_sample_pdf: misaligned array");
     if (n == 0) return RTPG_OK;
     k_sample_pdf<<<grid_for(n, 256, 8), 256, 0, as_stream(stream)>>>(h->dev, n, pos, seeds, seed_base, out_uv,
                                                                      out_pdf_uv, out_dir, out_pdf_dir);
@@ -697,6 +704,7 @@ int rtpg_sdtree_pdf(rtpg_sdtree* h, int64_t n, const float* pos, const float* di
                     float* out_pdf, void* stream) {
     if (!h) return fail(RTPG_EINVAL, "rtpg_sdtree_pdf: null handle");
     if (n < 0 || (n > 0 && (!pos || !dir || !out_pdf))) return fail(RTPG_EINVAL, "rtpg_sdtree_pdf: bad arguments");
+    if ((dir_is_canonical && !aligned8(dir)) || !aligned4(pos)) return fail(RTPG_EINVAL, "rtpg_sdtree_pdf: misaligned array");
     if (n == 0) return RTPG_OK;
     k_pdf<<<grid_for(n, 256, 8), 256, 0, as_stream(stream)>>>(h->dev, n, pos, dir, dir_is_canonical, out_pdf);
     RTPG_LAUNCH_CHECK();

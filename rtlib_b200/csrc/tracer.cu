@@ -1,0 +1,791 @@
+// Wavefront path tracer with SD-tree guiding, NEE and RIS (rtpg_tracer_*).
+//
+// RTLib renders with OptiX megakernels: __raygen__default loops over bounces and keeps up to
+// 10 trace vertices per path (SimpleGuide.cu:48-156); __closesthit__radiance shades, samples
+// the BSDF / guide mixture and does NEE or RIS with one shadow ray (SimpleGuide.cu:287-520,
+// SimpleTrace.cu for the unguided tracers).  Here the same per-path algorithm runs as a
+// wavefront over SoA path state, one frame of paths (one sample per pixel) per wave:
+//   raygen   camera rays, per-pixel Xorshift32 state from the seed buffer;
+//   extend   closest hit + shading of every active path: emission, BSDF / guide mixture
+//            sampling, NEE or RIS candidate selection (shadow ray left pending);
+//   connect  the pending shadow ray, the bounce radiance added to the path and to its earlier
+//            trace vertices, termination, compaction of survivors into the next queue;
+//   finish   accumulation in FP64, seed write-back, and the commit of trace vertices into
+//            the SD-tree (TraceVertexT::Commit, OPX7UtilsPathGuiding.h:830-866) with the
+//            fixed-point atomics of the record kernel.
+// A wave is captured once per configuration into a CUDA graph and replayed per sample.
+#include <map>
+#include <string.h>
+#include <new>
+#include <vector>
+
+#include "common.cuh"
+#include "bvh_dev.cuh"
+#include "sdtree_dev.cuh"
+#include "tracer_dev.cuh"
+
+struct rtpg_scene;
+struct rtpg_sdtree;
+namespace rtpg {
+SceneDev scene_device_view(const rtpg_scene* s);
+SDTreeDev sdtree_device_view(const rtpg_sdtree* t);
+}
+
+namespace rtpg {
+
+constexpr int kTV = 10;  // trace vertices per path (kTraceVertexSize, OPX7/CMakeLists.txt:90)
+constexpr int kTB = 128;
+
+struct TracerDev {
+    SceneDev scene;
+    const float* tri_v;     // 9 floats per triangle (original order)
+    const float* tri_uv;    // 6 floats per triangle or null
+    const uint32_t* tri_mat;
+    const Material* mats;
+    const float* const* tex;  // per texture: RGB float, tex_wh[t] = (w, h)
+    const uint2* tex_wh;
+    const uint32_t* light_tris;
+    const uint2* light_mesh;  // (first, count) into light_tris
+    const float3* light_emit;
+    uint32_t light_count;
+    float3 eye, cu, cv, cw, bg;
+    uint32_t width, height, npath, max_depth, num_candidates, flags;
+    // path state
+    float3 *org, *dir, *thr, *col, *brad, *sdir, *scontrib;
+    float* sdist;
+    uint32_t *rng, *depth, *hflags, *pending;
+    uint32_t* queue[2];
+    uint32_t* qcount;  // [0], [1]
+    // trace vertices, [kTV][npath]
+    float3 *v_pos, *v_dir, *v_thr, *v_rad, *v_bsdf;
+    float *v_wopdf, *v_cos;
+    uint8_t* v_flags;  // bit0 valid (a DTree exists), bit1 delta
+    uint32_t* seeds;
+    double* accum;  // 3 per pixel
+    SDTreeDev tree;
+    unsigned* status;
+    unsigned long long* counters;  // [0] extend visits (path-bounces), [1] shadow rays
+};
+
+// ------------------------------------------------------------------ raygen (SimpleGuide.cu:48-81)
+__global__ void __launch_bounds__(kTB) k_raygen(TracerDev T) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) T.qcount[0] = T.npath;
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < T.npath; p += gridDim.x * blockDim.x) {
+        const uint32_t x = p % T.width, y = p / T.width;
+        uint32_t rng = T.seeds[p];
+        const float jx = rnd1(rng);
+        const float jy = rnd1(rng);
+        const float dx = (2.0f * ((float)x + jx) / (float)T.width) - 1.0f;
+        const float dy = (2.0f * ((float)y + jy) / (float)T.height) - 1.0f;
+        T.org[p] = T.eye;
+        T.dir[p] = unit3(dx * T.cu + dy * T.cv + T.cw);
+        T.thr[p] = f3(1.0f, 1.0f, 1.0f);
+        T.col[p] = f3(0.0f, 0.0f, 0.0f);
+        T.rng[p] = rng;
+        T.depth[p] = 0;
+        T.hflags[p] = HF_COUNT_EMITTED;
+        T.queue[0][p] = p;
+    }
+}
+
+__device__ __forceinline__ float3 tex_fetch(const TracerDev& T, int t, float u, float v) {
+    const uint2 wh = T.tex_wh[t];
+    float fu = u - floorf(u), fv = v - floorf(v);
+    uint32_t x = min((uint32_t)(fu * wh.x), wh.x - 1), y = min((uint32_t)(fv * wh.y), wh.y - 1);
+    const float* px = T.tex[t] + 3 * (size_t(y) * wh.x + x);
+    return f3(px[0], px[1], px[2]);
+}
+
+struct LightSample {
+    float3 pos, dir, normal, emission;
+    float dist, inv_pdf;
+};
+// MeshLightList::Sample -> MeshLight::Sample (SimpleKernel.h:81-98, 114-120): mesh and
+// triangle by next() % count, barycentrics by random_in_unit_triangle.
+__device__ __forceinline__ LightSample sample_light(const TracerDev& T, float3 p_in, uint32_t& rng) {
+    const uint32_t mi = xs32_next(rng) % T.light_count;
+    const uint2 mesh = T.light_mesh[mi];
+    const uint32_t ti = T.light_tris[mesh.x + xs32_next(rng) % mesh.y];
+    const float* tv = T.tri_v + 9 * size_t(ti);
+    const float3 v0 = f3(tv[0], tv[1], tv[2]), v1 = f3(tv[3], tv[4], tv[5]), v2 = f3(tv[6], tv[7], tv[8]);
+    const float3 nf = cross3(v1 - v0, v2 - v0);
+    const float r0 = rnd1(rng);
+    const float r1 = rnd1(rng);
+    const float a = fminf(r0, r1), b = fmaxf(r0, r1);
+    const float3 p = a * v0 + (1.0f - b) * v1 + (b - a) * v2;
+    const float3 d = p - p_in;
+    LightSample l;
+    l.pos = p;
+    l.dist = len3(d);
+    l.dir = unit3(d);
+    l.emission = T.light_emit[mi];
+    l.normal = unit3(nf);
+    l.inv_pdf = len3(nf) / 2.0f * (float)mesh.y * (float)T.light_count;
+    return l;
+}
+
+// ------------------------------------------------------------------ extend
+// __closesthit__radiance / __miss__radiance (SimpleGuide.cu:220-520) for every active path.
+__global__ void __launch_bounds__(kTB) k_extend(TracerDev T, int in) {
+    const uint32_t n = T.qcount[in];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        T.qcount[in ^ 1] = 0;
+        atomicAdd(T.counters, (unsigned long long)n);
+    }
+    const bool use_tree = (T.flags & RTPG_TRACE_FLAG_USE_TREE) != 0;
+    const bool build = (T.flags & RTPG_TRACE_FLAG_BUILD) != 0;
+    const bool recording = use_tree && !(T.flags & RTPG_TRACE_FLAG_FINAL);
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        const uint32_t p = T.queue[in][q];
+        const float3 org = T.org[p], in_dir = T.dir[p], prev_thr = T.thr[p];
+        const uint32_t d = T.depth[p], prev_flags = T.hflags[p];
+        const Hit h = bvh_trace<false>(T.scene, org.x, org.y, org.z, in_dir.x, in_dir.y, in_dir.z, 0.0001f, 1.0e20f);
+        const size_t vi = size_t(d < kTV ? d : 0) * T.npath + p;
+        T.pending[p] = 0;
+        if (h.prim == 0xffffffffu) {
+            // __miss__radiance (SimpleGuide.cu:202-219)
+            T.brad[p] = prev_thr * T.bg;
+            T.hflags[p] = HF_FINISH;
+            T.thr[p] = prev_thr;
+            if (recording && d < kTV) T.v_flags[vi] = 0;
+            continue;
+        }
+        uint32_t rng = T.rng[p];
+        const float* tv = T.tri_v + 9 * size_t(h.prim);
+        const float3 v0 = f3(tv[0], tv[1], tv[2]), v1 = f3(tv[3], tv[4], tv[5]), v2 = f3(tv[6], tv[7], tv[8]);
+        const float3 fn = unit3(cross3(v1 - v0, v2 - v0));
+        float3 position = org + h.t * in_dir;
+        const Material m = T.mats[T.tri_mat[h.prim]];
+        float3 diffuse = m.diffuse;
+        if (m.tex >= 0 && T.tri_uv) {
+            const float* uv = T.tri_uv + 6 * size_t(h.prim);
+            const float w0 = 1.0f - h.u - h.v;
+            const float tu = w0 * uv[0] + h.u * uv[2] + h.v * uv[4];
+            const float tvv = w0 * uv[1] + h.u * uv[3] + h.v * uv[5];
+            diffuse = diffuse * tex_fetch(T, m.tex, tu, tvv);
+        }
+        const bool count_emitted = (prev_flags & HF_COUNT_EMITTED) || m.type == MAT_DEF_LIGHT;
+        float3 direction = f3(0.f, 0.f, 0.f), bsdf_val = f3(0.f, 0.f, 0.f), cur_thr = f3(0.f, 0.f, 0.f);
+        float cosine = 0.0f, bsdf_pdf = 0.0f, wo_pdf = 0.0f;
+        uint32_t flags = 0;
+        uint32_t dt = 0;
+        if (use_tree) dt = stree_lookup(T.tree.snode, T.tree.mn, T.tree.mx, position.x, position.y, position.z);
+        if (m.type == MAT_PHONG) {
+            const float3 refl = unit3(reflect3(in_dir, fn));
+            const float3 d0 = sample_cosine(fn, rng);
+            const float3 d1 = sample_phong(refl, m.shininess, rng);
+            const float c0 = dot3(d0, fn), c1 = dot3(d1, fn);
+            const float cp0 = fmaxf(c0 * kInvPi, 0.0f), cp1 = fmaxf(c1 * kInvPi, 0.0f);
+            const float pp0 = phong_pdf(d0, refl, m.shininess), pp1 = phong_pdf(d1, refl, m.shininess);
+            const float ad = 1.0e-10f + avg3(diffuse), as = 1.0e-10f + avg3(m.specular);
+            const float sel = ad / (ad + as);
+            const float sf = (m.shininess + 2.0f) / (m.shininess + 1.0f);
+            if (rnd1(rng) < sel) {
+                direction = d0; cosine = c0;
+                bsdf_val = diffuse * kInvPi + m.specular * sf * pp0;
+                bsdf_pdf = sel * cp0 + (1.0f - sel) * pp0;
+            } else {
+                direction = d1; cosine = c1;
+                bsdf_val = diffuse * kInvPi + m.specular * sf * pp1;
+                bsdf_pdf = sel * cp1 + (1.0f - sel) * pp1;
+            }
+            if (use_tree && build) {
+                const uint32_t soff = T.tree.s_off[dt];
+                const bool guided = dtree_mean(T.tree.s_statw[dt], T.tree.s_sum[dt]) > 0.0f;
+                if (rnd1(rng) < T.tree.fraction) {
+                    const float2 c = dtree_sample_g(T.tree.s_nodes, soff, guided, rng);
+                    direction = normalize3(canonical_to_dir(c.x, c.y));
+                    cosine = dot3(direction, fn);
+                    const float cp2 = fmaxf(cosine * kInvPi, 0.0f);
+                    const float pp2 = phong_pdf(direction, refl, m.shininess);
+                    bsdf_val = diffuse * kInvPi + m.specular * sf * pp2;
+                    bsdf_pdf = sel * cp2 + (1.0f - sel) * pp2;
+                }
+                const float2 c = dir_to_canonical(direction.x, direction.y, direction.z);
+                const float dtree_pdf = fmaxf(dtree_pdf_g(T.tree.s_nodes, soff, guided, c.x, c.y), 0.0f);
+                wo_pdf = (1.0f - T.tree.fraction) * bsdf_pdf + T.tree.fraction * dtree_pdf;
+            } else {
+                wo_pdf = bsdf_pdf;
+            }
+            cur_thr = prev_thr * ((wo_pdf > 0.0f) ? (bsdf_val * fmaxf(cosine, 0.0f) / wo_pdf) : f3(0.f, 0.f, 0.f));
+            if (T.flags & RTPG_TRACE_FLAG_NEE) {
+                if (d < T.max_depth - 1 && T.light_count > 0) {
+                    if (T.flags & RTPG_TRACE_FLAG_RIS) {
+                        // RIS over numCandidates light samples (SimpleGuide.cu:379-408)
+                        float w_sum = 0.0f, f_a_y = 0.0f, dist_y = 0.0f;
+                        uint32_t mcount = 0;
+                        float3 f_y = f3(0.f, 0.f, 0.f), ldir_y = f3(0.f, 0.f, 0.f);
+                        for (uint32_t c = 0; c < T.num_candidates; ++c) {
+                            const LightSample l = sample_light(T, position, rng);
+                            const float ndl = dot3(l.dir, fn), lndl = -dot3(l.dir, l.normal);
+                            const float3 b = phong_bsdf(diffuse, m.specular, m.shininess, l.dir, refl);
+                            const float g = fmaxf(ndl, 0.0f) * fmaxf(lndl, 0.0f) / (l.dist * l.dist);
+                            const float3 f = b * l.emission * g;
+                            const float fa = avg3(f);
+                            const float wi = fa * l.inv_pdf;
+                            // Reservoir::Update (SimpleKernel.h:124-143)
+                            w_sum += wi;
+                            ++mcount;
+                            if ((wi / w_sum) >= rnd1(rng)) {
+                                f_y = f; f_a_y = fa; ldir_y = l.dir; dist_y = l.dist;
+                            }
+                        }
+                        if (w_sum > 0.0f && f_a_y > 0.0f) {
+                            T.pending[p] = 1;
+                            T.sdir[p] = ldir_y;
+                            T.sdist[p] = dist_y - 0.0001f;
+                            T.scontrib[p] = prev_thr * f_y * (w_sum / (f_a_y * (float)mcount));
+                        }
+                    } else {
+                        // one light sample (SimpleGuide.cu:410-419)
+                        const LightSample l = sample_light(T, position, rng);
+                        const float3 b = phong_bsdf(diffuse, m.specular, m.shininess, l.dir, refl);
+                        const float g = fmaxf(-dot3(l.dir, l.normal), 0.0f) * fabsf(dot3(l.dir, fn)) / (l.dist * l.dist);
+                        T.pending[p] = 1;
+                        T.sdir[p] = l.dir;
+                        T.sdist[p] = l.dist - 0.0001f;
+                        T.scontrib[p] = prev_thr * b * l.emission * g * l.inv_pdf;
+                    }
+                }
+            } else {
+                flags |= HF_COUNT_EMITTED;
+            }
+        } else if (m.type == MAT_GLASS) {
+            // dielectric (SimpleGuide.cu:424-491), shading normal = face normal
+            float3 rn;
+            float rri;
+            float ci = dot3(fn, in_dir);
+            if (ci < 0.0f) { rn = fn; rri = 1.0f / m.ref_index; ci = -ci; }
+            else { rn = f3(-fn.x, -fn.y, -fn.z); rri = m.ref_index; }
+            const float so2 = (1.0f - ci * ci) * (rri * rri);
+            const float f0 = ((1.0f - rri) / (1.0f + rri)) * ((1.0f - rri) / (1.0f + rri));
+            const float om = 1.0f - ci;
+            const float fres = f0 + (1.0f - f0) * (om * om * om * om * om);
+            const float3 rd = unit3(reflect3(in_dir, rn));
+            if (rnd1(rng) < fres || so2 > 1.0f) {
+                position = position + 0.0001f * rn;
+                direction = rd;
+                cosine = fabsf(ci);
+                bsdf_val = m.specular;
+                cur_thr = prev_thr * m.specular;
+            } else {
+                position = position - 0.0001f * rn;
+                const float si2 = fmaxf(1.0f - ci * ci, 0.0f);
+                const float co = sqrtf(1.0f - so2);
+                float3 rf;
+                if (si2 > 0.0f) {
+                    const float3 k = (in_dir + ci * rn) / sqrtf(si2);
+                    rf = unit3(sqrtf(so2) * k - co * rn);
+                } else {
+                    rf = in_dir;
+                }
+                direction = rf;
+                cosine = fabsf(dot3(rf, rn));
+                bsdf_val = f3(1.f, 1.f, 1.f);
+                cur_thr = prev_thr;
+            }
+            wo_pdf = fabsf(cosine);
+            bsdf_pdf = 0.0f;
+            flags |= HF_COUNT_EMITTED | HF_DELTA;
+        }
+        float3 rad = f3(0.f, 0.f, 0.f);
+        if (dot3(in_dir, fn) < 0.0f && count_emitted) rad = prev_thr * m.emission;
+        if (m.emission.x + m.emission.y + m.emission.z > 0.0f) flags |= HF_FINISH;
+        T.brad[p] = rad;
+        T.org[p] = position;
+        T.dir[p] = direction;
+        T.thr[p] = cur_thr;
+        T.hflags[p] = flags;
+        T.rng[p] = rng;
+        if (recording && d < kTV) {
+            T.v_pos[vi] = position;
+            T.v_dir[vi] = direction;
+            T.v_thr[vi] = cur_thr;
+            T.v_rad[vi] = f3(0.f, 0.f, 0.f);
+            T.v_bsdf[vi] = bsdf_val;
+            T.v_wopdf[vi] = wo_pdf;
+            T.v_cos[vi] = cosine;
+            T.v_flags[vi] = (uint8_t)(1u | ((flags & HF_DELTA) ? 2u : 0u));
+        }
+    }
+}
+
+// ------------------------------------------------------------------ connect
+// Shadow ray of the pending NEE/RIS sample, then the raygen bookkeeping of one bounce
+// (SimpleGuide.cu:85-114): radiance into earlier trace vertices, color, termination.
+__global__ void __launch_bounds__(kTB) k_connect(TracerDev T, int in) {
+    const uint32_t n = T.qcount[in];
+    const bool recording = (T.flags & RTPG_TRACE_FLAG_USE_TREE) && !(T.flags & RTPG_TRACE_FLAG_FINAL);
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+        const uint32_t q = base + threadIdx.x;
+        bool keep = false;
+        uint32_t p = 0;
+        if (q < n) {
+            p = T.queue[in][q];
+            float3 L = T.brad[p];
+            if (T.pending[p]) {
+                const float3 o = T.org[p], sd = T.sdir[p];
+                const Hit h = bvh_trace<true>(T.scene, o.x, o.y, o.z, sd.x, sd.y, sd.z, 0.0001f, T.sdist[p]);
+                if (h.prim == 0xffffffffu) L = L + T.scontrib[p];
+            }
+            const uint32_t d = T.depth[p];
+            if (recording) {
+                const uint32_t tvd = d < kTV ? d : kTV;
+                for (uint32_t i = 0; i < tvd; ++i) {
+                    const size_t vi = size_t(i) * T.npath + p;
+                    T.v_rad[vi] = T.v_rad[vi] + L;
+                }
+            }
+            T.col[p] = T.col[p] + L;
+            const float3 dr = T.dir[p], th = T.thr[p];
+            const bool bad = any_nan3(dr) || any_nan3(th) || any_nan3(L);
+            const bool done = bad || (T.hflags[p] & HF_FINISH) || d >= T.max_depth - 1;
+            if (!done) {
+                T.depth[p] = d + 1;
+                keep = true;
+            }
+        }
+        const unsigned sh = __ballot_sync(0xffffffffu, q < n && T.pending[p]);
+        if ((threadIdx.x & 31) == 0 && sh) atomicAdd(T.counters + 1, (unsigned long long)__popc(sh));
+        // warp-aggregated append to the next queue
+        const unsigned m = __ballot_sync(0xffffffffu, keep);
+        if (m) {
+            const int lane = threadIdx.x & 31;
+            uint32_t base_q = 0;
+            if (lane == __ffs(m) - 1) base_q = atomicAdd(T.qcount + (in ^ 1), (uint32_t)__popc(m));
+            base_q = __shfl_sync(0xffffffffu, base_q, __ffs(m) - 1);
+            if (keep) T.queue[in ^ 1][base_q + __popc(m & ((1u << lane) - 1u))] = p;
+        }
+    }
+}
+
+// ------------------------------------------------------------------ finish
+// Accumulate, write the seed back, commit trace vertices (TraceVertexT::Commit,
+// OPX7UtilsPathGuiding.h:830-866 -> DTreeWrapperT::Record :514-520 with stat-weight 1).
+__global__ void __launch_bounds__(kTB) k_finish(TracerDev T) {
+    const bool recording = (T.flags & RTPG_TRACE_FLAG_USE_TREE) && !(T.flags & RTPG_TRACE_FLAG_FINAL);
+    for (uint32_t base = blockIdx.x * blockDim.x; base < T.npath; base += gridDim.x * blockDim.x) {
+        const uint32_t p = base + threadIdx.x;
+        uint32_t nv = 0;
+        if (p < T.npath) {
+            const float3 c = T.col[p];
+            double* a = T.accum + 3 * size_t(p);
+            a[0] += (double)c.x;
+            a[1] += (double)c.y;
+            a[2] += (double)c.z;
+            T.seeds[p] = T.rng[p];
+            const uint32_t d = T.depth[p];
+            nv = recording ? (d < kTV ? d : kTV) : 0;
+        }
+        for (uint32_t i = 0; i < kTV; ++i) {  // warp-uniform loop for the aggregated atomics
+            unsigned long long k_w = ~0ull, k_s = ~0ull, v_w = 0, v_s = 0;
+            if (i < nv) {
+                const size_t vi = size_t(i) * T.npath + p;
+                const uint8_t vf = T.v_flags[vi];
+                const float3 rad = T.v_rad[vi], bv = T.v_bsdf[vi], th = T.v_thr[vi];
+                const float wo = T.v_wopdf[vi];
+                const bool ok_r = isfinite(rad.x) && rad.x >= 0.f && isfinite(rad.y) && rad.y >= 0.f &&
+                                  isfinite(rad.z) && rad.z >= 0.f;
+                const bool ok_b = isfinite(bv.x) && bv.x >= 0.f && isfinite(bv.y) && bv.y >= 0.f &&
+                                  isfinite(bv.z) && bv.z >= 0.f;
+                if ((vf & 1) && wo > 0.0f && ok_r && ok_b && !(vf & 2)) {
+                    float3 lr = f3(0.f, 0.f, 0.f);
+                    if (th.x * wo > 1e-4f) lr.x = rad.x / th.x;
+                    if (th.y * wo > 1e-4f) lr.y = rad.y / th.y;
+                    if (th.z * wo > 1e-4f) lr.z = rad.z / th.z;
+                    lr = lr * fabsf(T.v_cos[vi]);
+                    const float lavg = (lr.x + lr.y + lr.z) / 3.0f;
+                    const float3 pos = T.v_pos[vi], dr = T.v_dir[vi];
+                    const uint32_t dt = stree_lookup(T.tree.snode, T.tree.mn, T.tree.mx, pos.x, pos.y, pos.z);
+                    k_w = dt;
+                    v_w = to_fx(1.0f, T.tree.fx, T.tree.status);
+                    const float irr = __fdiv_rn(lavg, wo);
+                    if (isfinite(irr) && irr > 0.0f) {
+                        const float2 c = dir_to_canonical(dr.x, dr.y, dr.z);
+                        k_s = dtree_record_slot(T.tree.b_child, T.tree.b_off[dt], c.x, c.y);
+                        v_s = to_fx(irr, T.tree.fx, T.tree.status);
+                    }
+                }
+            }
+            warp_add_u64(k_w, v_w, T.tree.b_statw);
+            warp_add_u64(k_s, v_s, T.tree.b_sums);
+        }
+    }
+}
+
+__global__ void k_seed_init(uint32_t* seeds, uint32_t n, uint32_t seed) {
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x)
+        seeds[p] = pcg1d(pcg1d(p) ^ (seed * 0x9E3779B9u)) | 1u;
+}
+
+__global__ void k_image(const double* accum, uint32_t n, double inv, float* out) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < 3 * n; i += gridDim.x * blockDim.x)
+        out[i] = (float)(accum[i] * inv);
+}
+
+}  // namespace rtpg
+
+using namespace rtpg;
+
+struct rtpg_tracer {
+    TracerDev dev{};
+    rtpg_scene* scene = nullptr;
+    std::vector<void*> allocs;
+    std::vector<const float*> tex_ptr;
+    std::vector<uint2> tex_wh;
+    const float** d_tex = nullptr;
+    uint2* d_tex_wh = nullptr;
+    uint32_t seed = 1;
+    bool timing = false;
+    double t_ms[4] = {0, 0, 0, 0};  // raygen, extend, connect, finish
+    uint64_t t_launch[4] = {0, 0, 0, 0};
+    cudaEvent_t ev[8] = {};
+    uint64_t samples = 0;
+    uint64_t paths = 0;
+    struct Cached {
+        cudaGraphExec_t exec;
+        SDTreeDev tree;
+    };
+    std::map<uint32_t, Cached> graphs;  // keyed by flags; the tree view is compared on use
+    template <class T>
+    int alloc(T** p, size_t count) {
+        void* q = nullptr;
+        cudaError_t e = cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T));
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return fail(RTPG_ENOMEM, "cudaMalloc(%zu bytes) failed: %s", count * sizeof(T), cudaGetErrorString(e));
+        }
+        allocs.push_back(q);
+        *p = static_cast<T*>(q);
+        return RTPG_OK;
+    }
+    void drop_graphs() {
+        for (auto& kv : graphs) cudaGraphExecDestroy(kv.second.exec);
+        graphs.clear();
+    }
+    ~rtpg_tracer() {
+        drop_graphs();
+        for (auto& e : ev)
+            if (e) cudaEventDestroy(e);
+        for (void* p : allocs) cudaFree(p);
+    }
+};
+
+// One wave with CUDA events around every kernel group; synchronises and accumulates the
+// per-group device time (used to measure the kernels, outside the graph-replayed path).
+static int timed_wave(rtpg_tracer* h, cudaStream_t st) {
+    TracerDev& T = h->dev;
+    const int g = kSMs * 8;
+    for (auto& e : h->ev)
+        if (!e) RTPG_CUDA(cudaEventCreate(&e));
+    std::vector<cudaEvent_t> marks;
+    std::vector<int> kind;
+    cudaEventRecord(h->ev[0], st);
+    k_raygen<<<g, kTB, 0, st>>>(T);
+    cudaEventRecord(h->ev[1], st);
+    RTPG_CUDA(cudaEventSynchronize(h->ev[1]));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, h->ev[0], h->ev[1]);
+    h->t_ms[0] += ms;
+    h->t_launch[0] += 1;
+    for (uint32_t b = 0; b < T.max_depth; ++b) {
+        cudaEventRecord(h->ev[2], st);
+        k_extend<<<g, kTB, 0, st>>>(T, int(b & 1));
+        cudaEventRecord(h->ev[3], st);
+        k_connect<<<g, kTB, 0, st>>>(T, int(b & 1));
+        cudaEventRecord(h->ev[4], st);
+        RTPG_CUDA(cudaEventSynchronize(h->ev[4]));
+        cudaEventElapsedTime(&ms, h->ev[2], h->ev[3]);
+        h->t_ms[1] += ms;
+        cudaEventElapsedTime(&ms, h->ev[3], h->ev[4]);
+        h->t_ms[2] += ms;
+        h->t_launch[1] += 1;
+        h->t_launch[2] += 1;
+    }
+    cudaEventRecord(h->ev[5], st);
+    k_finish<<<g, kTB, 0, st>>>(T);
+    cudaEventRecord(h->ev[6], st);
+    RTPG_CUDA(cudaEventSynchronize(h->ev[6]));
+    cudaEventElapsedTime(&ms, h->ev[5], h->ev[6]);
+    h->t_ms[3] += ms;
+    h->t_launch[3] += 1;
+    RTPG_LAUNCH_CHECK();
+    return RTPG_OK;
+}
+
+static void launch_wave(rtpg_tracer* h, cudaStream_t st) {
+    TracerDev& T = h->dev;
+    const int g = kSMs * 8;
+    k_raygen<<<g, kTB, 0, st>>>(T);
+    for (uint32_t b = 0; b < T.max_depth; ++b) {
+        k_extend<<<g, kTB, 0, st>>>(T, int(b & 1));
+        k_connect<<<g, kTB, 0, st>>>(T, int(b & 1));
+    }
+    k_finish<<<g, kTB, 0, st>>>(T);
+}
+
+extern "C" {
+
+int rtpg_tracer_create(rtpg_scene* scene, const float* tri_vertices, const uint32_t* tri_material, const float* tri_uv,
+                       const rtpg_material* host_materials, uint32_t num_materials, const uint32_t* light_tris,
+                       const uint32_t* host_light_mesh_first, const uint32_t* host_light_mesh_count,
+                       uint32_t num_light_meshes, const rtpg_camera* host_camera, const rtpg_tracer_desc* host_desc,
+                       rtpg_tracer** out) {
+    if (!scene || !tri_vertices || !tri_material || !host_materials || !num_materials || !host_camera || !host_desc || !out)
+        return fail(RTPG_EINVAL, "rtpg_tracer_create: null argument");
+    if (num_light_meshes && (!light_tris || !host_light_mesh_first || !host_light_mesh_count))
+        return fail(RTPG_EINVAL, "rtpg_tracer_create: light arrays missing");
+    const rtpg_tracer_desc& D = *host_desc;
+    if (!D.width || !D.height || D.max_depth < 1 || D.max_depth > 64)
+        return fail(RTPG_EINVAL, "rtpg_tracer_create: bad image size or max_depth");
+    auto* h = new (std::nothrow) rtpg_tracer();
+    if (!h) return fail(RTPG_ENOMEM, "rtpg_tracer_create: out of host memory");
+    h->scene = scene;
+    TracerDev& T = h->dev;
+    T.scene = scene_device_view(scene);
+    T.tri_v = tri_vertices;
+    T.tri_mat = tri_material;
+    T.tri_uv = tri_uv;
+    T.width = D.width;
+    T.height = D.height;
+    T.npath = D.width * D.height;
+    T.max_depth = D.max_depth;
+    T.num_candidates = D.num_candidates ? D.num_candidates : 32;
+    T.bg = make_float3(D.background[0], D.background[1], D.background[2]);
+    const rtpg_camera& c = *host_camera;
+    T.eye = make_float3(c.eye[0], c.eye[1], c.eye[2]);
+    T.cu = make_float3(c.u[0], c.u[1], c.u[2]);
+    T.cv = make_float3(c.v[0], c.v[1], c.v[2]);
+    T.cw = make_float3(c.w[0], c.w[1], c.w[2]);
+    h->seed = D.seed ? D.seed : 1;
+    const size_t P = T.npath;
+    Material* mats = nullptr;
+    uint2* lmesh = nullptr;
+    float3* lemit = nullptr;
+    int r;
+    if ((r = h->alloc(&mats, num_materials)) || (r = h->alloc(&lmesh, std::max(num_light_meshes, 1u))) ||
+        (r = h->alloc(&lemit, std::max(num_light_meshes, 1u))) || (r = h->alloc(&T.org, P)) ||
+        (r = h->alloc(&T.dir, P)) || (r = h->alloc(&T.thr, P)) || (r = h->alloc(&T.col, P)) ||
+        (r = h->alloc(&T.brad, P)) || (r = h->alloc(&T.sdir, P)) || (r = h->alloc(&T.scontrib, P)) ||
+        (r = h->alloc(&T.sdist, P)) || (r = h->alloc(&T.rng, P)) || (r = h->alloc(&T.depth, P)) ||
+        (r = h->alloc(&T.hflags, P)) || (r = h->alloc(&T.pending, P)) || (r = h->alloc(&T.queue[0], P)) ||
+        (r = h->alloc(&T.queue[1], P)) || (r = h->alloc(&T.qcount, 2)) || (r = h->alloc(&T.v_pos, P * kTV)) ||
+        (r = h->alloc(&T.v_dir, P * kTV)) || (r = h->alloc(&T.v_thr, P * kTV)) || (r = h->alloc(&T.v_rad, P * kTV)) ||
+        (r = h->alloc(&T.v_bsdf, P * kTV)) || (r = h->alloc(&T.v_wopdf, P * kTV)) ||
+        (r = h->alloc(&T.v_cos, P * kTV)) || (r = h->alloc(&T.v_flags, P * kTV)) || (r = h->alloc(&T.seeds, P)) ||
+        (r = h->alloc(&T.accum, 3 * P)) || (r = h->alloc(&T.status, 1)) || (r = h->alloc(&T.counters, 2)) || (r = h->alloc(&h->d_tex, 64)) ||
+        (r = h->alloc(&h->d_tex_wh, 64))) {
+        delete h;
+        return r;
+    }
+    std::vector<Material> hm(num_materials);
+    std::vector<float3> he(std::max(num_light_meshes, 1u));
+    for (uint32_t i = 0; i < num_materials; ++i) {
+        const rtpg_material& s = host_materials[i];
+        Material& m = hm[i];
+        m.diffuse = make_float3(s.diffuse[0], s.diffuse[1], s.diffuse[2]);
+        m.specular = make_float3(s.specular[0], s.specular[1], s.specular[2]);
+        m.emission = make_float3(s.emission[0], s.emission[1], s.emission[2]);
+        m.shininess = s.shininess;
+        m.ref_index = s.ref_index;
+        m.type = s.type;
+        m.tex = s.diffuse_texture;
+        m.pad[0] = m.pad[1] = m.pad[2] = 0;
+    }
+    std::vector<uint2> hl(std::max(num_light_meshes, 1u), make_uint2(0, 1));
+    for (uint32_t i = 0; i < num_light_meshes; ++i) {
+        hl[i] = make_uint2(host_light_mesh_first[i], host_light_mesh_count[i]);
+        if (!host_light_mesh_count[i]) {
+            delete h;
+            return fail(RTPG_EINVAL, "rtpg_tracer_create: empty light mesh %u", i);
+        }
+        he[i] = make_float3(host_desc->light_emission ? host_desc->light_emission[3 * i] : 0.f,
+                            host_desc->light_emission ? host_desc->light_emission[3 * i + 1] : 0.f,
+                            host_desc->light_emission ? host_desc->light_emission[3 * i + 2] : 0.f);
+    }
+    cudaError_t e;
+    if ((e = cudaMemcpy(mats, hm.data(), sizeof(Material) * num_materials, cudaMemcpyHostToDevice)) ||
+        (e = cudaMemcpy(lmesh, hl.data(), sizeof(uint2) * hl.size(), cudaMemcpyHostToDevice)) ||
+        (e = cudaMemcpy(lemit, he.data(), sizeof(float3) * he.size(), cudaMemcpyHostToDevice))) {
+        delete h;
+        return fail(RTPG_ECUDA, "rtpg_tracer_create: %s", cudaGetErrorString(e));
+    }
+    T.mats = mats;
+    T.light_mesh = lmesh;
+    T.light_emit = lemit;
+    T.light_tris = light_tris;
+    T.light_count = num_light_meshes;
+    T.tex = h->d_tex;
+    T.tex_wh = h->d_tex_wh;
+    *out = h;
+    return rtpg_tracer_clear(h, nullptr);
+}
+
+int rtpg_tracer_destroy(rtpg_tracer* h) {
+    if (!h) return fail(RTPG_EINVAL, "rtpg_tracer_destroy: null handle");
+    delete h;
+    return RTPG_OK;
+}
+
+int rtpg_tracer_set_texture(rtpg_tracer* h, uint32_t index, uint32_t width, uint32_t height, const float* rgb) {
+    if (!h || !rgb || !width || !height || index >= 64) return fail(RTPG_EINVAL, "rtpg_tracer_set_texture: bad arguments");
+    if (h->tex_ptr.size() <= index) {
+        h->tex_ptr.resize(index + 1, nullptr);
+        h->tex_wh.resize(index + 1, make_uint2(0, 0));
+    }
+    h->tex_ptr[index] = rgb;
+    h->tex_wh[index] = make_uint2(width, height);
+    RTPG_CUDA(cudaMemcpy(h->d_tex, h->tex_ptr.data(), sizeof(float*) * h->tex_ptr.size(), cudaMemcpyHostToDevice));
+    RTPG_CUDA(cudaMemcpy(h->d_tex_wh, h->tex_wh.data(), sizeof(uint2) * h->tex_wh.size(), cudaMemcpyHostToDevice));
+    return RTPG_OK;
+}
+
+// Zero the accumulation and reseed every pixel's Xorshift32 stream from `seed` (the
+// application reseeds from the host: RTLibExtOPX7TestApplication.cpp:2293-2299).
+int rtpg_tracer_clear(rtpg_tracer* h, void* stream) {
+    if (!h) return fail(RTPG_EINVAL, "rtpg_tracer_clear: null handle");
+    cudaStream_t st = as_stream(stream);
+    RTPG_CUDA(cudaMemsetAsync(h->dev.accum, 0, sizeof(double) * 3 * h->dev.npath, st));
+    RTPG_CUDA(cudaMemsetAsync(h->dev.status, 0, 4, st));
+    RTPG_CUDA(cudaMemsetAsync(h->dev.counters, 0, 16, st));
+    k_seed_init<<<grid_for(h->dev.npath, 256, 4), 256, 0, st>>>(h->dev.seeds, h->dev.npath, h->seed);
+    RTPG_LAUNCH_CHECK();
+    h->samples = 0;
+    return RTPG_OK;
+}
+
+int rtpg_tracer_set_seed(rtpg_tracer* h, uint32_t seed) {
+    if (!h) return fail(RTPG_EINVAL, "rtpg_tracer_set_seed: null handle");
+    h->seed = seed ? seed : 1;
+    return RTPG_OK;
+}
+
+// One launch of `spp` samples per pixel with the given RTPG_TRACE_FLAG_* (PARAM_FLAG_*,
+// SimpleKernel.h:145-154).  tree may be NULL when RTPG_TRACE_FLAG_USE_TREE is not set.
+int rtpg_tracer_render(rtpg_tracer* h, uint32_t spp, uint32_t flags, rtpg_sdtree* tree, void* stream) {
+    if (!h) return fail(RTPG_EINVAL, "rtpg_tracer_render: null handle");
+    if ((flags & RTPG_TRACE_FLAG_USE_TREE) && !tree) return fail(RTPG_EINVAL, "rtpg_tracer_render: USE_TREE without a tree");
+    if ((flags & RTPG_TRACE_FLAG_RIS) && !(flags & RTPG_TRACE_FLAG_NEE))
+        return fail(RTPG_EINVAL, "rtpg_tracer_render: RIS requires NEE");
+    cudaStream_t st = as_stream(stream);
+    h->dev.flags = flags;
+    if (tree) h->dev.tree = sdtree_device_view(tree);
+    if (h->timing) {
+        if (!tree) memset(&h->dev.tree, 0, sizeof(SDTreeDev));
+        for (uint32_t s = 0; s < spp; ++s) {
+            int r = timed_wave(h, st);
+            if (r) return r;
+        }
+        h->samples += spp;
+        h->paths += uint64_t(spp) * h->dev.npath;
+        return RTPG_OK;
+    }
+    // a captured wave bakes in the kernel arguments, so it is reused only for the same flags
+    // and an identical tree view (same device arrays)
+    if (!tree) memset(&h->dev.tree, 0, sizeof(SDTreeDev));
+    auto it = h->graphs.find(flags);
+    cudaGraphExec_t exec = nullptr;
+    if (it != h->graphs.end() && memcmp(&it->second.tree, &h->dev.tree, sizeof(SDTreeDev)) == 0) {
+        exec = it->second.exec;
+    } else {
+        if (it != h->graphs.end()) {
+            cudaGraphExecDestroy(it->second.exec);
+            h->graphs.erase(it);
+        }
+        cudaStream_t cs;
+        RTPG_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            launch_wave(h, cs);
+            e = cudaStreamEndCapture(cs, &g);
+        }
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, g, 0);
+        if (g) cudaGraphDestroy(g);
+        cudaStreamDestroy(cs);
+        if (e != cudaSuccess) return fail(RTPG_ECUDA, "rtpg_tracer_render: graph capture failed: %s", cudaGetErrorString(e));
+        h->graphs[flags] = {exec, h->dev.tree};
+    }
+    for (uint32_t s = 0; s < spp; ++s) RTPG_CUDA(cudaGraphLaunch(exec, st));
+    h->samples += spp;
+    h->paths += uint64_t(spp) * h->dev.npath;
+    return RTPG_OK;
+}
+
+// Mean radiance per pixel (accumulation / samples), RGB float, row-major, y = 0 first.
+int rtpg_tracer_image(rtpg_tracer* h, float* out_rgb, void* stream) {
+    if (!h || !out_rgb) return fail(RTPG_EINVAL, "rtpg_tracer_image: null argument");
+    const double inv = h->samples ? 1.0 / (double)h->samples : 0.0;
+    k_image<<<grid_for(3ull * h->dev.npath, 256, 4), 256, 0, as_stream(stream)>>>(h->dev.accum, h->dev.npath, inv, out_rgb);
+    RTPG_LAUNCH_CHECK();
+    return RTPG_OK;
+}
+
+// Device pointer to the FP64 accumulation buffer (3 doubles per pixel) and the sample count.
+int rtpg_tracer_accumulation(rtpg_tracer* h, const double** dev_accum, uint64_t* host_samples) {
+    if (!h) return fail(RTPG_EINVAL, "rtpg_tracer_accumulation: null handle");
+    if (dev_accum) *dev_accum = h->dev.accum;
+    if (host_samples) *host_samples = h->samples;
+    return RTPG_OK;
+}
+
+// Guided rendering driven by the pass controller, as TracePipeline does for the PG tracers
+// (RTLibExtOPX7TestApplication.cpp:2155-2230, flags by state as in GetParams,
+// RTLibExtOPX7TestApplication.h:399-424): per launch BegTrace, render samples_per_launch
+// with USE_TREE (+BUILD in RECORD_AND_SAMPLE, +BUILD|FINAL in SAMPLE), EndTrace.
+int rtpg_tracer_render_guided(rtpg_tracer* h, rtpg_sdtree* tree, rtpg_controller* ctrl, uint32_t base_flags,
+                              uint32_t samples_per_launch, uint32_t max_launches, void* stream) {
+    if (!h || !tree || !ctrl) return fail(RTPG_EINVAL, "rtpg_tracer_render_guided: null argument");
+    int r;
+    for (uint32_t k = 0; k < max_launches; ++k) {
+        if ((r = rtpg_controller_begin(ctrl, stream))) return r;
+        int32_t state, executing;
+        uint32_t it, tmp;
+        rtpg_controller_get(ctrl, &state, &it, &tmp, &executing);
+        if (!executing) break;
+        uint32_t flags = (base_flags & (RTPG_TRACE_FLAG_NEE | RTPG_TRACE_FLAG_RIS)) | RTPG_TRACE_FLAG_USE_TREE;
+        if (state == RTPG_TRACE_RECORD_AND_SAMPLE) flags |= RTPG_TRACE_FLAG_BUILD;
+        if (state == RTPG_TRACE_SAMPLE) flags |= RTPG_TRACE_FLAG_BUILD | RTPG_TRACE_FLAG_FINAL;
+        if ((r = rtpg_tracer_render(h, samples_per_launch, flags, tree, stream))) return r;
+        if ((r = rtpg_controller_end(ctrl, stream))) return r;
+    }
+    return RTPG_OK;
+}
+
+int rtpg_tracer_counters(rtpg_tracer* h, uint64_t* host_path_bounces, uint64_t* host_shadow_rays, void* stream) {
+    if (!h) return fail(RTPG_EINVAL, "rtpg_tracer_counters: null handle");
+    unsigned long long c[2];
+    RTPG_CUDA(cudaMemcpyAsync(c, h->dev.counters, sizeof(c), cudaMemcpyDeviceToHost, as_stream(stream)));
+    RTPG_CUDA(cudaStreamSynchronize(as_stream(stream)));
+    if (host_path_bounces) *host_path_bounces = c[0];
+    if (host_shadow_rays) *host_shadow_rays = c[1];
+    return RTPG_OK;
+}
+
+int rtpg_tracer_set_timing(rtpg_tracer* h, int enable) {
+    if (!h) return fail(RTPG_EINVAL, "rtpg_tracer_set_timing: null handle");
+    h->timing = enable != 0;
+    for (int k = 0; k < 4; ++k) {
+        h->t_ms[k] = 0.0;
+        h->t_launch[k] = 0;
+    }
+    return RTPG_OK;
+}
+
+int rtpg_tracer_timings(rtpg_tracer* h, double* host_ms, uint64_t* host_launches) {
+    if (!h || !host_ms) return fail(RTPG_EINVAL, "rtpg_tracer_timings: null argument");
+    for (int k = 0; k < 4; ++k) {
+        host_ms[k] = h->t_ms[k];
+        if (host_launches) host_launches[k] = h->t_launch[k];
+    }
+    return RTPG_OK;
+}
+
+int rtpg_tracer_stats(rtpg_tracer* h, uint64_t* host_samples, uint64_t* host_paths) {
+    if (!h) return fail(RTPG_EINVAL, "rtpg_tracer_stats: null handle");
+    if (host_samples) *host_samples = h->samples;
+    if (host_paths) *host_paths = h->paths;
+    return RTPG_OK;
+}
+
+}  // extern "C"

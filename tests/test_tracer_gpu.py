@@ -1,0 +1,125 @@
+"""Integrator parity: the wavefront tracer (C ABI) against the CPU restatement of RTLib's
+guided integrator on the same per-pixel Xorshift32 streams, and the BVH hit queries against
+a brute-force intersection.
+
+The GPU and the CPU draw the same random numbers in the same order, so most paths are
+identical; a path separates only where float differences of sin/cos/pow/atan2 between CUDA
+and libm flip a decision, which the image tolerances below absorb."""
+import numpy as np
+import pytest
+
+from rtlib_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+
+def _t(a, dev):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+
+
+def _mt(tri_v, o, d, tmin, tmax):
+    """Brute-force closest hit in float32 (numpy), the same formula as the device."""
+    v = tri_v.reshape(-1, 3, 3).astype(np.float32)
+    v0, e1, e2 = v[:, 0], v[:, 1] - v[:, 0], v[:, 2] - v[:, 0]
+    n = o.shape[0]
+    best_t = np.full(n, np.inf, np.float32)
+    best_p = np.full(n, 0xFFFFFFFF, np.uint32)
+    for i in range(n):
+        p = np.cross(d[i], e2)
+        det = np.einsum("ij,ij->i", e1, p)
+        with np.errstate(all="ignore"):
+            inv = np.float32(1) / det
+            s = o[i] - v0
+            u = np.einsum("ij,ij->i", s, p) * inv
+            q = np.cross(s, e1)
+            w = (q @ d[i]) * inv
+            t = np.einsum("ij,ij->i", e2, q) * inv
+        ok = (np.abs(det) >= 1e-20) & (u >= 0) & (u <= 1) & (w >= 0) & (u + w <= 1) & (t > tmin) & (t < tmax)
+        if ok.any():
+            k = np.argmin(np.where(ok, t, np.inf))
+            best_t[i], best_p[i] = t[k], k
+    return best_t, best_p
+
+
+def test_bvh_closest_and_any_hit(cuda):
+    import torch
+    from rtlib_b200.tracer import Scene
+    rng = np.random.default_rng(0)
+    c = rng.random((3000, 3)).astype(np.float32) * 4
+    tri = (c[:, None, :] + rng.normal(0, 0.15, (3000, 3, 3))).astype(np.float32).reshape(-1, 9)
+    tri = np.concatenate([tri, scenes.cornell_box()["tri_v"]])
+    sc = Scene(_t(tri, cuda))
+    n = 2048
+    o = (rng.random((n, 3)) * 5 - 0.5).astype(np.float32)
+    d = rng.normal(size=(n, 3)).astype(np.float32)
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    t = torch.empty(n, device=cuda)
+    pr = torch.empty(n, dtype=torch.int32, device=cuda)
+    sc.intersect(_t(o, cuda), _t(d, cuda), out_t=t, out_prim=pr)
+    anyh = torch.empty(n, dtype=torch.int32, device=cuda)
+    tmax = _t(np.full(n, 1.5, np.float32), cuda)
+    sc.intersect(_t(o, cuda), _t(d, cuda), tmax=tmax, any_hit=True, out_prim=anyh)
+    torch.cuda.synchronize()
+    bt, bp = _mt(tri, o, d, 0.0, 1e20)
+    gp = pr.cpu().numpy().view(np.uint32)
+    gt = t.cpu().numpy()
+    assert (gp == bp).mean() > 0.999
+    same = gp == bp
+    np.testing.assert_allclose(gt[same & (bp != 0xFFFFFFFF)], bt[same & (bp != 0xFFFFFFFF)], rtol=1e-5)
+    ga = anyh.cpu().numpy().view(np.uint32) != 0xFFFFFFFF
+    assert ((bt < 1.5) == ga).mean() > 0.999
+
+
+def _gpu_render(dev, sc, w, h, spp, flags, seed=1, tree=None, max_depth=8):
+    from rtlib_b200.tracer import Tracer
+    tr = Tracer(sc, dev, max_depth=max_depth, seed=seed, width=w, height=h)
+    tr.render(spp, flags, tree)
+    return tr.image().cpu().numpy(), tr
+
+
+def _compare(gimg, cimg, rel_mse=2e-3, frac=0.97):
+    denom = np.maximum(np.abs(cimg), 1e-2)
+    rel = np.abs(gimg - cimg) / denom
+    close = (rel < 1e-3).all(axis=2).mean()
+    rmse = np.mean((gimg - cimg) ** 2) / (np.mean(cimg ** 2) + 1e-12)
+    assert rmse < rel_mse, rmse
+    assert close > frac, close
+
+
+@pytest.mark.parametrize("flags", [0, 1, 3])
+def test_render_matches_oracle(cuda, oracle, flags):
+    """Unguided DEF (0), NEE (1), NEE + RIS (3) on the Cornell box, 64 x 64, 8 spp."""
+    from oracle.oracle import OracleRenderer
+    sc = scenes.cornell_box(64, 64)
+    gimg, _ = _gpu_render(cuda, sc, 64, 64, 8, flags)
+    r = OracleRenderer(oracle, sc, width=64, height=64)
+    r.render(8, flags)
+    _compare(gimg, r.image())
+
+
+def test_guided_render_matches_oracle(cuda, oracle):
+    """The controller-driven PGNEE schedule (1, 2, 4, ... spp passes, record -> build ->
+    refine between passes, guide fraction 0.5) on GPU and CPU."""
+    from oracle.oracle import OracleRenderer
+    from rtlib_b200.sdtree import SDTree, SDTreeController
+    from rtlib_b200.tracer import FLAG_NEE, Tracer
+    w = h = 48
+    budget = 31
+    sc = scenes.cornell_box(w, h)
+    mn, mx = (-0.005,) * 3, (1.005,) * 3
+    tree = SDTree(mn, mx, fraction=0.5)
+    ctrl = SDTreeController(tree, budget, iteration_for_built=0, ratio_for_budget=1.0, samples_per_launch=1)
+    tr = Tracer(sc, cuda, max_depth=8, width=w, height=h)
+    ctrl.start()
+    tr.render_guided(tree, ctrl, FLAG_NEE, samples_per_launch=1)
+    gimg = tr.image().cpu().numpy()
+    # the same schedule on the CPU (RTSTreeControllerT::BegTrace / EndTrace restated)
+    ot = oracle.sdtree(mn, mx)
+    r = OracleRenderer(oracle, sc, width=w, height=h, fraction=0.5)
+    r.render_guided(ot, budget, ratio_for_budget=1.0)
+    assert tr.stats()["samples"] == r.samples
+    _compare(gimg, r.image(), rel_mse=5e-3, frac=0.9)
+    st = tree.stats()
+    assert st["stree_nodes"] == ot.num_stree_nodes()
+    assert tree.status() == 0
