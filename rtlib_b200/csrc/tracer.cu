@@ -48,6 +48,7 @@ struct TracerDev {
     const uint2* light_mesh;  // (first, count) into light_tris
     const float3* light_emit;
     uint32_t light_count;
+    uint32_t num_materials, num_light_tris;
     float3 eye, cu, cv, cw, bg;
     uint32_t width, height, npath, max_depth, num_candidates, flags;
     // path state
@@ -105,7 +106,7 @@ struct LightSample {
 __device__ __forceinline__ LightSample sample_light(const TracerDev& T, float3 p_in, uint32_t& rng) {
     const uint32_t mi = xs32_next(rng) % T.light_count;
     const uint2 mesh = T.light_mesh[mi];
-    const uint32_t ti = T.light_tris[mesh.x + xs32_next(rng) % mesh.y];
+    const uint32_t ti = min(T.light_tris[mesh.x + xs32_next(rng) % mesh.y], T.scene.ntris - 1);
     const float* tv = T.tri_v + 9 * size_t(ti);
     const float3 v0 = f3(tv[0], tv[1], tv[2]), v1 = f3(tv[3], tv[4], tv[5]), v2 = f3(tv[6], tv[7], tv[8]);
     const float3 nf = cross3(v1 - v0, v2 - v0);
@@ -155,7 +156,8 @@ __global__ void __launch_bounds__(kTB) k_extend(TracerDev T, int in) {
         const float3 v0 = f3(tv[0], tv[1], tv[2]), v1 = f3(tv[3], tv[4], tv[5]), v2 = f3(tv[6], tv[7], tv[8]);
         const float3 fn = unit3(cross3(v1 - v0, v2 - v0));
         float3 position = org + h.t * in_dir;
-        const Material m = T.mats[T.tri_mat[h.prim]];
+        const uint32_t mi = T.tri_mat[h.prim];
+        const Material m = T.mats[mi < T.num_materials ? mi : T.num_materials - 1];
         float3 diffuse = m.diffuse;
         if (m.tex >= 0 && T.tri_uv) {
             const float* uv = T.tri_uv + 6 * size_t(h.prim);
@@ -432,6 +434,7 @@ struct rtpg_tracer {
     rtpg_scene* scene = nullptr;
     std::vector<void*> allocs;
     std::vector<const float*> tex_ptr;
+    std::vector<int32_t> mat_tex;  // texture index of every material (host copy for checks)
     std::vector<uint2> tex_wh;
     const float** d_tex = nullptr;
     uint2* d_tex_wh = nullptr;
@@ -611,6 +614,8 @@ int rtpg_tracer_create(rtpg_scene* scene, const float* tri_vertices, const uint3
         return fail(RTPG_ECUDA, "rtpg_tracer_create: %s", cudaGetErrorString(e));
     }
     T.mats = mats;
+    T.num_materials = num_materials;
+    for (uint32_t i = 0; i < num_materials; ++i) h->mat_tex.push_back(host_materials[i].diffuse_texture);
     T.light_mesh = lmesh;
     T.light_emit = lemit;
     T.light_tris = light_tris;
@@ -667,6 +672,10 @@ int rtpg_tracer_render(rtpg_tracer* h, uint32_t spp, uint32_t flags, rtpg_sdtree
     if ((flags & RTPG_TRACE_FLAG_USE_TREE) && !tree) return fail(RTPG_EINVAL, "rtpg_tracer_render: USE_TREE without a tree");
     if ((flags & RTPG_TRACE_FLAG_RIS) && !(flags & RTPG_TRACE_FLAG_NEE))
         return fail(RTPG_EINVAL, "rtpg_tracer_render: RIS requires NEE");
+    for (int32_t t : h->mat_tex)
+        if (t >= 0 && (size_t(t) >= h->tex_ptr.size() || !h->tex_ptr[t]))
+            return fail(RTPG_EINVAL, "rtpg_tracer_render: material texture %d was never set", t);
+    if (h->dev.scene.ntris == 0) return fail(RTPG_EINVAL, "rtpg_tracer_render: empty scene");
     cudaStream_t st = as_stream(stream);
     h->dev.flags = flags;
     if (tree) h->dev.tree = sdtree_device_view(tree);
