@@ -305,6 +305,11 @@ C_AABB = ((-0.005,) * 3, (1.005,) * 3)  # world AABB padded by 0.005 as the appl
 EXTEND_BYTES = 140
 
 
+def set_budget(b):
+    global C_BUDGET
+    C_BUDGET = int(b)
+
+
 def bench_cornell_ours(args, rank, world):
     import torch
     from rtlib_b200 import scenes
@@ -461,7 +466,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="cornell", choices=["cornell", "sdtree"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--budget", type=int, default=C_BUDGET,
+    ap.add_argument("--budget", type=int, default=2047,
                     help="cornell: total spp of the pass schedule (2047 = passes 1..1024); smaller values "
                          "give the short case used for profiling")
     args = ap.parse_args()
@@ -469,8 +474,7 @@ def main():
     rank = _env_int("RANK", 0)
     world = _env_int("WORLD_SIZE", 1)
     cornell = args.workload == "cornell"
-    global C_BUDGET
-    C_BUDGET = args.budget
+    set_budget(args.budget)
     if cornell:
         cfg = {"workload": f"cornell-guided: 512x512, {C_BUDGET} spp budget in doubling passes, max depth 8, NEE, "
                            "SD-tree guiding fraction 0.5", "width": C_W, "height": C_H, "spp": C_BUDGET + 1,

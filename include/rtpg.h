@@ -292,6 +292,9 @@ int rtpg_tracer_counters(rtpg_tracer* h, uint64_t* host_path_bounces, uint64_t* 
  * device milliseconds of raygen / extend / connect / finish (and their launch counts) are
  * read with rtpg_tracer_timings.  Enabling or disabling resets the sums. */
 int rtpg_tracer_set_timing(rtpg_tracer* h, int enable);
+/* Debug view: the final bounce index of every path of the last wave (uint32 per pixel,
+ * device); with recording on, a path commits min(depth, 10) trace vertices. */
+int rtpg_tracer_path_depths(rtpg_tracer* h, uint32_t* out_depth, void* stream);
 int rtpg_tracer_timings(rtpg_tracer* h, double* host_ms4, uint64_t* host_launches4);
 
 #ifdef __cplusplus

@@ -883,6 +883,14 @@ static void commit_vertex(OSDTree* t, const OVert* v) {
 
 /* One sample per pixel for pixels [p0, p1) of the frame; accum += color (double), seeds
  * updated.  tree: an or_sdtree handle or NULL.  Returns the number of paths traced. */
+static uint32_t* g_depth_out = NULL;
+static int64_t g_log_pixel = -1;
+static float* g_log = NULL; /* per bounce: org xyz, dir xyz, t, prim (as float bits) */
+/* log the rays of one pixel (debugging aid) */
+void or_render_log_pixel(int64_t pixel, float* out) { g_log_pixel = pixel; g_log = out; }
+/* where or_render writes the final bounce index of every path (NULL = nowhere) */
+void or_render_depth_output(uint32_t* out) { g_depth_out = out; }
+
 int64_t or_render(const OScene* s, uint32_t flags, void* tree_h, uint32_t p0, uint32_t p1, uint32_t* seeds,
                   double* accum) {
     OSDTree* tree = (OSDTree*)tree_h;
@@ -910,6 +918,13 @@ int64_t or_render(const OScene* s, uint32_t flags, void* tree_h, uint32_t p0, ui
             uint32_t hflags = 0;
             V3 position = org;
             int hit = o_trace(s, org, dir, 0.0001f, 1.0e20f, 0, &t, &prim, &hu, &hv);
+            if ((int64_t)p == g_log_pixel && g_log && depth < 16) {
+                float* lg = g_log + 8 * depth;
+                lg[0] = org.x; lg[1] = org.y; lg[2] = org.z; lg[3] = dir.x; lg[4] = dir.y; lg[5] = dir.z;
+                lg[6] = hit ? t : -1.0f;
+                uint32_t pb = hit ? prim : 0xffffffffu;
+                memcpy(&lg[7], &pb, 4);
+            }
             if (!hit) {
                 L = vmul(thr, v3(s->bg[0], s->bg[1], s->bg[2]));
                 hflags = 16u;
@@ -1066,6 +1081,7 @@ int64_t or_render(const OScene* s, uint32_t flags, void* tree_h, uint32_t p0, ui
             uint32_t nv = depth < O_KTV ? depth : O_KTV;
             for (uint32_t i = 0; i < nv; ++i) commit_vertex(tree, &verts[i]);
         }
+        if (g_depth_out) g_depth_out[p] = depth;
         accum[3 * (size_t)p] += col.x;
         accum[3 * (size_t)p + 1] += col.y;
         accum[3 * (size_t)p + 2] += col.z;

@@ -81,6 +81,7 @@ _SIGS = {
     "rtpg_tracer_stats": [P, P, P],
     "rtpg_tracer_set_timing": [P, C.c_int],
     "rtpg_tracer_counters": [P, P, P, P],
+    "rtpg_tracer_path_depths": [P, P, P],
     "rtpg_tracer_timings": [P, P, P],
 }
 _RESTYPE = {"rtpg_last_error": C.c_char_p}

@@ -771,6 +771,15 @@ int rtpg_tracer_counters(rtpg_tracer* h, uint64_t* host_path_bounces, uint64_t* 
     return RTPG_OK;
 }
 
+// Debug view of the last wave: final bounce index of every path and the number of trace
+// vertices it committed or would commit (n = min(depth, 10) when recording).
+int rtpg_tracer_path_depths(rtpg_tracer* h, uint32_t* out_depth, void* stream) {
+    if (!h || !out_depth) return fail(RTPG_EINVAL, "rtpg_tracer_path_depths: null argument");
+    RTPG_CUDA(cudaMemcpyAsync(out_depth, h->dev.depth, sizeof(uint32_t) * h->dev.npath, cudaMemcpyDeviceToDevice,
+                              as_stream(stream)));
+    return RTPG_OK;
+}
+
 int rtpg_tracer_set_timing(rtpg_tracer* h, int enable) {
     if (!h) return fail(RTPG_EINVAL, "rtpg_tracer_set_timing: null handle");
     h->timing = enable != 0;

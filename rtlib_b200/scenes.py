@@ -90,8 +90,10 @@ def cornell_box(width=512, height=512, light_grid=1, back_texture=False):
     b.quad((0, 0, 0), (1, 0, 0), (0, 1, 0), BK)     # back wall z=0, normal +z
     b.quad((0, 0, 0), (0, 1, 0), (0, 0, 1), R)      # left wall x=0, normal +x
     b.quad((1, 0, 0), (0, 0, 1), (0, 1, 0), G)      # right wall x=1, normal -x
-    b.box((0.33, 0.15, 0.62), (0.3, 0.3, 0.3), -18.0, W)
-    b.box((0.66, 0.3, 0.36), (0.3, 0.6, 0.3), 18.0, W)
+    # the boxes stand 1 mm above the floor: a bottom face coplanar with the floor would make
+    # the closest hit a tie between two triangles with opposite normals
+    b.box((0.33, 0.151, 0.62), (0.3, 0.3, 0.3), -18.0, W)
+    b.box((0.66, 0.301, 0.36), (0.3, 0.6, 0.3), 18.0, W)
     n_geom = len(b.tris)
     light_first, light_count, light_emit = [], [], []
     s = 0.25 / light_grid

@@ -139,6 +139,12 @@ class Tracer:
         call("rtpg_tracer_counters", self.h, C.byref(a), C.byref(b), stream_ptr(stream))
         return {"path_bounces": a.value, "shadow_rays": b.value}
 
+    def path_depths(self, stream=None):
+        import torch
+        out = torch.empty((self.height, self.width), dtype=torch.int32, device=self.device)
+        call("rtpg_tracer_path_depths", self.h, ptr(out), stream_ptr(stream))
+        return out
+
     def set_timing(self, enable):
         call("rtpg_tracer_set_timing", self.h, int(bool(enable)))
 
