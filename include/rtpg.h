@@ -175,6 +175,23 @@ int rtpg_hashgrid_export(rtpg_hashgrid* h, int previous, uint64_t* host_table, v
 int rtpg_hashgrid_status(rtpg_hashgrid* h, uint32_t* host_status, int clear, void* stream);
 /* Device pointers of the two tables (uint64 keys), for kernels that probe them directly. */
 int rtpg_hashgrid_device_view(rtpg_hashgrid* h, void** dev_current, void** dev_previous);
+/* Allocation-free batch insert.  No counterpart in the reference: RTLib only inserts from
+ * inside its OptiX programs.  It is for callers that cannot allocate device memory -- a host
+ * application that owns every allocation under a fixed budget, code that enqueues work while
+ * another component captures the stream into a CUDA graph (where cudaMalloc is not allowed),
+ * or a real-time loop that must not block in the allocator.  Same slots and table contents as
+ * rtpg_hashgrid_insert on a handle with the same grid: the caller passes the grid parameters,
+ * the current table (num_slots uint64 keys, device, in/out, zero = empty), an optional device
+ * status word (RTPG_STATUS_HASH_FULL; NULL = not reported), and the points and out_slot.
+ * At most 65536 points per call (RTPG_ECAPACITY beyond).  The sort scratch is one
+ * file-scope device array of about 7.8 MB that every GPU loading the library reserves until
+ * the process exits; the first call on a device looks up its address (make that first call
+ * before any stream capture).  All calls share that array, so calls that overlap on the GPU
+ * (different streams, or different host threads on one device) race and must be ordered by
+ * the caller; each call overwrites the scratch it reads, so nothing carries over. */
+int rtpg_hashgrid_insert_noalloc(const float host_aabb_min[3], const float host_aabb_max[3],
+                                 const uint32_t host_bounds[3], uint32_t num_slots, int32_t keying, uint64_t* table,
+                                 uint32_t* status, int64_t n, const float* pos, uint32_t* out_slot, void* stream);
 
 /* ================================================================ Morton quadtrees
  * Replaces MortonQuadTreeT / MortonQuadTreeWrapperT / RTMortonQuadTreeWrapperT

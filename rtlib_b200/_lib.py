@@ -57,6 +57,7 @@ _SIGS = {
     "rtpg_hashgrid_export": [P, C.c_int, P, P],
     "rtpg_hashgrid_status": [P, P, C.c_int, P],
     "rtpg_hashgrid_device_view": [P, P, P],
+    "rtpg_hashgrid_insert_noalloc": [P, P, P, U32, I32, P, P, I64, P, P, P],
     "rtpg_mqt_create": [U32, U32, F32, I32, P],
     "rtpg_mqt_destroy": [P],
     "rtpg_mqt_clear": [P, P],

@@ -14,6 +14,7 @@
 // keys of a bucket are ranked by first occurrence and appended after the bucket's occupied
 // prefix.  Lookups (FindFromPrv) read the previous snapshot and stop at the first empty slot.
 #include <cub/cub.cuh>
+#include <mutex>
 #include <new>
 #include <vector>
 
@@ -318,3 +319,127 @@ int rtpg_hashgrid_device_view(rtpg_hashgrid* h, void** dev_cur, void** dev_prv) 
 }
 
 }  // extern "C"
+
+// ================================================================ allocation-free insert
+// The batch insert above keeps its sort buffers in the handle, allocated by
+// rtpg_hashgrid_create.  Some callers cannot allocate device memory at all: a renderer or
+// simulation that hands this library a fixed memory budget and owns every allocation, code
+// that enqueues work while another component captures the stream into a CUDA graph (where
+// cudaMalloc is not allowed), or a real-time loop that must never block in the allocator.
+// rtpg_hashgrid_insert_noalloc serves them: the caller passes the table and the outputs, and
+// the scratch lives in one file-scope device array of fixed size, reserved in every GPU's
+// memory when the library loads and held until the process exits.
+namespace rtpg {
+
+constexpr uint32_t kNoAllocMaxPoints = 1u << 16;  // points per call
+constexpr size_t kNoAllocSortBytes = size_t(4) << 20;  // radix-sort temporary storage
+constexpr size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+constexpr size_t kNA_skey = 0;
+constexpr size_t kNA_sval = kNA_skey + align256(2ull * 8 * kNoAllocMaxPoints);
+constexpr size_t kNA_comp = kNA_sval + align256(2ull * 4 * kNoAllocMaxPoints);
+constexpr size_t kNA_cval = kNA_comp + align256(2ull * 8 * kNoAllocMaxPoints);
+constexpr size_t kNA_bucket = kNA_cval + align256(2ull * 4 * kNoAllocMaxPoints);
+constexpr size_t kNA_run = kNA_bucket + align256(4ull * kNoAllocMaxPoints);
+constexpr size_t kNA_occ = kNA_run + align256(4ull * kNoAllocMaxPoints);
+constexpr size_t kNA_status = kNA_occ + align256(kNoAllocMaxPoints);
+constexpr size_t kNA_temp = kNA_status + 256;
+constexpr size_t kNoAllocScratchBytes = kNA_temp + kNoAllocSortBytes;  // about 7.8 MB
+
+static __device__ __align__(256) unsigned char g_insert_scratch[kNoAllocScratchBytes];
+
+// Device address of g_insert_scratch per device, looked up once per device with that device
+// current (host code cannot use the symbol itself as a device address).
+static std::mutex g_na_mutex;
+static unsigned char* g_na_ptr[64] = {};
+
+static int noalloc_scratch(unsigned char** out) {
+    int dev = 0;
+    RTPG_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return fail(RTPG_EINVAL, "rtpg_hashgrid_insert_noalloc: device ordinal %d out of range", dev);
+    std::lock_guard<std::mutex> lock(g_na_mutex);
+    if (!g_na_ptr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_insert_scratch);
+        if (e != cudaSuccess)
+            return fail(RTPG_ECUDA, "rtpg_hashgrid_insert_noalloc: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
+        // the sort's temporary storage for the largest batch must fit the reserved bytes
+        cub::DoubleBuffer<unsigned long long> dk(nullptr, nullptr);
+        cub::DoubleBuffer<uint32_t> dv(nullptr, nullptr);
+        size_t tb = 0;
+        e = cub::DeviceRadixSort::SortPairs(nullptr, tb, dk, dv, (int)kNoAllocMaxPoints, 0, 64);
+        if (e != cudaSuccess) return fail(RTPG_ECUDA, "rtpg_hashgrid_insert_noalloc: %s", cudaGetErrorString(e));
+        if (tb > kNoAllocSortBytes)
+            return fail(RTPG_ECAPACITY, "rtpg_hashgrid_insert_noalloc: sort needs %zu bytes, %zu reserved", tb,
+                        kNoAllocSortBytes);
+        g_na_ptr[dev] = static_cast<unsigned char*>(p);
+    }
+    *out = g_na_ptr[dev];
+    return RTPG_OK;
+}
+
+}  // namespace rtpg
+
+extern "C" int rtpg_hashgrid_insert_noalloc(const float* aabb_min, const float* aabb_max, const uint32_t* bounds,
+                                            uint32_t num_slots, int32_t keying, uint64_t* table, uint32_t* status,
+                                            int64_t n, const float* pos, uint32_t* out_slot, void* stream) {
+    if (!aabb_min || !aabb_max || !bounds || !table) return fail(RTPG_EINVAL, "rtpg_hashgrid_insert_noalloc: null argument");
+    if (n < 0 || (n > 0 && (!pos || !out_slot))) return fail(RTPG_EINVAL, "rtpg_hashgrid_insert_noalloc: bad arguments");
+    if (n > (int64_t)kNoAllocMaxPoints)
+        return fail(RTPG_ECAPACITY, "rtpg_hashgrid_insert_noalloc: %lld points exceed the limit of %u per call",
+                    (long long)n, kNoAllocMaxPoints);
+    if (num_slots < kHashBlock || num_slots % kHashBlock)
+        return fail(RTPG_EINVAL, "rtpg_hashgrid_insert_noalloc: num_slots must be a positive multiple of %u", kHashBlock);
+    if (keying != RTPG_HASH_KEY_REFERENCE && keying != RTPG_HASH_KEY_MORTON)
+        return fail(RTPG_EINVAL, "rtpg_hashgrid_insert_noalloc: unknown keying %d", keying);
+    if (!aligned8(table) || !aligned4(pos) || !aligned4(out_slot))
+        return fail(RTPG_EINVAL, "rtpg_hashgrid_insert_noalloc: misaligned array");
+    for (int k = 0; k < 3; ++k) {
+        if (bounds[k] == 0 || !(aabb_max[k] > aabb_min[k]))
+            return fail(RTPG_EINVAL, "rtpg_hashgrid_insert_noalloc: empty grid or AABB");
+        if (keying == RTPG_HASH_KEY_MORTON && bounds[k] > (1u << 21))
+            return fail(RTPG_EINVAL, "rtpg_hashgrid_insert_noalloc: Morton keying supports at most 2^21 cells per axis");
+    }
+    unsigned char* s = nullptr;
+    int r = noalloc_scratch(&s);
+    if (r) return r;
+    if (n == 0) return RTPG_OK;
+    HashGridDev g{};
+    g.off = make_float3(aabb_min[0], aabb_min[1], aabb_min[2]);
+    g.size = make_float3(aabb_max[0] - aabb_min[0], aabb_max[1] - aabb_min[1], aabb_max[2] - aabb_min[2]);
+    g.bounds = make_uint3(bounds[0], bounds[1], bounds[2]);
+    g.nslots = num_slots;
+    g.nbuckets = num_slots / kHashBlock;
+    g.keying = keying;
+    g.cur = reinterpret_cast<unsigned long long*>(table);
+    g.prv = nullptr;
+    g.status = status ? reinterpret_cast<unsigned*>(status) : reinterpret_cast<unsigned*>(s + kNA_status);
+    auto* skey = reinterpret_cast<unsigned long long*>(s + kNA_skey);
+    auto* sval = reinterpret_cast<uint32_t*>(s + kNA_sval);
+    auto* comp = reinterpret_cast<unsigned long long*>(s + kNA_comp);
+    auto* cval = reinterpret_cast<uint32_t*>(s + kNA_cval);
+    auto* bucket_of = reinterpret_cast<uint32_t*>(s + kNA_bucket);
+    auto* run_slot = reinterpret_cast<uint32_t*>(s + kNA_run);
+    auto* occ_of = reinterpret_cast<uint8_t*>(s + kNA_occ);
+    void* temp = s + kNA_temp;
+    // every scratch word read below is written earlier in the same call, so nothing left
+    // by a previous call needs clearing
+    cudaStream_t st = as_stream(stream);
+    const int64_t m = n;
+    const int grid = grid_for(m, 256, 8);
+    k_hash_prepare<<<grid, 256, 0, st>>>(g, 0, m, pos, skey, sval, bucket_of, occ_of, out_slot, nullptr);
+    RTPG_LAUNCH_CHECK();
+    cub::DoubleBuffer<unsigned long long> dk(skey, skey + kNoAllocMaxPoints);
+    cub::DoubleBuffer<uint32_t> dv(sval, sval + kNoAllocMaxPoints);
+    size_t tb = kNoAllocSortBytes;
+    RTPG_CUDA(cub::DeviceRadixSort::SortPairs(temp, tb, dk, dv, (int)m, 0, 64, st));
+    k_hash_heads<<<grid, 256, 0, st>>>(m, dk.Current(), dv.Current(), bucket_of, comp, cval);
+    RTPG_LAUNCH_CHECK();
+    cub::DoubleBuffer<unsigned long long> ck(comp, comp + kNoAllocMaxPoints);
+    cub::DoubleBuffer<uint32_t> cv(cval, cval + kNoAllocMaxPoints);
+    tb = kNoAllocSortBytes;
+    RTPG_CUDA(cub::DeviceRadixSort::SortPairs(temp, tb, ck, cv, (int)m, 0, 64, st));
+    k_hash_assign<<<grid, 256, 0, st>>>(g, m, ck.Current(), cv.Current(), dk.Current(), occ_of, run_slot);
+    k_hash_scatter<<<grid, 256, 0, st>>>(0, m, dk.Current(), dv.Current(), run_slot, out_slot);
+    RTPG_LAUNCH_CHECK();
+    return RTPG_OK;
+}

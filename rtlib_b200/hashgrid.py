@@ -59,6 +59,25 @@ class HashGrid:
         return s.value
 
 
+NOALLOC_MAX_POINTS = 1 << 16
+
+
+def insert_noalloc(aabb_min, aabb_max, bounds, table, pos, out_slot, keying=KEY_REFERENCE, status=None, stream=None):
+    """Batch insert without any device allocation (rtpg_hashgrid_insert_noalloc).
+
+    For callers that cannot allocate device memory -- an application that owns every
+    allocation under a fixed budget, work enqueued while the stream is being captured into a
+    CUDA graph, or a real-time loop that must not block in the allocator.  `table` is the
+    caller's current table (uint64 keys, num_slots entries, zero = empty), updated in place.
+    At most NOALLOC_MAX_POINTS points per call.  Calls share one fixed scratch array on the
+    device, so overlapping calls must be ordered by the caller."""
+    mn = (C.c_float * 3)(*[float(v) for v in aabb_min])
+    mx = (C.c_float * 3)(*[float(v) for v in aabb_max])
+    b = (C.c_uint32 * 3)(*[int(v) for v in bounds])
+    call("rtpg_hashgrid_insert_noalloc", mn, mx, b, int(table.shape[0]), int(keying), ptr(table), ptr(status),
+         int(pos.shape[0]), ptr(pos), ptr(out_slot), stream_ptr(stream))
+
+
 class MortonQuadTrees:
     def __init__(self, num_cells, level=6, fraction=0.3, fixed_point_bits=0):
         h = C.c_void_p()
