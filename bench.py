@@ -298,11 +298,12 @@ C_BUDGET = 2047          # passes of 1, 2, 4, ..., 512, 1024 spp
 C_MAX_DEPTH = 8
 C_FRACTION = 0.5
 C_AABB = ((-0.005,) * 3, (1.005,) * 3)  # world AABB padded by 0.005 as the application does
-# compulsory SoA bytes of one extend visit (one path-bounce): reads queue index, origin,
-# direction, throughput, depth, flags, rng (52 B); writes pending flag, bounce radiance,
-# origin, direction, throughput, flags, rng (60 B) and the NEE shadow ray (28 B).  Scene,
-# material and tree reads are L2-resident and not counted; trace-vertex writes are excluded.
-EXTEND_BYTES = 140
+# compulsory SoA bytes of one bounce visit (one path-bounce): reads queue index, origin,
+# direction, throughput, depth, flags, rng, color (64 B); writes origin, direction,
+# throughput, flags, rng, color, depth and the next-queue index (64 B).  Scene, material and
+# tree reads are L2-resident and not counted; per-bounce radiance and trace-vertex writes
+# (recording passes only) are excluded.
+BOUNCE_BYTES = 128
 
 
 def set_budget(b):
@@ -367,9 +368,9 @@ def bench_cornell_ours(args, rank, world):
     torch.cuda.synchronize()
     tk = tr.timings()
     tr.set_timing(False)
-    ext_ms = tk["extend"][0]
+    ext_ms = tk["bounce"][0]
     peak, peak_kind = _peaks()
-    achieved = cnt["path_bounces"] * EXTEND_BYTES / (ext_ms * 1e-3) / 1e9
+    achieved = cnt["path_bounces"] * BOUNCE_BYTES / (ext_ms * 1e-3) / 1e9
 
     # e2e: scene from host memory through the C ABI, image back to host
     e2e_ms = []
@@ -399,16 +400,16 @@ def bench_cornell_ours(args, rank, world):
         "ms_per_step": ms,
         "e2e": {"value": paths / (e2e * 1e-3) / 1e6, "unit": "Mpaths/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(h_img.numel() * 4)},
-        "roofline": {"kernel": "k_extend", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+        "roofline": {"kernel": "k_bounce", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs (burst copy)",
-                     "traffic": _traffic("k_extend"), "algorithmic_bytes_per_path_bounce": EXTEND_BYTES,
+                     "traffic": _traffic("k_bounce"), "algorithmic_bytes_per_path_bounce": BOUNCE_BYTES,
                      "path_bounces_per_step": cnt["path_bounces"],
-                     "launch_ms": ext_ms / max(1, tk["extend"][1]),
+                     "launch_ms": ext_ms / max(1, tk["bounce"][1]),
                      "kernel_ms_per_step": {kk: v[0] for kk, v in tk.items()},
-                     "note": "extend = BVH closest hit + shading; its bound is instruction and latency, "
-                             "the HBM figure is the SoA state traffic"},
+                     "note": "bounce = BVH closest hit + shading + shadow ray; its bound is instruction "
+                             "issue and traversal latency, the HBM figure is the SoA state traffic"},
         "clocks": clk,
-        "gpu_launches": (1 + 2 * C_MAX_DEPTH + 1) * (C_BUDGET + 1) * args.steps,
+        "gpu_launches": (1 + C_MAX_DEPTH + 1) * (C_BUDGET + 1) * args.steps,
         "counters_per_step": cnt,
         "sdtree": st,
     }

@@ -224,6 +224,24 @@ int rtpg_mqt_pdf(rtpg_mqt* h, int64_t n, const uint32_t* cell, const float* dir,
 int rtpg_mqt_export(rtpg_mqt* h, int64_t* host_leaves, float* host_pyramid, void* stream);
 int rtpg_mqt_status(rtpg_mqt* h, uint32_t* host_status, int clear, void* stream);
 
+/* RTMortonQuadTreeControllerT (MO.h:766-993): the doubling pass schedule of the hash-grid
+ * guide.  States as its TraceState enum; begin at a start clears the quadtrees (Allocate),
+ * end after a finished pass beyond iteration_for_built calls rtpg_mqt_update. */
+typedef struct rtpg_mqt_controller rtpg_mqt_controller;
+#define RTPG_MQT_TRACE_RECORD 0
+#define RTPG_MQT_TRACE_RECORD_AND_SAMPLE 1
+#define RTPG_MQT_TRACE_SAMPLE 2
+#define RTPG_MQT_TRACE_LOCATE 3
+int rtpg_mqt_controller_create(rtpg_mqt* tree, uint32_t sample_for_budget, uint32_t iteration_for_built,
+                               uint32_t iteration_for_locate, float ratio_for_budget, uint32_t samples_per_launch,
+                               rtpg_mqt_controller** out);
+int rtpg_mqt_controller_destroy(rtpg_mqt_controller* c);
+int rtpg_mqt_controller_start(rtpg_mqt_controller* c);
+int rtpg_mqt_controller_begin(rtpg_mqt_controller* c, void* stream);
+int rtpg_mqt_controller_end(rtpg_mqt_controller* c, void* stream);
+int rtpg_mqt_controller_get(rtpg_mqt_controller* c, int32_t* host_state, uint32_t* host_iteration,
+                            uint32_t* host_samples_in_pass, int32_t* host_executing);
+
 /* ================================================================ scene / hit queries
  * The integrator's closest-hit and any-hit queries (RTLib: optixTrace inside TraceRadiance /
  * TraceOccluded, RTLib/Src/Ext/OPX7/Test/cuda/SimpleKernel.h:347-366, "SK.h") answered by a
@@ -273,9 +291,11 @@ typedef struct rtpg_tracer_desc {
 /* Params::flags (SK.h:145-154) */
 #define RTPG_TRACE_FLAG_NEE 1u
 #define RTPG_TRACE_FLAG_RIS 2u
-#define RTPG_TRACE_FLAG_USE_TREE 8u
+#define RTPG_TRACE_FLAG_USE_GRID 4u /* hash-grid + Morton quadtree guide (SimpleGuide2.cu) */
+#define RTPG_TRACE_FLAG_USE_TREE 8u /* SD-tree guide (SimpleGuide.cu) */
 #define RTPG_TRACE_FLAG_BUILD 16u
 #define RTPG_TRACE_FLAG_FINAL 32u
+#define RTPG_TRACE_FLAG_LOCATE 64u /* insert unseen cells into the current hash table */
 /* tri_vertices: num_triangles x 9 floats (v0, v1, v2 of triangle i, the scene's order);
  * tri_material: uint32 per triangle; tri_uv: 6 floats per triangle or NULL; light_tris:
  * triangle ids of the emitters, light mesh i = light_tris[first[i] .. first[i] + count[i])
@@ -297,22 +317,38 @@ int rtpg_tracer_render(rtpg_tracer* h, uint32_t spp, uint32_t flags, rtpg_sdtree
  * max_launches launches of samples_per_launch samples, flags from the controller state. */
 int rtpg_tracer_render_guided(rtpg_tracer* h, rtpg_sdtree* tree, rtpg_controller* ctrl, uint32_t base_flags,
                               uint32_t samples_per_launch, uint32_t max_launches, void* stream);
+/* `spp` samples per pixel guided by the hash grid and its Morton quadtrees
+ * (SimpleGuide2.cu:48-520): flags must hold RTPG_TRACE_FLAG_USE_GRID and not USE_TREE.
+ * Every Phong hit looks its cell up in the grid's previous table; with BUILD a found cell's
+ * quadtree is mixed into the direction pdf; with LOCATE an unseen cell is inserted into the
+ * current table; trace vertices are committed into the quadtrees' building leaves unless
+ * FINAL.  mqt must have at least as many cells as the grid has slots. */
+int rtpg_tracer_render_grid(rtpg_tracer* h, uint32_t spp, uint32_t flags, rtpg_hashgrid* grid, rtpg_mqt* mqt,
+                            void* stream);
+/* TracePipeline's loop for the hash-grid tracers (RTLibExtOPX7TestApplication.cpp:2174-2222):
+ * controller begin, flags by state (LOCATE: USE_GRID|LOCATE, RECORD: USE_GRID,
+ * RECORD_AND_SAMPLE: +BUILD, SAMPLE: +BUILD|FINAL, plus NEE / RIS of base_flags), render,
+ * controller end, and the grid's current -> previous copy (rtpg_hashgrid_swap) after every
+ * finished pass. */
+int rtpg_tracer_render_grid_guided(rtpg_tracer* h, rtpg_hashgrid* grid, rtpg_mqt* mqt, rtpg_mqt_controller* ctrl,
+                                   uint32_t base_flags, uint32_t samples_per_launch, uint32_t max_launches,
+                                   void* stream);
 /* mean radiance per pixel, width x height x RGB float (device) */
 int rtpg_tracer_image(rtpg_tracer* h, float* out_rgb, void* stream);
 int rtpg_tracer_accumulation(rtpg_tracer* h, const double** dev_accum, uint64_t* host_samples);
 int rtpg_tracer_stats(rtpg_tracer* h, uint64_t* host_samples, uint64_t* host_paths);
-/* Device counters since the last clear: path-bounces shaded (extend visits) and shadow rays
+/* Device counters since the last clear: path-bounces shaded (bounce visits) and shadow rays
  * traced.  Synchronises the stream. */
 int rtpg_tracer_counters(rtpg_tracer* h, uint64_t* host_path_bounces, uint64_t* host_shadow_rays, void* stream);
 /* Measurement mode: enable = 1 makes rtpg_tracer_render launch waves without the CUDA graph,
  * bracket every kernel with CUDA events on the stream and synchronise per wave; the summed
- * device milliseconds of raygen / extend / connect / finish (and their launch counts) are
- * read with rtpg_tracer_timings.  Enabling or disabling resets the sums. */
+ * device milliseconds of raygen / bounce / finish (and their launch counts) are read into
+ * three-element arrays with rtpg_tracer_timings.  Enabling or disabling resets the sums. */
 int rtpg_tracer_set_timing(rtpg_tracer* h, int enable);
 /* Debug view: the final bounce index of every path of the last wave (uint32 per pixel,
  * device); with recording on, a path commits min(depth, 10) trace vertices. */
 int rtpg_tracer_path_depths(rtpg_tracer* h, uint32_t* out_depth, void* stream);
-int rtpg_tracer_timings(rtpg_tracer* h, double* host_ms4, uint64_t* host_launches4);
+int rtpg_tracer_timings(rtpg_tracer* h, double* host_ms3, uint64_t* host_launches3);
 
 #ifdef __cplusplus
 }

@@ -686,7 +686,50 @@ void or_mqt_build(uint32_t ncells, uint32_t level, int bits, const int64_t* leav
     }
     free(tmp);
 }
-/* MortonQuadTreeT::SampleAndPdf (OPX7UtilsMorton.h:286-344) and ::Pdf (:401-414). */
+/* MortonQuadTreeT::SampleAndPdf (OPX7UtilsMorton.h:286-344) for one pyramid w; an empty tree
+ * samples uniformly with pdf 1. */
+static void mqt_sample_one(const float* w, uint32_t level, uint32_t* rng, float* ux, float* uy, float* pdf) {
+    float total = w[0];
+    if (total <= 0.0f) {
+        *ux = rnd1(rng); *uy = rnd1(rng); *pdf = 1.0f;
+        return;
+    }
+    uint32_t size = 4, offset = 1, code = 0;
+    for (uint32_t l = 0; l < level; ++l) {
+        const float* q = w + offset + (code << 2);
+        uint32_t cl = 0;
+        float partial = q[0] + q[2];
+        float boundary = partial / total;
+        float sample = rnd1(rng);
+        if (sample < boundary) { sample /= boundary; boundary = q[0] / partial; }
+        else {
+            partial = q[1] + q[3];
+            sample = (sample - boundary) / (1.0f - boundary);
+            boundary = q[1] / partial;
+            cl |= 1;
+        }
+        if (sample >= boundary) cl |= 2;
+        total = q[cl];
+        code = (code << 2) + cl;
+        offset += size;
+        size *= 4;
+    }
+    const float nn = ldexpf(1.0f, (int)level);
+    const uint32_t xi = compact1by1(code), yi = compact1by1(code >> 1);
+    *ux = ((float)xi + rnd1(rng)) / nn;
+    *uy = ((float)yi + rnd1(rng)) / nn;
+    *pdf = total / w[0] * ldexpf(1.0f, (int)(2 * level));
+}
+/* MortonQuadTreeT::Pdf (OPX7UtilsMorton.h:401-414); an empty tree has pdf 1 */
+static float mqt_pdf_one(const float* w, uint32_t level, float u, float v) {
+    if (w[0] <= 0.0f) return 1.0f;
+    const float nn = ldexpf(1.0f, (int)level);
+    const uint32_t maxi = (1u << level) - 1u;
+    uint32_t px = (uint32_t)(u * nn), py = (uint32_t)(v * nn);
+    px = px > maxi ? maxi : px;
+    py = py > maxi ? maxi : py;
+    return w[mqt_off(level) + or_morton2(px, py)] / w[0] * nn * nn;
+}
 void or_mqt_sample_pdf(int64_t n, uint32_t level, const float* pyramid, const uint32_t* cell, const uint32_t* seeds,
                        float* out_uv, float* out_pdf, float* out_pdf_eval) {
     const uint32_t per = mqt_off(level + 1);
@@ -694,51 +737,10 @@ void or_mqt_sample_pdf(int64_t n, uint32_t level, const float* pyramid, const ui
         const float* w = pyramid + (uint64_t)cell[i] * per;
         uint32_t rng = seeds[i];
         float ux, uy, pdf;
-        float total = w[0];
-        if (total <= 0.0f) {
-            ux = rnd1(&rng); uy = rnd1(&rng); pdf = 1.0f;
-        } else {
-            uint32_t size = 4, offset = 1, code = 0;
-            for (uint32_t l = 0; l < level; ++l) {
-                const float* q = w + offset + (code << 2);
-                uint32_t cl = 0;
-                float partial = q[0] + q[2];
-                float boundary = partial / total;
-                float sample = rnd1(&rng);
-                if (sample < boundary) { sample /= boundary; boundary = q[0] / partial; }
-                else {
-                    partial = q[1] + q[3];
-                    sample = (sample - boundary) / (1.0f - boundary);
-                    boundary = q[1] / partial;
-                    cl |= 1;
-                }
-                if (sample >= boundary) cl |= 2;
-                total = q[cl];
-                code = (code << 2) + cl;
-                offset += size;
-                size *= 4;
-            }
-            const float nn = ldexpf(1.0f, (int)level);
-            const uint32_t xi = compact1by1(code), yi = compact1by1(code >> 1);
-            ux = ((float)xi + rnd1(&rng)) / nn;
-            uy = ((float)yi + rnd1(&rng)) / nn;
-            pdf = total / w[0] * ldexpf(1.0f, (int)(2 * level));
-        }
+        mqt_sample_one(w, level, &rng, &ux, &uy, &pdf);
         out_uv[2 * i] = ux; out_uv[2 * i + 1] = uy;
         out_pdf[i] = pdf;
-        if (out_pdf_eval) {
-            float pe;
-            if (w[0] <= 0.0f) pe = 1.0f;
-            else {
-                const float nn = ldexpf(1.0f, (int)level);
-                const uint32_t maxi = (1u << level) - 1u;
-                uint32_t px = (uint32_t)(ux * nn), py = (uint32_t)(uy * nn);
-                px = px > maxi ? maxi : px;
-                py = py > maxi ? maxi : py;
-                pe = w[mqt_off(level) + or_morton2(px, py)] / w[0] * nn * nn;
-            }
-            out_pdf_eval[i] = pe;
-        }
+        if (out_pdf_eval) out_pdf_eval[i] = mqt_pdf_one(w, level, ux, uy);
     }
 }
 
@@ -857,11 +859,81 @@ static OLight o_sample_light(const OScene* s, V3 p_in, uint32_t* rng) {
 }
 #define O_NEE 1u
 #define O_RIS 2u
+#define O_GRID 4u
 #define O_TREE 8u
 #define O_BUILD 16u
 #define O_FINAL 32u
+#define O_LOCATE 64u
 #define O_KTV 10
-typedef struct { V3 pos, dir, thr, rad, bsdf; float wopdf, cosine; int valid, delta; } OVert;
+typedef struct { V3 pos, dir, thr, rad, bsdf; float wopdf, cosine; int valid, delta; uint32_t cell; } OVert;
+
+/* The hash-grid guide of SimpleGuide2.cu: DoubleBufferedHashGrid3T (cur / prv tables of
+ * 64-bit keys, 0 = empty) and one Morton quadtree per slot (int64 building leaves, float
+ * sampling pyramid).  keying 0: the reference's pcg1d bucket and checksum key; 1: 63-bit
+ * Morton key + 1 with a 64-bit mixed bucket. */
+typedef struct {
+    float off[3], size[3];
+    uint32_t bounds[3], nslots;
+    int32_t keying;
+    uint64_t* cur;
+    uint64_t* prv;
+    uint32_t level;
+    int32_t bits;
+    int64_t* leaves;
+    const float* pyramid;
+    float fraction;
+    uint32_t status;
+} OGrid;
+static uint64_t grid_key(const OGrid* g, V3 p, uint32_t* bucket) {
+    float pp[3] = {p.x, p.y, p.z};
+    uint32_t c[3];
+    grid_cell(pp, g->off, g->size, g->bounds, c);
+    const uint32_t nb = g->nslots / 32;
+    if (g->keying == 0) {
+        *bucket = or_pcg1d(g->nslots + c[2] + or_pcg1d(c[1] + or_pcg1d(c[0]))) % nb;
+        return (uint64_t)(1u + g->bounds[0] * g->bounds[1] * c[2] + g->bounds[0] * c[1] + c[0]);
+    }
+    const uint64_t key = or_morton3(c[0], c[1], c[2]) + 1ull;
+    *bucket = (uint32_t)(mix64(key) % nb);
+    return key;
+}
+/* FindFromPrv (OPX7UtilsGrid.h:278-300) */
+static uint32_t grid_find_prv(const OGrid* g, uint64_t key, uint32_t b) {
+    for (uint32_t k = 0; k < 32; ++k) {
+        const uint64_t v = g->prv[32 * (uint64_t)b + k];
+        if (v == 0) return UINT32_MAX;
+        if (v == key) return 32 * b + k;
+    }
+    return UINT32_MAX;
+}
+/* FindFromCur (OPX7UtilsGrid.h:189-226) */
+static uint32_t grid_insert_cur(OGrid* g, uint64_t key, uint32_t b) {
+    for (uint32_t k = 0; k < 32; ++k) {
+        uint64_t* v = &g->cur[32 * (uint64_t)b + k];
+        if (*v == 0) { *v = key; return 32 * b + k; }
+        if (*v == key) return 32 * b + k;
+    }
+    g->status |= 0x10u;
+    return UINT32_MAX;
+}
+/* MortonTraceVertexT::Commit (OPX7UtilsMorton.h:550-585) -> MortonQuadTreeWrapperT::Record */
+static void commit_vertex_grid(OGrid* g, const OVert* v) {
+    if (!v->valid || v->delta) return;
+    V3 r = v->rad, b = v->bsdf;
+    int okr = isfinite(r.x) && r.x >= 0.f && isfinite(r.y) && r.y >= 0.f && isfinite(r.z) && r.z >= 0.f;
+    int okb = isfinite(b.x) && b.x >= 0.f && isfinite(b.y) && b.y >= 0.f && isfinite(b.z) && b.z >= 0.f;
+    if (v->wopdf <= 0.0f || !okr || !okb) return;
+    V3 lr = v3(0, 0, 0);
+    if (v->thr.x * v->wopdf > 1e-4f) lr.x = r.x / v->thr.x;
+    if (v->thr.y * v->wopdf > 1e-4f) lr.y = r.y / v->thr.y;
+    if (v->thr.z * v->wopdf > 1e-4f) lr.z = r.z / v->thr.z;
+    lr = vs(fabsf(v->cosine), lr);
+    float lavg = (lr.x + lr.y + lr.z) / 3.0f;
+    float irr = lavg / v->wopdf;
+    float d[3] = {v->dir.x, v->dir.y, v->dir.z}, uv[2];
+    or_dir_to_canonical(1, d, uv);
+    or_mqt_record(1, g->level, g->bits, g->leaves, &v->cell, uv, &irr, &g->status);
+}
 
 static void commit_vertex(OSDTree* t, const OVert* v) {
     if (!v->valid || v->delta) return;
@@ -891,11 +963,13 @@ void or_render_log_pixel(int64_t pixel, float* out) { g_log_pixel = pixel; g_log
 /* where or_render writes the final bounce index of every path (NULL = nowhere) */
 void or_render_depth_output(uint32_t* out) { g_depth_out = out; }
 
-int64_t or_render(const OScene* s, uint32_t flags, void* tree_h, uint32_t p0, uint32_t p1, uint32_t* seeds,
-                  double* accum) {
+int64_t or_render(const OScene* s, uint32_t flags, void* tree_h, void* grid_h, uint32_t p0, uint32_t p1,
+                  uint32_t* seeds, double* accum) {
     OSDTree* tree = (OSDTree*)tree_h;
-    const int use_tree = (flags & O_TREE) != 0, build = (flags & O_BUILD) != 0;
-    const int recording = use_tree && !(flags & O_FINAL);
+    OGrid* grid = (OGrid*)grid_h;
+    const int use_tree = (flags & O_TREE) != 0, use_grid = (flags & O_GRID) != 0, build = (flags & O_BUILD) != 0;
+    const int recording = (use_tree || use_grid) && !(flags & O_FINAL);
+    const uint32_t mqt_per = use_grid ? mqt_off(grid->level + 1) : 0;
     const float inv_pi = (float)0.318309886183790691216444201927515678107738494873046875;
     for (uint32_t p = p0; p < p1; ++p) {
         uint32_t x = p % s->width, y = p / s->width;
@@ -949,9 +1023,15 @@ int64_t or_render(const OScene* s, uint32_t flags, void* tree_h, uint32_t p0, ui
                     diffuse = vmul(diffuse, v3(px[0], px[1], px[2]));
                 }
                 int count_emitted = (pflags & 8u) || m->type == 3;
-                uint32_t dt = 0;
+                uint32_t dt = 0, cell = UINT32_MAX;
                 if (use_tree) dt = (uint32_t)leaf_dtree(tree, &position.x);
                 if (m->type == 0) {
+                    uint32_t gb = 0, prv_cell = UINT32_MAX;
+                    uint64_t gk = 0;
+                    if (use_grid) {
+                        gk = grid_key(grid, position, &gb);
+                        prv_cell = grid_find_prv(grid, gk, gb);
+                    }
                     V3 refl = vunit(reflect_o(dir, fn));
                     float a = rnd1(&rng), c = rnd1(&rng);
                     float r = sqrtf(a), z = sqrtf(1.0f - a);
@@ -999,6 +1079,34 @@ int64_t or_render(const OScene* s, uint32_t flags, void* tree_h, uint32_t p0, ui
                         or_dir_to_canonical(1, dd3, c2);
                         float dpdf = fmaxf(dtree_pdf(dd, c2[0], c2[1]), 0.0f);
                         wo_pdf = (1.0f - s->fraction) * bsdf_pdf + s->fraction * dpdf;
+                    } else if (use_grid && build && prv_cell != UINT32_MAX) {
+                        /* SimpleGuide2.cu:350-377 */
+                        const float* w = grid->pyramid + (uint64_t)prv_cell * mqt_per;
+                        float dpdf;
+                        if (rnd1(&rng) < grid->fraction) {
+                            float uv[2], tp;
+                            mqt_sample_one(w, grid->level, &rng, &uv[0], &uv[1], &tp);
+                            dpdf = (float)((double)tp * (0.25 * 0.318309886183790691216444201927515678107738494873046875));
+                            float dv[3];
+                            const float cosTheta = 2.0f * uv[0] - 1.0f;
+                            const float sinTheta = sqrtf(fmaxf(1.0f - cosTheta * cosTheta, 0.0f));
+                            dv[0] = sinTheta * cospi_f(2.0f * uv[1]);
+                            dv[1] = sinTheta * sinpi_f(2.0f * uv[1]);
+                            dv[2] = cosTheta;
+                            float l = 1.0f / sqrtf(dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2]);
+                            direction = v3(dv[0] * l, dv[1] * l, dv[2] * l);
+                            cosine = vdot(direction, fn);
+                            float cp2 = fmaxf(cosine * inv_pi, 0.0f);
+                            float pp2 = phong_pdf_o(direction, refl, m->shininess);
+                            bsdf_val = vadd(vs(inv_pi, diffuse), vs(pp2, vs(sf, spec)));
+                            bsdf_pdf = sel * cp2 + (1.0f - sel) * pp2;
+                        } else {
+                            float dd3[3] = {direction.x, direction.y, direction.z}, c2[2];
+                            or_dir_to_canonical(1, dd3, c2);
+                            const float tp = mqt_pdf_one(w, grid->level, c2[0], c2[1]);
+                            dpdf = fmaxf((float)((double)(tp * 0.25f) * 0.318309886183790691216444201927515678107738494873046875), 0.0f);
+                        }
+                        wo_pdf = grid->fraction * dpdf + (1.0f - grid->fraction) * bsdf_pdf;
                     } else {
                         wo_pdf = bsdf_pdf;
                     }
@@ -1034,6 +1142,8 @@ int64_t or_render(const OScene* s, uint32_t flags, void* tree_h, uint32_t p0, ui
                     } else {
                         hflags |= 8u;
                     }
+                    if (use_grid)
+                        cell = ((flags & O_LOCATE) && prv_cell == UINT32_MAX) ? grid_insert_cur(grid, gk, gb) : prv_cell;
                 } else if (m->type == 1) {
                     V3 rn;
                     float rri, ci = vdot(fn, dir);
@@ -1063,7 +1173,9 @@ int64_t or_render(const OScene* s, uint32_t flags, void* tree_h, uint32_t p0, ui
                 if (recording && depth < O_KTV) {
                     OVert* v = &verts[depth];
                     v->pos = position; v->dir = direction; v->thr = cur_thr; v->rad = v3(0, 0, 0);
-                    v->bsdf = bsdf_val; v->wopdf = wo_pdf; v->cosine = cosine; v->valid = 1; v->delta = (hflags & 2u) != 0;
+                    v->bsdf = bsdf_val; v->wopdf = wo_pdf; v->cosine = cosine; v->delta = (hflags & 2u) != 0;
+                    v->valid = use_grid ? cell != UINT32_MAX : 1;
+                    v->cell = cell;
                 }
             }
             if (recording)
@@ -1079,7 +1191,10 @@ int64_t or_render(const OScene* s, uint32_t flags, void* tree_h, uint32_t p0, ui
         }
         if (recording) {
             uint32_t nv = depth < O_KTV ? depth : O_KTV;
-            for (uint32_t i = 0; i < nv; ++i) commit_vertex(tree, &verts[i]);
+            for (uint32_t i = 0; i < nv; ++i) {
+                if (use_grid) commit_vertex_grid(grid, &verts[i]);
+                else commit_vertex(tree, &verts[i]);
+            }
         }
         if (g_depth_out) g_depth_out[p] = depth;
         accum[3 * (size_t)p] += col.x;

@@ -67,6 +67,12 @@ _SIGS = {
     "rtpg_mqt_pdf": [P, I64, P, P, C.c_int, P, C.c_int, P],
     "rtpg_mqt_export": [P, P, P, P],
     "rtpg_mqt_status": [P, P, C.c_int, P],
+    "rtpg_mqt_controller_create": [P, U32, U32, U32, F32, U32, P],
+    "rtpg_mqt_controller_destroy": [P],
+    "rtpg_mqt_controller_start": [P],
+    "rtpg_mqt_controller_begin": [P, P],
+    "rtpg_mqt_controller_end": [P, P],
+    "rtpg_mqt_controller_get": [P, P, P, P, P],
     "rtpg_scene_create": [P, U32, P, U32, P, P],
     "rtpg_scene_destroy": [P],
     "rtpg_scene_intersect": [P, I64, P, P, P, P, C.c_int, P, P, P, P],
@@ -77,6 +83,8 @@ _SIGS = {
     "rtpg_tracer_clear": [P, P],
     "rtpg_tracer_render": [P, U32, U32, P, P],
     "rtpg_tracer_render_guided": [P, P, P, U32, U32, U32, P],
+    "rtpg_tracer_render_grid": [P, U32, U32, P, P, P],
+    "rtpg_tracer_render_grid_guided": [P, P, P, P, U32, U32, U32, P],
     "rtpg_tracer_image": [P, P, P],
     "rtpg_tracer_accumulation": [P, P, P],
     "rtpg_tracer_stats": [P, P, P],

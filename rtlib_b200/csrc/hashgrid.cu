@@ -320,6 +320,10 @@ int rtpg_hashgrid_device_view(rtpg_hashgrid* h, void** dev_cur, void** dev_prv) 
 
 }  // extern "C"
 
+namespace rtpg {
+HashGridDev hashgrid_device_view(const rtpg_hashgrid* h) { return h->dev; }
+}
+
 // ================================================================ allocation-free insert
 // The batch insert above keeps its sort buffers in the handle, allocated by
 // rtpg_hashgrid_create.  Some callers cannot allocate device memory at all: a renderer or

@@ -64,15 +64,32 @@ __device__ __forceinline__ unsigned long long hash_key(const HashGridDev& g, flo
 
 // FindFromPrv (OPX7UtilsGrid.h:278-300): probe the previous snapshot, stop at the first empty
 // slot; UINT32_MAX when absent.
-__device__ __forceinline__ uint32_t hash_find_prv(const HashGridDev& g, float px, float py, float pz) {
-    uint32_t b;
-    const unsigned long long key = hash_key(g, px, py, pz, b);
+__device__ __forceinline__ uint32_t hash_find_prv_key(const HashGridDev& g, unsigned long long key, uint32_t b) {
     const unsigned long long* row = g.prv + size_t(b) * kHashBlock;
     for (uint32_t k = 0; k < kHashBlock; ++k) {
         const unsigned long long v = row[k];
         if (v == 0ull) return 0xffffffffu;
         if (v == key) return b * kHashBlock + k;
     }
+    return 0xffffffffu;
+}
+__device__ __forceinline__ uint32_t hash_find_prv(const HashGridDev& g, float px, float py, float pz) {
+    uint32_t b;
+    const unsigned long long key = hash_key(g, px, py, pz, b);
+    return hash_find_prv_key(g, key, b);
+}
+
+// FindFromCur (OPX7UtilsGrid.h:189-226): claim the first empty slot of the bucket with a
+// compare-and-swap or find the key already there; slots only ever go from empty to a key,
+// so the occupied slots of a bucket stay a prefix and lookups may stop at the first empty
+// one.  A full bucket returns UINT32_MAX and raises RTPG_STATUS_HASH_FULL.
+__device__ __forceinline__ uint32_t hash_insert_cur_key(const HashGridDev& g, unsigned long long key, uint32_t b) {
+    unsigned long long* row = g.cur + size_t(b) * kHashBlock;
+    for (uint32_t k = 0; k < kHashBlock; ++k) {
+        const unsigned long long old = atomicCAS(row + k, 0ull, key);
+        if (old == 0ull || old == key) return b * kHashBlock + k;
+    }
+    atomicOr(g.status, RTPG_STATUS_HASH_FULL);
     return 0xffffffffu;
 }
 

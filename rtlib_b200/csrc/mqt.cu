@@ -12,6 +12,7 @@
 // kernel: a CTA per cell reads the cell's leaves, reduces the pyramid in shared memory with
 // exact integer sums, writes it as float to the sampling buffer and zeroes the leaves
 // (RTLib launches 1024x more blocks than cells and loops serially per cell).
+#include <algorithm>
 #include <new>
 #include <vector>
 
@@ -256,6 +257,114 @@ int rtpg_mqt_status(rtpg_mqt* h, uint32_t* host_status, int clear, void* stream)
     RTPG_CUDA(cudaMemcpyAsync(host_status, h->dev.status, 4, cudaMemcpyDeviceToHost, st));
     if (clear) RTPG_CUDA(cudaMemsetAsync(h->dev.status, 0, 4, st));
     RTPG_CUDA(cudaStreamSynchronize(st));
+    return RTPG_OK;
+}
+
+}  // extern "C"
+
+namespace rtpg {
+MqtDev mqt_device_view(const rtpg_mqt* h) { return h->dev; }
+}
+
+// ================================================================== pass controller
+// RTMortonQuadTreeControllerT (OPX7UtilsMorton.h:766-993): the doubling pass schedule of the
+// hash-grid guide with a LOCATE phase.  BegTrace at Start clears both quadtree buffers
+// (RTMortonQuadTreeWrapperT::Allocate); EndTrace after a finished pass beyond
+// iteration_for_built runs Update + mortonBuildKernel (rtpg_mqt_update here).
+struct rtpg_mqt_controller {
+    rtpg_mqt* tree;
+    uint32_t sample_for_budget, samples_per_launch, iteration_for_built, iteration_for_locate;
+    float ratio_for_budget;
+    bool start = false, executing = false;
+    uint32_t per_all = 0, per_tmp = 0, remain = 0, pass = 0, iteration = 0;
+    int32_t state = RTPG_MQT_TRACE_RECORD;
+};
+
+extern "C" {
+
+int rtpg_mqt_controller_create(rtpg_mqt* tree, uint32_t sample_for_budget, uint32_t iteration_for_built,
+                               uint32_t iteration_for_locate, float ratio_for_budget, uint32_t samples_per_launch,
+                               rtpg_mqt_controller** out) {
+    if (!tree || !out || samples_per_launch == 0) return fail(RTPG_EINVAL, "rtpg_mqt_controller_create: bad arguments");
+    auto* c = new (std::nothrow) rtpg_mqt_controller();
+    if (!c) return fail(RTPG_ENOMEM, "rtpg_mqt_controller_create: out of host memory");
+    c->tree = tree;
+    c->sample_for_budget = sample_for_budget;
+    c->samples_per_launch = samples_per_launch;
+    c->iteration_for_built = iteration_for_built;
+    c->iteration_for_locate = iteration_for_locate;
+    c->ratio_for_budget = ratio_for_budget;
+    *out = c;
+    return RTPG_OK;
+}
+int rtpg_mqt_controller_destroy(rtpg_mqt_controller* c) {
+    if (!c) return fail(RTPG_EINVAL, "rtpg_mqt_controller_destroy: null handle");
+    delete c;
+    return RTPG_OK;
+}
+int rtpg_mqt_controller_start(rtpg_mqt_controller* c) {
+    if (!c) return fail(RTPG_EINVAL, "rtpg_mqt_controller_start: null handle");
+    c->start = true;
+    return RTPG_OK;
+}
+// BegTrace (OPX7UtilsMorton.h:818-889)
+int rtpg_mqt_controller_begin(rtpg_mqt_controller* c, void* stream) {
+    if (!c) return fail(RTPG_EINVAL, "rtpg_mqt_controller_begin: null handle");
+    if (c->start) {
+        c->per_all = 0;
+        c->per_tmp = 0;
+        c->iteration = 0;
+        c->start = false;
+        c->executing = true;
+        c->remain = ((c->sample_for_budget - 1 + c->samples_per_launch) / c->samples_per_launch) * c->samples_per_launch;
+        c->pass = 0;
+        c->state = RTPG_MQT_TRACE_RECORD;
+        int r = rtpg_mqt_clear(c->tree, stream);
+        if (r) return r;
+    }
+    if (!c->executing) return RTPG_OK;
+    if (c->per_tmp == 0) {
+        c->remain -= c->pass;
+        c->pass = std::min<uint32_t>(c->remain, (1u << c->iteration) * c->samples_per_launch);
+        if ((c->remain - c->pass < 2 * c->pass) ||
+            (c->per_all >= c->ratio_for_budget * static_cast<float>(c->sample_for_budget)))
+            c->pass = c->remain;
+    }
+    if (c->iteration > c->iteration_for_built)
+        c->state = c->remain > c->pass ? RTPG_MQT_TRACE_RECORD_AND_SAMPLE : RTPG_MQT_TRACE_SAMPLE;
+    else if (c->iteration > c->iteration_for_locate)
+        c->state = RTPG_MQT_TRACE_RECORD;
+    else
+        c->state = RTPG_MQT_TRACE_LOCATE;
+    return RTPG_OK;
+}
+// EndTrace (OPX7UtilsMorton.h:891-922)
+int rtpg_mqt_controller_end(rtpg_mqt_controller* c, void* stream) {
+    if (!c) return fail(RTPG_EINVAL, "rtpg_mqt_controller_end: null handle");
+    if (!c->executing) return RTPG_OK;
+    c->per_all += c->samples_per_launch;
+    c->per_tmp += c->samples_per_launch;
+    if (c->per_tmp >= c->pass) {
+        c->iteration++;
+        if (c->iteration > c->iteration_for_built) {
+            int r = rtpg_mqt_update(c->tree, stream);
+            if (r) return r;
+        }
+        c->per_tmp = 0;
+    }
+    if (c->per_all > c->sample_for_budget) {
+        c->executing = false;
+        c->per_all = 0;
+    }
+    return RTPG_OK;
+}
+int rtpg_mqt_controller_get(rtpg_mqt_controller* c, int32_t* state, uint32_t* iteration, uint32_t* samples_in_pass,
+                            int32_t* executing) {
+    if (!c) return fail(RTPG_EINVAL, "rtpg_mqt_controller_get: null handle");
+    if (state) *state = c->state;
+    if (iteration) *iteration = c->iteration;
+    if (samples_in_pass) *samples_in_pass = c->per_tmp;
+    if (executing) *executing = c->executing ? 1 : 0;
     return RTPG_OK;
 }
 

@@ -6,10 +6,9 @@
 // SimpleTrace.cu for the unguided tracers).  Here the same per-path algorithm runs as a
 // wavefront over SoA path state, one frame of paths (one sample per pixel) per wave:
 //   raygen   camera rays, per-pixel Xorshift32 state from the seed buffer;
-//   extend   closest hit + shading of every active path: emission, BSDF / guide mixture
-//            sampling, NEE or RIS candidate selection (shadow ray left pending);
-//   connect  the pending shadow ray, the bounce radiance added to the path and to its earlier
-//            trace vertices, termination, compaction of survivors into the next queue;
+//   bounce   closest hit + shading of every active path: emission, BSDF / guide mixture
+//            sampling, NEE or RIS candidate selection and its shadow ray, the bounce radiance
+//            added to the path, termination, compaction of survivors into the next queue;
 //   finish   accumulation in FP64, seed write-back, and the commit of trace vertices into
 //            the SD-tree (TraceVertexT::Commit, OPX7UtilsPathGuiding.h:830-866) with the
 //            fixed-point atomics of the record kernel.
@@ -21,14 +20,20 @@
 
 #include "common.cuh"
 #include "bvh_dev.cuh"
+#include "hashgrid_dev.cuh"
+#include "mqt_dev.cuh"
 #include "sdtree_dev.cuh"
 #include "tracer_dev.cuh"
 
 struct rtpg_scene;
 struct rtpg_sdtree;
+struct rtpg_hashgrid;
+struct rtpg_mqt;
 namespace rtpg {
 SceneDev scene_device_view(const rtpg_scene* s);
 SDTreeDev sdtree_device_view(const rtpg_sdtree* t);
+HashGridDev hashgrid_device_view(const rtpg_hashgrid* h);
+MqtDev mqt_device_view(const rtpg_mqt* h);
 }
 
 namespace rtpg {
@@ -52,20 +57,23 @@ struct TracerDev {
     float3 eye, cu, cv, cw, bg;
     uint32_t width, height, npath, max_depth, num_candidates, flags;
     // path state
-    float3 *org, *dir, *thr, *col, *brad, *sdir, *scontrib;
-    float* sdist;
-    uint32_t *rng, *depth, *hflags, *pending;
+    float3 *org, *dir, *thr, *col;
+    uint32_t *rng, *depth, *hflags;
     uint32_t* queue[2];
     uint32_t* qcount;  // [0], [1]
     // trace vertices, [kTV][npath]
-    float3 *v_pos, *v_dir, *v_thr, *v_rad, *v_bsdf;
+    float3 *v_pos, *v_dir, *v_thr, *v_bsdf;
+    float3* b_rad;  // radiance of bounce k of every path, [max_depth][npath] (recording only)
     float *v_wopdf, *v_cos;
-    uint8_t* v_flags;  // bit0 valid (a DTree exists), bit1 delta
+    uint8_t* v_flags;  // bit0 valid (a DTree exists / a grid cell was found), bit1 delta
+    uint32_t* v_cell;  // hash-grid slot of the vertex (grid guide only)
     uint32_t* seeds;
     double* accum;  // 3 per pixel
     SDTreeDev tree;
+    HashGridDev grid;
+    MqtDev mqt;
     unsigned* status;
-    unsigned long long* counters;  // [0] extend visits (path-bounces), [1] shadow rays
+    unsigned long long* counters;  // [0] bounce visits (path-bounces), [1] shadow rays
 };
 
 // ------------------------------------------------------------------ raygen (SimpleGuide.cu:48-81)
@@ -125,229 +133,263 @@ __device__ __forceinline__ LightSample sample_light(const TracerDev& T, float3 p
     return l;
 }
 
-// ------------------------------------------------------------------ extend
-// __closesthit__radiance / __miss__radiance (SimpleGuide.cu:220-520) for every active path.
-__global__ void __launch_bounds__(kTB) k_extend(TracerDev T, int in) {
+// ------------------------------------------------------------------ bounce
+// One bounce of every active path: closest hit + shading (__closesthit__radiance /
+// __miss__radiance, SimpleGuide.cu:202-520), the NEE/RIS shadow ray traced right away as the
+// closest-hit program does, then the raygen bookkeeping (SimpleGuide.cu:85-114): bounce
+// radiance into the color (and, recording, into the per-bounce store from which k_finish forms
+// the trace-vertex radiance), termination, compaction of the survivors into the next queue.
+// Returns whether the path continues; *shadow tells whether a shadow ray was traced.
+__device__ __forceinline__ bool bounce_path(const TracerDev& T, uint32_t p, bool use_tree, bool use_grid, bool build,
+                                            bool recording, bool& shadow) {
+    const float3 org = T.org[p], in_dir = T.dir[p], prev_thr = T.thr[p];
+    const uint32_t d = T.depth[p], prev_flags = T.hflags[p];
+    const Hit h = bvh_trace<false>(T.scene, org.x, org.y, org.z, in_dir.x, in_dir.y, in_dir.z, 0.0001f, 1.0e20f);
+    const size_t vi = size_t(d < kTV ? d : 0) * T.npath + p;
+    bool pend = false;
+    float3 sdir = f3(0.f, 0.f, 0.f), scontrib = f3(0.f, 0.f, 0.f);
+    float sdist = 0.0f;
+    if (h.prim == 0xffffffffu) {
+        // __miss__radiance (SimpleGuide.cu:202-219): the ray keeps its direction
+        const float3 L = prev_thr * T.bg;
+        if (recording) T.b_rad[size_t(d) * T.npath + p] = L;
+        T.col[p] = T.col[p] + L;
+        if (recording && d < kTV) T.v_flags[vi] = 0;
+        return false;
+    }
+    uint32_t rng = T.rng[p];
+    const float* tv = T.tri_v + 9 * size_t(h.prim);
+    const float3 v0 = f3(tv[0], tv[1], tv[2]), v1 = f3(tv[3], tv[4], tv[5]), v2 = f3(tv[6], tv[7], tv[8]);
+    const float3 fn = unit3(cross3(v1 - v0, v2 - v0));
+    float3 position = org + h.t * in_dir;
+    const uint32_t mi = T.tri_mat[h.prim];
+    const Material m = T.mats[mi < T.num_materials ? mi : T.num_materials - 1];
+    float3 diffuse = m.diffuse;
+    if (m.tex >= 0 && T.tri_uv) {
+        const float* uv = T.tri_uv + 6 * size_t(h.prim);
+        const float w0 = 1.0f - h.u - h.v;
+        const float tu = w0 * uv[0] + h.u * uv[2] + h.v * uv[4];
+        const float tvv = w0 * uv[1] + h.u * uv[3] + h.v * uv[5];
+        diffuse = diffuse * tex_fetch(T, m.tex, tu, tvv);
+    }
+    const bool count_emitted = (prev_flags & HF_COUNT_EMITTED) || m.type == MAT_DEF_LIGHT;
+    float3 direction = f3(0.f, 0.f, 0.f), bsdf_val = f3(0.f, 0.f, 0.f), cur_thr = f3(0.f, 0.f, 0.f);
+    float cosine = 0.0f, bsdf_pdf = 0.0f, wo_pdf = 0.0f;
+    uint32_t flags = 0;
+    uint32_t dt = 0;
+    uint32_t cell = 0xffffffffu;  // hash-grid slot of this vertex (SimpleGuide2.cu: curGridIndex)
+    if (use_tree) dt = stree_lookup(T.tree.snode, T.tree.mn, T.tree.mx, position.x, position.y, position.z);
+    if (m.type == MAT_PHONG) {
+        uint32_t gbucket = 0, prv_cell = 0xffffffffu;
+        unsigned long long gkey = 0;
+        if (use_grid) {
+            gkey = hash_key(T.grid, position.x, position.y, position.z, gbucket);
+            prv_cell = hash_find_prv_key(T.grid, gkey, gbucket);
+        }
+        // With specular == 0 (every Lambertian surface) the Phong lobe only ever enters
+        // multiplied by zero: skip its math but draw its two random numbers, so the stream
+        // and every result stay bit-identical to the full evaluation.
+        const float ad = 1.0e-10f + avg3(diffuse), as = 1.0e-10f + avg3(m.specular);
+        const float sel = ad / (ad + as);
+        // (sel == 1 as well: then the lobe choice and the pdf mixture never use it either)
+        const bool glossy = m.specular.x != 0.0f || m.specular.y != 0.0f || m.specular.z != 0.0f || sel != 1.0f;
+        const float3 refl = unit3(reflect3(in_dir, fn));
+        const float3 d0 = sample_cosine(fn, rng);
+        float3 d1 = d0;
+        if (glossy) {
+            d1 = sample_phong(refl, m.shininess, rng);
+        } else {
+            xs32_next(rng);
+            xs32_next(rng);
+        }
+        const float c0 = dot3(d0, fn), c1 = dot3(d1, fn);
+        const float cp0 = fmaxf(c0 * kInvPi, 0.0f), cp1 = fmaxf(c1 * kInvPi, 0.0f);
+        const float pp0 = glossy ? phong_pdf(d0, refl, m.shininess) : 0.0f;
+        const float pp1 = glossy ? phong_pdf(d1, refl, m.shininess) : 0.0f;
+        const float sf = (m.shininess + 2.0f) / (m.shininess + 1.0f);
+        if (rnd1(rng) < sel) {
+            direction = d0; cosine = c0;
+            bsdf_val = diffuse * kInvPi + m.specular * sf * pp0;
+            bsdf_pdf = sel * cp0 + (1.0f - sel) * pp0;
+        } else {
+            direction = d1; cosine = c1;
+            bsdf_val = diffuse * kInvPi + m.specular * sf * pp1;
+            bsdf_pdf = sel * cp1 + (1.0f - sel) * pp1;
+        }
+        if (use_tree && build) {
+            const uint32_t soff = T.tree.s_off[dt];
+            const bool guided = dtree_mean(T.tree.s_statw[dt], T.tree.s_sum[dt]) > 0.0f;
+            if (rnd1(rng) < T.tree.fraction) {
+                const float2 c = dtree_sample_g(T.tree.s_nodes, soff, guided, rng);
+                direction = normalize3(canonical_to_dir(c.x, c.y));
+                cosine = dot3(direction, fn);
+                const float cp2 = fmaxf(cosine * kInvPi, 0.0f);
+                const float pp2 = glossy ? phong_pdf(direction, refl, m.shininess) : 0.0f;
+                bsdf_val = diffuse * kInvPi + m.specular * sf * pp2;
+                bsdf_pdf = sel * cp2 + (1.0f - sel) * pp2;
+            }
+            const float2 c = dir_to_canonical(direction.x, direction.y, direction.z);
+            const float dtree_pdf = fmaxf(dtree_pdf_g(T.tree.s_nodes, soff, guided, c.x, c.y), 0.0f);
+            wo_pdf = (1.0f - T.tree.fraction) * bsdf_pdf + T.tree.fraction * dtree_pdf;
+        } else if (use_grid && build && prv_cell != 0xffffffffu) {
+            // the Morton quadtree of the cell (SimpleGuide2.cu:350-377)
+            float dtree_pdf;
+            if (rnd1(rng) < T.mqt.fraction) {
+                float tp;
+                const float2 c = mqt_sample_and_pdf(T.mqt, prv_cell, rng, tp);
+                dtree_pdf = (float)((double)tp * (0.25 * kInvPiD));
+                direction = normalize3(canonical_to_dir(c.x, c.y));
+                cosine = dot3(direction, fn);
+                const float cp2 = fmaxf(cosine * kInvPi, 0.0f);
+                const float pp2 = glossy ? phong_pdf(direction, refl, m.shininess) : 0.0f;
+                bsdf_val = diffuse * kInvPi + m.specular * sf * pp2;
+                bsdf_pdf = sel * cp2 + (1.0f - sel) * pp2;
+            } else {
+                const float2 c = dir_to_canonical(direction.x, direction.y, direction.z);
+                const float tp = mqt_pdf(T.mqt, prv_cell, c.x, c.y);
+                dtree_pdf = fmaxf((float)((double)(tp * 0.25f) * kInvPiD), 0.0f);
+            }
+            wo_pdf = T.mqt.fraction * dtree_pdf + (1.0f - T.mqt.fraction) * bsdf_pdf;
+        } else {
+            wo_pdf = bsdf_pdf;
+        }
+        cur_thr = prev_thr * ((wo_pdf > 0.0f) ? (bsdf_val * fmaxf(cosine, 0.0f) / wo_pdf) : f3(0.f, 0.f, 0.f));
+        if (T.flags & RTPG_TRACE_FLAG_NEE) {
+            if (d < T.max_depth - 1 && T.light_count > 0) {
+                if (T.flags & RTPG_TRACE_FLAG_RIS) {
+                    // RIS over numCandidates light samples (SimpleGuide.cu:379-408)
+                    float w_sum = 0.0f, f_a_y = 0.0f, dist_y = 0.0f;
+                    uint32_t mcount = 0;
+                    float3 f_y = f3(0.f, 0.f, 0.f), ldir_y = f3(0.f, 0.f, 0.f);
+                    for (uint32_t c = 0; c < T.num_candidates; ++c) {
+                        const LightSample l = sample_light(T, position, rng);
+                        const float ndl = dot3(l.dir, fn), lndl = -dot3(l.dir, l.normal);
+                        const float3 b = glossy ? phong_bsdf(diffuse, m.specular, m.shininess, l.dir, refl)
+                                                : diffuse * kInvPi;
+                        const float g = fmaxf(ndl, 0.0f) * fmaxf(lndl, 0.0f) / (l.dist * l.dist);
+                        const float3 f = b * l.emission * g;
+                        const float fa = avg3(f);
+                        const float wi = fa * l.inv_pdf;
+                        // Reservoir::Update (SimpleKernel.h:124-143)
+                        w_sum += wi;
+                        ++mcount;
+                        if ((wi / w_sum) >= rnd1(rng)) {
+                            f_y = f; f_a_y = fa; ldir_y = l.dir; dist_y = l.dist;
+                        }
+                    }
+                    if (w_sum > 0.0f && f_a_y > 0.0f) {
+                        pend = true;
+                        sdir = ldir_y;
+                        sdist = dist_y - 0.0001f;
+                        scontrib = prev_thr * f_y * (w_sum / (f_a_y * (float)mcount));
+                    }
+                } else {
+                    // one light sample (SimpleGuide.cu:410-419)
+                    const LightSample l = sample_light(T, position, rng);
+                    const float3 b = glossy ? phong_bsdf(diffuse, m.specular, m.shininess, l.dir, refl)
+                                            : diffuse * kInvPi;
+                    const float g = fmaxf(-dot3(l.dir, l.normal), 0.0f) * fabsf(dot3(l.dir, fn)) / (l.dist * l.dist);
+                    pend = true;
+                    sdir = l.dir;
+                    sdist = l.dist - 0.0001f;
+                    scontrib = prev_thr * b * l.emission * g * l.inv_pdf;
+                }
+            }
+        } else {
+            flags |= HF_COUNT_EMITTED;
+        }
+        if (use_grid)
+            cell = ((T.flags & RTPG_TRACE_FLAG_LOCATE) && prv_cell == 0xffffffffu) ? hash_insert_cur_key(T.grid, gkey, gbucket)
+                                                                                  : prv_cell;
+    } else if (m.type == MAT_GLASS) {
+        // dielectric (SimpleGuide.cu:424-491), shading normal = face normal
+        float3 rn;
+        float rri;
+        float ci = dot3(fn, in_dir);
+        if (ci < 0.0f) { rn = fn; rri = 1.0f / m.ref_index; ci = -ci; }
+        else { rn = f3(-fn.x, -fn.y, -fn.z); rri = m.ref_index; }
+        const float so2 = (1.0f - ci * ci) * (rri * rri);
+        const float f0 = ((1.0f - rri) / (1.0f + rri)) * ((1.0f - rri) / (1.0f + rri));
+        const float om = 1.0f - ci;
+        const float fres = f0 + (1.0f - f0) * (om * om * om * om * om);
+        const float3 rd = unit3(reflect3(in_dir, rn));
+        if (rnd1(rng) < fres || so2 > 1.0f) {
+            position = position + 0.0001f * rn;
+            direction = rd;
+            cosine = fabsf(ci);
+            bsdf_val = m.specular;
+            cur_thr = prev_thr * m.specular;
+        } else {
+            position = position - 0.0001f * rn;
+            const float si2 = fmaxf(1.0f - ci * ci, 0.0f);
+            const float co = sqrtf(1.0f - so2);
+            float3 rf;
+            if (si2 > 0.0f) {
+                const float3 k = (in_dir + ci * rn) / sqrtf(si2);
+                rf = unit3(sqrtf(so2) * k - co * rn);
+            } else {
+                rf = in_dir;
+            }
+            direction = rf;
+            cosine = fabsf(dot3(rf, rn));
+            bsdf_val = f3(1.f, 1.f, 1.f);
+            cur_thr = prev_thr;
+        }
+        wo_pdf = fabsf(cosine);
+        bsdf_pdf = 0.0f;
+        flags |= HF_COUNT_EMITTED | HF_DELTA;
+    }
+    float3 rad = f3(0.f, 0.f, 0.f);
+    if (dot3(in_dir, fn) < 0.0f && count_emitted) rad = prev_thr * m.emission;
+    if (m.emission.x + m.emission.y + m.emission.z > 0.0f) flags |= HF_FINISH;
+    T.org[p] = position;
+    T.dir[p] = direction;
+    T.thr[p] = cur_thr;
+    T.hflags[p] = flags;
+    T.rng[p] = rng;
+    if (recording && d < kTV) {
+        T.v_pos[vi] = position;
+        T.v_dir[vi] = direction;
+        T.v_thr[vi] = cur_thr;
+        T.v_bsdf[vi] = bsdf_val;
+        T.v_wopdf[vi] = wo_pdf;
+        T.v_cos[vi] = cosine;
+        T.v_flags[vi] = (uint8_t)((use_grid ? (cell != 0xffffffffu ? 1u : 0u) : 1u) | ((flags & HF_DELTA) ? 2u : 0u));
+        if (use_grid) T.v_cell[vi] = cell;
+    }
+    float3 L = rad;
+    if (pend) {
+        shadow = true;
+        const Hit sh = bvh_trace<true>(T.scene, position.x, position.y, position.z, sdir.x, sdir.y, sdir.z, 0.0001f, sdist);
+        if (sh.prim == 0xffffffffu) L = L + scontrib;
+    }
+    if (recording) T.b_rad[size_t(d) * T.npath + p] = L;
+    T.col[p] = T.col[p] + L;
+    const bool bad = any_nan3(direction) || any_nan3(cur_thr) || any_nan3(L);
+    if (bad || (flags & HF_FINISH) || d >= T.max_depth - 1) return false;
+    T.depth[p] = d + 1;
+    return true;
+}
+
+__global__ void __launch_bounds__(kTB, 6) k_bounce(TracerDev T, int in) {
     const uint32_t n = T.qcount[in];
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         T.qcount[in ^ 1] = 0;
         atomicAdd(T.counters, (unsigned long long)n);
     }
     const bool use_tree = (T.flags & RTPG_TRACE_FLAG_USE_TREE) != 0;
+    const bool use_grid = (T.flags & RTPG_TRACE_FLAG_USE_GRID) != 0;
     const bool build = (T.flags & RTPG_TRACE_FLAG_BUILD) != 0;
-    const bool recording = use_tree && !(T.flags & RTPG_TRACE_FLAG_FINAL);
-    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
-        const uint32_t p = T.queue[in][q];
-        const float3 org = T.org[p], in_dir = T.dir[p], prev_thr = T.thr[p];
-        const uint32_t d = T.depth[p], prev_flags = T.hflags[p];
-        const Hit h = bvh_trace<false>(T.scene, org.x, org.y, org.z, in_dir.x, in_dir.y, in_dir.z, 0.0001f, 1.0e20f);
-        const size_t vi = size_t(d < kTV ? d : 0) * T.npath + p;
-        T.pending[p] = 0;
-        if (h.prim == 0xffffffffu) {
-            // __miss__radiance (SimpleGuide.cu:202-219)
-            T.brad[p] = prev_thr * T.bg;
-            T.hflags[p] = HF_FINISH;
-            T.thr[p] = prev_thr;
-            if (recording && d < kTV) T.v_flags[vi] = 0;
-            continue;
-        }
-        uint32_t rng = T.rng[p];
-        const float* tv = T.tri_v + 9 * size_t(h.prim);
-        const float3 v0 = f3(tv[0], tv[1], tv[2]), v1 = f3(tv[3], tv[4], tv[5]), v2 = f3(tv[6], tv[7], tv[8]);
-        const float3 fn = unit3(cross3(v1 - v0, v2 - v0));
-        float3 position = org + h.t * in_dir;
-        const uint32_t mi = T.tri_mat[h.prim];
-        const Material m = T.mats[mi < T.num_materials ? mi : T.num_materials - 1];
-        float3 diffuse = m.diffuse;
-        if (m.tex >= 0 && T.tri_uv) {
-            const float* uv = T.tri_uv + 6 * size_t(h.prim);
-            const float w0 = 1.0f - h.u - h.v;
-            const float tu = w0 * uv[0] + h.u * uv[2] + h.v * uv[4];
-            const float tvv = w0 * uv[1] + h.u * uv[3] + h.v * uv[5];
-            diffuse = diffuse * tex_fetch(T, m.tex, tu, tvv);
-        }
-        const bool count_emitted = (prev_flags & HF_COUNT_EMITTED) || m.type == MAT_DEF_LIGHT;
-        float3 direction = f3(0.f, 0.f, 0.f), bsdf_val = f3(0.f, 0.f, 0.f), cur_thr = f3(0.f, 0.f, 0.f);
-        float cosine = 0.0f, bsdf_pdf = 0.0f, wo_pdf = 0.0f;
-        uint32_t flags = 0;
-        uint32_t dt = 0;
-        if (use_tree) dt = stree_lookup(T.tree.snode, T.tree.mn, T.tree.mx, position.x, position.y, position.z);
-        if (m.type == MAT_PHONG) {
-            const float3 refl = unit3(reflect3(in_dir, fn));
-            const float3 d0 = sample_cosine(fn, rng);
-            const float3 d1 = sample_phong(refl, m.shininess, rng);
-            const float c0 = dot3(d0, fn), c1 = dot3(d1, fn);
-            const float cp0 = fmaxf(c0 * kInvPi, 0.0f), cp1 = fmaxf(c1 * kInvPi, 0.0f);
-            const float pp0 = phong_pdf(d0, refl, m.shininess), pp1 = phong_pdf(d1, refl, m.shininess);
-            const float ad = 1.0e-10f + avg3(diffuse), as = 1.0e-10f + avg3(m.specular);
-            const float sel = ad / (ad + as);
-            const float sf = (m.shininess + 2.0f) / (m.shininess + 1.0f);
-            if (rnd1(rng) < sel) {
-                direction = d0; cosine = c0;
-                bsdf_val = diffuse * kInvPi + m.specular * sf * pp0;
-                bsdf_pdf = sel * cp0 + (1.0f - sel) * pp0;
-            } else {
-                direction = d1; cosine = c1;
-                bsdf_val = diffuse * kInvPi + m.specular * sf * pp1;
-                bsdf_pdf = sel * cp1 + (1.0f - sel) * pp1;
-            }
-            if (use_tree && build) {
-                const uint32_t soff = T.tree.s_off[dt];
-                const bool guided = dtree_mean(T.tree.s_statw[dt], T.tree.s_sum[dt]) > 0.0f;
-                if (rnd1(rng) < T.tree.fraction) {
-                    const float2 c = dtree_sample_g(T.tree.s_nodes, soff, guided, rng);
-                    direction = normalize3(canonical_to_dir(c.x, c.y));
-                    cosine = dot3(direction, fn);
-                    const float cp2 = fmaxf(cosine * kInvPi, 0.0f);
-                    const float pp2 = phong_pdf(direction, refl, m.shininess);
-                    bsdf_val = diffuse * kInvPi + m.specular * sf * pp2;
-                    bsdf_pdf = sel * cp2 + (1.0f - sel) * pp2;
-                }
-                const float2 c = dir_to_canonical(direction.x, direction.y, direction.z);
-                const float dtree_pdf = fmaxf(dtree_pdf_g(T.tree.s_nodes, soff, guided, c.x, c.y), 0.0f);
-                wo_pdf = (1.0f - T.tree.fraction) * bsdf_pdf + T.tree.fraction * dtree_pdf;
-            } else {
-                wo_pdf = bsdf_pdf;
-            }
-            cur_thr = prev_thr * ((wo_pdf > 0.0f) ? (bsdf_val * fmaxf(cosine, 0.0f) / wo_pdf) : f3(0.f, 0.f, 0.f));
-            if (T.flags & RTPG_TRACE_FLAG_NEE) {
-                if (d < T.max_depth - 1 && T.light_count > 0) {
-                    if (T.flags & RTPG_TRACE_FLAG_RIS) {
-                        // RIS over numCandidates light samples (SimpleGuide.cu:379-408)
-                        float w_sum = 0.0f, f_a_y = 0.0f, dist_y = 0.0f;
-                        uint32_t mcount = 0;
-                        float3 f_y = f3(0.f, 0.f, 0.f), ldir_y = f3(0.f, 0.f, 0.f);
-                        for (uint32_t c = 0; c < T.num_candidates; ++c) {
-                            const LightSample l = sample_light(T, position, rng);
-                            const float ndl = dot3(l.dir, fn), lndl = -dot3(l.dir, l.normal);
-                            const float3 b = phong_bsdf(diffuse, m.specular, m.shininess, l.dir, refl);
-                            const float g = fmaxf(ndl, 0.0f) * fmaxf(lndl, 0.0f) / (l.dist * l.dist);
-                            const float3 f = b * l.emission * g;
-                            const float fa = avg3(f);
-                            const float wi = fa * l.inv_pdf;
-                            // Reservoir::Update (SimpleKernel.h:124-143)
-                            w_sum += wi;
-                            ++mcount;
-                            if ((wi / w_sum) >= rnd1(rng)) {
-                                f_y = f; f_a_y = fa; ldir_y = l.dir; dist_y = l.dist;
-                            }
-                        }
-                        if (w_sum > 0.0f && f_a_y > 0.0f) {
-                            T.pending[p] = 1;
-                            T.sdir[p] = ldir_y;
-                            T.sdist[p] = dist_y - 0.0001f;
-                            T.scontrib[p] = prev_thr * f_y * (w_sum / (f_a_y * (float)mcount));
-                        }
-                    } else {
-                        // one light sample (SimpleGuide.cu:410-419)
-                        const LightSample l = sample_light(T, position, rng);
-                        const float3 b = phong_bsdf(diffuse, m.specular, m.shininess, l.dir, refl);
-                        const float g = fmaxf(-dot3(l.dir, l.normal), 0.0f) * fabsf(dot3(l.dir, fn)) / (l.dist * l.dist);
-                        T.pending[p] = 1;
-                        T.sdir[p] = l.dir;
-                        T.sdist[p] = l.dist - 0.0001f;
-                        T.scontrib[p] = prev_thr * b * l.emission * g * l.inv_pdf;
-                    }
-                }
-            } else {
-                flags |= HF_COUNT_EMITTED;
-            }
-        } else if (m.type == MAT_GLASS) {
-            // dielectric (SimpleGuide.cu:424-491), shading normal = face normal
-            float3 rn;
-            float rri;
-            float ci = dot3(fn, in_dir);
-            if (ci < 0.0f) { rn = fn; rri = 1.0f / m.ref_index; ci = -ci; }
-            else { rn = f3(-fn.x, -fn.y, -fn.z); rri = m.ref_index; }
-            const float so2 = (1.0f - ci * ci) * (rri * rri);
-            const float f0 = ((1.0f - rri) / (1.0f + rri)) * ((1.0f - rri) / (1.0f + rri));
-            const float om = 1.0f - ci;
-            const float fres = f0 + (1.0f - f0) * (om * om * om * om * om);
-            const float3 rd = unit3(reflect3(in_dir, rn));
-            if (rnd1(rng) < fres || so2 > 1.0f) {
-                position = position + 0.0001f * rn;
-                direction = rd;
-                cosine = fabsf(ci);
-                bsdf_val = m.specular;
-                cur_thr = prev_thr * m.specular;
-            } else {
-                position = position - 0.0001f * rn;
-                const float si2 = fmaxf(1.0f - ci * ci, 0.0f);
-                const float co = sqrtf(1.0f - so2);
-                float3 rf;
-                if (si2 > 0.0f) {
-                    const float3 k = (in_dir + ci * rn) / sqrtf(si2);
-                    rf = unit3(sqrtf(so2) * k - co * rn);
-                } else {
-                    rf = in_dir;
-                }
-                direction = rf;
-                cosine = fabsf(dot3(rf, rn));
-                bsdf_val = f3(1.f, 1.f, 1.f);
-                cur_thr = prev_thr;
-            }
-            wo_pdf = fabsf(cosine);
-            bsdf_pdf = 0.0f;
-            flags |= HF_COUNT_EMITTED | HF_DELTA;
-        }
-        float3 rad = f3(0.f, 0.f, 0.f);
-        if (dot3(in_dir, fn) < 0.0f && count_emitted) rad = prev_thr * m.emission;
-        if (m.emission.x + m.emission.y + m.emission.z > 0.0f) flags |= HF_FINISH;
-        T.brad[p] = rad;
-        T.org[p] = position;
-        T.dir[p] = direction;
-        T.thr[p] = cur_thr;
-        T.hflags[p] = flags;
-        T.rng[p] = rng;
-        if (recording && d < kTV) {
-            T.v_pos[vi] = position;
-            T.v_dir[vi] = direction;
-            T.v_thr[vi] = cur_thr;
-            T.v_rad[vi] = f3(0.f, 0.f, 0.f);
-            T.v_bsdf[vi] = bsdf_val;
-            T.v_wopdf[vi] = wo_pdf;
-            T.v_cos[vi] = cosine;
-            T.v_flags[vi] = (uint8_t)(1u | ((flags & HF_DELTA) ? 2u : 0u));
-        }
-    }
-}
-
-// ------------------------------------------------------------------ connect
-// Shadow ray of the pending NEE/RIS sample, then the raygen bookkeeping of one bounce
-// (SimpleGuide.cu:85-114): radiance into earlier trace vertices, color, termination.
-__global__ void __launch_bounds__(kTB) k_connect(TracerDev T, int in) {
-    const uint32_t n = T.qcount[in];
-    const bool recording = (T.flags & RTPG_TRACE_FLAG_USE_TREE) && !(T.flags & RTPG_TRACE_FLAG_FINAL);
+    const bool recording = (use_tree || use_grid) && !(T.flags & RTPG_TRACE_FLAG_FINAL);
     for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
         const uint32_t q = base + threadIdx.x;
-        bool keep = false;
+        bool keep = false, shadow = false;
         uint32_t p = 0;
         if (q < n) {
             p = T.queue[in][q];
-            float3 L = T.brad[p];
-            if (T.pending[p]) {
-                const float3 o = T.org[p], sd = T.sdir[p];
-                const Hit h = bvh_trace<true>(T.scene, o.x, o.y, o.z, sd.x, sd.y, sd.z, 0.0001f, T.sdist[p]);
-                if (h.prim == 0xffffffffu) L = L + T.scontrib[p];
-            }
-            const uint32_t d = T.depth[p];
-            if (recording) {
-                const uint32_t tvd = d < kTV ? d : kTV;
-                for (uint32_t i = 0; i < tvd; ++i) {
-                    const size_t vi = size_t(i) * T.npath + p;
-                    T.v_rad[vi] = T.v_rad[vi] + L;
-                }
-            }
-            T.col[p] = T.col[p] + L;
-            const float3 dr = T.dir[p], th = T.thr[p];
-            const bool bad = any_nan3(dr) || any_nan3(th) || any_nan3(L);
-            const bool done = bad || (T.hflags[p] & HF_FINISH) || d >= T.max_depth - 1;
-            if (!done) {
-                T.depth[p] = d + 1;
-                keep = true;
-            }
+            keep = bounce_path(T, p, use_tree, use_grid, build, recording, shadow);
         }
-        const unsigned sh = __ballot_sync(0xffffffffu, q < n && T.pending[p]);
+        const unsigned sh = __ballot_sync(0xffffffffu, shadow);
         if ((threadIdx.x & 31) == 0 && sh) atomicAdd(T.counters + 1, (unsigned long long)__popc(sh));
         // warp-aggregated append to the next queue
         const unsigned m = __ballot_sync(0xffffffffu, keep);
@@ -363,9 +405,12 @@ __global__ void __launch_bounds__(kTB) k_connect(TracerDev T, int in) {
 
 // ------------------------------------------------------------------ finish
 // Accumulate, write the seed back, commit trace vertices (TraceVertexT::Commit,
-// OPX7UtilsPathGuiding.h:830-866 -> DTreeWrapperT::Record :514-520 with stat-weight 1).
+// OPX7UtilsPathGuiding.h:830-866 -> DTreeWrapperT::Record :514-520 with stat-weight 1, or
+// MortonTraceVertexT::Commit for the grid guide).
 __global__ void __launch_bounds__(kTB) k_finish(TracerDev T) {
-    const bool recording = (T.flags & RTPG_TRACE_FLAG_USE_TREE) && !(T.flags & RTPG_TRACE_FLAG_FINAL);
+    const bool use_grid = (T.flags & RTPG_TRACE_FLAG_USE_GRID) != 0;
+    const bool recording = (T.flags & (RTPG_TRACE_FLAG_USE_TREE | RTPG_TRACE_FLAG_USE_GRID)) &&
+                           !(T.flags & RTPG_TRACE_FLAG_FINAL);
     for (uint32_t base = blockIdx.x * blockDim.x; base < T.npath; base += gridDim.x * blockDim.x) {
         const uint32_t p = base + threadIdx.x;
         uint32_t nv = 0;
@@ -379,12 +424,29 @@ __global__ void __launch_bounds__(kTB) k_finish(TracerDev T) {
             const uint32_t d = T.depth[p];
             nv = recording ? (d < kTV ? d : kTV) : 0;
         }
+        // radiance of vertex i = L_{i+1} + L_{i+2} + ... added in bounce order, exactly the
+        // float sums RTLib's raygen loop accumulates into traceVertices[i].radiance; each
+        // bounce radiance is read once and added to every earlier vertex in registers
+        const uint32_t dfin = nv ? T.depth[p] : 0u;
+        float3 acc[kTV];
+#pragma unroll
+        for (int i = 0; i < kTV; ++i) acc[i] = f3(0.f, 0.f, 0.f);
+        for (uint32_t k = 1; k <= dfin; ++k) {
+            const float3 L = T.b_rad[size_t(k) * T.npath + p];
+#pragma unroll
+            for (uint32_t i = 0; i < kTV; ++i)
+                if (i < k) acc[i] = acc[i] + L;
+        }
         for (uint32_t i = 0; i < kTV; ++i) {  // warp-uniform loop for the aggregated atomics
             unsigned long long k_w = ~0ull, k_s = ~0ull, v_w = 0, v_s = 0;
             if (i < nv) {
                 const size_t vi = size_t(i) * T.npath + p;
                 const uint8_t vf = T.v_flags[vi];
-                const float3 rad = T.v_rad[vi], bv = T.v_bsdf[vi], th = T.v_thr[vi];
+                float3 rad = acc[0];
+#pragma unroll
+                for (uint32_t j = 1; j < kTV; ++j)
+                    if (j == i) rad = acc[j];
+                const float3 bv = T.v_bsdf[vi], th = T.v_thr[vi];
                 const float wo = T.v_wopdf[vi];
                 const bool ok_r = isfinite(rad.x) && rad.x >= 0.f && isfinite(rad.y) && rad.y >= 0.f &&
                                   isfinite(rad.z) && rad.z >= 0.f;
@@ -397,20 +459,36 @@ __global__ void __launch_bounds__(kTB) k_finish(TracerDev T) {
                     if (th.z * wo > 1e-4f) lr.z = rad.z / th.z;
                     lr = lr * fabsf(T.v_cos[vi]);
                     const float lavg = (lr.x + lr.y + lr.z) / 3.0f;
-                    const float3 pos = T.v_pos[vi], dr = T.v_dir[vi];
-                    const uint32_t dt = stree_lookup(T.tree.snode, T.tree.mn, T.tree.mx, pos.x, pos.y, pos.z);
-                    k_w = dt;
-                    v_w = to_fx(1.0f, T.tree.fx, T.tree.status);
+                    const float3 dr = T.v_dir[vi];
                     const float irr = __fdiv_rn(lavg, wo);
-                    if (isfinite(irr) && irr > 0.0f) {
-                        const float2 c = dir_to_canonical(dr.x, dr.y, dr.z);
-                        k_s = dtree_record_slot(T.tree.b_child, T.tree.b_off[dt], c.x, c.y);
-                        v_s = to_fx(irr, T.tree.fx, T.tree.status);
+                    if (use_grid) {
+                        // MortonTraceVertexT::Commit (OPX7UtilsMorton.h:550-585) ->
+                        // MortonQuadTreeWrapperT::Record: leaf of the cell's building quadtree
+                        if (isfinite(irr) && irr > 0.0f) {
+                            const uint32_t cell = T.v_cell[vi];
+                            const float2 c = dir_to_canonical(dr.x, dr.y, dr.z);
+                            k_s = ((unsigned long long)cell << (2 * T.mqt.level)) + mqt_leaf_code(T.mqt.level, c.x, c.y);
+                            v_s = to_fx(irr, T.mqt.fx, T.mqt.status);
+                        }
+                    } else {
+                        const float3 pos = T.v_pos[vi];
+                        const uint32_t dt = stree_lookup(T.tree.snode, T.tree.mn, T.tree.mx, pos.x, pos.y, pos.z);
+                        k_w = dt;
+                        v_w = to_fx(1.0f, T.tree.fx, T.tree.status);
+                        if (isfinite(irr) && irr > 0.0f) {
+                            const float2 c = dir_to_canonical(dr.x, dr.y, dr.z);
+                            k_s = dtree_record_slot(T.tree.b_child, T.tree.b_off[dt], c.x, c.y);
+                            v_s = to_fx(irr, T.tree.fx, T.tree.status);
+                        }
                     }
                 }
             }
-            warp_add_u64(k_w, v_w, T.tree.b_statw);
-            warp_add_u64(k_s, v_s, T.tree.b_sums);
+            if (use_grid) {
+                warp_add_u64(k_s, v_s, T.mqt.leaves);
+            } else {
+                warp_add_u64(k_w, v_w, T.tree.b_statw);
+                warp_add_u64(k_s, v_s, T.tree.b_sums);
+            }
         }
     }
 }
@@ -440,16 +518,18 @@ struct rtpg_tracer {
     uint2* d_tex_wh = nullptr;
     uint32_t seed = 1;
     bool timing = false;
-    double t_ms[4] = {0, 0, 0, 0};  // raygen, extend, connect, finish
-    uint64_t t_launch[4] = {0, 0, 0, 0};
+    double t_ms[3] = {0, 0, 0};  // raygen, bounce, finish
+    uint64_t t_launch[3] = {0, 0, 0};
     cudaEvent_t ev[8] = {};
     uint64_t samples = 0;
     uint64_t paths = 0;
     struct Cached {
         cudaGraphExec_t exec;
         SDTreeDev tree;
+        HashGridDev grid;
+        MqtDev mqt;
     };
-    std::map<uint32_t, Cached> graphs;  // keyed by flags; the tree view is compared on use
+    std::map<uint32_t, Cached> graphs;  // keyed by flags; the guide views are compared on use
     template <class T>
     int alloc(T** p, size_t count) {
         void* q = nullptr;
@@ -481,8 +561,6 @@ static int timed_wave(rtpg_tracer* h, cudaStream_t st) {
     const int g = kSMs * 8;
     for (auto& e : h->ev)
         if (!e) RTPG_CUDA(cudaEventCreate(&e));
-    std::vector<cudaEvent_t> marks;
-    std::vector<int> kind;
     cudaEventRecord(h->ev[0], st);
     k_raygen<<<g, kTB, 0, st>>>(T);
     cudaEventRecord(h->ev[1], st);
@@ -493,25 +571,20 @@ static int timed_wave(rtpg_tracer* h, cudaStream_t st) {
     h->t_launch[0] += 1;
     for (uint32_t b = 0; b < T.max_depth; ++b) {
         cudaEventRecord(h->ev[2], st);
-        k_extend<<<g, kTB, 0, st>>>(T, int(b & 1));
+        k_bounce<<<g, kTB, 0, st>>>(T, int(b & 1));
         cudaEventRecord(h->ev[3], st);
-        k_connect<<<g, kTB, 0, st>>>(T, int(b & 1));
-        cudaEventRecord(h->ev[4], st);
-        RTPG_CUDA(cudaEventSynchronize(h->ev[4]));
+        RTPG_CUDA(cudaEventSynchronize(h->ev[3]));
         cudaEventElapsedTime(&ms, h->ev[2], h->ev[3]);
         h->t_ms[1] += ms;
-        cudaEventElapsedTime(&ms, h->ev[3], h->ev[4]);
-        h->t_ms[2] += ms;
         h->t_launch[1] += 1;
-        h->t_launch[2] += 1;
     }
-    cudaEventRecord(h->ev[5], st);
+    cudaEventRecord(h->ev[4], st);
     k_finish<<<g, kTB, 0, st>>>(T);
-    cudaEventRecord(h->ev[6], st);
-    RTPG_CUDA(cudaEventSynchronize(h->ev[6]));
-    cudaEventElapsedTime(&ms, h->ev[5], h->ev[6]);
-    h->t_ms[3] += ms;
-    h->t_launch[3] += 1;
+    cudaEventRecord(h->ev[5], st);
+    RTPG_CUDA(cudaEventSynchronize(h->ev[5]));
+    cudaEventElapsedTime(&ms, h->ev[4], h->ev[5]);
+    h->t_ms[2] += ms;
+    h->t_launch[2] += 1;
     RTPG_LAUNCH_CHECK();
     return RTPG_OK;
 }
@@ -521,8 +594,7 @@ static void launch_wave(rtpg_tracer* h, cudaStream_t st) {
     const int g = kSMs * 8;
     k_raygen<<<g, kTB, 0, st>>>(T);
     for (uint32_t b = 0; b < T.max_depth; ++b) {
-        k_extend<<<g, kTB, 0, st>>>(T, int(b & 1));
-        k_connect<<<g, kTB, 0, st>>>(T, int(b & 1));
+        k_bounce<<<g, kTB, 0, st>>>(T, int(b & 1));
     }
     k_finish<<<g, kTB, 0, st>>>(T);
 }
@@ -569,13 +641,12 @@ int rtpg_tracer_create(rtpg_scene* scene, const float* tri_vertices, const uint3
     if ((r = h->alloc(&mats, num_materials)) || (r = h->alloc(&lmesh, std::max(num_light_meshes, 1u))) ||
         (r = h->alloc(&lemit, std::max(num_light_meshes, 1u))) || (r = h->alloc(&T.org, P)) ||
         (r = h->alloc(&T.dir, P)) || (r = h->alloc(&T.thr, P)) || (r = h->alloc(&T.col, P)) ||
-        (r = h->alloc(&T.brad, P)) || (r = h->alloc(&T.sdir, P)) || (r = h->alloc(&T.scontrib, P)) ||
-        (r = h->alloc(&T.sdist, P)) || (r = h->alloc(&T.rng, P)) || (r = h->alloc(&T.depth, P)) ||
-        (r = h->alloc(&T.hflags, P)) || (r = h->alloc(&T.pending, P)) || (r = h->alloc(&T.queue[0], P)) ||
+        (r = h->alloc(&T.rng, P)) || (r = h->alloc(&T.depth, P)) ||
+        (r = h->alloc(&T.hflags, P)) || (r = h->alloc(&T.queue[0], P)) ||
         (r = h->alloc(&T.queue[1], P)) || (r = h->alloc(&T.qcount, 2)) || (r = h->alloc(&T.v_pos, P * kTV)) ||
-        (r = h->alloc(&T.v_dir, P * kTV)) || (r = h->alloc(&T.v_thr, P * kTV)) || (r = h->alloc(&T.v_rad, P * kTV)) ||
+        (r = h->alloc(&T.v_dir, P * kTV)) || (r = h->alloc(&T.v_thr, P * kTV)) || (r = h->alloc(&T.b_rad, P * std::max<uint32_t>(D.max_depth, 1))) ||
         (r = h->alloc(&T.v_bsdf, P * kTV)) || (r = h->alloc(&T.v_wopdf, P * kTV)) ||
-        (r = h->alloc(&T.v_cos, P * kTV)) || (r = h->alloc(&T.v_flags, P * kTV)) || (r = h->alloc(&T.seeds, P)) ||
+        (r = h->alloc(&T.v_cos, P * kTV)) || (r = h->alloc(&T.v_flags, P * kTV)) || (r = h->alloc(&T.v_cell, P * kTV)) || (r = h->alloc(&T.seeds, P)) ||
         (r = h->alloc(&T.accum, 3 * P)) || (r = h->alloc(&T.status, 1)) || (r = h->alloc(&T.counters, 2)) || (r = h->alloc(&h->d_tex, 64)) ||
         (r = h->alloc(&h->d_tex_wh, 64))) {
         delete h;
@@ -665,22 +736,24 @@ int rtpg_tracer_set_seed(rtpg_tracer* h, uint32_t seed) {
     return RTPG_OK;
 }
 
-// One launch of `spp` samples per pixel with the given RTPG_TRACE_FLAG_* (PARAM_FLAG_*,
-// SimpleKernel.h:145-154).  tree may be NULL when RTPG_TRACE_FLAG_USE_TREE is not set.
-int rtpg_tracer_render(rtpg_tracer* h, uint32_t spp, uint32_t flags, rtpg_sdtree* tree, void* stream) {
-    if (!h) return fail(RTPG_EINVAL, "rtpg_tracer_render: null handle");
-    if ((flags & RTPG_TRACE_FLAG_USE_TREE) && !tree) return fail(RTPG_EINVAL, "rtpg_tracer_render: USE_TREE without a tree");
+static int check_render(rtpg_tracer* h, uint32_t flags, const char* fn) {
     if ((flags & RTPG_TRACE_FLAG_RIS) && !(flags & RTPG_TRACE_FLAG_NEE))
-        return fail(RTPG_EINVAL, "rtpg_tracer_render: RIS requires NEE");
+        return fail(RTPG_EINVAL, "%s: RIS requires NEE", fn);
+    if ((flags & RTPG_TRACE_FLAG_USE_TREE) && (flags & RTPG_TRACE_FLAG_USE_GRID))
+        return fail(RTPG_EINVAL, "%s: USE_TREE and USE_GRID are exclusive", fn);
     for (int32_t t : h->mat_tex)
         if (t >= 0 && (size_t(t) >= h->tex_ptr.size() || !h->tex_ptr[t]))
-            return fail(RTPG_EINVAL, "rtpg_tracer_render: material texture %d was never set", t);
-    if (h->dev.scene.ntris == 0) return fail(RTPG_EINVAL, "rtpg_tracer_render: empty scene");
-    cudaStream_t st = as_stream(stream);
+            return fail(RTPG_EINVAL, "%s: material texture %d was never set", fn, t);
+    if (h->dev.scene.ntris == 0) return fail(RTPG_EINVAL, "%s: empty scene", fn);
+    return RTPG_OK;
+}
+
+// `spp` waves with the flags and guide views already in h->dev.  A captured wave bakes in
+// the kernel arguments, so it is reused only for the same flags and identical guide views
+// (the same device arrays).
+static int render_waves(rtpg_tracer* h, uint32_t spp, uint32_t flags, cudaStream_t st) {
     h->dev.flags = flags;
-    if (tree) h->dev.tree = sdtree_device_view(tree);
     if (h->timing) {
-        if (!tree) memset(&h->dev.tree, 0, sizeof(SDTreeDev));
         for (uint32_t s = 0; s < spp; ++s) {
             int r = timed_wave(h, st);
             if (r) return r;
@@ -689,12 +762,11 @@ int rtpg_tracer_render(rtpg_tracer* h, uint32_t spp, uint32_t flags, rtpg_sdtree
         h->paths += uint64_t(spp) * h->dev.npath;
         return RTPG_OK;
     }
-    // a captured wave bakes in the kernel arguments, so it is reused only for the same flags
-    // and an identical tree view (same device arrays)
-    if (!tree) memset(&h->dev.tree, 0, sizeof(SDTreeDev));
     auto it = h->graphs.find(flags);
     cudaGraphExec_t exec = nullptr;
-    if (it != h->graphs.end() && memcmp(&it->second.tree, &h->dev.tree, sizeof(SDTreeDev)) == 0) {
+    if (it != h->graphs.end() && memcmp(&it->second.tree, &h->dev.tree, sizeof(SDTreeDev)) == 0 &&
+        memcmp(&it->second.grid, &h->dev.grid, sizeof(HashGridDev)) == 0 &&
+        memcmp(&it->second.mqt, &h->dev.mqt, sizeof(MqtDev)) == 0) {
         exec = it->second.exec;
     } else {
         if (it != h->graphs.end()) {
@@ -713,12 +785,46 @@ int rtpg_tracer_render(rtpg_tracer* h, uint32_t spp, uint32_t flags, rtpg_sdtree
         if (g) cudaGraphDestroy(g);
         cudaStreamDestroy(cs);
         if (e != cudaSuccess) return fail(RTPG_ECUDA, "rtpg_tracer_render: graph capture failed: %s", cudaGetErrorString(e));
-        h->graphs[flags] = {exec, h->dev.tree};
+        h->graphs[flags] = {exec, h->dev.tree, h->dev.grid, h->dev.mqt};
     }
     for (uint32_t s = 0; s < spp; ++s) RTPG_CUDA(cudaGraphLaunch(exec, st));
     h->samples += spp;
     h->paths += uint64_t(spp) * h->dev.npath;
     return RTPG_OK;
+}
+
+// One launch of `spp` samples per pixel with the given RTPG_TRACE_FLAG_* (PARAM_FLAG_*,
+// SimpleKernel.h:145-158).  tree may be NULL when RTPG_TRACE_FLAG_USE_TREE is not set.
+int rtpg_tracer_render(rtpg_tracer* h, uint32_t spp, uint32_t flags, rtpg_sdtree* tree, void* stream) {
+    if (!h) return fail(RTPG_EINVAL, "rtpg_tracer_render: null handle");
+    if ((flags & RTPG_TRACE_FLAG_USE_TREE) && !tree) return fail(RTPG_EINVAL, "rtpg_tracer_render: USE_TREE without a tree");
+    if (flags & (RTPG_TRACE_FLAG_USE_GRID | RTPG_TRACE_FLAG_LOCATE))
+        return fail(RTPG_EINVAL, "rtpg_tracer_render: grid flags need rtpg_tracer_render_grid");
+    int r = check_render(h, flags, "rtpg_tracer_render");
+    if (r) return r;
+    memset(&h->dev.grid, 0, sizeof(HashGridDev));
+    memset(&h->dev.mqt, 0, sizeof(MqtDev));
+    if (tree) h->dev.tree = sdtree_device_view(tree);
+    else memset(&h->dev.tree, 0, sizeof(SDTreeDev));
+    return render_waves(h, spp, flags, as_stream(stream));
+}
+
+// One launch guided by the hash grid and its Morton quadtrees (the HT* tracers of
+// SimpleGuide2.cu).
+int rtpg_tracer_render_grid(rtpg_tracer* h, uint32_t spp, uint32_t flags, rtpg_hashgrid* grid, rtpg_mqt* mqt,
+                            void* stream) {
+    if (!h || !grid || !mqt) return fail(RTPG_EINVAL, "rtpg_tracer_render_grid: null argument");
+    if (!(flags & RTPG_TRACE_FLAG_USE_GRID)) return fail(RTPG_EINVAL, "rtpg_tracer_render_grid: USE_GRID not set");
+    int r = check_render(h, flags, "rtpg_tracer_render_grid");
+    if (r) return r;
+    const HashGridDev g = hashgrid_device_view(grid);
+    const MqtDev q = mqt_device_view(mqt);
+    if (q.ncells < g.nslots)
+        return fail(RTPG_EINVAL, "rtpg_tracer_render_grid: %u quadtrees for %u grid slots", q.ncells, g.nslots);
+    memset(&h->dev.tree, 0, sizeof(SDTreeDev));
+    h->dev.grid = g;
+    h->dev.mqt = q;
+    return render_waves(h, spp, flags, as_stream(stream));
 }
 
 // Mean radiance per pixel (accumulation / samples), RGB float, row-major, y = 0 first.
@@ -761,6 +867,32 @@ int rtpg_tracer_render_guided(rtpg_tracer* h, rtpg_sdtree* tree, rtpg_controller
     return RTPG_OK;
 }
 
+// TracePipeline for the HT* tracers (RTLibExtOPX7TestApplication.cpp:2174-2222): flags by
+// the Morton controller's state, the grid's current table copied to the previous one after
+// every finished pass (GetSamplePerTmp() == 0 after EndTrace).
+int rtpg_tracer_render_grid_guided(rtpg_tracer* h, rtpg_hashgrid* grid, rtpg_mqt* mqt, rtpg_mqt_controller* ctrl,
+                                   uint32_t base_flags, uint32_t samples_per_launch, uint32_t max_launches,
+                                   void* stream) {
+    if (!h || !grid || !mqt || !ctrl) return fail(RTPG_EINVAL, "rtpg_tracer_render_grid_guided: null argument");
+    int r;
+    for (uint32_t k = 0; k < max_launches; ++k) {
+        if ((r = rtpg_mqt_controller_begin(ctrl, stream))) return r;
+        int32_t state, executing;
+        uint32_t it, tmp;
+        rtpg_mqt_controller_get(ctrl, &state, &it, &tmp, &executing);
+        if (!executing) break;
+        uint32_t flags = (base_flags & (RTPG_TRACE_FLAG_NEE | RTPG_TRACE_FLAG_RIS)) | RTPG_TRACE_FLAG_USE_GRID;
+        if (state == RTPG_MQT_TRACE_LOCATE) flags |= RTPG_TRACE_FLAG_LOCATE;
+        if (state == RTPG_MQT_TRACE_RECORD_AND_SAMPLE) flags |= RTPG_TRACE_FLAG_BUILD;
+        if (state == RTPG_MQT_TRACE_SAMPLE) flags |= RTPG_TRACE_FLAG_BUILD | RTPG_TRACE_FLAG_FINAL;
+        if ((r = rtpg_tracer_render_grid(h, samples_per_launch, flags, grid, mqt, stream))) return r;
+        if ((r = rtpg_mqt_controller_end(ctrl, stream))) return r;
+        rtpg_mqt_controller_get(ctrl, &state, &it, &tmp, &executing);
+        if (tmp == 0 && (r = rtpg_hashgrid_swap(grid, stream))) return r;
+    }
+    return RTPG_OK;
+}
+
 int rtpg_tracer_counters(rtpg_tracer* h, uint64_t* host_path_bounces, uint64_t* host_shadow_rays, void* stream) {
     if (!h) return fail(RTPG_EINVAL, "rtpg_tracer_counters: null handle");
     unsigned long long c[2];
@@ -783,7 +915,7 @@ int rtpg_tracer_path_depths(rtpg_tracer* h, uint32_t* out_depth, void* stream) {
 int rtpg_tracer_set_timing(rtpg_tracer* h, int enable) {
     if (!h) return fail(RTPG_EINVAL, "rtpg_tracer_set_timing: null handle");
     h->timing = enable != 0;
-    for (int k = 0; k < 4; ++k) {
+    for (int k = 0; k < 3; ++k) {
         h->t_ms[k] = 0.0;
         h->t_launch[k] = 0;
     }
@@ -792,7 +924,7 @@ int rtpg_tracer_set_timing(rtpg_tracer* h, int enable) {
 
 int rtpg_tracer_timings(rtpg_tracer* h, double* host_ms, uint64_t* host_launches) {
     if (!h || !host_ms) return fail(RTPG_EINVAL, "rtpg_tracer_timings: null argument");
-    for (int k = 0; k < 4; ++k) {
+    for (int k = 0; k < 3; ++k) {
         host_ms[k] = h->t_ms[k];
         if (host_launches) host_launches[k] = h->t_launch[k];
     }

@@ -3,7 +3,8 @@
 ``HashGrid`` stands for DoubleBufferedHashGrid3Buffer (RTLibExtOPX7Test.h:1472-1570) with the
 device routines DoubleBufferedHashGrid3T::FindFromCur / FindFromPrv batched;
 ``MortonQuadTrees`` for RTMortonQuadTreeWrapperT (OPX7UtilsMorton.h:590-764) with
-MortonQuadTreeWrapperT::Record / SampleAndPdf / Pdf batched and the pyramid build.
+MortonQuadTreeWrapperT::Record / SampleAndPdf / Pdf batched and the pyramid build;
+``MortonQuadTreeController`` for RTMortonQuadTreeControllerT (OPX7UtilsMorton.h:766-993).
 """
 from __future__ import annotations
 
@@ -127,3 +128,37 @@ class MortonQuadTrees:
         s = C.c_uint32()
         call("rtpg_mqt_status", self.h, C.byref(s), int(clear), stream_ptr(stream))
         return s.value
+
+
+TRACE_RECORD, TRACE_RECORD_AND_SAMPLE, TRACE_SAMPLE, TRACE_LOCATE = 0, 1, 2, 3
+
+
+class MortonQuadTreeController:
+    """The doubling pass schedule of the hash-grid guide, with the LOCATE phase."""
+
+    def __init__(self, trees, sample_for_budget, iteration_for_built=3, iteration_for_locate=0,
+                 ratio_for_budget=0.3, samples_per_launch=1):
+        h = C.c_void_p()
+        call("rtpg_mqt_controller_create", trees.h, int(sample_for_budget), int(iteration_for_built),
+             int(iteration_for_locate), float(ratio_for_budget), int(samples_per_launch), C.byref(h))
+        self.h = h
+        self.trees = trees
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            call("rtpg_mqt_controller_destroy", self.h)
+            self.h = None
+
+    def start(self):
+        call("rtpg_mqt_controller_start", self.h)
+
+    def begin(self, stream=None):
+        call("rtpg_mqt_controller_begin", self.h, stream_ptr(stream))
+
+    def end(self, stream=None):
+        call("rtpg_mqt_controller_end", self.h, stream_ptr(stream))
+
+    def get(self):
+        st, it, tmp, ex = C.c_int32(), C.c_uint32(), C.c_uint32(), C.c_int32()
+        call("rtpg_mqt_controller_get", self.h, C.byref(st), C.byref(it), C.byref(tmp), C.byref(ex))
+        return {"state": st.value, "iteration": it.value, "samples_in_pass": tmp.value, "executing": bool(ex.value)}

@@ -3,7 +3,8 @@
 ``Scene`` owns the BVH of a triangle soup; ``Tracer`` plays the part of RTLib's test
 application for one scene (RTLibExtOPX7TestApplication: Params, TracePipeline, accumulation);
 ``render`` is one launch with explicit PARAM_FLAG_* flags, ``render_guided`` the controller-
-driven loop of the PG tracers.
+driven loop of the PG tracers; ``render_grid`` / ``render_grid_guided`` the same for the HT
+tracers (hash grid + Morton quadtrees, SimpleGuide2.cu).
 """
 from __future__ import annotations
 
@@ -13,7 +14,7 @@ import numpy as np
 
 from ._lib import call, ptr, stream_ptr
 
-FLAG_NEE, FLAG_RIS, FLAG_USE_TREE, FLAG_BUILD, FLAG_FINAL = 1, 2, 8, 16, 32
+FLAG_NEE, FLAG_RIS, FLAG_USE_GRID, FLAG_USE_TREE, FLAG_BUILD, FLAG_FINAL, FLAG_LOCATE = 1, 2, 4, 8, 16, 32, 64
 
 
 class _Material(C.Structure):
@@ -121,6 +122,14 @@ class Tracer:
         call("rtpg_tracer_render_guided", self.h, tree.h, controller.h, int(base_flags), int(samples_per_launch),
              int(max_launches), stream_ptr(stream))
 
+    def render_grid(self, spp, flags, grid, mqt, stream=None):
+        call("rtpg_tracer_render_grid", self.h, int(spp), int(flags), grid.h, mqt.h, stream_ptr(stream))
+
+    def render_grid_guided(self, grid, mqt, controller, base_flags=FLAG_NEE, samples_per_launch=1,
+                           max_launches=1 << 30, stream=None):
+        call("rtpg_tracer_render_grid_guided", self.h, grid.h, mqt.h, controller.h, int(base_flags),
+             int(samples_per_launch), int(max_launches), stream_ptr(stream))
+
     def image(self, out=None, stream=None):
         import torch
         if out is None:
@@ -149,11 +158,11 @@ class Tracer:
         call("rtpg_tracer_set_timing", self.h, int(bool(enable)))
 
     def timings(self):
-        """Summed device ms and launch counts of raygen / extend / connect / finish."""
-        ms = np.zeros(4, np.float64)
-        n = np.zeros(4, np.uint64)
+        """Summed device ms and launch counts of raygen / bounce / finish."""
+        ms = np.zeros(3, np.float64)
+        n = np.zeros(3, np.uint64)
         call("rtpg_tracer_timings", self.h, ms.ctypes.data, n.ctypes.data)
-        return dict(zip(("raygen", "extend", "connect", "finish"), zip(ms.tolist(), n.tolist())))
+        return dict(zip(("raygen", "bounce", "finish"), zip(ms.tolist(), n.tolist())))
 
     def stats(self):
         a, b = C.c_uint64(), C.c_uint64()
