@@ -402,7 +402,11 @@ def bench_cornell_ours(args, rank, world):
                 "d2h_bytes_per_step": int(h_img.numel() * 4)},
         "roofline": {"kernel": "k_bounce", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs (burst copy)",
-                     "traffic": _traffic("k_bounce"), "algorithmic_bytes_per_path_bounce": BOUNCE_BYTES,
+                     "traffic": (None if _traffic("k_bounce_bytes_per_path_bounce") is None else
+                                 _traffic("k_bounce_bytes_per_path_bounce") * cnt["path_bounces"]
+                                 / max(1, C_MAX_DEPTH * (C_BUDGET + 1))),
+                     "traffic_bytes_per_path_bounce": _traffic("k_bounce_bytes_per_path_bounce"),
+                     "algorithmic_bytes_per_path_bounce": BOUNCE_BYTES,
                      "path_bounces_per_step": cnt["path_bounces"],
                      "launch_ms": ext_ms / max(1, tk["bounce"][1]),
                      "kernel_ms_per_step": {kk: v[0] for kk, v in tk.items()},

@@ -333,6 +333,24 @@ int rtpg_tracer_render_grid(rtpg_tracer* h, uint32_t spp, uint32_t flags, rtpg_h
 int rtpg_tracer_render_grid_guided(rtpg_tracer* h, rtpg_hashgrid* grid, rtpg_mqt* mqt, rtpg_mqt_controller* ctrl,
                                    uint32_t base_flags, uint32_t samples_per_launch, uint32_t max_launches,
                                    void* stream);
+/* Emitter radiances (no counterpart in RTLib, which fixes them at load): light mesh i gets
+ * host_rgb[3i..3i+2], both as MeshLight::emission for NEE and as the emission of its material.
+ * Every light mesh must have its own emissive material. */
+int rtpg_tracer_set_light_emission(rtpg_tracer* h, const float* host_rgb, uint32_t num_lights);
+/* Path-replay backpropagation (no counterpart in RTLib).  Replays the spp samples that
+ * rtpg_tracer_render(h, spp, flags, NULL) would draw from the current per-pixel streams
+ * (call rtpg_tracer_clear first to restart them) and ADDS to the gradient buffers the
+ * derivatives of a loss whose gradient with respect to the mean image of those samples is
+ * d_image (RGB float per pixel, device):
+ *   grad_texture        3 floats per texel of diffuse texture texture_index (-1: none);
+ *   grad_light_emission 3 floats per light mesh (NULL: none).
+ * flags: 0 or RTPG_TRACE_FLAG_NEE (RIS resampling depends on the radiances, guiding on
+ * recorded radiance; neither is differentiated).  Per sample, one primal wave recomputes every
+ * path's radiance and one adjoint wave replays the path, subtracting each term as it passes
+ * it: nothing per vertex is stored.  The accumulation is not touched; the streams advance
+ * as the render would advance them. */
+int rtpg_tracer_render_adjoint(rtpg_tracer* h, uint32_t spp, uint32_t flags, const float* d_image,
+                               int32_t texture_index, float* grad_texture, float* grad_light_emission, void* stream);
 /* mean radiance per pixel, width x height x RGB float (device) */
 int rtpg_tracer_image(rtpg_tracer* h, float* out_rgb, void* stream);
 int rtpg_tracer_accumulation(rtpg_tracer* h, const double** dev_accum, uint64_t* host_samples);

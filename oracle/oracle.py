@@ -404,7 +404,7 @@ class OracleRenderer:
     def __init__(self, oracle, scene, max_depth=8, num_candidates=32, seed=1, fraction=0.3, width=None, height=None,
                  texture=None, background=(0.0, 0.0, 0.0)):
         L = self.L = oracle.L
-        L.or_render.argtypes = [P, C.c_uint32, P, C.c_uint32, C.c_uint32, _u32, np.ctypeslib.ndpointer(np.float64)]
+        L.or_render.argtypes = [P, C.c_uint32, P, P, C.c_uint32, C.c_uint32, _u32, np.ctypeslib.ndpointer(np.float64)]
         L.or_render.restype = C.c_int64
         s = scene
         self.keep = {k: np.ascontiguousarray(s[k]) for k in ("tri_v", "tri_mat", "tri_uv", "light_tris", "light_first",
@@ -440,14 +440,28 @@ class OracleRenderer:
         self.accum = np.zeros(3 * o.width * o.height, np.float64)
         self.samples = 0
 
-    def render(self, spp, flags, tree=None):
+    def render(self, spp, flags, tree=None, grid=None):
         for _ in range(spp):
-            self.L.or_render(C.byref(self.sc), int(flags), tree.h if tree is not None else None, 0,
-                             self.width * self.height, self.seeds, self.accum)
+            self.L.or_render(C.byref(self.sc), int(flags), tree.h if tree is not None else None,
+                             C.byref(grid.g) if grid is not None else None, 0, self.width * self.height, self.seeds,
+                             self.accum)
         self.samples += spp
 
     def image(self):
         return (self.accum / max(self.samples, 1)).reshape(self.height, self.width, 3).astype(np.float32)
+
+    def restart(self, seed=1):
+        """Zero the accumulation and restart the per-pixel streams (rtpg_tracer_clear)."""
+        self.seeds = tracer_seeds(self.width, self.height, seed)
+        self.accum[:] = 0
+        self.samples = 0
+
+    def set_light_emission(self, rgb, light_material_first):
+        """Emitter radiances for NEE and the emissive materials light i = material first + i."""
+        rgb = np.asarray(rgb, np.float32).reshape(-1, 3)
+        self.keep["light_emission"][:] = rgb.reshape(-1)
+        for i, c in enumerate(rgb):
+            self.mats[light_material_first + i].emission[:] = [float(x) for x in c]
 
     def render_guided(self, tree, budget, ratio_for_budget=1.0, iteration_for_built=0, base_flags=1):
         """RTSTreeControllerT::BegTrace / EndTrace (OPX7UtilsPathGuiding.h:1808-1887) with one
@@ -473,3 +487,84 @@ class OracleRenderer:
                 per_tmp = 0
             if per_all > budget:
                 break
+
+    def render_grid_guided(self, grid, budget, iteration_for_built=3, iteration_for_locate=0, ratio_for_budget=0.3,
+                           base_flags=1, max_launches=1 << 30):
+        """RTMortonQuadTreeControllerT::BegTrace / EndTrace (OPX7UtilsMorton.h:818-922) with one
+        sample per launch, flags by state and the hash grid's current -> previous copy after
+        every finished pass, as TracePipeline does for the HT tracers
+        (RTLibExtOPX7TestApplication.cpp:2174-2222)."""
+        grid.clear_trees()
+        remain = ((budget - 1 + 1) // 1) * 1
+        pas, per_all, per_tmp, it = 0, 0, 0, 0
+        for _ in range(max_launches):
+            if per_tmp == 0:
+                remain -= pas
+                pas = min(remain, 1 << it)
+                if remain - pas < 2 * pas or per_all >= ratio_for_budget * budget:
+                    pas = remain
+            flags = (base_flags & 3) | 4
+            if it > iteration_for_built:
+                flags |= 16 if remain > pas else 16 | 32
+            elif not it > iteration_for_locate:
+                flags |= 64
+            self.render(1, flags, grid=grid)
+            per_all += 1
+            per_tmp += 1
+            if per_tmp >= pas:
+                it += 1
+                if it > iteration_for_built:
+                    grid.update()
+                per_tmp = 0
+            if per_tmp == 0:
+                grid.swap()
+            if per_all > budget:
+                break
+
+
+class _OGrid(C.Structure):
+    _fields_ = [("off", C.c_float * 3), ("size", C.c_float * 3), ("bounds", C.c_uint32 * 3), ("nslots", C.c_uint32),
+                ("keying", C.c_int32), ("cur", P), ("prv", P), ("level", C.c_uint32), ("bits", C.c_int32),
+                ("leaves", P), ("pyramid", P), ("fraction", C.c_float), ("status", C.c_uint32)]
+
+
+class OracleGrid:
+    """Hash grid (current / previous tables of 64-bit keys) with one Morton quadtree per slot,
+    the state of the HT tracers (DoubleBufferedHashGrid3Buffer + RTMortonQuadTreeWrapperT)."""
+
+    def __init__(self, oracle, aabb_min, aabb_max, bounds, nslots, keying=0, level=4, fraction=0.3, frac_bits=24):
+        self.o = oracle
+        self.nslots, self.level, self.bits = int(nslots), int(level), int(frac_bits)
+        self.cur = np.zeros(self.nslots, np.uint64)
+        self.prv = np.zeros(self.nslots, np.uint64)
+        self.per = ((1 << (2 * (self.level + 1))) - 1) // 3
+        self.leaves = np.zeros(self.nslots << (2 * self.level), np.int64)
+        self.pyramid = np.zeros(self.nslots * self.per, np.float32)
+        g = self.g = _OGrid()
+        g.off[:] = [float(v) for v in aabb_min]
+        g.size[:] = [float(np.float32(b) - np.float32(a)) for a, b in zip(aabb_min, aabb_max)]
+        g.bounds[:] = [int(b) for b in bounds]
+        g.nslots, g.keying = self.nslots, int(keying)
+        g.cur, g.prv = self.cur.ctypes.data, self.prv.ctypes.data
+        g.level, g.bits = self.level, self.bits
+        g.leaves, g.pyramid = self.leaves.ctypes.data, self.pyramid.ctypes.data
+        g.fraction = float(fraction)
+
+    def clear(self):
+        self.cur[:] = 0
+        self.prv[:] = 0
+
+    def clear_trees(self):
+        self.leaves[:] = 0
+        self.pyramid[:] = 0
+
+    def swap(self):
+        self.prv[:] = self.cur
+
+    def update(self):
+        self.pyramid[:] = self.o.mqt_build(self.nslots, self.level, self.bits, self.leaves)
+        self.leaves[:] = 0
+
+    @property
+    def status(self):
+        return self.g.status

@@ -84,6 +84,8 @@ _SIGS = {
     "rtpg_tracer_render": [P, U32, U32, P, P],
     "rtpg_tracer_render_guided": [P, P, P, U32, U32, U32, P],
     "rtpg_tracer_render_grid": [P, U32, U32, P, P, P],
+    "rtpg_tracer_set_light_emission": [P, P, U32],
+    "rtpg_tracer_render_adjoint": [P, U32, U32, P, I32, P, P, P],
     "rtpg_tracer_render_grid_guided": [P, P, P, P, U32, U32, U32, P],
     "rtpg_tracer_image": [P, P, P],
     "rtpg_tracer_accumulation": [P, P, P],

@@ -74,6 +74,15 @@ struct TracerDev {
     MqtDev mqt;
     unsigned* status;
     unsigned long long* counters;  // [0] bounce visits (path-bounces), [1] shadow rays
+    // adjoint replay (path-replay backpropagation)
+    const float3* adj_c;   // radiance of every path from the primal replay of this sample
+    float3* lrem;          // radiance still ahead of the path during the adjoint replay
+    const float* adj_dimg; // dLoss/dImage, RGB per pixel
+    float adj_scale;       // 1 / samples of the image
+    int32_t adj_tex;       // texture whose texels get gradients (-1: none)
+    float* grad_tex;       // 3 per texel of adj_tex
+    float* grad_light;     // 3 per light mesh
+    const int32_t* mat_light;  // light mesh of an emissive material, -1 otherwise
 };
 
 // ------------------------------------------------------------------ raygen (SimpleGuide.cu:48-81)
@@ -94,20 +103,23 @@ __global__ void __launch_bounds__(kTB) k_raygen(TracerDev T) {
         T.depth[p] = 0;
         T.hflags[p] = HF_COUNT_EMITTED;
         T.queue[0][p] = p;
+        if (T.adj_c) T.lrem[p] = T.adj_c[p];
     }
 }
 
-__device__ __forceinline__ float3 tex_fetch(const TracerDev& T, int t, float u, float v) {
+__device__ __forceinline__ float3 tex_fetch(const TracerDev& T, int t, float u, float v, uint32_t& texel) {
     const uint2 wh = T.tex_wh[t];
     float fu = u - floorf(u), fv = v - floorf(v);
     uint32_t x = min((uint32_t)(fu * wh.x), wh.x - 1), y = min((uint32_t)(fv * wh.y), wh.y - 1);
-    const float* px = T.tex[t] + 3 * (size_t(y) * wh.x + x);
+    texel = y * wh.x + x;
+    const float* px = T.tex[t] + 3 * size_t(texel);
     return f3(px[0], px[1], px[2]);
 }
 
 struct LightSample {
     float3 pos, dir, normal, emission;
     float dist, inv_pdf;
+    uint32_t mesh;
 };
 // MeshLightList::Sample -> MeshLight::Sample (SimpleKernel.h:81-98, 114-120): mesh and
 // triangle by next() % count, barycentrics by random_in_unit_triangle.
@@ -130,6 +142,7 @@ __device__ __forceinline__ LightSample sample_light(const TracerDev& T, float3 p
     l.emission = T.light_emit[mi];
     l.normal = unit3(nf);
     l.inv_pdf = len3(nf) / 2.0f * (float)mesh.y * (float)T.light_count;
+    l.mesh = mi;
     return l;
 }
 
@@ -140,8 +153,17 @@ __device__ __forceinline__ LightSample sample_light(const TracerDev& T, float3 p
 // radiance into the color (and, recording, into the per-bounce store from which k_finish forms
 // the trace-vertex radiance), termination, compaction of the survivors into the next queue.
 // Returns whether the path continues; *shadow tells whether a shadow ray was traced.
-__device__ __forceinline__ bool bounce_path(const TracerDev& T, uint32_t p, bool use_tree, bool use_grid, bool build,
-                                            bool recording, bool& shadow) {
+constexpr int kGuideNone = 0, kGuideTree = 1, kGuideGrid = 2, kAdjoint = 3;
+
+// The adjoint replay (kAdjoint) runs the unguided path again from the same random numbers and
+// scatters d(loss)/d(parameter) as it goes (path-replay backpropagation): lrem starts as the
+// path's radiance from the primal replay and loses each term once the path has passed it, so
+// at a textured vertex it holds exactly the terms that carry the vertex's albedo as a factor
+// (its NEE term and everything after it); the albedo gradient is delta * lrem / albedo per
+// channel.  An emitter's gradient is delta * (the term's factor in front of its radiance).
+template <int G>
+__device__ __forceinline__ bool bounce_path(const TracerDev& T, uint32_t p, bool build, bool recording, bool& shadow) {
+    constexpr bool use_tree = G == kGuideTree, use_grid = G == kGuideGrid, adjoint = G == kAdjoint;
     const float3 org = T.org[p], in_dir = T.dir[p], prev_thr = T.thr[p];
     const uint32_t d = T.depth[p], prev_flags = T.hflags[p];
     const Hit h = bvh_trace<false>(T.scene, org.x, org.y, org.z, in_dir.x, in_dir.y, in_dir.z, 0.0001f, 1.0e20f);
@@ -149,6 +171,8 @@ __device__ __forceinline__ bool bounce_path(const TracerDev& T, uint32_t p, bool
     bool pend = false;
     float3 sdir = f3(0.f, 0.f, 0.f), scontrib = f3(0.f, 0.f, 0.f);
     float sdist = 0.0f;
+    uint32_t nee_mesh = 0xffffffffu;                 // adjoint: light mesh of the NEE sample
+    float3 nee_factor = f3(0.f, 0.f, 0.f);           // adjoint: NEE term / light radiance
     if (h.prim == 0xffffffffu) {
         // __miss__radiance (SimpleGuide.cu:202-219): the ray keeps its direction
         const float3 L = prev_thr * T.bg;
@@ -164,13 +188,16 @@ __device__ __forceinline__ bool bounce_path(const TracerDev& T, uint32_t p, bool
     float3 position = org + h.t * in_dir;
     const uint32_t mi = T.tri_mat[h.prim];
     const Material m = T.mats[mi < T.num_materials ? mi : T.num_materials - 1];
-    float3 diffuse = m.diffuse;
+    float3 diffuse = m.diffuse, texv = f3(1.f, 1.f, 1.f);
+    uint32_t texel = 0xffffffffu;
     if (m.tex >= 0 && T.tri_uv) {
         const float* uv = T.tri_uv + 6 * size_t(h.prim);
         const float w0 = 1.0f - h.u - h.v;
         const float tu = w0 * uv[0] + h.u * uv[2] + h.v * uv[4];
         const float tvv = w0 * uv[1] + h.u * uv[3] + h.v * uv[5];
-        diffuse = diffuse * tex_fetch(T, m.tex, tu, tvv);
+        texv = tex_fetch(T, m.tex, tu, tvv, texel);
+        diffuse = diffuse * texv;
+        if (adjoint && m.tex != T.adj_tex) texel = 0xffffffffu;
     }
     const bool count_emitted = (prev_flags & HF_COUNT_EMITTED) || m.type == MAT_DEF_LIGHT;
     float3 direction = f3(0.f, 0.f, 0.f), bsdf_val = f3(0.f, 0.f, 0.f), cur_thr = f3(0.f, 0.f, 0.f);
@@ -293,6 +320,10 @@ __device__ __forceinline__ bool bounce_path(const TracerDev& T, uint32_t p, bool
                     sdir = l.dir;
                     sdist = l.dist - 0.0001f;
                     scontrib = prev_thr * b * l.emission * g * l.inv_pdf;
+                    if (adjoint) {
+                        nee_mesh = l.mesh;
+                        nee_factor = prev_thr * b * g * l.inv_pdf;
+                    }
                 }
             }
         } else {
@@ -340,7 +371,8 @@ __device__ __forceinline__ bool bounce_path(const TracerDev& T, uint32_t p, bool
         flags |= HF_COUNT_EMITTED | HF_DELTA;
     }
     float3 rad = f3(0.f, 0.f, 0.f);
-    if (dot3(in_dir, fn) < 0.0f && count_emitted) rad = prev_thr * m.emission;
+    const bool emitted = dot3(in_dir, fn) < 0.0f && count_emitted;
+    if (emitted) rad = prev_thr * m.emission;
     if (m.emission.x + m.emission.y + m.emission.z > 0.0f) flags |= HF_FINISH;
     T.org[p] = position;
     T.dir[p] = direction;
@@ -358,10 +390,44 @@ __device__ __forceinline__ bool bounce_path(const TracerDev& T, uint32_t p, bool
         if (use_grid) T.v_cell[vi] = cell;
     }
     float3 L = rad;
+    bool lit = false;
     if (pend) {
         shadow = true;
         const Hit sh = bvh_trace<true>(T.scene, position.x, position.y, position.z, sdir.x, sdir.y, sdir.z, 0.0001f, sdist);
-        if (sh.prim == 0xffffffffu) L = L + scontrib;
+        if (sh.prim == 0xffffffffu) {
+            L = L + scontrib;
+            lit = true;
+        }
+    }
+    if (adjoint) {
+        const float3 delta = f3(T.adj_dimg[3 * size_t(p)], T.adj_dimg[3 * size_t(p) + 1], T.adj_dimg[3 * size_t(p) + 2]) * T.adj_scale;
+        float3 lr = T.lrem[p] - rad;  // the emission term does not depend on this vertex
+        if (emitted) {
+            const int32_t li = T.mat_light[mi < T.num_materials ? mi : T.num_materials - 1];
+            if (li >= 0 && T.grad_light) {
+                const float3 gl = delta * prev_thr;
+                atomicAdd(T.grad_light + 3 * li, gl.x);
+                atomicAdd(T.grad_light + 3 * li + 1, gl.y);
+                atomicAdd(T.grad_light + 3 * li + 2, gl.z);
+            }
+        }
+        if (texel != 0xffffffffu && T.grad_tex && m.type == MAT_PHONG) {
+            // albedo enters the NEE term and the throughput linearly, per channel
+            float* gt = T.grad_tex + 3 * size_t(texel);
+            if (texv.x > 0.f) atomicAdd(gt, delta.x * lr.x / texv.x);
+            if (texv.y > 0.f) atomicAdd(gt + 1, delta.y * lr.y / texv.y);
+            if (texv.z > 0.f) atomicAdd(gt + 2, delta.z * lr.z / texv.z);
+        }
+        if (lit && nee_mesh != 0xffffffffu) {
+            if (T.grad_light) {
+                const float3 gl = delta * nee_factor;
+                atomicAdd(T.grad_light + 3 * nee_mesh, gl.x);
+                atomicAdd(T.grad_light + 3 * nee_mesh + 1, gl.y);
+                atomicAdd(T.grad_light + 3 * nee_mesh + 2, gl.z);
+            }
+            lr = lr - scontrib;
+        }
+        T.lrem[p] = lr;
     }
     if (recording) T.b_rad[size_t(d) * T.npath + p] = L;
     T.col[p] = T.col[p] + L;
@@ -371,23 +437,28 @@ __device__ __forceinline__ bool bounce_path(const TracerDev& T, uint32_t p, bool
     return true;
 }
 
+// guide kinds (and the adjoint replay), a template argument so that each variant carries only
+// its own code
+__host__ __device__ constexpr int guide_of(uint32_t flags) {
+    return (flags & RTPG_TRACE_FLAG_USE_TREE) ? kGuideTree : ((flags & RTPG_TRACE_FLAG_USE_GRID) ? kGuideGrid : kGuideNone);
+}
+
+template <int G>
 __global__ void __launch_bounds__(kTB, 6) k_bounce(TracerDev T, int in) {
     const uint32_t n = T.qcount[in];
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         T.qcount[in ^ 1] = 0;
         atomicAdd(T.counters, (unsigned long long)n);
     }
-    const bool use_tree = (T.flags & RTPG_TRACE_FLAG_USE_TREE) != 0;
-    const bool use_grid = (T.flags & RTPG_TRACE_FLAG_USE_GRID) != 0;
     const bool build = (T.flags & RTPG_TRACE_FLAG_BUILD) != 0;
-    const bool recording = (use_tree || use_grid) && !(T.flags & RTPG_TRACE_FLAG_FINAL);
+    const bool recording = (G == kGuideTree || G == kGuideGrid) && !(T.flags & RTPG_TRACE_FLAG_FINAL);
     for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
         const uint32_t q = base + threadIdx.x;
         bool keep = false, shadow = false;
         uint32_t p = 0;
         if (q < n) {
             p = T.queue[in][q];
-            keep = bounce_path(T, p, use_tree, use_grid, build, recording, shadow);
+            keep = bounce_path<G>(T, p, build, recording, shadow);
         }
         const unsigned sh = __ballot_sync(0xffffffffu, shadow);
         if ((threadIdx.x & 31) == 0 && sh) atomicAdd(T.counters + 1, (unsigned long long)__popc(sh));
@@ -407,10 +478,10 @@ __global__ void __launch_bounds__(kTB, 6) k_bounce(TracerDev T, int in) {
 // Accumulate, write the seed back, commit trace vertices (TraceVertexT::Commit,
 // OPX7UtilsPathGuiding.h:830-866 -> DTreeWrapperT::Record :514-520 with stat-weight 1, or
 // MortonTraceVertexT::Commit for the grid guide).
+template <int G>
 __global__ void __launch_bounds__(kTB) k_finish(TracerDev T) {
-    const bool use_grid = (T.flags & RTPG_TRACE_FLAG_USE_GRID) != 0;
-    const bool recording = (T.flags & (RTPG_TRACE_FLAG_USE_TREE | RTPG_TRACE_FLAG_USE_GRID)) &&
-                           !(T.flags & RTPG_TRACE_FLAG_FINAL);
+    constexpr bool use_grid = G == kGuideGrid;
+    const bool recording = G != kGuideNone && !(T.flags & RTPG_TRACE_FLAG_FINAL);
     for (uint32_t base = blockIdx.x * blockDim.x; base < T.npath; base += gridDim.x * blockDim.x) {
         const uint32_t p = base + threadIdx.x;
         uint32_t nv = 0;
@@ -511,6 +582,14 @@ struct rtpg_tracer {
     TracerDev dev{};
     rtpg_scene* scene = nullptr;
     std::vector<void*> allocs;
+    // host copies for parameter updates and the adjoint
+    std::vector<Material> hmats;
+    std::vector<float3> hemit;
+    std::vector<int32_t> light_mat;  // material of every light mesh (-1: its triangles differ)
+    bool light_mat_shared = false;   // some material belongs to two light meshes
+    float3* col_adj = nullptr;       // path colour of the adjoint replay
+    float3* lrem = nullptr;
+    int32_t* d_mat_light = nullptr;
     std::vector<const float*> tex_ptr;
     std::vector<int32_t> mat_tex;  // texture index of every material (host copy for checks)
     std::vector<uint2> tex_wh;
@@ -554,6 +633,21 @@ struct rtpg_tracer {
     }
 };
 
+static void launch_bounce(const TracerDev& T, int g, cudaStream_t st, int in) {
+    switch (guide_of(T.flags)) {
+        case kGuideTree: k_bounce<kGuideTree><<<g, kTB, 0, st>>>(T, in); break;
+        case kGuideGrid: k_bounce<kGuideGrid><<<g, kTB, 0, st>>>(T, in); break;
+        default: k_bounce<kGuideNone><<<g, kTB, 0, st>>>(T, in); break;
+    }
+}
+static void launch_finish(const TracerDev& T, int g, cudaStream_t st) {
+    switch (guide_of(T.flags)) {
+        case kGuideTree: k_finish<kGuideTree><<<g, kTB, 0, st>>>(T); break;
+        case kGuideGrid: k_finish<kGuideGrid><<<g, kTB, 0, st>>>(T); break;
+        default: k_finish<kGuideNone><<<g, kTB, 0, st>>>(T); break;
+    }
+}
+
 // One wave with CUDA events around every kernel group; synchronises and accumulates the
 // per-group device time (used to measure the kernels, outside the graph-replayed path).
 static int timed_wave(rtpg_tracer* h, cudaStream_t st) {
@@ -571,7 +665,7 @@ static int timed_wave(rtpg_tracer* h, cudaStream_t st) {
     h->t_launch[0] += 1;
     for (uint32_t b = 0; b < T.max_depth; ++b) {
         cudaEventRecord(h->ev[2], st);
-        k_bounce<<<g, kTB, 0, st>>>(T, int(b & 1));
+        launch_bounce(T, g, st, int(b & 1));
         cudaEventRecord(h->ev[3], st);
         RTPG_CUDA(cudaEventSynchronize(h->ev[3]));
         cudaEventElapsedTime(&ms, h->ev[2], h->ev[3]);
@@ -579,7 +673,7 @@ static int timed_wave(rtpg_tracer* h, cudaStream_t st) {
         h->t_launch[1] += 1;
     }
     cudaEventRecord(h->ev[4], st);
-    k_finish<<<g, kTB, 0, st>>>(T);
+    launch_finish(T, g, st);
     cudaEventRecord(h->ev[5], st);
     RTPG_CUDA(cudaEventSynchronize(h->ev[5]));
     cudaEventElapsedTime(&ms, h->ev[4], h->ev[5]);
@@ -593,10 +687,8 @@ static void launch_wave(rtpg_tracer* h, cudaStream_t st) {
     TracerDev& T = h->dev;
     const int g = kSMs * 8;
     k_raygen<<<g, kTB, 0, st>>>(T);
-    for (uint32_t b = 0; b < T.max_depth; ++b) {
-        k_bounce<<<g, kTB, 0, st>>>(T, int(b & 1));
-    }
-    k_finish<<<g, kTB, 0, st>>>(T);
+    for (uint32_t b = 0; b < T.max_depth; ++b) launch_bounce(T, g, st, int(b & 1));
+    launch_finish(T, g, st);
 }
 
 extern "C" {
@@ -691,6 +783,51 @@ int rtpg_tracer_create(rtpg_scene* scene, const float* tri_vertices, const uint3
     T.light_emit = lemit;
     T.light_tris = light_tris;
     T.light_count = num_light_meshes;
+    // light mesh <-> emissive material, for emitter parameters and their gradients
+    h->hmats = hm;
+    h->hemit = he;
+    {
+        std::vector<int32_t> ml(num_materials, -1);
+        h->light_mat.assign(num_light_meshes, -1);
+        uint32_t nlt = 0;
+        for (uint32_t i = 0; i < num_light_meshes; ++i) nlt = std::max(nlt, hl[i].x + hl[i].y);
+        std::vector<uint32_t> lt(nlt), tm;
+        if (nlt && (e = cudaMemcpy(lt.data(), light_tris, 4ull * nlt, cudaMemcpyDeviceToHost))) {
+            delete h;
+            return fail(RTPG_ECUDA, "rtpg_tracer_create: %s", cudaGetErrorString(e));
+        }
+        const uint32_t nt = T.scene.ntris;
+        tm.resize(nt);
+        if (nlt && (e = cudaMemcpy(tm.data(), tri_material, 4ull * nt, cudaMemcpyDeviceToHost))) {
+            delete h;
+            return fail(RTPG_ECUDA, "rtpg_tracer_create: %s", cudaGetErrorString(e));
+        }
+        for (uint32_t i = 0; i < num_light_meshes; ++i) {
+            int32_t mat = -1;
+            for (uint32_t k = 0; k < hl[i].y; ++k) {
+                const uint32_t t = lt[hl[i].x + k];
+                const int32_t mk = t < nt ? (int32_t)std::min(tm[t], num_materials - 1) : -1;
+                mat = (k == 0) ? mk : (mat == mk ? mat : -1);
+            }
+            h->light_mat[i] = mat;
+            if (mat >= 0) {
+                if (ml[mat] >= 0 && ml[mat] != (int32_t)i) h->light_mat_shared = true;
+                ml[mat] = (int32_t)i;
+            }
+        }
+        if (h->light_mat_shared) std::fill(ml.begin(), ml.end(), -1);
+        if ((r = h->alloc(&h->d_mat_light, num_materials)) || (r = h->alloc(&h->col_adj, P)) ||
+            (r = h->alloc(&h->lrem, P))) {
+            delete h;
+            return r;
+        }
+        if ((e = cudaMemcpy(h->d_mat_light, ml.data(), 4ull * num_materials, cudaMemcpyHostToDevice))) {
+            delete h;
+            return fail(RTPG_ECUDA, "rtpg_tracer_create: %s", cudaGetErrorString(e));
+        }
+        T.mat_light = h->d_mat_light;
+        T.adj_tex = -1;
+    }
     T.tex = h->d_tex;
     T.tex_wh = h->d_tex_wh;
     *out = h;
@@ -890,6 +1027,79 @@ int rtpg_tracer_render_grid_guided(rtpg_tracer* h, rtpg_hashgrid* grid, rtpg_mqt
         rtpg_mqt_controller_get(ctrl, &state, &it, &tmp, &executing);
         if (tmp == 0 && (r = rtpg_hashgrid_swap(grid, stream))) return r;
     }
+    return RTPG_OK;
+}
+
+// Emitter radiances: light mesh i gets rgb[3i..3i+2] for NEE (MeshLight::emission) and as the
+// emission of its material (what a ray that hits it sees).
+int rtpg_tracer_set_light_emission(rtpg_tracer* h, const float* host_rgb, uint32_t num_lights) {
+    if (!h || !host_rgb) return fail(RTPG_EINVAL, "rtpg_tracer_set_light_emission: null argument");
+    if (num_lights != h->dev.light_count)
+        return fail(RTPG_EINVAL, "rtpg_tracer_set_light_emission: %u values for %u lights", num_lights, h->dev.light_count);
+    if (h->light_mat_shared)
+        return fail(RTPG_EINVAL, "rtpg_tracer_set_light_emission: light meshes share an emissive material");
+    for (uint32_t i = 0; i < num_lights; ++i) {
+        if (h->light_mat[i] < 0)
+            return fail(RTPG_EINVAL, "rtpg_tracer_set_light_emission: light mesh %u has triangles of several materials", i);
+        h->hemit[i] = make_float3(host_rgb[3 * i], host_rgb[3 * i + 1], host_rgb[3 * i + 2]);
+        h->hmats[h->light_mat[i]].emission = h->hemit[i];
+    }
+    RTPG_CUDA(cudaMemcpy(const_cast<float3*>(h->dev.light_emit), h->hemit.data(), sizeof(float3) * num_lights,
+                         cudaMemcpyHostToDevice));
+    RTPG_CUDA(cudaMemcpy(const_cast<Material*>(h->dev.mats), h->hmats.data(), sizeof(Material) * h->hmats.size(),
+                         cudaMemcpyHostToDevice));
+    return RTPG_OK;
+}
+
+__global__ void k_seed_store(TracerDev T) {
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < T.npath; p += gridDim.x * blockDim.x)
+        T.seeds[p] = T.rng[p];
+}
+
+// Path-replay backpropagation of an image loss.  Replays the `spp` samples that
+// rtpg_tracer_render(h, spp, flags) draws from the current per-pixel streams: per sample one
+// primal wave gives every path's radiance, one adjoint wave runs the same path again and
+// scatters gradients.  The streams advance as that render would advance them; the
+// accumulation is not touched.
+int rtpg_tracer_render_adjoint(rtpg_tracer* h, uint32_t spp, uint32_t flags, const float* d_image,
+                               int32_t texture_index, float* grad_texture, float* grad_light_emission, void* stream) {
+    if (!h || !d_image) return fail(RTPG_EINVAL, "rtpg_tracer_render_adjoint: null argument");
+    if (flags & ~RTPG_TRACE_FLAG_NEE)
+        return fail(RTPG_EINVAL, "rtpg_tracer_render_adjoint: only the unguided tracer with or without NEE is differentiated "
+                                 "(RIS resampling weights depend on the emitter radiances)");
+    if (texture_index >= 0 && (!grad_texture || size_t(texture_index) >= h->tex_ptr.size() || !h->tex_ptr[texture_index]))
+        return fail(RTPG_EINVAL, "rtpg_tracer_render_adjoint: texture %d not set or no gradient buffer", texture_index);
+    if (grad_light_emission && h->light_mat_shared)
+        return fail(RTPG_EINVAL, "rtpg_tracer_render_adjoint: light meshes share an emissive material");
+    int r = check_render(h, flags, "rtpg_tracer_render_adjoint");
+    if (r) return r;
+    if (!aligned4(d_image) || (grad_texture && !aligned4(grad_texture)) || (grad_light_emission && !aligned4(grad_light_emission)))
+        return fail(RTPG_EINVAL, "rtpg_tracer_render_adjoint: misaligned buffer");
+    cudaStream_t st = as_stream(stream);
+    TracerDev A = h->dev;
+    A.flags = flags;
+    memset(&A.tree, 0, sizeof(SDTreeDev));
+    memset(&A.grid, 0, sizeof(HashGridDev));
+    memset(&A.mqt, 0, sizeof(MqtDev));
+    A.adj_c = nullptr;
+    TracerDev B = A;
+    B.col = h->col_adj;
+    B.adj_c = A.col;
+    B.lrem = h->lrem;
+    B.adj_dimg = d_image;
+    B.adj_scale = spp ? 1.0f / (float)spp : 0.0f;
+    B.adj_tex = texture_index;
+    B.grad_tex = texture_index >= 0 ? grad_texture : nullptr;
+    B.grad_light = grad_light_emission;
+    const int g = kSMs * 8;
+    for (uint32_t s = 0; s < spp; ++s) {
+        k_raygen<<<g, kTB, 0, st>>>(A);
+        for (uint32_t b = 0; b < A.max_depth; ++b) k_bounce<kGuideNone><<<g, kTB, 0, st>>>(A, int(b & 1));
+        k_raygen<<<g, kTB, 0, st>>>(B);
+        for (uint32_t b = 0; b < B.max_depth; ++b) k_bounce<kAdjoint><<<g, kTB, 0, st>>>(B, int(b & 1));
+        k_seed_store<<<g, kTB, 0, st>>>(B);
+    }
+    RTPG_LAUNCH_CHECK();
     return RTPG_OK;
 }
 

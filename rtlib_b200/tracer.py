@@ -130,6 +130,18 @@ class Tracer:
         call("rtpg_tracer_render_grid_guided", self.h, grid.h, mqt.h, controller.h, int(base_flags),
              int(samples_per_launch), int(max_launches), stream_ptr(stream))
 
+    def set_light_emission(self, rgb):
+        """rgb: (num_lights, 3) host array; NEE radiance and material emission of every light."""
+        a = np.ascontiguousarray(rgb, np.float32).reshape(-1)
+        call("rtpg_tracer_set_light_emission", self.h, a.ctypes.data, a.size // 3)
+
+    def render_adjoint(self, spp, d_image, flags=FLAG_NEE, texture_index=-1, grad_texture=None, grad_light=None,
+                       stream=None):
+        """Adds d(loss)/d(texture texels) and d(loss)/d(light radiances) for a loss with gradient
+        d_image w.r.t. the mean image of the spp samples rtpg_tracer_render would draw next."""
+        call("rtpg_tracer_render_adjoint", self.h, int(spp), int(flags), ptr(d_image), int(texture_index),
+             ptr(grad_texture), ptr(grad_light), stream_ptr(stream))
+
     def image(self, out=None, stream=None):
         import torch
         if out is None:

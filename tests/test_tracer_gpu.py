@@ -126,3 +126,97 @@ def test_guided_render_matches_oracle(cuda, oracle):
     st = tree.stats()
     assert st["stree_nodes"] == ot.num_stree_nodes()
     assert tree.status() == 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("keying", [0, 1])
+def test_grid_guided_render_matches_oracle(cuda, oracle, keying):
+    """The HTNEE schedule (SimpleGuide2.cu + RTMortonQuadTreeControllerT): a LOCATE pass that
+    inserts cells, record passes, then record-and-sample passes guided by the per-cell
+    Morton quadtrees, on GPU and CPU.  Slot numbers may differ (concurrent inserts claim
+    slots in any order); the cell sets and each cell's quadtree must agree."""
+    from oracle.oracle import OracleGrid, OracleRenderer
+    from rtlib_b200.hashgrid import HashGrid, MortonQuadTreeController, MortonQuadTrees
+    from rtlib_b200.tracer import FLAG_NEE, Tracer
+    w = h = 48
+    budget, level, fraction = 31, 4, 0.5
+    bounds, nslots = (16, 16, 16), 4096
+    sc = scenes.cornell_box(w, h)
+    mn, mx = (-0.005,) * 3, (1.005,) * 3
+    grid = HashGrid(mn, mx, bounds, nslots, keying=keying)
+    trees = MortonQuadTrees(nslots, level=level, fraction=fraction)
+    ctrl = MortonQuadTreeController(trees, budget, iteration_for_built=1, iteration_for_locate=0,
+                                    ratio_for_budget=0.5, samples_per_launch=1)
+    tr = Tracer(sc, cuda, max_depth=8, width=w, height=h)
+    grid.clear()
+    ctrl.start()
+    # passes of 1 (locate), 2 (record), 4 and 8 (record + sample) launches, then compare the
+    # grid and the quadtrees built from the last pass; then the rest of the schedule
+    tr.render_grid_guided(grid, trees, ctrl, FLAG_NEE, samples_per_launch=1, max_launches=15)
+    og = OracleGrid(oracle, mn, mx, bounds, nslots, keying=keying, level=level, fraction=fraction)
+    r = OracleRenderer(oracle, sc, width=w, height=h)
+    r.render_grid_guided(og, budget, iteration_for_built=1, iteration_for_locate=0, ratio_for_budget=0.5,
+                         max_launches=15)
+    assert grid.status() == 0 and og.status == 0 and trees.status() == 0
+    gcur, ocur = grid.export(), og.cur
+    assert np.array_equal(np.sort(gcur[gcur != 0]), np.sort(ocur[ocur != 0]))
+    gslot = {int(k): i for i, k in enumerate(gcur) if k}
+    oslot = {int(k): i for i, k in enumerate(ocur) if k}
+    _, gpyr = trees.export()
+    per = trees.per_cell
+    gp = np.stack([gpyr[gslot[k] * per:(gslot[k] + 1) * per] for k in sorted(oslot)])
+    op = np.stack([og.pyramid[oslot[k] * per:(oslot[k] + 1) * per] for k in sorted(oslot)])
+    assert op[:, 0].sum() > 0
+    np.testing.assert_allclose(gp, op, rtol=1e-4, atol=1e-3)
+    tr.render_grid_guided(grid, trees, ctrl, FLAG_NEE, samples_per_launch=1)
+    og2 = OracleGrid(oracle, mn, mx, bounds, nslots, keying=keying, level=level, fraction=fraction)
+    r2 = OracleRenderer(oracle, sc, width=w, height=h)
+    r2.render_grid_guided(og2, budget, iteration_for_built=1, iteration_for_locate=0, ratio_for_budget=0.5)
+    assert tr.stats()["samples"] == r2.samples
+    _compare(tr.image().cpu().numpy(), r2.image(), rel_mse=1e-4, frac=0.99)
+
+
+def _small_occluded():
+    # the occluded-light scene with few objects and lights, so the CPU oracle's brute-force
+    # intersection stays fast; 20 objects of 20-triangle icospheres and boxes, 64 emitters
+    return scenes.occluded_rooms(64, 36, n_objects=20, n_lights=64, seed=5, sphere_level=0)
+
+
+@pytest.mark.parametrize("flags", [1, 3])
+def test_occluded_nee_ris_matches_oracle(cuda, oracle, flags):
+    """NEE and NEE + RIS (32 candidates, max depth 16) on the occluded-light scene: light
+    reaches the main room only through the doorway."""
+    from oracle.oracle import OracleRenderer
+    sc = _small_occluded()
+    gimg, tr = _gpu_render(cuda, sc, 64, 36, 4, flags, max_depth=16)
+    r = OracleRenderer(oracle, sc, width=64, height=36, max_depth=16, num_candidates=32)
+    r.render(4, flags)
+    assert r.image().mean() > 0
+    _compare(gimg, r.image())
+
+
+@pytest.mark.parametrize("keying", [0, 1])
+def test_occluded_grid_guided_ris_matches_oracle(cuda, oracle, keying):
+    """HTRIS on the occluded-light scene: hash-grid + Morton quadtree guide with RIS."""
+    from oracle.oracle import OracleGrid, OracleRenderer
+    from rtlib_b200.hashgrid import HashGrid, MortonQuadTreeController, MortonQuadTrees
+    from rtlib_b200.tracer import FLAG_NEE, FLAG_RIS, Tracer
+    sc = _small_occluded()
+    w, h, budget, level = 64, 36, 15, 4
+    mn, mx = (-0.005, -0.005, -0.005), (14.005, 4.005, 10.005)
+    bounds, nslots = (64, 16, 48), 1 << 15
+    grid = HashGrid(mn, mx, bounds, nslots, keying=keying)
+    trees = MortonQuadTrees(nslots, level=level, fraction=0.3)
+    ctrl = MortonQuadTreeController(trees, budget, iteration_for_built=1, ratio_for_budget=0.5)
+    tr = Tracer(sc, cuda, max_depth=16, width=w, height=h)
+    grid.clear()
+    ctrl.start()
+    tr.render_grid_guided(grid, trees, ctrl, FLAG_NEE | FLAG_RIS)
+    og = OracleGrid(oracle, mn, mx, bounds, nslots, keying=keying, level=level, fraction=0.3)
+    r = OracleRenderer(oracle, sc, width=w, height=h, max_depth=16, num_candidates=32)
+    r.render_grid_guided(og, budget, iteration_for_built=1, ratio_for_budget=0.5, base_flags=3)
+    assert tr.stats()["samples"] == r.samples
+    assert grid.status() == 0 and og.status == 0
+    gcur = grid.export()
+    assert np.array_equal(np.sort(gcur[gcur != 0]), np.sort(og.cur[og.cur != 0]))
+    _compare(tr.image().cpu().numpy(), r.image(), rel_mse=2e-3, frac=0.97)
