@@ -40,6 +40,7 @@ extern "C" {
 #define RTPG_STATUS_DNODE_CAPACITY 0x8u    /* quadtree pool capacity exhausted */
 #define RTPG_STATUS_HASH_FULL 0x10u        /* a hash bucket was full (slot = UINT32_MAX) */
 #define RTPG_STATUS_QUEUE_OVERFLOW 0x20u   /* a wavefront queue overflowed */
+#define RTPG_STATUS_TIMEOUT 0x40u          /* a bounded wait on the tensor cores gave up */
 
 const char* rtpg_last_error(void);
 /* Library version as MAJOR*10000 + MINOR*100 + PATCH. */
@@ -242,6 +243,38 @@ int rtpg_mqt_controller_end(rtpg_mqt_controller* c, void* stream);
 int rtpg_mqt_controller_get(rtpg_mqt_controller* c, int32_t* host_state, uint32_t* host_iteration,
                             uint32_t* host_samples_in_pass, int32_t* host_executing);
 
+/* ================================================================ learned guide
+ * No counterpart in RTLib: a 3 x 64 ReLU MLP (inputs: position with 12 sin/cos frequencies per
+ * axis, shading normal, outgoing direction) emitting an 8-lobe von Mises-Fisher mixture, with
+ * BF16 weights and FP32 accumulation on the tensor cores, trained online by Adam on the
+ * radiance records the tracer writes (the SD-tree's record: luminance of incident radiance x
+ * |cos| / pdf in the sampled direction), minimising -sum w log q(wi) / sum w. */
+typedef struct rtpg_mlp rtpg_mlp;
+#define RTPG_MLP_PARAMS 16384 /* fp32 parameters: W0 80x64, W1 64x64, W2 64x64, W3 64x48, [in][out] */
+/* aabb: the positions' box (features use the normalised position); seed: initialisation;
+ * learning_rate <= 0: 1e-3; record_capacity: records the tracer may write per pass. */
+int rtpg_mlp_create(const float* aabb_min, const float* aabb_max, uint32_t seed, float learning_rate,
+                    uint32_t record_capacity, rtpg_mlp** out);
+int rtpg_mlp_destroy(rtpg_mlp* h);
+/* copy the fp32 parameters out (host_get) and / or in (host_set, which also resets Adam) */
+int rtpg_mlp_params(rtpg_mlp* h, float* host_get, const float* host_set, void* stream);
+/* n samples (device, 3 floats each): raw outputs (48 per sample) and / or the mixture
+ * (8 lobes x mu xyz, kappa, weight = 40 per sample); either output may be NULL */
+int rtpg_mlp_eval(rtpg_mlp* h, int64_t n, const float* pos, const float* nrm, const float* wo, float* out_raw,
+                  float* out_lobes, void* stream);
+/* gradient of the loss over n records ADDED to grads (device, RTPG_MLP_PARAMS floats, [in][out]);
+ * host_loss: the loss (NULL: not read) */
+int rtpg_mlp_loss_grad(rtpg_mlp* h, int64_t n, const float* pos, const float* nrm, const float* wo, const float* wi,
+                       const float* w, float* grads, float* host_loss, void* stream);
+/* epochs x (n / batch) Adam steps on the given records, or on the record buffer when pos is
+ * NULL; host_last_loss: the last minibatch's loss (NULL: not read) */
+int rtpg_mlp_train(rtpg_mlp* h, int64_t n, const float* pos, const float* nrm, const float* wo, const float* wi,
+                   const float* w, uint32_t batch, uint32_t epochs, float* host_last_loss, void* stream);
+/* records written so far (may exceed the capacity: the excess was dropped); clear = 1 empties */
+int rtpg_mlp_records(rtpg_mlp* h, uint32_t* host_count, int clear, void* stream);
+int rtpg_mlp_record_arrays(rtpg_mlp* h, float** pos, float** nrm, float** wo, float** wi, float** w);
+int rtpg_mlp_status(rtpg_mlp* h, uint32_t* host_status, int clear, void* stream);
+
 /* ================================================================ scene / hit queries
  * The integrator's closest-hit and any-hit queries (RTLib: optixTrace inside TraceRadiance /
  * TraceOccluded, RTLib/Src/Ext/OPX7/Test/cuda/SimpleKernel.h:347-366, "SK.h") answered by a
@@ -353,6 +386,8 @@ int rtpg_tracer_render_adjoint(rtpg_tracer* h, uint32_t spp, uint32_t flags, con
                                int32_t texture_index, float* grad_texture, float* grad_light_emission, void* stream);
 /* mean radiance per pixel, width x height x RGB float (device) */
 int rtpg_tracer_image(rtpg_tracer* h, float* out_rgb, void* stream);
+/* the same in FP64 (double per channel) */
+int rtpg_tracer_image_f64(rtpg_tracer* h, double* out_rgb, void* stream);
 int rtpg_tracer_accumulation(rtpg_tracer* h, const double** dev_accum, uint64_t* host_samples);
 int rtpg_tracer_stats(rtpg_tracer* h, uint64_t* host_samples, uint64_t* host_paths);
 /* Device counters since the last clear: path-bounces shaded (bounce visits) and shadow rays

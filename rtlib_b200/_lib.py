@@ -84,7 +84,17 @@ _SIGS = {
     "rtpg_tracer_render": [P, U32, U32, P, P],
     "rtpg_tracer_render_guided": [P, P, P, U32, U32, U32, P],
     "rtpg_tracer_render_grid": [P, U32, U32, P, P, P],
+    "rtpg_mlp_create": [P, P, U32, F32, U32, P],
+    "rtpg_mlp_destroy": [P],
+    "rtpg_mlp_params": [P, P, P, P],
+    "rtpg_mlp_eval": [P, I64, P, P, P, P, P, P],
+    "rtpg_mlp_loss_grad": [P, I64, P, P, P, P, P, P, P, P],
+    "rtpg_mlp_train": [P, I64, P, P, P, P, P, U32, U32, P, P],
+    "rtpg_mlp_records": [P, P, C.c_int, P],
+    "rtpg_mlp_record_arrays": [P, P, P, P, P, P],
+    "rtpg_mlp_status": [P, P, C.c_int, P],
     "rtpg_tracer_set_light_emission": [P, P, U32],
+    "rtpg_tracer_image_f64": [P, P, P],
     "rtpg_tracer_render_adjoint": [P, U32, U32, P, I32, P, P, P],
     "rtpg_tracer_render_grid_guided": [P, P, P, P, U32, U32, U32, P],
     "rtpg_tracer_image": [P, P, P],

@@ -569,9 +569,10 @@ __global__ void k_seed_init(uint32_t* seeds, uint32_t n, uint32_t seed) {
         seeds[p] = pcg1d(pcg1d(p) ^ (seed * 0x9E3779B9u)) | 1u;
 }
 
-__global__ void k_image(const double* accum, uint32_t n, double inv, float* out) {
+template <class T>
+__global__ void k_image(const double* accum, uint32_t n, double inv, T* out) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < 3 * n; i += gridDim.x * blockDim.x)
-        out[i] = (float)(accum[i] * inv);
+        out[i] = (T)(accum[i] * inv);
 }
 
 }  // namespace rtpg
@@ -967,6 +968,15 @@ int rtpg_tracer_render_grid(rtpg_tracer* h, uint32_t spp, uint32_t flags, rtpg_h
 // Mean radiance per pixel (accumulation / samples), RGB float, row-major, y = 0 first.
 int rtpg_tracer_image(rtpg_tracer* h, float* out_rgb, void* stream) {
     if (!h || !out_rgb) return fail(RTPG_EINVAL, "rtpg_tracer_image: null argument");
+    const double inv = h->samples ? 1.0 / (double)h->samples : 0.0;
+    k_image<<<grid_for(3ull * h->dev.npath, 256, 4), 256, 0, as_stream(stream)>>>(h->dev.accum, h->dev.npath, inv, out_rgb);
+    RTPG_LAUNCH_CHECK();
+    return RTPG_OK;
+}
+
+// Mean radiance per pixel in FP64 (accumulation / samples).
+int rtpg_tracer_image_f64(rtpg_tracer* h, double* out_rgb, void* stream) {
+    if (!h || !out_rgb) return fail(RTPG_EINVAL, "rtpg_tracer_image_f64: null argument");
     const double inv = h->samples ? 1.0 / (double)h->samples : 0.0;
     k_image<<<grid_for(3ull * h->dev.npath, 256, 4), 256, 0, as_stream(stream)>>>(h->dev.accum, h->dev.npath, inv, out_rgb);
     RTPG_LAUNCH_CHECK();

@@ -1,0 +1,51 @@
+"""Image error metrics and the result-image format of the test application.
+
+``rmae`` / ``smape`` restate the comparison tool RTLibExtOPX7Comp.cpp:124-145 (all-range
+branch); ``relmse`` is the relative mean squared error used for equal-time comparisons:
+mean over pixels and channels of (img - ref)^2 / (ref^2 + eps).  ``save_result_bin`` writes
+what SaveResultImage writes (RTLibExtOPX7TestApplication.cpp:2590-2610): float RGB mean
+radiance with the pixel order reversed."""
+from __future__ import annotations
+
+import numpy as np
+
+
+def relmse(img, ref, eps=1e-2):
+    img = np.asarray(img, np.float64)
+    ref = np.asarray(ref, np.float64)
+    ok = np.isfinite(img).all(axis=-1) & np.isfinite(ref).all(axis=-1)
+    return float(np.mean(((img - ref) ** 2 / (ref ** 2 + eps))[ok]))
+
+
+def rmae(img, ref):
+    """sum |img - ref| (Euclidean RGB distance) / sum (|ref| + |img|) / 2 over pixels with ref != 0."""
+    b = np.asarray(ref, np.float32).reshape(-1, 3)
+    c = np.asarray(img, np.float32).reshape(-1, 3)
+    ok = ~(np.isnan(b).any(1) | np.isnan(c).any(1))
+    nb = np.sqrt((b ** 2).sum(1))
+    m = ok & (nb > 0)
+    d = np.sqrt(((b - c) ** 2).sum(1))
+    mean = ((nb + np.sqrt((c ** 2).sum(1))) * 0.5)[m].sum()
+    return float(d[m].sum() / mean) if mean > 0 else 0.0
+
+
+def smape(img, ref):
+    """mean over all pixels of |img - ref| / |ref| (Euclidean RGB), pixels with ref = 0 adding 0."""
+    b = np.asarray(ref, np.float32).reshape(-1, 3)
+    c = np.asarray(img, np.float32).reshape(-1, 3)
+    ok = ~(np.isnan(b).any(1) | np.isnan(c).any(1))
+    nb = np.sqrt((b ** 2).sum(1))
+    m = ok & (nb > 0)
+    d = np.sqrt(((b - c) ** 2).sum(1))
+    return float((d[m] / nb[m]).sum() / b.shape[0])
+
+
+def save_result_bin(path, mean_rgb):
+    """mean_rgb: (h, w, 3) float; written with the pixel order reversed, float32."""
+    a = np.asarray(mean_rgb, np.float32).reshape(-1, 3)[::-1]
+    a.tofile(path)
+
+
+def load_result_bin(path, width, height):
+    a = np.fromfile(path, np.float32).reshape(-1, 3)[::-1]
+    return a.reshape(height, width, 3)

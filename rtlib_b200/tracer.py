@@ -149,6 +149,13 @@ class Tracer:
         call("rtpg_tracer_image", self.h, ptr(out), stream_ptr(stream))
         return out
 
+    def image64(self, out=None, stream=None):
+        import torch
+        if out is None:
+            out = torch.empty((self.height, self.width, 3), dtype=torch.float64, device=self.device)
+        call("rtpg_tracer_image_f64", self.h, ptr(out), stream_ptr(stream))
+        return out
+
     def accumulation(self):
         """(device pointer of the FP64 accumulation, samples so far)."""
         p, s = C.c_void_p(), C.c_uint64()

@@ -1,0 +1,21 @@
+"""Error metrics and the result-image format (CPU)."""
+import numpy as np
+
+from rtlib_b200 import metrics
+
+
+def test_relmse_rmae_smape_small_cases(tmp_path):
+    ref = np.array([[[1.0, 1.0, 1.0], [0.0, 0.0, 0.0]]], np.float32)
+    img = np.array([[[1.1, 1.0, 0.9], [0.0, 0.0, 0.0]]], np.float32)
+    # relMSE: (0.01 / 1.01 + 0 + 0.01 / 1.01) / 6
+    assert abs(metrics.relmse(img, ref) - (0.02 / 1.01) / 6) < 1e-7
+    d = np.sqrt(0.02)
+    assert abs(metrics.smape(img, ref) - d / np.sqrt(3) / 2) < 1e-6
+    mean = (np.sqrt(3) + np.sqrt(1.21 + 1 + 0.81)) / 2
+    assert abs(metrics.rmae(img, ref) - d / mean) < 1e-6
+    assert metrics.relmse(ref, ref) == 0.0
+    p = tmp_path / "r.bin"
+    metrics.save_result_bin(p, img)
+    raw = np.fromfile(p, np.float32).reshape(-1, 3)
+    assert np.array_equal(raw[0], img[0, 1]) and np.array_equal(raw[1], img[0, 0])
+    assert np.array_equal(metrics.load_result_bin(p, 2, 1), img)
