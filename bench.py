@@ -10,6 +10,13 @@ build -> refine between passes.  One step = one complete guided render.  Metric:
 (camera paths = pixels x spp).  "e2e" repeats the step through the C ABI from host arrays:
 the scene goes host->device, the image comes back device->host, both inside the timed region.
 
+Workload "occluded": the occluded-light scene (1280 x 720, ~1M triangles in a 10 x 4 x 10 room lit
+only through a 1 x 2 doorway by 4096 emitters) with NEE + RIS (32 candidates), max depth 16 and
+the hash-grid guide (2^20 slots, Morton keys, Morton quadtrees) under its pass controller.
+
+Workload "learned": equal-time relMSE of the learned guide against plain SD-tree guiding on the
+occluded scene (budgets --budgets, reference --ref-seconds of SD-tree rendering).
+
 Workload "sdtree" (SD-tree standalone): 2^20 seeded radiance records (uniform positions,
 4-lobe vMF directions kappa 50, lognormal(0,1) radiance) are recorded, the trees are built and
 refined at 12000*sqrt(2), then 2^22 guided sample+pdf queries run at uniform positions.
@@ -446,6 +453,177 @@ def _cornell_cpu(threads, seconds, scene_px=32):
     return paths / dt / 1e6, dt, paths
 
 
+# ---------------------------------------------------------------------------- occluded workload
+O_W, O_H, O_DEPTH = 1280, 720, 16
+O_AABB = ((-0.005,) * 3, (14.005, 4.005, 10.005))
+O_GRID_BOUNDS, O_SLOTS, O_LEVEL = (256, 64, 192), 1 << 20, 4
+O_BUDGET = 15  # passes of 1 (locate), 2 (record), 4 and 8 spp (record + sample)
+
+
+def bench_occluded_ours(args, rank, world):
+    """The occluded-light scene with NEE + RIS (32 candidates) and the hash-grid guide (Morton
+    keys, 2^20 slots): one step = one HT-guided render of O_BUDGET spp under the Morton pass
+    controller (locate, record, record + sample)."""
+    import torch
+    from rtlib_b200 import scenes
+    from rtlib_b200.hashgrid import KEY_MORTON, HashGrid, MortonQuadTreeController, MortonQuadTrees
+    from rtlib_b200.tracer import FLAG_NEE, FLAG_RIS, Tracer
+
+    dev = torch.device("cuda", rank % max(1, torch.cuda.device_count()))
+    torch.cuda.set_device(dev)
+    sc = scenes.occluded_rooms(O_W, O_H)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    flags = FLAG_NEE | FLAG_RIS
+    tr = Tracer(sc, dev, max_depth=O_DEPTH, num_candidates=32, seed=1)
+    grid = HashGrid(*O_AABB, O_GRID_BOUNDS, O_SLOTS, keying=KEY_MORTON)
+    trees = MortonQuadTrees(O_SLOTS, level=O_LEVEL, fraction=0.3)
+    ctrl = MortonQuadTreeController(trees, O_BUDGET, iteration_for_built=1, ratio_for_budget=0.5)
+    stream = torch.cuda.current_stream()
+
+    def step(t=tr, g=grid, q=trees, c=ctrl):
+        t.clear()
+        g.clear()
+        c.start()
+        t.render_grid_guided(g, q, c, flags, samples_per_launch=1)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    samples = tr.stats()["samples"]
+    clocks = ClockSampler(dev.index)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    _barrier(world)
+    torch.cuda.synchronize()
+    clocks.start()
+    for k in range(args.steps):
+        flush.fill_(k & 0xff)
+        a, c = ev[k]
+        a.record(stream)
+        step()
+        c.record(stream)
+    torch.cuda.synchronize()
+    _barrier(world)
+    clk = clocks.stop()
+    ms = _max_over_ranks(sum(a.elapsed_time(c) for a, c in ev) / len(ev), world, dev)
+    cnt = tr.counters()
+    assert grid.status() == 0 and trees.status() == 0
+    cells = int((grid.export() != 0).sum())
+    # unguided NEE + RIS on the same tracer, and kernel times of one guided step
+    a, c = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    tr.clear()
+    a.record(stream)
+    tr.render(samples, flags)
+    c.record(stream)
+    torch.cuda.synchronize()
+    plain_ms = a.elapsed_time(c)
+    tr.set_timing(True)
+    step()
+    tk = tr.timings()
+    tr.set_timing(False)
+    peak, peak_kind = _peaks()
+    bpb = _traffic("k_bounce_bytes_per_path_bounce")
+    achieved = cnt["path_bounces"] * BOUNCE_BYTES / (tk["bounce"][0] * 1e-3) / 1e9
+    # e2e: scene and structures from host arrays, image back to host
+    h_img = torch.empty((O_H, O_W, 3), dtype=torch.float32).pin_memory()
+    h2d = sum(np.asarray(sc[k]).nbytes for k in ("tri_v", "tri_mat", "tri_uv", "light_tris"))
+    e2e_ms = []
+    for k in range(max(1, args.steps // 2)):
+        flush.fill_(k & 0xff)
+        torch.cuda.synchronize()
+        a, c = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        tr2 = Tracer(sc, dev, max_depth=O_DEPTH, num_candidates=32, seed=1)
+        g2 = HashGrid(*O_AABB, O_GRID_BOUNDS, O_SLOTS, keying=KEY_MORTON)
+        q2 = MortonQuadTrees(O_SLOTS, level=O_LEVEL, fraction=0.3)
+        c2 = MortonQuadTreeController(q2, O_BUDGET, iteration_for_built=1, ratio_for_budget=0.5)
+        step(tr2, g2, q2, c2)
+        h_img.copy_(tr2.image(), non_blocking=True)
+        c.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms.append(a.elapsed_time(c))
+        del tr2, g2, q2, c2
+    e2e = _max_over_ranks(sum(e2e_ms) / len(e2e_ms), world, dev)
+    paths = O_W * O_H * samples * world
+    return {
+        "metric": "Mpaths/s", "value": paths / (ms * 1e-3) / 1e6, "unit": "Mpaths/s", "ms_per_step": ms,
+        "e2e": {"value": paths / (e2e * 1e-3) / 1e6, "unit": "Mpaths/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(h_img.numel() * 4)},
+        "roofline": {"kernel": "k_bounce", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs (burst copy)",
+                     "traffic": None if bpb is None else bpb * cnt["path_bounces"] / max(1, O_DEPTH * samples),
+                     "algorithmic_bytes_per_path_bounce": BOUNCE_BYTES,
+                     "kernel_ms_per_step": {kk: v[0] for kk, v in tk.items()},
+                     "note": "bounce = BVH closest hit over 1M triangles + shading + RIS over 32 light samples + "
+                             "one shadow ray; bound by traversal latency and issue"},
+        "clocks": clk,
+        "gpu_launches": (1 + O_DEPTH + 1) * samples * args.steps,
+        "counters_per_step": cnt,
+        "unguided_nee_ris_Mpaths_s": O_W * O_H * samples / (plain_ms * 1e-3) / 1e6,
+        "grid_cells": cells, "spp_per_step": samples,
+    }
+
+
+# ---------------------------------------------------------------------------- learned-guide workload
+def _timed_render(fn, seconds):
+    import torch
+    t0 = time.perf_counter()
+    n = 0
+    while time.perf_counter() - t0 < seconds:
+        fn()
+        torch.cuda.synchronize()
+        n += 1
+    return n
+
+
+def bench_learned(args):
+    """Equal-time comparison on the occluded-light scene (NEE + RIS, 32 candidates, max depth 16):
+    plain SD-tree guiding against the learned guide (the SD-tree's pass schedule, network trained
+    on the tracer's records between passes), relMSE against a long SD-tree render.  Wall-clock
+    budgets include every training step; each method synchronises per launch."""
+    import torch
+    from rtlib_b200 import metrics, scenes
+    from rtlib_b200.learned import render_learned
+    from rtlib_b200.mlp import MLPGuide
+    from rtlib_b200.sdtree import SDTree, SDTreeController
+    from rtlib_b200.tracer import FLAG_NEE, FLAG_RIS, Tracer
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    w, h = args.size
+    sc = scenes.occluded_rooms(w, h)
+    flags = FLAG_NEE | FLAG_RIS
+
+    def sdtree_run(tr, seconds):
+        tree = SDTree(*O_AABB, fraction=0.5)
+        ctrl = SDTreeController(tree, 1 << 20, iteration_for_built=0, ratio_for_budget=0.5, samples_per_launch=1)
+        ctrl.start()
+        return _timed_render(lambda: tr.render_guided(tree, ctrl, flags, max_launches=1), seconds)
+
+    warm = Tracer(sc, dev, max_depth=O_DEPTH, seed=5)
+    sdtree_run(warm, 2.0)
+    del warm
+    ref_tr = Tracer(sc, dev, max_depth=O_DEPTH, seed=99)
+    ref_spp = sdtree_run(ref_tr, args.ref_seconds)
+    ref = ref_tr.image().cpu().numpy()
+    del ref_tr
+    out = []
+    for budget in args.budgets:
+        tr = Tracer(sc, dev, max_depth=O_DEPTH, seed=3)
+        n_sd = sdtree_run(tr, budget)
+        e_sd = metrics.relmse(tr.image().cpu().numpy(), ref, normalize=True)
+        del tr
+        tr = Tracer(sc, dev, max_depth=O_DEPTH, seed=3)
+        g = MLPGuide((-0.1, -0.1, -0.1), (14.1, 4.1, 10.1), seed=1, learning_rate=1e-3, record_capacity=1 << 18)
+        log = []
+        n_ml = render_learned(tr, g, time_budget_s=budget, base_flags=flags, fraction=0.5, ratio=0.5,
+                              epochs=args.epochs, batch=4096, log=log)
+        e_ml = metrics.relmse(tr.image().cpu().numpy(), ref, normalize=True)
+        out.append({"budget_s": budget, "relmse_sdtree": e_sd, "relmse_learned": e_ml, "ratio": e_ml / e_sd,
+                    "spp_sdtree": n_sd, "spp_learned": n_ml, "train_log": log[-3:], "mlp_status": g.status()})
+        del tr, g
+    return {"budgets": out, "ref_spp": ref_spp, "ref_seconds": args.ref_seconds}
+
+
 # ---------------------------------------------------------------------------- plumbing
 def _barrier(world):
     if world > 1:
@@ -469,7 +647,11 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="cornell", choices=["cornell", "sdtree"])
+    ap.add_argument("--workload", default="cornell", choices=["cornell", "sdtree", "occluded", "learned"])
+    ap.add_argument("--budgets", default="30,120", help="learned: equal-time budgets in seconds")
+    ap.add_argument("--ref-seconds", type=float, default=300.0, help="learned: reference render time")
+    ap.add_argument("--epochs", type=int, default=16, help="learned: Adam epochs over each pass's records")
+    ap.add_argument("--size", default="1280x720", help="learned: image size")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--budget", type=int, default=2047,
                     help="cornell: total spp of the pass schedule (2047 = passes 1..1024); smaller values "
@@ -478,9 +660,43 @@ def main():
     args.warmup = max(args.warmup, 3)
     rank = _env_int("RANK", 0)
     world = _env_int("WORLD_SIZE", 1)
+    if args.workload == "learned":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the learned guide has no counterpart in RTLib; "
+                              "its judge is the SD-tree arm of the same run"}), flush=True)
+            return 0
+        if rank != 0:
+            return 0
+        args.budgets = [float(x) for x in args.budgets.split(",")]
+        args.size = tuple(int(x) for x in args.size.split("x"))
+        r = bench_learned(args)
+        last = r["budgets"][-1]
+        line = {"metric": "equal-time relMSE, learned guide / SD-tree guide (occluded scene)", "value": last["ratio"],
+                "unit": "ratio", "n_gpus": 1, "steps": len(r["budgets"]), "warmup": args.warmup,
+                "ms_per_step": last["budget_s"] * 1e3, "higher_is_better": False, "scaling": "weak",
+                "vs_baseline": None, "dtype": "bf16 network / f32 tracer", "data": "synthetic",
+                "config": {"workload": f"occluded-rooms {args.size[0]}x{args.size[1]}, NEE+RIS 32, depth 16; "
+                                       f"equal wall-clock budgets {args.budgets} s; reference: SD-tree "
+                                       f"{r['ref_seconds']} s ({r['ref_spp']} spp)", "relmse": "normalised by the "
+                                       "reference mean, eps 1e-2"},
+                "budgets": r["budgets"]}
+        print(json.dumps(line), flush=True)
+        return 0
+    if args.workload == "occluded" and args.impl == "reference":
+        if rank == 0:
+            print(json.dumps({"impl": "reference", "unavailable": "RTLib's integrator exists only as OptiX "
+                              "programs and the CPU restatement intersects by brute force, which is not a "
+                              "meaningful baseline over 1M triangles; see the cornell workload"}), flush=True)
+        return 0
     cornell = args.workload == "cornell"
+    occluded = args.workload == "occluded"
     set_budget(args.budget)
-    if cornell:
+    if occluded:
+        cfg = {"workload": f"occluded-rooms HTRIS: {O_W}x{O_H}, ~1M triangles, 4096 emitters, NEE + RIS 32 "
+                           f"candidates, max depth 16, hash grid 2^20 slots (Morton keys) + level-{O_LEVEL} "
+                           f"Morton quadtrees, {O_BUDGET} spp budget", "width": O_W, "height": O_H, "max_depth": O_DEPTH}
+        metric, unit = "Mpaths/s", "Mpaths/s"
+    elif cornell:
         cfg = {"workload": f"cornell-guided: 512x512, {C_BUDGET} spp budget in doubling passes, max depth 8, NEE, "
                            "SD-tree guiding fraction 0.5", "width": C_W, "height": C_H, "spp": C_BUDGET + 1,
                "max_depth": C_MAX_DEPTH}
@@ -524,7 +740,7 @@ def main():
         from datetime import timedelta
         torch.cuda.set_device(_env_int("LOCAL_RANK", rank))
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
-    res = (bench_cornell_ours if cornell else bench_sdtree_ours)(args, rank, world)
+    res = (bench_occluded_ours if occluded else bench_cornell_ours if cornell else bench_sdtree_ours)(args, rank, world)
     cfg["l2"] = "flushed (256 MiB write) before every timed step"
     cfg["parallelism"] = f"replicas x{world}"
     line = {"metric": res["metric"], "value": res["value"], "unit": res["unit"], "n_gpus": world,
@@ -532,10 +748,10 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic", "config": cfg, "e2e": res["e2e"], "roofline": res["roofline"],
             "clocks": res["clocks"], "gpu_launches": res["gpu_launches"]}
-    for k in ("sdtree", "counters_per_step"):
+    for k in ("sdtree", "counters_per_step", "unguided_nee_ris_Mpaths_s", "grid_cells", "spp_per_step"):
         if k in res:
             line[k] = res[k]
-    if rank == 0 and not args.no_cpu_baseline:
+    if rank == 0 and not args.no_cpu_baseline and not occluded:
         if cornell:
             cores = os.cpu_count() or 1
             v, dt, paths = _cornell_cpu(cores, 10.0)

@@ -329,6 +329,7 @@ typedef struct rtpg_tracer_desc {
 #define RTPG_TRACE_FLAG_BUILD 16u
 #define RTPG_TRACE_FLAG_FINAL 32u
 #define RTPG_TRACE_FLAG_LOCATE 64u /* insert unseen cells into the current hash table */
+#define RTPG_TRACE_FLAG_USE_MLP 128u /* learned vMF-mixture guide (rtpg_tracer_render_mlp) */
 /* tri_vertices: num_triangles x 9 floats (v0, v1, v2 of triangle i, the scene's order);
  * tri_material: uint32 per triangle; tri_uv: 6 floats per triangle or NULL; light_tris:
  * triangle ids of the emitters, light mesh i = light_tris[first[i] .. first[i] + count[i])
@@ -366,6 +367,13 @@ int rtpg_tracer_render_grid(rtpg_tracer* h, uint32_t spp, uint32_t flags, rtpg_h
 int rtpg_tracer_render_grid_guided(rtpg_tracer* h, rtpg_hashgrid* grid, rtpg_mqt* mqt, rtpg_mqt_controller* ctrl,
                                    uint32_t base_flags, uint32_t samples_per_launch, uint32_t max_launches,
                                    void* stream);
+/* `spp` samples per pixel with the learned guide (no counterpart in RTLib): flags = USE_MLP
+ * [| NEE | RIS] [| BUILD: sample the mixture with probability `fraction`, woPdf = (1 - fraction)
+ * bsdfPdf + fraction q] [| FINAL: no training records].  Unless FINAL, every committed trace
+ * vertex (the SD-tree's record) is appended to the guide's record buffer with probability
+ * record_keep, up to its capacity.  The tracer and the guide must be on the same device. */
+int rtpg_tracer_render_mlp(rtpg_tracer* h, uint32_t spp, uint32_t flags, rtpg_mlp* mlp, float fraction,
+                           float record_keep, void* stream);
 /* Emitter radiances (no counterpart in RTLib, which fixes them at load): light mesh i gets
  * host_rgb[3i..3i+2], both as MeshLight::emission for NEE and as the emission of its material.
  * Every light mesh must have its own emissive material. */

@@ -16,85 +16,6 @@
 
 namespace rtpg {
 
-constexpr int kMlpThreads = kMlpTile;
-constexpr size_t kSmemW = size_t(kMlpParams) * 2;             // 32 KB of bf16 weights
-constexpr size_t kSmemX = size_t(kMlpTile) * kMlpIn * 2;       // 20 KB input features
-constexpr size_t kSmemH = size_t(kMlpTile) * kMlpHidden * 2;   // 16 KB per hidden activation
-constexpr size_t kSmemEval = kSmemW + kSmemX + 64;
-constexpr size_t kSmemTrain = kSmemW + kSmemX + 4 * kSmemH + 64;  // X0, H1, H2, H3, dY
-// TMEM columns of the training kernel: forward / dX accumulator, then dW^T of layers 3..0
-constexpr uint32_t kColD = 0, kColW3 = 64, kColW2 = 128, kColW1 = 192, kColW0 = 256, kTrainCols = 512;
-constexpr uint32_t kEvalCols = 64;
-
-struct MlpDev {
-    const __nv_bfloat16* wq;  // bf16 weights, each matrix in the core-matrix layout
-    float3 mn, inv_ext;       // AABB of the positions
-    unsigned* status;
-};
-
-struct Records {
-    const float* pos;  // 3 per record
-    const float* nrm;
-    const float* wo;
-    const float* wi;
-    const float* w;    // weight (>= 0)
-};
-
-// ------------------------------------------------------------------ shared building blocks
-__device__ __forceinline__ void load_weights(__nv_bfloat16* ws, const __nv_bfloat16* wq) {
-    const uint4* s = reinterpret_cast<const uint4*>(wq);
-    uint4* d = reinterpret_cast<uint4*>(ws);
-    for (int i = threadIdx.x; i < kMlpParams / 8; i += blockDim.x) d[i] = __ldg(s + i);
-}
-// features of sample t into row t of X0
-__device__ __forceinline__ void store_features(__nv_bfloat16* x0, int t, const float* f) {
-#pragma unroll
-    for (int c = 0; c < kMlpIn; c += 8) st_bf16x8(x0 + blk(t, c, kMlpIn), f + c);
-}
-// all threads: make the shared-memory operands written by this CTA visible to the tensor
-// cores and order earlier TMEM loads before the next MMA
-__device__ __forceinline__ void mma_barrier() {
-    fence_async_smem();
-    tc_fence_before();
-    __syncthreads();
-    tc_fence_after();
-}
-// D[128 x n] (+)= A[128 x k] (K-major, a_cols columns) x W[k x n] (MN-major, n columns)
-__device__ __forceinline__ void issue_fwd(uint32_t d, uint32_t a, uint32_t a_cols, uint32_t k, uint32_t w, uint32_t n) {
-    const uint32_t id = umma_idesc(128, n, false, true);
-    for (uint32_t kk = 0; kk < k; kk += 16) umma_f16(d, desc_kmajor(a, kk, a_cols), desc_mnmajor(w, kk, n), id, kk > 0);
-}
-// D[128 x nin] = dY[128 x kout] (K-major, 64 columns) x W^T, W stored [nin x kout]
-__device__ __forceinline__ void issue_dx(uint32_t d, uint32_t dy, uint32_t kout, uint32_t w, uint32_t nin) {
-    const uint32_t id = umma_idesc(128, nin, false, false);
-    for (uint32_t kk = 0; kk < kout; kk += 16)
-        umma_f16(d, desc_kmajor(dy, kk, kMlpHidden), desc_kmajor(w, kk, kout), id, kk > 0);
-}
-// D[64 x nin] (+)= dY^T[64 x 128] x X[128 x nin]  (dW^T of a layer over one tile)
-__device__ __forceinline__ void issue_dw(uint32_t d, uint32_t dy, uint32_t x, uint32_t x_cols, uint32_t nin, bool acc) {
-    const uint32_t id = umma_idesc(64, nin, true, true);
-    for (uint32_t kk = 0; kk < kMlpTile; kk += 16)
-        umma_f16(d, desc_mnmajor(dy, kk, kMlpHidden), desc_mnmajor(x, kk, x_cols), id, (acc || kk > 0) ? 1u : 0u);
-}
-// thread t: accumulator row t, columns c0 .. c0+15
-__device__ __forceinline__ void ld_row16(uint32_t tmem, uint32_t col, float* v) {
-    const uint32_t lane = (threadIdx.x & ~31u);
-    tmem_ld16(tmem + (lane << 16) + col, v);
-}
-// hidden epilogue: ReLU, bf16, row t of h [128 x 64]
-__device__ __forceinline__ void epilogue_relu(uint32_t tmem, __nv_bfloat16* h) {
-    const int t = threadIdx.x;
-#pragma unroll
-    for (int c = 0; c < kMlpHidden; c += 16) {
-        float v[16];
-        ld_row16(tmem, kColD + c, v);
-#pragma unroll
-        for (int i = 0; i < 16; ++i) v[i] = fmaxf(v[i], 0.0f);
-        st_bf16x8(h + blk(t, c, kMlpHidden), v);
-        st_bf16x8(h + blk(t, c + 8, kMlpHidden), v + 8);
-    }
-}
-
 // ------------------------------------------------------------------ inference
 // out_raw: 48 floats per sample (the network output); out_lobes: 40 floats per sample, lobe k
 // = (mu xyz, kappa, weight).  Either may be null.
@@ -104,7 +25,6 @@ __global__ void __launch_bounds__(kMlpThreads) k_mlp_eval(MlpDev P, int64_t n, c
     extern __shared__ __align__(128) uint8_t sm[];
     __nv_bfloat16* ws = reinterpret_cast<__nv_bfloat16*>(sm);
     __nv_bfloat16* x0 = reinterpret_cast<__nv_bfloat16*>(sm + kSmemW);
-    __nv_bfloat16* h = x0;  // a hidden activation overwrites the consumed input
     uint64_t* mbar = reinterpret_cast<uint64_t*>(sm + kSmemW + kSmemX);
     uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + kSmemW + kSmemX + 8);
     const int t = threadIdx.x;
@@ -115,7 +35,7 @@ __global__ void __launch_bounds__(kMlpThreads) k_mlp_eval(MlpDev P, int64_t n, c
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *tslot;
-    const uint32_t sw = smem_u32(ws), sx = smem_u32(x0);
+    const uint32_t sw = smem_u32(ws);
     uint32_t phase = 0;
     bool ok = true;
     for (int64_t base = int64_t(blockIdx.x) * kMlpTile; base < n; base += int64_t(gridDim.x) * kMlpTile) {
@@ -129,23 +49,8 @@ __global__ void __launch_bounds__(kMlpThreads) k_mlp_eval(MlpDev P, int64_t n, c
             for (int k = 0; k < kMlpIn; ++k) f[k] = 0.0f;
         }
         store_features(x0, t, f);
-        // layer 0 .. 2 with ReLU, layer 3 linear
-        for (int l = 0; l < 4; ++l) {
-            mma_barrier();
-            if (t == 0) {
-                if (l == 0) issue_fwd(tmem + kColD, sx, kMlpIn, kMlpIn, sw + 2 * kW0, kMlpHidden);
-                else if (l < 3) issue_fwd(tmem + kColD, sx, kMlpHidden, kMlpHidden, sw + 2 * (l == 1 ? kW1 : kW2), kMlpHidden);
-                else issue_fwd(tmem + kColD, sx, kMlpHidden, kMlpHidden, sw + 2 * kW3, kMlpOut);
-                umma_commit(mbar);
-            }
-            ok &= mbar_wait(mbar, phase);
-            phase ^= 1u;
-            tc_fence_after();
-            if (l < 3) epilogue_relu(tmem, h);
-        }
         float o[kMlpOut];
-#pragma unroll
-        for (int c = 0; c < kMlpOut; c += 16) ld_row16(tmem, kColD + c, o + c);
+        ok &= mlp_forward_tile(tmem, sw, x0, mbar, phase, o);
         if (i < n) {
             if (out_raw)
                 for (int c = 0; c < kMlpOut; ++c) out_raw[i * kMlpOut + c] = o[c];
@@ -403,12 +308,6 @@ struct rtpg_mlp {
 };
 
 namespace rtpg {
-struct MlpView {
-    MlpDev dev;
-    float *r_pos, *r_nrm, *r_wo, *r_wi, *r_w;
-    uint32_t* r_count;
-    uint32_t capacity;
-};
 MlpView mlp_view(const rtpg_mlp* h) {
     return MlpView{h->dev, h->r_pos, h->r_nrm, h->r_wo, h->r_wi, h->r_w, h->r_count, h->capacity};
 }

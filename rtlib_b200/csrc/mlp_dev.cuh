@@ -208,4 +208,118 @@ __device__ __forceinline__ float3 vmf_mixture_sample(const VmfLobe* L, float u0,
     return t * (sz * cp) + bt * (sz * sp) + n * cz;
 }
 
+// ------------------------------------------------------------------ network building blocks
+constexpr int kMlpThreads = kMlpTile;
+constexpr size_t kSmemW = size_t(kMlpParams) * 2;             // 32 KB of bf16 weights
+constexpr size_t kSmemX = size_t(kMlpTile) * kMlpIn * 2;       // 20 KB input features
+constexpr size_t kSmemH = size_t(kMlpTile) * kMlpHidden * 2;   // 16 KB per hidden activation
+constexpr size_t kSmemEval = kSmemW + kSmemX + 64;
+constexpr size_t kSmemTrain = kSmemW + kSmemX + 4 * kSmemH + 64;  // X0, H1, H2, H3, dY
+// TMEM columns of the training kernel: forward / dX accumulator, then dW^T of layers 3..0
+constexpr uint32_t kColD = 0, kColW3 = 64, kColW2 = 128, kColW1 = 192, kColW0 = 256, kTrainCols = 512;
+constexpr uint32_t kEvalCols = 64;
+
+struct MlpDev {
+    const __nv_bfloat16* wq;  // bf16 weights, each matrix in the core-matrix layout
+    float3 mn, inv_ext;       // AABB of the positions
+    unsigned* status;
+};
+
+// the learned guide as the tracer sees it: weights and the record buffer it appends to
+struct MlpView {
+    MlpDev dev;
+    float *r_pos, *r_nrm, *r_wo, *r_wi, *r_w;
+    uint32_t* r_count;
+    uint32_t capacity;
+};
+
+struct Records {
+    const float* pos;  // 3 per record
+    const float* nrm;
+    const float* wo;
+    const float* wi;
+    const float* w;    // weight (>= 0)
+};
+
+// ------------------------------------------------------------------ shared building blocks
+__device__ __forceinline__ void load_weights(__nv_bfloat16* ws, const __nv_bfloat16* wq) {
+    const uint4* s = reinterpret_cast<const uint4*>(wq);
+    uint4* d = reinterpret_cast<uint4*>(ws);
+    for (int i = threadIdx.x; i < kMlpParams / 8; i += blockDim.x) d[i] = __ldg(s + i);
+}
+// features of sample t into row t of X0
+__device__ __forceinline__ void store_features(__nv_bfloat16* x0, int t, const float* f) {
+#pragma unroll
+    for (int c = 0; c < kMlpIn; c += 8) st_bf16x8(x0 + blk(t, c, kMlpIn), f + c);
+}
+// all threads: make the shared-memory operands written by this CTA visible to the tensor
+// cores and order earlier TMEM loads before the next MMA
+__device__ __forceinline__ void mma_barrier() {
+    fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+}
+// D[128 x n] (+)= A[128 x k] (K-major, a_cols columns) x W[k x n] (MN-major, n columns)
+__device__ __forceinline__ void issue_fwd(uint32_t d, uint32_t a, uint32_t a_cols, uint32_t k, uint32_t w, uint32_t n) {
+    const uint32_t id = umma_idesc(128, n, false, true);
+    for (uint32_t kk = 0; kk < k; kk += 16) umma_f16(d, desc_kmajor(a, kk, a_cols), desc_mnmajor(w, kk, n), id, kk > 0);
+}
+// D[128 x nin] = dY[128 x kout] (K-major, 64 columns) x W^T, W stored [nin x kout]
+__device__ __forceinline__ void issue_dx(uint32_t d, uint32_t dy, uint32_t kout, uint32_t w, uint32_t nin) {
+    const uint32_t id = umma_idesc(128, nin, false, false);
+    for (uint32_t kk = 0; kk < kout; kk += 16)
+        umma_f16(d, desc_kmajor(dy, kk, kMlpHidden), desc_kmajor(w, kk, kout), id, kk > 0);
+}
+// D[64 x nin] (+)= dY^T[64 x 128] x X[128 x nin]  (dW^T of a layer over one tile)
+__device__ __forceinline__ void issue_dw(uint32_t d, uint32_t dy, uint32_t x, uint32_t x_cols, uint32_t nin, bool acc) {
+    const uint32_t id = umma_idesc(64, nin, true, true);
+    for (uint32_t kk = 0; kk < kMlpTile; kk += 16)
+        umma_f16(d, desc_mnmajor(dy, kk, kMlpHidden), desc_mnmajor(x, kk, x_cols), id, (acc || kk > 0) ? 1u : 0u);
+}
+// thread t: accumulator row t, columns c0 .. c0+15
+__device__ __forceinline__ void ld_row16(uint32_t tmem, uint32_t col, float* v) {
+    const uint32_t lane = (threadIdx.x & ~31u);
+    tmem_ld16(tmem + (lane << 16) + col, v);
+}
+// hidden epilogue: ReLU, bf16, row t of h [128 x 64]
+__device__ __forceinline__ void epilogue_relu(uint32_t tmem, __nv_bfloat16* h) {
+    const int t = threadIdx.x;
+#pragma unroll
+    for (int c = 0; c < kMlpHidden; c += 16) {
+        float v[16];
+        ld_row16(tmem, kColD + c, v);
+#pragma unroll
+        for (int i = 0; i < 16; ++i) v[i] = fmaxf(v[i], 0.0f);
+        st_bf16x8(h + blk(t, c, kMlpHidden), v);
+        st_bf16x8(h + blk(t, c + 8, kMlpHidden), v + 8);
+    }
+}
+
+// Forward pass of one tile: the features of sample t are in row t of x0 (which the hidden
+// activations then overwrite); returns sample t's 48 raw outputs in o.  Every thread of the
+// 128-thread CTA calls it; thread 0 issues the MMAs.  False if a wait on the tensor cores gave
+// up.
+__device__ __forceinline__ bool mlp_forward_tile(uint32_t tmem, uint32_t sw, __nv_bfloat16* x0, uint64_t* mbar,
+                                                 uint32_t& phase, float* o) {
+    const uint32_t sx = smem_u32(x0);
+    bool ok = true;
+    for (int l = 0; l < 4; ++l) {
+        mma_barrier();
+        if (threadIdx.x == 0) {
+            if (l == 0) issue_fwd(tmem + kColD, sx, kMlpIn, kMlpIn, sw + 2 * kW0, kMlpHidden);
+            else if (l < 3) issue_fwd(tmem + kColD, sx, kMlpHidden, kMlpHidden, sw + 2 * (l == 1 ? kW1 : kW2), kMlpHidden);
+            else issue_fwd(tmem + kColD, sx, kMlpHidden, kMlpHidden, sw + 2 * kW3, kMlpOut);
+            umma_commit(mbar);
+        }
+        ok &= mbar_wait(mbar, phase);
+        phase ^= 1u;
+        tc_fence_after();
+        if (l < 3) epilogue_relu(tmem, x0);
+    }
+#pragma unroll
+    for (int c = 0; c < kMlpOut; c += 16) ld_row16(tmem, kColD + c, o + c);
+    return ok;
+}
+
 }  // namespace rtpg

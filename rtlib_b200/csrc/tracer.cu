@@ -21,6 +21,7 @@
 #include "common.cuh"
 #include "bvh_dev.cuh"
 #include "hashgrid_dev.cuh"
+#include "mlp_dev.cuh"
 #include "mqt_dev.cuh"
 #include "sdtree_dev.cuh"
 #include "tracer_dev.cuh"
@@ -29,7 +30,9 @@ struct rtpg_scene;
 struct rtpg_sdtree;
 struct rtpg_hashgrid;
 struct rtpg_mqt;
+struct rtpg_mlp;
 namespace rtpg {
+MlpView mlp_view(const rtpg_mlp* h);
 SceneDev scene_device_view(const rtpg_scene* s);
 SDTreeDev sdtree_device_view(const rtpg_sdtree* t);
 HashGridDev hashgrid_device_view(const rtpg_hashgrid* h);
@@ -62,11 +65,11 @@ struct TracerDev {
     uint32_t* queue[2];
     uint32_t* qcount;  // [0], [1]
     // trace vertices, [kTV][npath]
-    float3 *v_pos, *v_dir, *v_thr, *v_bsdf;
+    float3 *v_pos, *v_dir, *v_thr;
     float3* b_rad;  // radiance of bounce k of every path, [max_depth][npath] (recording only)
     float *v_wopdf, *v_cos;
     uint8_t* v_flags;  // bit0 valid (a DTree exists / a grid cell was found), bit1 delta
-    uint32_t* v_cell;  // hash-grid slot of the vertex (grid guide only)
+    uint32_t* v_cell;  // hash-grid slot (grid guide) or DTree (SD-tree guide) of the vertex
     uint32_t* seeds;
     double* accum;  // 3 per pixel
     SDTreeDev tree;
@@ -83,6 +86,13 @@ struct TracerDev {
     float* grad_tex;       // 3 per texel of adj_tex
     float* grad_light;     // 3 per light mesh
     const int32_t* mat_light;  // light mesh of an emissive material, -1 otherwise
+    // learned guide: hits found ahead of shading, the mixture of every path, record appends
+    MlpView ml;
+    float mlp_fraction, mlp_keep;
+    uint32_t* hit_prim;
+    float4* hit_tuv;
+    __half* lobes;  // 40 per path: 8 x (mu xyz, kappa, weight)
+    float3 *v_nrm, *v_wo;
 };
 
 // ------------------------------------------------------------------ raygen (SimpleGuide.cu:48-81)
@@ -153,7 +163,7 @@ __device__ __forceinline__ LightSample sample_light(const TracerDev& T, float3 p
 // radiance into the color (and, recording, into the per-bounce store from which k_finish forms
 // the trace-vertex radiance), termination, compaction of the survivors into the next queue.
 // Returns whether the path continues; *shadow tells whether a shadow ray was traced.
-constexpr int kGuideNone = 0, kGuideTree = 1, kGuideGrid = 2, kAdjoint = 3;
+constexpr int kGuideNone = 0, kGuideTree = 1, kGuideGrid = 2, kAdjoint = 3, kGuideMlp = 4;
 
 // The adjoint replay (kAdjoint) runs the unguided path again from the same random numbers and
 // scatters d(loss)/d(parameter) as it goes (path-replay backpropagation): lrem starts as the
@@ -164,9 +174,19 @@ constexpr int kGuideNone = 0, kGuideTree = 1, kGuideGrid = 2, kAdjoint = 3;
 template <int G>
 __device__ __forceinline__ bool bounce_path(const TracerDev& T, uint32_t p, bool build, bool recording, bool& shadow) {
     constexpr bool use_tree = G == kGuideTree, use_grid = G == kGuideGrid, adjoint = G == kAdjoint;
+    constexpr bool use_mlp = G == kGuideMlp;
     const float3 org = T.org[p], in_dir = T.dir[p], prev_thr = T.thr[p];
     const uint32_t d = T.depth[p], prev_flags = T.hflags[p];
-    const Hit h = bvh_trace<false>(T.scene, org.x, org.y, org.z, in_dir.x, in_dir.y, in_dir.z, 0.0001f, 1.0e20f);
+    Hit h;
+    if (use_mlp) {  // found by k_hit ahead of the mixture inference
+        const float4 tuv = T.hit_tuv[p];
+        h.prim = T.hit_prim[p];
+        h.t = tuv.x;
+        h.u = tuv.y;
+        h.v = tuv.z;
+    } else {
+        h = bvh_trace<false>(T.scene, org.x, org.y, org.z, in_dir.x, in_dir.y, in_dir.z, 0.0001f, 1.0e20f);
+    }
     const size_t vi = size_t(d < kTV ? d : 0) * T.npath + p;
     bool pend = false;
     float3 sdir = f3(0.f, 0.f, 0.f), scontrib = f3(0.f, 0.f, 0.f);
@@ -258,6 +278,28 @@ __device__ __forceinline__ bool bounce_path(const TracerDev& T, uint32_t p, bool
             const float2 c = dir_to_canonical(direction.x, direction.y, direction.z);
             const float dtree_pdf = fmaxf(dtree_pdf_g(T.tree.s_nodes, soff, guided, c.x, c.y), 0.0f);
             wo_pdf = (1.0f - T.tree.fraction) * bsdf_pdf + T.tree.fraction * dtree_pdf;
+        } else if (use_mlp && build) {
+            // the learned mixture of this path's hit (k_mlp_lobes)
+            VmfLobe Lb[kMlpLobes];
+            const __half* lp = T.lobes + size_t(p) * 40;
+#pragma unroll
+            for (int k = 0; k < kMlpLobes; ++k) {
+                Lb[k].mu = f3(__half2float(lp[5 * k]), __half2float(lp[5 * k + 1]), __half2float(lp[5 * k + 2]));
+                Lb[k].kappa = __half2float(lp[5 * k + 3]);
+                Lb[k].weight = __half2float(lp[5 * k + 4]);
+            }
+            if (rnd1(rng) < T.mlp_fraction) {
+                const float u0 = rnd1(rng);
+                const float u1 = rnd1(rng);
+                const float u2 = rnd1(rng);
+                direction = normalize3(vmf_mixture_sample(Lb, u0, u1, u2));
+                cosine = dot3(direction, fn);
+                const float cp2 = fmaxf(cosine * kInvPi, 0.0f);
+                const float pp2 = glossy ? phong_pdf(direction, refl, m.shininess) : 0.0f;
+                bsdf_val = diffuse * kInvPi + m.specular * sf * pp2;
+                bsdf_pdf = sel * cp2 + (1.0f - sel) * pp2;
+            }
+            wo_pdf = (1.0f - T.mlp_fraction) * bsdf_pdf + T.mlp_fraction * vmf_mixture_pdf(Lb, direction);
         } else if (use_grid && build && prv_cell != 0xffffffffu) {
             // the Morton quadtree of the cell (SimpleGuide2.cu:350-377)
             float dtree_pdf;
@@ -380,14 +422,23 @@ __device__ __forceinline__ bool bounce_path(const TracerDev& T, uint32_t p, bool
     T.hflags[p] = flags;
     T.rng[p] = rng;
     if (recording && d < kTV) {
-        T.v_pos[vi] = position;
+        if (use_mlp) T.v_pos[vi] = position;
         T.v_dir[vi] = direction;
         T.v_thr[vi] = cur_thr;
-        T.v_bsdf[vi] = bsdf_val;
         T.v_wopdf[vi] = wo_pdf;
         T.v_cos[vi] = cosine;
-        T.v_flags[vi] = (uint8_t)((use_grid ? (cell != 0xffffffffu ? 1u : 0u) : 1u) | ((flags & HF_DELTA) ? 2u : 0u));
+        // bit 0: the commit may use the vertex -- a DTree / found cell, and a finite,
+        // non-negative BSDF value (isValidBsdfVal of TraceVertexT::Commit); bit 1: delta
+        const bool ok_b = isfinite(bsdf_val.x) && bsdf_val.x >= 0.f && isfinite(bsdf_val.y) && bsdf_val.y >= 0.f &&
+                          isfinite(bsdf_val.z) && bsdf_val.z >= 0.f;
+        const bool has_guide = use_grid ? cell != 0xffffffffu : true;
+        T.v_flags[vi] = (uint8_t)((has_guide && ok_b ? 1u : 0u) | ((flags & HF_DELTA) ? 2u : 0u));
         if (use_grid) T.v_cell[vi] = cell;
+        if (use_tree) T.v_cell[vi] = dt;  // the vertex's DTree, found once here for the commit
+        if (use_mlp) {
+            T.v_nrm[vi] = fn;
+            T.v_wo[vi] = f3(-in_dir.x, -in_dir.y, -in_dir.z);
+        }
     }
     float3 L = rad;
     bool lit = false;
@@ -440,7 +491,89 @@ __device__ __forceinline__ bool bounce_path(const TracerDev& T, uint32_t p, bool
 // guide kinds (and the adjoint replay), a template argument so that each variant carries only
 // its own code
 __host__ __device__ constexpr int guide_of(uint32_t flags) {
-    return (flags & RTPG_TRACE_FLAG_USE_TREE) ? kGuideTree : ((flags & RTPG_TRACE_FLAG_USE_GRID) ? kGuideGrid : kGuideNone);
+    return (flags & RTPG_TRACE_FLAG_USE_TREE) ? kGuideTree
+           : (flags & RTPG_TRACE_FLAG_USE_GRID) ? kGuideGrid
+           : (flags & RTPG_TRACE_FLAG_USE_MLP)  ? kGuideMlp
+                                                 : kGuideNone;
+}
+
+// learned guide, stage 1 of a bounce: closest hits of the queue
+__global__ void __launch_bounds__(kTB) k_hit(TracerDev T, int in) {
+    const uint32_t n = T.qcount[in];
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        const uint32_t p = T.queue[in][q];
+        const float3 o = T.org[p], d = T.dir[p];
+        const Hit h = bvh_trace<false>(T.scene, o.x, o.y, o.z, d.x, d.y, d.z, 0.0001f, 1.0e20f);
+        T.hit_prim[p] = h.prim;
+        T.hit_tuv[p] = make_float4(h.t, h.u, h.v, 0.0f);
+    }
+}
+
+// learned guide, stage 2: the mixture of every queued path that hit a Phong surface, 128
+// paths per tile on the tensor cores (features of path q in row q of the tile)
+__global__ void __launch_bounds__(kMlpThreads) k_mlp_lobes(TracerDev T, int in) {
+    extern __shared__ __align__(128) uint8_t sm[];
+    __nv_bfloat16* ws = reinterpret_cast<__nv_bfloat16*>(sm);
+    __nv_bfloat16* x0 = reinterpret_cast<__nv_bfloat16*>(sm + kSmemW);
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(sm + kSmemW + kSmemX);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + kSmemW + kSmemX + 8);
+    const int t = threadIdx.x;
+    if (t < 32) tmem_alloc(tslot, kEvalCols);
+    if (t == 0) mbar_init(mbar, 1);
+    load_weights(ws, T.ml.dev.wq);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tslot, sw = smem_u32(ws);
+    uint32_t phase = 0;
+    bool ok = true;
+    const uint32_t n = T.qcount[in];
+    for (uint32_t base = blockIdx.x * kMlpTile; base < n; base += gridDim.x * kMlpTile) {
+        const uint32_t q = base + t;
+        bool live = false;
+        uint32_t p = 0;
+        float f[kMlpIn];
+        if (q < n) {
+            p = T.queue[in][q];
+            const uint32_t prim = T.hit_prim[p];
+            if (prim != 0xffffffffu) {
+                const uint32_t mi = T.tri_mat[prim];
+                live = T.mats[mi < T.num_materials ? mi : T.num_materials - 1].type == MAT_PHONG;
+            }
+            if (live) {
+                const float4 tuv = T.hit_tuv[p];
+                const float3 o = T.org[p], d = T.dir[p];
+                const float* tv = T.tri_v + 9 * size_t(prim);
+                const float3 v0 = f3(tv[0], tv[1], tv[2]), v1 = f3(tv[3], tv[4], tv[5]), v2 = f3(tv[6], tv[7], tv[8]);
+                const float3 fn = unit3(cross3(v1 - v0, v2 - v0));
+                mlp_features(o + tuv.x * d, fn, f3(-d.x, -d.y, -d.z), T.ml.dev.mn, T.ml.dev.inv_ext, f);
+            }
+        }
+        if (!live)
+#pragma unroll
+            for (int k = 0; k < kMlpIn; ++k) f[k] = 0.0f;
+        store_features(x0, t, f);
+        float o[kMlpOut];
+        ok &= mlp_forward_tile(tmem, sw, x0, mbar, phase, o);
+        if (live) {
+            VmfLobe L[kMlpLobes];
+            mlp_head(o, L);
+            __half* lp = T.lobes + size_t(p) * 40;
+#pragma unroll
+            for (int k = 0; k < kMlpLobes; ++k) {
+                lp[5 * k] = __float2half_rn(L[k].mu.x);
+                lp[5 * k + 1] = __float2half_rn(L[k].mu.y);
+                lp[5 * k + 2] = __float2half_rn(L[k].mu.z);
+                lp[5 * k + 3] = __float2half_rn(L[k].kappa);
+                lp[5 * k + 4] = __float2half_rn(L[k].weight);
+            }
+        }
+    }
+    if (!ok) atomicOr(T.status, RTPG_STATUS_TIMEOUT);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (t < 32) tmem_dealloc(tmem, kEvalCols);
 }
 
 template <int G>
@@ -451,7 +584,7 @@ __global__ void __launch_bounds__(kTB, 6) k_bounce(TracerDev T, int in) {
         atomicAdd(T.counters, (unsigned long long)n);
     }
     const bool build = (T.flags & RTPG_TRACE_FLAG_BUILD) != 0;
-    const bool recording = (G == kGuideTree || G == kGuideGrid) && !(T.flags & RTPG_TRACE_FLAG_FINAL);
+    const bool recording = (G == kGuideTree || G == kGuideGrid || G == kGuideMlp) && !(T.flags & RTPG_TRACE_FLAG_FINAL);
     for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
         const uint32_t q = base + threadIdx.x;
         bool keep = false, shadow = false;
@@ -481,7 +614,7 @@ __global__ void __launch_bounds__(kTB, 6) k_bounce(TracerDev T, int in) {
 template <int G>
 __global__ void __launch_bounds__(kTB) k_finish(TracerDev T) {
     constexpr bool use_grid = G == kGuideGrid;
-    const bool recording = G != kGuideNone && !(T.flags & RTPG_TRACE_FLAG_FINAL);
+    const bool recording = (G == kGuideTree || G == kGuideGrid || G == kGuideMlp) && !(T.flags & RTPG_TRACE_FLAG_FINAL);
     for (uint32_t base = blockIdx.x * blockDim.x; base < T.npath; base += gridDim.x * blockDim.x) {
         const uint32_t p = base + threadIdx.x;
         uint32_t nv = 0;
@@ -517,13 +650,11 @@ __global__ void __launch_bounds__(kTB) k_finish(TracerDev T) {
 #pragma unroll
                 for (uint32_t j = 1; j < kTV; ++j)
                     if (j == i) rad = acc[j];
-                const float3 bv = T.v_bsdf[vi], th = T.v_thr[vi];
-                const float wo = T.v_wopdf[vi];
                 const bool ok_r = isfinite(rad.x) && rad.x >= 0.f && isfinite(rad.y) && rad.y >= 0.f &&
                                   isfinite(rad.z) && rad.z >= 0.f;
-                const bool ok_b = isfinite(bv.x) && bv.x >= 0.f && isfinite(bv.y) && bv.y >= 0.f &&
-                                  isfinite(bv.z) && bv.z >= 0.f;
-                if ((vf & 1) && wo > 0.0f && ok_r && ok_b && !(vf & 2)) {
+                const float wo = (vf & 1) && !(vf & 2) && ok_r ? T.v_wopdf[vi] : 0.0f;
+                if (wo > 0.0f) {
+                    const float3 th = T.v_thr[vi];
                     float3 lr = f3(0.f, 0.f, 0.f);
                     if (th.x * wo > 1e-4f) lr.x = rad.x / th.x;
                     if (th.y * wo > 1e-4f) lr.y = rad.y / th.y;
@@ -532,7 +663,26 @@ __global__ void __launch_bounds__(kTB) k_finish(TracerDev T) {
                     const float lavg = (lr.x + lr.y + lr.z) / 3.0f;
                     const float3 dr = T.v_dir[vi];
                     const float irr = __fdiv_rn(lavg, wo);
-                    if (use_grid) {
+                    if (G == kGuideMlp) {
+                        // a training record of the learned guide: the SD-tree's record with the
+                        // vertex's normal and outgoing direction, kept with probability mlp_keep
+                        if (isfinite(irr) && irr > 0.0f &&
+                            to_uniform_float(pcg1d(T.rng[p] ^ (i * 0x9E3779B9u))) < T.mlp_keep) {
+                            const uint32_t idx = atomicAdd(T.ml.r_count, 1u);
+                            if (idx < T.ml.capacity) {
+                                const float3 ps = T.v_pos[vi], nm = T.v_nrm[vi], wo = T.v_wo[vi];
+                                float* rp = T.ml.r_pos + 3 * size_t(idx);
+                                float* rn = T.ml.r_nrm + 3 * size_t(idx);
+                                float* ro = T.ml.r_wo + 3 * size_t(idx);
+                                float* ri = T.ml.r_wi + 3 * size_t(idx);
+                                rp[0] = ps.x; rp[1] = ps.y; rp[2] = ps.z;
+                                rn[0] = nm.x; rn[1] = nm.y; rn[2] = nm.z;
+                                ro[0] = wo.x; ro[1] = wo.y; ro[2] = wo.z;
+                                ri[0] = dr.x; ri[1] = dr.y; ri[2] = dr.z;
+                                T.ml.r_w[idx] = irr;
+                            }
+                        }
+                    } else if (use_grid) {
                         // MortonTraceVertexT::Commit (OPX7UtilsMorton.h:550-585) ->
                         // MortonQuadTreeWrapperT::Record: leaf of the cell's building quadtree
                         if (isfinite(irr) && irr > 0.0f) {
@@ -542,8 +692,7 @@ __global__ void __launch_bounds__(kTB) k_finish(TracerDev T) {
                             v_s = to_fx(irr, T.mqt.fx, T.mqt.status);
                         }
                     } else {
-                        const float3 pos = T.v_pos[vi];
-                        const uint32_t dt = stree_lookup(T.tree.snode, T.tree.mn, T.tree.mx, pos.x, pos.y, pos.z);
+                        const uint32_t dt = T.v_cell[vi];  // stree_lookup of the vertex, from k_bounce
                         k_w = dt;
                         v_w = to_fx(1.0f, T.tree.fx, T.tree.status);
                         if (isfinite(irr) && irr > 0.0f) {
@@ -554,7 +703,8 @@ __global__ void __launch_bounds__(kTB) k_finish(TracerDev T) {
                     }
                 }
             }
-            if (use_grid) {
+            if (G == kGuideMlp) {
+            } else if (use_grid) {
                 warp_add_u64(k_s, v_s, T.mqt.leaves);
             } else {
                 warp_add_u64(k_w, v_w, T.tree.b_statw);
@@ -605,9 +755,7 @@ struct rtpg_tracer {
     uint64_t paths = 0;
     struct Cached {
         cudaGraphExec_t exec;
-        SDTreeDev tree;
-        HashGridDev grid;
-        MqtDev mqt;
+        TracerDev dev;  // a captured wave bakes in every kernel argument
     };
     std::map<uint32_t, Cached> graphs;  // keyed by flags; the guide views are compared on use
     template <class T>
@@ -635,6 +783,12 @@ struct rtpg_tracer {
 };
 
 static void launch_bounce(const TracerDev& T, int g, cudaStream_t st, int in) {
+    if (guide_of(T.flags) == kGuideMlp) {
+        k_hit<<<g, kTB, 0, st>>>(T, in);
+        if (T.flags & RTPG_TRACE_FLAG_BUILD) k_mlp_lobes<<<kSMs * 4, kMlpThreads, kSmemEval, st>>>(T, in);
+        k_bounce<kGuideMlp><<<g, kTB, 0, st>>>(T, in);
+        return;
+    }
     switch (guide_of(T.flags)) {
         case kGuideTree: k_bounce<kGuideTree><<<g, kTB, 0, st>>>(T, in); break;
         case kGuideGrid: k_bounce<kGuideGrid><<<g, kTB, 0, st>>>(T, in); break;
@@ -645,6 +799,7 @@ static void launch_finish(const TracerDev& T, int g, cudaStream_t st) {
     switch (guide_of(T.flags)) {
         case kGuideTree: k_finish<kGuideTree><<<g, kTB, 0, st>>>(T); break;
         case kGuideGrid: k_finish<kGuideGrid><<<g, kTB, 0, st>>>(T); break;
+        case kGuideMlp: k_finish<kGuideMlp><<<g, kTB, 0, st>>>(T); break;
         default: k_finish<kGuideNone><<<g, kTB, 0, st>>>(T); break;
     }
 }
@@ -736,9 +891,9 @@ int rtpg_tracer_create(rtpg_scene* scene, const float* tri_vertices, const uint3
         (r = h->alloc(&T.dir, P)) || (r = h->alloc(&T.thr, P)) || (r = h->alloc(&T.col, P)) ||
         (r = h->alloc(&T.rng, P)) || (r = h->alloc(&T.depth, P)) ||
         (r = h->alloc(&T.hflags, P)) || (r = h->alloc(&T.queue[0], P)) ||
-        (r = h->alloc(&T.queue[1], P)) || (r = h->alloc(&T.qcount, 2)) || (r = h->alloc(&T.v_pos, P * kTV)) ||
+        (r = h->alloc(&T.queue[1], P)) || (r = h->alloc(&T.qcount, 2)) ||
         (r = h->alloc(&T.v_dir, P * kTV)) || (r = h->alloc(&T.v_thr, P * kTV)) || (r = h->alloc(&T.b_rad, P * std::max<uint32_t>(D.max_depth, 1))) ||
-        (r = h->alloc(&T.v_bsdf, P * kTV)) || (r = h->alloc(&T.v_wopdf, P * kTV)) ||
+        (r = h->alloc(&T.v_wopdf, P * kTV)) ||
         (r = h->alloc(&T.v_cos, P * kTV)) || (r = h->alloc(&T.v_flags, P * kTV)) || (r = h->alloc(&T.v_cell, P * kTV)) || (r = h->alloc(&T.seeds, P)) ||
         (r = h->alloc(&T.accum, 3 * P)) || (r = h->alloc(&T.status, 1)) || (r = h->alloc(&T.counters, 2)) || (r = h->alloc(&h->d_tex, 64)) ||
         (r = h->alloc(&h->d_tex_wh, 64))) {
@@ -902,9 +1057,7 @@ static int render_waves(rtpg_tracer* h, uint32_t spp, uint32_t flags, cudaStream
     }
     auto it = h->graphs.find(flags);
     cudaGraphExec_t exec = nullptr;
-    if (it != h->graphs.end() && memcmp(&it->second.tree, &h->dev.tree, sizeof(SDTreeDev)) == 0 &&
-        memcmp(&it->second.grid, &h->dev.grid, sizeof(HashGridDev)) == 0 &&
-        memcmp(&it->second.mqt, &h->dev.mqt, sizeof(MqtDev)) == 0) {
+    if (it != h->graphs.end() && memcmp(&it->second.dev, &h->dev, sizeof(TracerDev)) == 0) {
         exec = it->second.exec;
     } else {
         if (it != h->graphs.end()) {
@@ -923,7 +1076,7 @@ static int render_waves(rtpg_tracer* h, uint32_t spp, uint32_t flags, cudaStream
         if (g) cudaGraphDestroy(g);
         cudaStreamDestroy(cs);
         if (e != cudaSuccess) return fail(RTPG_ECUDA, "rtpg_tracer_render: graph capture failed: %s", cudaGetErrorString(e));
-        h->graphs[flags] = {exec, h->dev.tree, h->dev.grid, h->dev.mqt};
+        h->graphs[flags] = {exec, h->dev};
     }
     for (uint32_t s = 0; s < spp; ++s) RTPG_CUDA(cudaGraphLaunch(exec, st));
     h->samples += spp;
@@ -942,6 +1095,7 @@ int rtpg_tracer_render(rtpg_tracer* h, uint32_t spp, uint32_t flags, rtpg_sdtree
     if (r) return r;
     memset(&h->dev.grid, 0, sizeof(HashGridDev));
     memset(&h->dev.mqt, 0, sizeof(MqtDev));
+    memset(&h->dev.ml, 0, sizeof(MlpView));
     if (tree) h->dev.tree = sdtree_device_view(tree);
     else memset(&h->dev.tree, 0, sizeof(SDTreeDev));
     return render_waves(h, spp, flags, as_stream(stream));
@@ -960,8 +1114,38 @@ int rtpg_tracer_render_grid(rtpg_tracer* h, uint32_t spp, uint32_t flags, rtpg_h
     if (q.ncells < g.nslots)
         return fail(RTPG_EINVAL, "rtpg_tracer_render_grid: %u quadtrees for %u grid slots", q.ncells, g.nslots);
     memset(&h->dev.tree, 0, sizeof(SDTreeDev));
+    memset(&h->dev.ml, 0, sizeof(MlpView));
     h->dev.grid = g;
     h->dev.mqt = q;
+    return render_waves(h, spp, flags, as_stream(stream));
+}
+
+// One launch guided by the learned mixture (no counterpart in RTLib): every bounce runs the
+// closest-hit queries, the network on the tensor cores for the hit points (with BUILD), then
+// shading; unless FINAL, committed trace vertices become training records of the guide, each
+// kept with probability record_keep.
+int rtpg_tracer_render_mlp(rtpg_tracer* h, uint32_t spp, uint32_t flags, rtpg_mlp* mlp, float fraction,
+                           float record_keep, void* stream) {
+    if (!h || !mlp) return fail(RTPG_EINVAL, "rtpg_tracer_render_mlp: null argument");
+    if (!(flags & RTPG_TRACE_FLAG_USE_MLP) || (flags & (RTPG_TRACE_FLAG_USE_TREE | RTPG_TRACE_FLAG_USE_GRID)))
+        return fail(RTPG_EINVAL, "rtpg_tracer_render_mlp: flags must hold USE_MLP and no other guide");
+    if (!(fraction >= 0.0f && fraction <= 1.0f)) return fail(RTPG_EINVAL, "rtpg_tracer_render_mlp: fraction outside [0, 1]");
+    int r = check_render(h, flags, "rtpg_tracer_render_mlp");
+    if (r) return r;
+    TracerDev& T = h->dev;
+    if (!T.hit_prim) {
+        const size_t P = T.npath;
+        if ((r = h->alloc(&T.hit_prim, P)) || (r = h->alloc(&T.hit_tuv, P)) || (r = h->alloc(&T.lobes, P * 40)) ||
+            (r = h->alloc(&T.v_nrm, P * kTV)) || (r = h->alloc(&T.v_wo, P * kTV)) || (r = h->alloc(&T.v_pos, P * kTV)))
+            return r;
+        RTPG_CUDA(cudaFuncSetAttribute(k_mlp_lobes, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemEval));
+    }
+    memset(&T.tree, 0, sizeof(SDTreeDev));
+    memset(&T.grid, 0, sizeof(HashGridDev));
+    memset(&T.mqt, 0, sizeof(MqtDev));
+    T.ml = mlp_view(mlp);
+    T.mlp_fraction = fraction;
+    T.mlp_keep = record_keep;
     return render_waves(h, spp, flags, as_stream(stream));
 }
 

@@ -2,7 +2,8 @@
 
 ``rmae`` / ``smape`` restate the comparison tool RTLibExtOPX7Comp.cpp:124-145 (all-range
 branch); ``relmse`` is the relative mean squared error used for equal-time comparisons:
-mean over pixels and channels of (img - ref)^2 / (ref^2 + eps).  ``save_result_bin`` writes
+mean over pixels and channels of (img - ref)^2 / (ref^2 + eps), optionally after scaling both
+images by the reference's mean.  ``save_result_bin`` writes
 what SaveResultImage writes (RTLibExtOPX7TestApplication.cpp:2590-2610): float RGB mean
 radiance with the pixel order reversed."""
 from __future__ import annotations
@@ -10,9 +11,15 @@ from __future__ import annotations
 import numpy as np
 
 
-def relmse(img, ref, eps=1e-2):
+def relmse(img, ref, eps=1e-2, normalize=False):
+    """normalize: divide both images by the reference's mean first, so that eps = 1e-2 means
+    1% of the mean brightness (dark scenes otherwise compare only in their brightest pixels)."""
     img = np.asarray(img, np.float64)
     ref = np.asarray(ref, np.float64)
+    if normalize:
+        m = float(np.mean(ref[np.isfinite(ref)]))
+        if m > 0:
+            img, ref = img / m, ref / m
     ok = np.isfinite(img).all(axis=-1) & np.isfinite(ref).all(axis=-1)
     return float(np.mean(((img - ref) ** 2 / (ref ** 2 + eps))[ok]))
 

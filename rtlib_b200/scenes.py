@@ -144,8 +144,8 @@ def _icosphere(level):
 def occluded_rooms(width=1280, height=720, n_objects=2048, n_lights=4096, seed=3, sphere_level=3):
     """The occluded-light scene: a 10 x 4 x 10 room filled with n_objects random icospheres and
     boxes (radii U[0.05, 0.4]); light enters only through a 1 x 2 doorway in the x = 10 wall
-    from a neighbouring 4 x 4 x 10 room whose ceiling holds n_lights emissive triangles, each
-    its own NEE light with radiance lognormal(0, 1.5) (grey).  With level-3 icospheres (1280
+    from a neighbouring 4 x 4 x 10 room whose far wall (x = 14, facing the doorway) holds
+    n_lights emissive triangles, each its own NEE light with radiance lognormal(0, 1.5) (grey).  With level-3 icospheres (1280
     triangles) for 807 of the objects and boxes for the rest the scene has about 2^20
     triangles."""
     rng = np.random.default_rng(seed)
@@ -172,27 +172,33 @@ def occluded_rooms(width=1280, height=720, n_objects=2048, n_lights=4096, seed=3
     n_sph = min(n_objects, 807)
     kinds = np.array([1] * n_sph + [0] * (n_objects - n_sph))
     rng.shuffle(kinds)
+    eye = np.array([7.5, 1.6, 3.6])
     for k in kinds:
         r = rng.uniform(0.05, 0.4)
-        c = np.array([rng.uniform(r, 10 - r), rng.uniform(r, 4 - r), rng.uniform(r, 10 - r)])
+        # nothing within 1.5 m of the camera (its view would start inside an object)
+        while True:
+            c = np.array([rng.uniform(r, 10 - r), rng.uniform(r, 4 - r), rng.uniform(r, 10 - r)])
+            if np.linalg.norm(c - eye) > r * 1.8 + 1.5:
+                break
         m = int(rng.integers(0, 3))
         if k:
             b.mesh(sv * r + c, sf, m)
         else:
             b.box(c, (2 * r, 2 * r, 2 * r), rng.uniform(0, 90), m)
     n_geom = len(b.tris)
-    # emissive triangles tiling the light-room ceiling just below y = 4, facing down
+    # emissive triangles tiling the light room's far wall (x = 14) just in front of it, facing
+    # the doorway (-x): gz x gy quads of two triangles
     nq = n_lights // 2
-    gx = 32 if nq % 32 == 0 else int(np.sqrt(nq * 0.4))
-    gz = nq // gx
-    rad = rng.lognormal(0.0, 1.5, 2 * gx * gz).astype(np.float32)
+    gz = 1 << int(np.floor(np.log2(max(1.0, np.sqrt(nq * 2.5)))))
+    gy = max(1, nq // gz)
+    rad = rng.lognormal(0.0, 1.5, 2 * gy * gz).astype(np.float32)
     light_emit, light_first = [], []
     k = 0
-    for i in range(gx):
+    for i in range(gy):
         for j in range(gz):
-            p = (10 + 4 * i / gx, 3.99, 10 * j / gz)
-            e1, e2 = (4 / gx, 0, 0), (0, 0, 10 / gz)
-            # quad(p, e1, e2): normal e1 x e2 = -y
+            p = (13.99, 4 * i / gy, 10 * j / gz)
+            e1, e2 = (0, 0, 10 / gz), (0, 4 / gy, 0)
+            # quad(p, e1, e2): normal e1 x e2 = -x
             for tri in range(2):
                 mats.append(_mat(emission=(rad[k],) * 3, type=NEE_LIGHT))
                 k += 1
@@ -205,5 +211,5 @@ def occluded_rooms(width=1280, height=720, n_objects=2048, n_lights=4096, seed=3
     return {"tri_v": tri_v, "tri_mat": tri_mat, "tri_uv": tri_uv, "materials": mats, "light_tris": light_tris,
             "light_first": np.array(light_first, np.uint32), "light_count": np.ones(len(light_first), np.uint32),
             "light_emission": np.array(light_emit, np.float32).reshape(-1),
-            "camera": _camera((1.0, 1.7, 5.0), (9.0, 1.0, 5.0), (0, 1, 0), 60.0, width / height),
+            "camera": _camera(tuple(eye), (10.0, 1.0, 5.0), (0, 1, 0), 60.0, width / height),
             "width": width, "height": height, "geometry_triangles": n_geom}

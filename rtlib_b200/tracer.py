@@ -15,6 +15,7 @@ import numpy as np
 from ._lib import call, ptr, stream_ptr
 
 FLAG_NEE, FLAG_RIS, FLAG_USE_GRID, FLAG_USE_TREE, FLAG_BUILD, FLAG_FINAL, FLAG_LOCATE = 1, 2, 4, 8, 16, 32, 64
+FLAG_USE_MLP = 128
 
 
 class _Material(C.Structure):
@@ -129,6 +130,10 @@ class Tracer:
                            max_launches=1 << 30, stream=None):
         call("rtpg_tracer_render_grid_guided", self.h, grid.h, mqt.h, controller.h, int(base_flags),
              int(samples_per_launch), int(max_launches), stream_ptr(stream))
+
+    def render_mlp(self, spp, flags, mlp, fraction=0.5, record_keep=1.0, stream=None):
+        call("rtpg_tracer_render_mlp", self.h, int(spp), int(flags) | FLAG_USE_MLP, mlp.h, float(fraction),
+             float(record_keep), stream_ptr(stream))
 
     def set_light_emission(self, rgb):
         """rgb: (num_lights, 3) host array; NEE radiance and material emission of every light."""

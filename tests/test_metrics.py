@@ -14,6 +14,9 @@ def test_relmse_rmae_smape_small_cases(tmp_path):
     mean = (np.sqrt(3) + np.sqrt(1.21 + 1 + 0.81)) / 2
     assert abs(metrics.rmae(img, ref) - d / mean) < 1e-6
     assert metrics.relmse(ref, ref) == 0.0
+    # normalised: scale invariant
+    a, b = metrics.relmse(img * 1e-3, ref * 1e-3, normalize=True), metrics.relmse(img, ref, normalize=True)
+    assert b > 0 and abs(a - b) < 1e-5 * b
     p = tmp_path / "r.bin"
     metrics.save_result_bin(p, img)
     raw = np.fromfile(p, np.float32).reshape(-1, 3)

@@ -220,3 +220,80 @@ def test_occluded_grid_guided_ris_matches_oracle(cuda, oracle, keying):
     gcur = grid.export()
     assert np.array_equal(np.sort(gcur[gcur != 0]), np.sort(og.cur[og.cur != 0]))
     _compare(tr.image().cpu().numpy(), r.image(), rel_mse=2e-3, frac=0.97)
+
+
+def test_mlp_pipeline_without_guiding_equals_unguided(cuda):
+    """USE_MLP without BUILD runs the split pipeline (hit kernel, then shading) and records; the
+    image must be bit-identical to the unguided render of the same streams."""
+    from rtlib_b200.mlp import MLPGuide
+    from rtlib_b200.tracer import FLAG_NEE, FLAG_RIS
+    sc = _small_occluded()
+    a, _ = _gpu_render(cuda, sc, 64, 36, 4, FLAG_NEE | FLAG_RIS, max_depth=16)
+    from rtlib_b200.tracer import Tracer
+    tr = Tracer(sc, cuda, max_depth=16, width=64, height=36)
+    g = MLPGuide((-0.1, -0.1, -0.1), (14.1, 4.1, 10.1), record_capacity=1 << 14)
+    tr.render_mlp(4, FLAG_NEE | FLAG_RIS, g, 0.5)
+    assert np.array_equal(tr.image().cpu().numpy(), a)
+    assert g.records() > 0 and g.status() == 0
+
+
+def test_learned_guide_lowers_error(cuda):
+    """The trained network against the same tracer without it (BSDF sampling + NEE + RIS), equal
+    samples per pixel, relMSE against a high-sample unguided reference."""
+    import torch
+    from rtlib_b200 import metrics
+    from rtlib_b200.learned import render_learned
+    from rtlib_b200.mlp import MLPGuide
+    from rtlib_b200.tracer import FLAG_NEE, FLAG_RIS, Tracer
+    sc = scenes.occluded_rooms(128, 72, n_objects=60, n_lights=256, seed=5, sphere_level=1)
+    flags = FLAG_NEE | FLAG_RIS
+    ref_tr = Tracer(sc, cuda, max_depth=16, width=128, height=72, seed=99)
+    ref_tr.render(2048, flags)
+    ref = ref_tr.image().cpu().numpy()
+    spp = 64
+    base = Tracer(sc, cuda, max_depth=16, width=128, height=72, seed=3)
+    base.render(spp, flags)
+    e_base = metrics.relmse(base.image().cpu().numpy(), ref, normalize=True)
+    tr = Tracer(sc, cuda, max_depth=16, width=128, height=72, seed=3)
+    g = MLPGuide((-0.1, -0.1, -0.1), (14.1, 4.1, 10.1), seed=1, learning_rate=1e-3, record_capacity=1 << 16)
+    log = []
+    n = render_learned(tr, g, budget_spp=spp, base_flags=flags, fraction=0.5, ratio=0.5, epochs=16, batch=4096,
+                       log=log)
+    assert n == spp and g.status() == 0
+    e_mlp = metrics.relmse(tr.image().cpu().numpy(), ref, normalize=True)
+    assert e_mlp < 0.8 * e_base, (e_mlp, e_base, log)
+
+
+def test_convergence_4096_spp_within_one_percent(cuda):
+    """Guided (SD-tree schedule) and unguided renders of the Cornell box at 4096 spp against a
+    65536-spp FP64-accumulated image of the same integrator: relMSE < 1%."""
+    from rtlib_b200 import metrics
+    from rtlib_b200.sdtree import SDTree, SDTreeController
+    from rtlib_b200.tracer import FLAG_NEE, Tracer
+    w = h = 96
+    sc = scenes.cornell_box(w, h)
+    ref_tr = Tracer(sc, cuda, max_depth=8, width=w, height=h, seed=1234)
+    ref_tr.render(65536, FLAG_NEE)
+    ref = ref_tr.image64().cpu().numpy()
+    tr = Tracer(sc, cuda, max_depth=8, width=w, height=h, seed=7)
+    tr.render(4096, FLAG_NEE)
+    e_plain = metrics.relmse(tr.image64().cpu().numpy(), ref)
+    tree = SDTree((-0.005,) * 3, (1.005,) * 3, fraction=0.5)
+    ctrl = SDTreeController(tree, 4095, iteration_for_built=0, ratio_for_budget=1.0, samples_per_launch=1)
+    tr2 = Tracer(sc, cuda, max_depth=8, width=w, height=h, seed=9)
+    ctrl.start()
+    tr2.render_guided(tree, ctrl, FLAG_NEE)
+    e_guided = metrics.relmse(tr2.image64().cpu().numpy(), ref)
+    assert e_plain < 0.01 and e_guided < 0.01, (e_plain, e_guided)
+
+
+@pytest.mark.parametrize("name", ["DEF", "NEE", "RIS", "PGNEE", "PGRIS", "HTNEE", "HTRIS"])
+def test_config_tracers_run(cuda, name):
+    """Every tracer of the application runs from a trace configuration."""
+    from rtlib_b200.config import TraceConfig, run
+    cfg = TraceConfig.from_json({"Width": 48, "Height": 48, "Samples": 1, "SamplesPerSave": 8, "MaxSamples": 15,
+                                 "MaxDepth": 8, "DefTracer": name,
+                                 "Custom": {"MortonTree.IterationForBuilt": 1, "MortonTree.Level": 4,
+                                            "HashGrid.CellSize": 4096, "HashGrid.GridSize": [16, 16, 16]}})
+    tr, img, spp, dt = run(cfg, scenes.cornell_box(48, 48), cuda)
+    assert spp >= 15 and img.shape == (48, 48, 3) and np.isfinite(img).all() and img.mean() > 0.05
