@@ -624,6 +624,110 @@ def bench_learned(args):
     return {"budgets": out, "ref_spp": ref_spp, "ref_seconds": args.ref_seconds}
 
 
+# ---------------------------------------------------------------------------- learned-guide kernels
+# tensor-core FLOPs executed per sample (padding included): forward 2*(80*64 + 2*64*64 + 64*48);
+# training adds dX of layers 3..1 (2*(48*64 + 2*64*64)) and dW^T of layers 3..0 at M = 64
+# (2*(3*64*64 + 64*80))
+MLP_FWD_FLOP = 2 * (80 * 64 + 2 * 64 * 64 + 64 * 48)
+MLP_TRAIN_FLOP = MLP_FWD_FLOP + 2 * (48 * 64 + 2 * 64 * 64) + 2 * (3 * 64 * 64 + 64 * 80)
+MLP_N_TRAIN, MLP_BATCH, MLP_N_EVAL = 1 << 18, 1 << 14, 1 << 20
+
+
+def bench_mlp_ours(args, rank, world):
+    """The learned guide's tcgen05 kernels: one training epoch over 2^18 records (16 Adam steps
+    of 16384) and inference of 2^20 samples.  Metric: training records per second."""
+    import torch
+    from rtlib_b200.mlp import MLPGuide
+
+    dev = torch.device("cuda", rank % max(1, torch.cuda.device_count()))
+    torch.cuda.set_device(dev)
+    rng = np.random.default_rng(1)
+
+    def unit(n):
+        v = rng.normal(size=(n, 3)).astype(np.float32)
+        return v / np.linalg.norm(v, axis=1, keepdims=True)
+
+    def T(a):
+        return torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+
+    n = MLP_N_TRAIN
+    rec = (T(rng.uniform(0, 10, (n, 3)).astype(np.float32)), T(unit(n)), T(unit(n)), T(unit(n)),
+           T(rng.lognormal(0, 1, n).astype(np.float32)))
+    q = (T(rng.uniform(0, 10, (MLP_N_EVAL, 3)).astype(np.float32)), T(unit(MLP_N_EVAL)), T(unit(MLP_N_EVAL)))
+    g = MLPGuide((0, 0, 0), (10, 10, 10), seed=1)
+    out = torch.empty((MLP_N_EVAL, 40), dtype=torch.float32, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream()
+    for _ in range(args.warmup):
+        g.train(rec, batch=MLP_BATCH, epochs=1)
+        g.eval(*q, raw=False)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(dev.index)
+    tr_ms, ev_ms = [], []
+    _barrier(world)
+    clocks.start()
+    for k in range(args.steps):
+        flush.fill_(k & 0xff)
+        a, b, c = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        a.record(stream)
+        g.train(rec, batch=MLP_BATCH, epochs=1)
+        b.record(stream)
+        g.eval(*q, raw=False)
+        c.record(stream)
+        torch.cuda.synchronize()
+        tr_ms.append(a.elapsed_time(b))
+        ev_ms.append(b.elapsed_time(c))
+    _barrier(world)
+    clk = clocks.stop()
+    assert g.status() == 0
+    t_ms = _max_over_ranks(sum(tr_ms) / len(tr_ms), world, dev)
+    e_ms = sum(ev_ms) / len(ev_ms)
+    # e2e: records from pinned host memory, the mixture of the queries back to host
+    hrec = [x.cpu().pin_memory() for x in rec]
+    hq = [x.cpu().pin_memory() for x in q]
+    hout = torch.empty((MLP_N_EVAL, 40), dtype=torch.float32).pin_memory()
+    e2e = []
+    for k in range(max(1, args.steps // 2)):
+        a, c = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        drec = tuple(x.to(dev, non_blocking=True) for x in hrec)
+        g.train(drec, batch=MLP_BATCH, epochs=1)
+        dq = tuple(x.to(dev, non_blocking=True) for x in hq)
+        hout.copy_(g.eval(*dq, raw=False), non_blocking=True)
+        c.record(stream)
+        torch.cuda.synchronize()
+        e2e.append(a.elapsed_time(c))
+    e2e_ms = _max_over_ranks(sum(e2e) / len(e2e), world, dev)
+    peak = _peaks_tensor()
+    achieved = MLP_TRAIN_FLOP * n / (t_ms * 1e-3) / 1e12
+    steps = n // MLP_BATCH
+    return {
+        "metric": "learned-guide training throughput (records/s, 2^18 records, Adam steps of 16384)",
+        "value": n * world / (t_ms * 1e-3) / 1e6, "unit": "Mrecords/s", "ms_per_step": t_ms,
+        "e2e": {"value": n * world / (e2e_ms * 1e-3) / 1e6, "unit": "Mrecords/s",
+                "h2d_bytes_per_step": int(sum(x.numel() * 4 for x in hrec + hq)),
+                "d2h_bytes_per_step": int(hout.numel() * 4)},
+        "roofline": {"kernel": "k_mlp_train", "bound": "tensor", "achieved": achieved, "peak": peak[0],
+                     "unit": "TFLOP/s", "frac": achieved / peak[0], "peak_source": peak[1],
+                     "traffic": None, "flop_per_record": MLP_TRAIN_FLOP,
+                     "note": "64-wide layers: 128-row tiles of dependent tcgen05 MMAs, latency bound; the "
+                             "step time includes the weight-sum and Adam kernels"},
+        "inference": {"Msamples_s": MLP_N_EVAL / (e_ms * 1e-3) / 1e6, "ms": e_ms,
+                      "tflops": MLP_FWD_FLOP * MLP_N_EVAL / (e_ms * 1e-3) / 1e12},
+        "clocks": clk,
+        "gpu_launches": (3 * steps + 1) * args.steps,
+    }
+
+
+def _peaks_tensor():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d.get("bf16_tflops", 1590.0), "measured bf16_tflops (cuBLAS burst)"
+    return 1590.0, "fallback bf16 TFLOP/s"
+
+
 # ---------------------------------------------------------------------------- plumbing
 def _barrier(world):
     if world > 1:
@@ -647,7 +751,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="cornell", choices=["cornell", "sdtree", "occluded", "learned"])
+    ap.add_argument("--workload", default="cornell", choices=["cornell", "sdtree", "occluded", "learned", "mlp"])
     ap.add_argument("--budgets", default="30,120", help="learned: equal-time budgets in seconds")
     ap.add_argument("--ref-seconds", type=float, default=300.0, help="learned: reference render time")
     ap.add_argument("--epochs", type=int, default=16, help="learned: Adam epochs over each pass's records")
@@ -682,6 +786,11 @@ def main():
                 "budgets": r["budgets"]}
         print(json.dumps(line), flush=True)
         return 0
+    if args.workload == "mlp" and args.impl == "reference":
+        if rank == 0:
+            print(json.dumps({"impl": "reference", "unavailable": "the learned guide has no counterpart in RTLib"}),
+                  flush=True)
+        return 0
     if args.workload == "occluded" and args.impl == "reference":
         if rank == 0:
             print(json.dumps({"impl": "reference", "unavailable": "RTLib's integrator exists only as OptiX "
@@ -690,8 +799,13 @@ def main():
         return 0
     cornell = args.workload == "cornell"
     occluded = args.workload == "occluded"
+    mlp = args.workload == "mlp"
     set_budget(args.budget)
-    if occluded:
+    if mlp:
+        cfg = {"workload": "learned-guide kernels: 3x64 ReLU MLP -> 8 vMF lobes, BF16 tcgen05 / FP32 TMEM; "
+                           "train 2^18 records (batch 16384, Adam), infer 2^20 samples"}
+        metric, unit = "learned-guide training throughput", "Mrecords/s"
+    elif occluded:
         cfg = {"workload": f"occluded-rooms HTRIS: {O_W}x{O_H}, ~1M triangles, 4096 emitters, NEE + RIS 32 "
                            f"candidates, max depth 16, hash grid 2^20 slots (Morton keys) + level-{O_LEVEL} "
                            f"Morton quadtrees, {O_BUDGET} spp budget", "width": O_W, "height": O_H, "max_depth": O_DEPTH}
@@ -740,18 +854,19 @@ def main():
         from datetime import timedelta
         torch.cuda.set_device(_env_int("LOCAL_RANK", rank))
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
-    res = (bench_occluded_ours if occluded else bench_cornell_ours if cornell else bench_sdtree_ours)(args, rank, world)
+    res = (bench_mlp_ours if mlp else bench_occluded_ours if occluded else bench_cornell_ours if cornell
+           else bench_sdtree_ours)(args, rank, world)
     cfg["l2"] = "flushed (256 MiB write) before every timed step"
     cfg["parallelism"] = f"replicas x{world}"
     line = {"metric": res["metric"], "value": res["value"], "unit": res["unit"], "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["ms_per_step"],
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": ("bf16" if mlp else "f32"),
             "data": "synthetic", "config": cfg, "e2e": res["e2e"], "roofline": res["roofline"],
             "clocks": res["clocks"], "gpu_launches": res["gpu_launches"]}
-    for k in ("sdtree", "counters_per_step", "unguided_nee_ris_Mpaths_s", "grid_cells", "spp_per_step"):
+    for k in ("sdtree", "counters_per_step", "unguided_nee_ris_Mpaths_s", "grid_cells", "spp_per_step", "inference"):
         if k in res:
             line[k] = res[k]
-    if rank == 0 and not args.no_cpu_baseline and not occluded:
+    if rank == 0 and not args.no_cpu_baseline and not occluded and not mlp:
         if cornell:
             cores = os.cpu_count() or 1
             v, dt, paths = _cornell_cpu(cores, 10.0)

@@ -13,6 +13,7 @@ N_IN, N_H, N_OUT, LOBES, FREQS = 80, 64, 48, 8, 12
 OFF = (0, 80 * 64, 80 * 64 + 64 * 64, 80 * 64 + 2 * 64 * 64)
 SHAPES = ((80, 64), (64, 64), (64, 64), (64, 48))
 LK_MIN, LK_MAX = -2.3, 6.9
+W_CLAMP = 20.0
 
 
 def bf16(x):
@@ -85,9 +86,11 @@ def loss_grad(w, x, wi, weight):
     W = [bf16(m).astype(np.float64) for m in unpack(w)]
     o, acts = forward(w, x)
     wi = np.asarray(wi, np.float64)
-    weight = np.maximum(np.asarray(weight, np.float64), 0.0)
-    sw = weight.sum()
+    weight = np.maximum(np.asarray(weight, np.float32), 0.0)
+    sw = float(weight.astype(np.float64).sum())
     scale = 1.0 / sw if sw > 0 else 0.0
+    # the weight clamp of the training kernel: 20 x the mean weight of the call
+    weight = np.minimum(weight, np.float32(20.0) * np.float32(sw / weight.shape[0])).astype(np.float64)
     mu, kappa, wgt, ln, s = head(o)
     fk = vmf_pdf(mu, kappa, wi)
     q = np.maximum((wgt * fk).sum(1), 1e-30)

@@ -130,6 +130,9 @@ __global__ void __launch_bounds__(kMlpThreads, 1) k_mlp_train(MlpDev P, int64_t 
     const uint32_t sw = smem_u32(ws), sx = smem_u32(x0), sdy = smem_u32(dy);
     const uint32_t sh[3] = {smem_u32(hs[0]), smem_u32(hs[1]), smem_u32(hs[2])};
     const float scale = (wsum && *wsum > 0.0f) ? 1.0f / *wsum : 0.0f;
+    // record weights are Monte Carlo estimates with a heavy tail: clamp at kWeightClamp times
+    // their mean so that single rare paths do not dominate a step
+    const float wmax = (wsum && n > 0) ? kWeightClamp * (*wsum / (float)n) : 0.0f;
     uint32_t phase = 0;
     bool ok = true, first = true;
     float lsum = 0.0f;
@@ -149,7 +152,7 @@ __global__ void __launch_bounds__(kMlpThreads, 1) k_mlp_train(MlpDev P, int64_t 
                          f3(R.nrm[3 * i], R.nrm[3 * i + 1], R.nrm[3 * i + 2]),
                          f3(R.wo[3 * i], R.wo[3 * i + 1], R.wo[3 * i + 2]), P.mn, P.inv_ext, f);
             wi = f3(R.wi[3 * i], R.wi[3 * i + 1], R.wi[3 * i + 2]);
-            w = R.w[i];
+            w = fminf(fmaxf(R.w[i], 0.0f), wmax);
         } else {
 #pragma unroll
             for (int k = 0; k < kMlpIn; ++k) f[k] = 0.0f;

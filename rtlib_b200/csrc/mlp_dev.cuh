@@ -29,6 +29,7 @@ constexpr int kMlpFreqs = 12;
 constexpr int kW0 = 0, kW1 = kMlpIn * kMlpHidden, kW2 = kW1 + kMlpHidden * kMlpHidden,
               kW3 = kW2 + kMlpHidden * kMlpHidden, kMlpParams = kW3 + kMlpHidden * kMlpOut;  // 16384
 constexpr float kLogKappaMin = -2.3f, kLogKappaMax = 6.9f;  // kappa in [0.1, ~1000]
+constexpr float kWeightClamp = 20.0f;  // training weights clamped at 20 x their minibatch mean
 
 // element offset of (row, col) of a matrix with `ncols` columns in the core-matrix layout
 __host__ __device__ __forceinline__ uint32_t blk(uint32_t row, uint32_t col, uint32_t ncols) {

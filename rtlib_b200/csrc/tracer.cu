@@ -641,7 +641,9 @@ __global__ void __launch_bounds__(kTB) k_finish(TracerDev T) {
             for (uint32_t i = 0; i < kTV; ++i)
                 if (i < k) acc[i] = acc[i] + L;
         }
-        for (uint32_t i = 0; i < kTV; ++i) {  // warp-uniform loop for the aggregated atomics
+        // warp-uniform loop (the aggregated atomics need the whole warp) up to the warp's deepest path
+        const uint32_t nv_warp = __reduce_max_sync(0xffffffffu, nv);
+        for (uint32_t i = 0; i < nv_warp; ++i) {
             unsigned long long k_w = ~0ull, k_s = ~0ull, v_w = 0, v_s = 0;
             if (i < nv) {
                 const size_t vi = size_t(i) * T.npath + p;

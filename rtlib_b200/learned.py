@@ -17,7 +17,7 @@ from .tracer import FLAG_BUILD, FLAG_FINAL
 
 
 def render_learned(tracer, mlp, budget_spp=None, time_budget_s=None, base_flags=1, fraction=0.5, ratio=0.5,
-                   epochs=4, batch=1 << 14, sync=None, log=None):
+                   epochs=32, batch=4096, sync=None, log=None):
     """Returns the number of samples rendered.  Either budget_spp or time_budget_s (seconds,
     wall clock with a device synchronisation per pass) must be given."""
     import torch

@@ -64,6 +64,7 @@ def test_loss_gradient_matches_oracle(cuda):
     wi = _unit(rng, n)
     w = rng.lognormal(0.0, 1.0, n).astype(np.float32)
     w[::9] = 0.0
+    w[5] = 1000.0  # above the training clamp (20 x the mean weight)
     loss, grad = g.loss_grad(*(_t(a, cuda) for a in (pos, nrm, wo, wi, w)))
     grad = grad.cpu().numpy().astype(np.float64)
     lo, go = M.loss_grad(g.params(), M.features(pos, nrm, wo, MN, MX), wi, w)
