@@ -51,7 +51,7 @@ N_Q = 1 << 22
 # algorithmic bytes of one sample+pdf query: position in (12 B), direction (12 B) and pdf
 # (4 B) out; the Xorshift32 seed is derived from the query index
 Q_BYTES = 28
-LAUNCHES_PER_STEP = 21  # clear 1, record 1, build 1, refine 17, sample 1
+LAUNCHES_PER_STEP = 21  # clear 1, record 1, build 1, refine 17, sample 1 (three CUDA graphs)
 
 
 def _env_int(k, d):
@@ -153,11 +153,17 @@ def bench_sdtree_ours(args, rank, world):
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     tree = SDTree((0, 0, 0), (1, 1, 1))
 
-    def build_part(p, u, r):
+    def record_part(p, u, r):
         tree.clear()
         tree.record(p, u, r)
+
+    def refine_part():
         tree.build()
         tree.refine(th)
+
+    def build_part(p, u, r):
+        record_part(p, u, r)
+        refine_part()
 
     def sample_part(qp):
         # guided direction + pdf of the sampled point (DTreeT::Sample + DTreeT::Pdf)
@@ -171,39 +177,47 @@ def bench_sdtree_ours(args, rank, world):
             build_part(pos, uv, rad)
             sample_part(qpos)
     torch.cuda.current_stream().wait_stream(side)
-    g_build, g_sample = torch.cuda.CUDAGraph(), torch.cuda.CUDAGraph()
-    with torch.cuda.graph(g_build):
-        build_part(pos, uv, rad)
+    # one CUDA graph per phase of the step (record, build + refine, sample) so that each is
+    # timed alone
+    g_record, g_refine, g_sample = torch.cuda.CUDAGraph(), torch.cuda.CUDAGraph(), torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g_record):
+        record_part(pos, uv, rad)
+    with torch.cuda.graph(g_refine):
+        refine_part()
     with torch.cuda.graph(g_sample):
         sample_part(qpos)
     stream = torch.cuda.current_stream()
     t0 = time.perf_counter()
     k = 0
     while k < args.warmup or time.perf_counter() - t0 < 0.5:  # also lets the clocks ramp up
-        g_build.replay()
+        g_record.replay()
+        g_refine.replay()
         g_sample.replay()
         k += 1
     torch.cuda.synchronize()
 
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
-           torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    ev = [tuple(torch.cuda.Event(enable_timing=True) for _ in range(4)) for _ in range(args.steps)]
     clocks = ClockSampler(dev.index)
     _barrier(world)
     torch.cuda.synchronize()
     clocks.start()
     for k in range(args.steps):
         flush.fill_(k & 0xff)
-        a, b, c = ev[k]
+        a, r, b, c = ev[k]
         a.record(stream)
-        g_build.replay()
+        g_record.replay()
+        r.record(stream)
+        g_refine.replay()
         b.record(stream)
         g_sample.replay()
         c.record(stream)
     torch.cuda.synchronize()
     _barrier(world)
     clk = clocks.stop()
-    step_ms = [a.elapsed_time(c) for a, b, c in ev]
-    sample_ms = [b.elapsed_time(c) for a, b, c in ev]
+    step_ms = [a.elapsed_time(c) for a, r, b, c in ev]
+    sample_ms = [b.elapsed_time(c) for a, r, b, c in ev]
+    record_ms = [a.elapsed_time(r) for a, r, b, c in ev]
+    refine_ms = [r.elapsed_time(b) for a, r, b, c in ev]
     ms = sum(step_ms) / len(step_ms)
     ms = _max_over_ranks(ms, world, dev)
     st = tree.stats()
@@ -253,10 +267,13 @@ def bench_sdtree_ours(args, rank, world):
         "clocks": clk,
         "gpu_launches": LAUNCHES_PER_STEP * args.steps,
         "sdtree": st,
+        "phases": {"record_Mrec_s": N_REC / (statistics.mean(record_ms) * 1e-3) / 1e6,
+                   "build_refine_ms": statistics.mean(refine_ms),
+                   "sample_pdf_Mq_s": N_Q / (s_ms * 1e-3) / 1e6},
     }
 
 
-def _ref_workload(lib_kind, threads, reps=1):
+def _ref_workload(lib_kind, threads, reps=1, phases=None):
     """One config-1 pass on the host: record (single thread), build + refine (single
     thread), sample+pdf over `threads` threads.  Returns seconds per pass."""
     from oracle.oracle import Oracle, Reference
@@ -269,13 +286,18 @@ def _ref_workload(lib_kind, threads, reps=1):
             t = Oracle().sdtree((0, 0, 0), (1, 1, 1))
         t0 = time.perf_counter()
         t.record(rec["pos"], rec["uv"], rec["radiance"])
+        t1 = time.perf_counter()
         t.build()
         t.refine(th)
+        t2 = time.perf_counter()
         if lib_kind == "reference":
             t.sample_pdf(q["pos"], q["seeds"], threads=threads, with_dir=True)
         else:
             t.sample_pdf(q["pos"], q["seeds"], with_dir=True)
-        times.append(time.perf_counter() - t0)
+        t3 = time.perf_counter()
+        times.append(t3 - t0)
+        if phases is not None:
+            phases.append((t1 - t0, t2 - t1, t3 - t2))
     return times
 
 
@@ -288,15 +310,18 @@ def cpu_baseline_sdtree():
     kind = _ref_kind()
     cores = os.cpu_count() or 1
     threads = cores if kind == "reference" else 1
-    times = []
+    times, ph = [], []
     t_start = time.perf_counter()
     while time.perf_counter() - t_start < 10.0 and len(times) < 30:
-        times += _ref_workload(kind, threads)
+        times += _ref_workload(kind, threads, phases=ph)
     s = statistics.median(times)
     return {"value": (N_REC + N_Q) / s / 1e6, "unit": "Mops/s", "cores": threads, "kind": kind,
             "sample": f"{len(times)} full config-1 passes (2^20 records, refine, 2^22 queries); record/build/"
                       f"refine single-threaded as in RTLib, sample+pdf on {threads} thread(s)",
-            "seconds_per_pass": s}
+            "seconds_per_pass": s,
+            "phases": {"record_Mrec_s": N_REC / statistics.median(p[0] for p in ph) / 1e6,
+                       "build_refine_ms": 1e3 * statistics.median(p[1] for p in ph),
+                       "sample_pdf_Mq_s": N_Q / statistics.median(p[2] for p in ph) / 1e6}}
 
 
 # ---------------------------------------------------------------------------- Cornell workload
@@ -863,7 +888,8 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": ("bf16" if mlp else "f32"),
             "data": "synthetic", "config": cfg, "e2e": res["e2e"], "roofline": res["roofline"],
             "clocks": res["clocks"], "gpu_launches": res["gpu_launches"]}
-    for k in ("sdtree", "counters_per_step", "unguided_nee_ris_Mpaths_s", "grid_cells", "spp_per_step", "inference"):
+    for k in ("sdtree", "phases", "counters_per_step", "unguided_nee_ris_Mpaths_s", "grid_cells", "spp_per_step",
+              "inference"):
         if k in res:
             line[k] = res[k]
     if rank == 0 and not args.no_cpu_baseline and not occluded and not mlp:
