@@ -51,6 +51,8 @@ N_Q = 1 << 22
 # algorithmic bytes of one sample+pdf query: position in (12 B), direction (12 B) and pdf
 # (4 B) out; the Xorshift32 seed is derived from the query index
 Q_BYTES = 28
+# algorithmic bytes of one record: position 12 B, canonical direction 8 B, radiance 4 B
+REC_BYTES = 24
 LAUNCHES_PER_STEP = 21  # clear 1, record 1, build 1, refine 17, sample 1 (three CUDA graphs)
 
 
@@ -267,6 +269,12 @@ def bench_sdtree_ours(args, rank, world):
         "clocks": clk,
         "gpu_launches": LAUNCHES_PER_STEP * args.steps,
         "sdtree": st,
+        "roofline_record": {"kernel": "k_record (with clear)", "bound": "L2 atomics", "unit": "GB/s",
+                            "achieved": REC_BYTES * N_REC / (statistics.mean(record_ms) * 1e-3) / 1e9,
+                            "peak": peak, "frac": REC_BYTES * N_REC / (statistics.mean(record_ms) * 1e-3) / 1e9 / peak,
+                            "algorithmic_bytes_per_record": REC_BYTES,
+                            "atomics_per_s": 2 * N_REC / (statistics.mean(record_ms) * 1e-3),
+                            "note": "2 int64 atomics per record before warp / CTA aggregation"},
         "phases": {"record_Mrec_s": N_REC / (statistics.mean(record_ms) * 1e-3) / 1e6,
                    "build_refine_ms": statistics.mean(refine_ms),
                    "sample_pdf_Mq_s": N_Q / (s_ms * 1e-3) / 1e6},
@@ -888,7 +896,7 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": ("bf16" if mlp else "f32"),
             "data": "synthetic", "config": cfg, "e2e": res["e2e"], "roofline": res["roofline"],
             "clocks": res["clocks"], "gpu_launches": res["gpu_launches"]}
-    for k in ("sdtree", "phases", "counters_per_step", "unguided_nee_ris_Mpaths_s", "grid_cells", "spp_per_step",
+    for k in ("sdtree", "phases", "roofline_record", "counters_per_step", "unguided_nee_ris_Mpaths_s", "grid_cells", "spp_per_step",
               "inference"):
         if k in res:
             line[k] = res[k]

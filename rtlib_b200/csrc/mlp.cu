@@ -172,8 +172,7 @@ __global__ void __launch_bounds__(kMlpThreads, 1) k_mlp_train(MlpDev P, int64_t 
         // loss gradient at the outputs -> dY [128 x 64] (columns 40..63 zero)
         {
             float o[kMlpOut], g[kMlpHidden];
-#pragma unroll
-            for (int c = 0; c < kMlpOut; c += 16) ld_row16(tmem, kColD + c, o + c);
+            ld_row<kMlpOut>(tmem, kColD, o);
             const float nl = head_grad(o, wi, w * scale, g);
             if (w > 0.0f) lsum += w * nl;
 #pragma unroll
@@ -198,15 +197,17 @@ __global__ void __launch_bounds__(kMlpThreads, 1) k_mlp_train(MlpDev P, int64_t 
             if (l > 0) {
                 // dH = dX masked by ReLU' of the activation it came from, back into dY
                 const __nv_bfloat16* hl = hs[l - 1];
+                float v[kMlpHidden];
+                ld_row<kMlpHidden>(tmem, kColD, v);
 #pragma unroll
-                for (int c = 0; c < kMlpHidden; c += 16) {
-                    float v[16];
-                    ld_row16(tmem, kColD + c, v);
+                for (int c = 0; c < kMlpHidden; c += 8) {
+                    // the activation's 8 bf16 of this chunk in one 16-byte load
+                    const uint4 hv = *reinterpret_cast<const uint4*>(hl + blk(t, c, kMlpHidden));
+                    const __nv_bfloat16* hb = reinterpret_cast<const __nv_bfloat16*>(&hv);
 #pragma unroll
-                    for (int k = 0; k < 16; ++k)
-                        if (!(__bfloat162float(hl[blk(t, c + k, kMlpHidden)]) > 0.0f)) v[k] = 0.0f;
-                    st_bf16x8(dy + blk(t, c, kMlpHidden), v);
-                    st_bf16x8(dy + blk(t, c + 8, kMlpHidden), v + 8);
+                    for (int k = 0; k < 8; ++k)
+                        if (!(__bfloat162float(hb[k]) > 0.0f)) v[c + k] = 0.0f;
+                    st_bf16x8(dy + blk(t, c, kMlpHidden), v + c);
                 }
             }
         }

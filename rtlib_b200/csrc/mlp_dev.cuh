@@ -104,17 +104,32 @@ __device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-// 16 consecutive FP32 columns of this thread's TMEM lane (warp w reads lanes 32w .. 32w+31)
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
-    uint32_t r[16];
+// 16 consecutive FP32 columns of this thread's TMEM lane (warp w reads lanes 32w .. 32w+31);
+// the load is asynchronous until tmem_wait_ld()
+__device__ __forceinline__ void tmem_ld16_async(uint32_t taddr, uint32_t* r) {
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
           "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
         : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+    uint32_t r[16];
+    tmem_ld16_async(taddr, r);
+    tmem_wait_ld();
 #pragma unroll
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+// `n` (a multiple of 16, at most 64) columns with the loads in flight together
+template <int N>
+__device__ __forceinline__ void tmem_ld_cols(uint32_t taddr, float* v) {
+    uint32_t r[N];
+#pragma unroll
+    for (int c = 0; c < N; c += 16) tmem_ld16_async(taddr + c, r + c);
+    tmem_wait_ld();
+#pragma unroll
+    for (int i = 0; i < N; ++i) v[i] = __uint_as_float(r[i]);
 }
 
 // 8 floats -> 8 bf16 (round to nearest even) stored as one 16-byte core-matrix row chunk
@@ -283,18 +298,21 @@ __device__ __forceinline__ void ld_row16(uint32_t tmem, uint32_t col, float* v) 
     const uint32_t lane = (threadIdx.x & ~31u);
     tmem_ld16(tmem + (lane << 16) + col, v);
 }
+// thread t: accumulator row t, columns c0 .. c0+N-1 in one batch of loads
+template <int N>
+__device__ __forceinline__ void ld_row(uint32_t tmem, uint32_t col, float* v) {
+    const uint32_t lane = (threadIdx.x & ~31u);
+    tmem_ld_cols<N>(tmem + (lane << 16) + col, v);
+}
 // hidden epilogue: ReLU, bf16, row t of h [128 x 64]
 __device__ __forceinline__ void epilogue_relu(uint32_t tmem, __nv_bfloat16* h) {
     const int t = threadIdx.x;
+    float v[kMlpHidden];
+    ld_row<kMlpHidden>(tmem, kColD, v);
 #pragma unroll
-    for (int c = 0; c < kMlpHidden; c += 16) {
-        float v[16];
-        ld_row16(tmem, kColD + c, v);
+    for (int i = 0; i < kMlpHidden; ++i) v[i] = fmaxf(v[i], 0.0f);
 #pragma unroll
-        for (int i = 0; i < 16; ++i) v[i] = fmaxf(v[i], 0.0f);
-        st_bf16x8(h + blk(t, c, kMlpHidden), v);
-        st_bf16x8(h + blk(t, c + 8, kMlpHidden), v + 8);
-    }
+    for (int c = 0; c < kMlpHidden; c += 8) st_bf16x8(h + blk(t, c, kMlpHidden), v + c);
 }
 
 // Forward pass of one tile: the features of sample t are in row t of x0 (which the hidden
@@ -318,8 +336,7 @@ __device__ __forceinline__ bool mlp_forward_tile(uint32_t tmem, uint32_t sw, __n
         tc_fence_after();
         if (l < 3) epilogue_relu(tmem, x0);
     }
-#pragma unroll
-    for (int c = 0; c < kMlpOut; c += 16) ld_row16(tmem, kColD + c, o + c);
+    ld_row<kMlpOut>(tmem, kColD, o);
     return ok;
 }
 
