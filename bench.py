@@ -147,6 +147,7 @@ def bench_sdtree_ours(args, rank, world):
     dev = torch.device("cuda", rank % max(1, torch.cuda.device_count()))
     torch.cuda.set_device(dev)
     rec, q, th = _sdtree_inputs()
+    from rtlib_b200.workloads import spatial_threshold as W_th
     T = lambda a: torch.from_numpy(a).to(dev)
     pos, uv, rad = T(rec["pos"]), T(rec["uv"]), T(rec["radiance"])
     qpos = T(q["pos"])
@@ -159,13 +160,18 @@ def bench_sdtree_ours(args, rank, world):
         tree.clear()
         tree.record(p, u, r)
 
-    def refine_part():
+    def refine_part(p, u, r):
         tree.build()
         tree.refine(th)
+        for it in range(2, args.passes + 1):
+            # the same records again into the refined topology (deeper quadtrees to sample)
+            tree.record(p, u, r)
+            tree.build()
+            tree.refine(W_th(it))
 
     def build_part(p, u, r):
         record_part(p, u, r)
-        refine_part()
+        refine_part(p, u, r)
 
     def sample_part(qp):
         # guided direction + pdf of the sampled point (DTreeT::Sample + DTreeT::Pdf)
@@ -185,7 +191,7 @@ def bench_sdtree_ours(args, rank, world):
     with torch.cuda.graph(g_record):
         record_part(pos, uv, rad)
     with torch.cuda.graph(g_refine):
-        refine_part()
+        refine_part(pos, uv, rad)
     with torch.cuda.graph(g_sample):
         sample_part(qpos)
     stream = torch.cuda.current_stream()
@@ -267,7 +273,7 @@ def bench_sdtree_ours(args, rank, world):
                      "traffic": _traffic("k_sample_pdf"), "algorithmic_bytes_per_launch": Q_BYTES * N_Q,
                      "launch_ms": s_ms},
         "clocks": clk,
-        "gpu_launches": LAUNCHES_PER_STEP * args.steps,
+        "gpu_launches": (LAUNCHES_PER_STEP + (args.passes - 1) * 20) * args.steps,
         "sdtree": st,
         "roofline_record": {"kernel": "k_record (with clear)", "bound": "L2 atomics", "unit": "GB/s",
                             "achieved": REC_BYTES * N_REC / (statistics.mean(record_ms) * 1e-3) / 1e9,
@@ -329,7 +335,24 @@ def cpu_baseline_sdtree():
             "seconds_per_pass": s,
             "phases": {"record_Mrec_s": N_REC / statistics.median(p[0] for p in ph) / 1e6,
                        "build_refine_ms": 1e3 * statistics.median(p[1] for p in ph),
-                       "sample_pdf_Mq_s": N_Q / statistics.median(p[2] for p in ph) / 1e6}}
+                       "sample_pdf_Mq_s": N_Q / statistics.median(p[2] for p in ph) / 1e6,
+                       "sample_pdf_1thread_Mq_s": _ref_sample_1thread(kind)}}
+
+
+def _ref_sample_1thread(kind, n=1 << 18):
+    """Single-threaded sample+pdf rate of the host implementation on the first n queries."""
+    from oracle.oracle import Oracle, Reference
+    rec, q, th = _sdtree_inputs()
+    t = Reference().sdtree((0, 0, 0), (1, 1, 1)) if kind == "reference" else Oracle().sdtree((0, 0, 0), (1, 1, 1))
+    t.record(rec["pos"], rec["uv"], rec["radiance"])
+    t.build()
+    t.refine(th)
+    t0 = time.perf_counter()
+    if kind == "reference":
+        t.sample_pdf(q["pos"][:n], q["seeds"][:n], threads=1, with_dir=True)
+    else:
+        t.sample_pdf(q["pos"][:n], q["seeds"][:n], with_dir=True)
+    return n / (time.perf_counter() - t0) / 1e6
 
 
 # ---------------------------------------------------------------------------- Cornell workload
@@ -789,6 +812,9 @@ def main():
     ap.add_argument("--ref-seconds", type=float, default=300.0, help="learned: reference render time")
     ap.add_argument("--epochs", type=int, default=16, help="learned: Adam epochs over each pass's records")
     ap.add_argument("--size", default="1280x720", help="learned: image size")
+    ap.add_argument("--passes", type=int, default=1,
+                    help="sdtree: record+build+refine passes before the queries (1 = the literal config; 2 = "
+                         "the same records again into the refined topology)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--budget", type=int, default=2047,
                     help="cornell: total spp of the pass schedule (2047 = passes 1..1024); smaller values "
@@ -849,8 +875,9 @@ def main():
                "max_depth": C_MAX_DEPTH}
         metric, unit = "Mpaths/s", "Mpaths/s"
     else:
-        cfg = {"workload": "sdtree-standalone: 2^20 records, refine at 12000*sqrt(2), 2^22 sample+pdf",
-               "records": N_REC, "queries": N_Q}
+        cfg = {"workload": "sdtree-standalone: 2^20 records, refine at 12000*sqrt(2), 2^22 sample+pdf"
+                           + (f" ({args.passes} record+refine passes)" if args.passes > 1 else ""),
+               "records": N_REC, "queries": N_Q, "passes": args.passes}
         metric, unit = "SD-tree record+refine+sample throughput (config 1)", "Mops/s"
 
     if args.impl == "reference":
