@@ -633,12 +633,14 @@ def _timed_render(fn, seconds):
 
 def bench_learned(args):
     """Equal-time comparison on the occluded-light scene (NEE + RIS, 32 candidates, max depth 16):
-    plain SD-tree guiding against the learned guide (the SD-tree's pass schedule, network trained
-    on the tracer's records between passes), relMSE against a long SD-tree render.  Wall-clock
-    budgets include every training step; each method synchronises per launch."""
+    plain SD-tree guiding against the learned guide with the SD-tree as its fallback (the same
+    pass schedule; guide density half network, half SD-tree; network trained on the tracer's
+    records after every pass) and against the network alone, relMSE against a long SD-tree
+    render.  Wall-clock budgets include every training step; each method synchronises per
+    launch."""
     import torch
     from rtlib_b200 import metrics, scenes
-    from rtlib_b200.learned import render_learned
+    from rtlib_b200.learned import render_learned, render_learned_with_fallback
     from rtlib_b200.mlp import MLPGuide
     from rtlib_b200.sdtree import SDTree, SDTreeController
     from rtlib_b200.tracer import FLAG_NEE, FLAG_RIS, Tracer
@@ -668,15 +670,26 @@ def bench_learned(args):
         n_sd = sdtree_run(tr, budget)
         e_sd = metrics.relmse(tr.image().cpu().numpy(), ref, normalize=True)
         del tr
+        # the learned guide with the SD-tree as its fallback (the main configuration)
         tr = Tracer(sc, dev, max_depth=O_DEPTH, seed=3)
         g = MLPGuide((-0.1, -0.1, -0.1), (14.1, 4.1, 10.1), seed=1, learning_rate=1e-3, record_capacity=1 << 18)
+        tree = SDTree(*O_AABB, fraction=0.5)
         log = []
-        n_ml = render_learned(tr, g, time_budget_s=budget, base_flags=flags, fraction=0.5, ratio=0.5,
-                              epochs=args.epochs, batch=4096, log=log)
+        n_ml = render_learned_with_fallback(tr, g, tree, time_budget_s=budget, base_flags=flags, fraction=0.5,
+                                            mlp_share=0.5, epochs=args.epochs, batch=4096, log=log)
         e_ml = metrics.relmse(tr.image().cpu().numpy(), ref, normalize=True)
-        out.append({"budget_s": budget, "relmse_sdtree": e_sd, "relmse_learned": e_ml, "ratio": e_ml / e_sd,
-                    "spp_sdtree": n_sd, "spp_learned": n_ml, "train_log": log[-3:], "mlp_status": g.status()})
+        st_ml = g.status()
+        del tr, g, tree
+        # the network alone (its own doubling schedule, no SD-tree)
+        tr = Tracer(sc, dev, max_depth=O_DEPTH, seed=3)
+        g = MLPGuide((-0.1, -0.1, -0.1), (14.1, 4.1, 10.1), seed=1, learning_rate=1e-3, record_capacity=1 << 18)
+        n_mo = render_learned(tr, g, time_budget_s=budget, base_flags=flags, fraction=0.5, ratio=0.5,
+                              epochs=args.epochs, batch=4096)
+        e_mo = metrics.relmse(tr.image().cpu().numpy(), ref, normalize=True)
         del tr, g
+        out.append({"budget_s": budget, "relmse_sdtree": e_sd, "relmse_learned": e_ml, "ratio": e_ml / e_sd,
+                    "relmse_network_only": e_mo, "spp_sdtree": n_sd, "spp_learned": n_ml, "spp_network_only": n_mo,
+                    "train_log": log[-3:], "mlp_status": st_ml})
     return {"budgets": out, "ref_spp": ref_spp, "ref_seconds": args.ref_seconds}
 
 
@@ -834,7 +847,8 @@ def main():
         args.size = tuple(int(x) for x in args.size.split("x"))
         r = bench_learned(args)
         last = r["budgets"][-1]
-        line = {"metric": "equal-time relMSE, learned guide / SD-tree guide (occluded scene)", "value": last["ratio"],
+        line = {"metric": "equal-time relMSE, learned guide (SD-tree fallback) / plain SD-tree guide (occluded scene)",
+                "value": last["ratio"],
                 "unit": "ratio", "n_gpus": 1, "steps": len(r["budgets"]), "warmup": args.warmup,
                 "ms_per_step": last["budget_s"] * 1e3, "higher_is_better": False, "scaling": "weak",
                 "vs_baseline": None, "dtype": "bf16 network / f32 tracer", "data": "synthetic",

@@ -371,9 +371,12 @@ int rtpg_tracer_render_grid_guided(rtpg_tracer* h, rtpg_hashgrid* grid, rtpg_mqt
  * [| NEE | RIS] [| BUILD: sample the mixture with probability `fraction`, woPdf = (1 - fraction)
  * bsdfPdf + fraction q] [| FINAL: no training records].  Unless FINAL, every committed trace
  * vertex (the SD-tree's record) is appended to the guide's record buffer with probability
- * record_keep, up to its capacity.  The tracer and the guide must be on the same device. */
-int rtpg_tracer_render_mlp(rtpg_tracer* h, uint32_t spp, uint32_t flags, rtpg_mlp* mlp, float fraction,
-                           float record_keep, void* stream);
+ * record_keep, up to its capacity.  fallback (may be NULL): an SD-tree mixed into the guide
+ * density, q = mlp_share * network + (1 - mlp_share) * SD-tree, which then also receives the
+ * vertices' records (its build / refine stay with the caller or its controller).  The tracer
+ * and the guide must be on the same device. */
+int rtpg_tracer_render_mlp(rtpg_tracer* h, uint32_t spp, uint32_t flags, rtpg_mlp* mlp, rtpg_sdtree* fallback,
+                           float fraction, float mlp_share, float record_keep, void* stream);
 /* Emitter radiances (no counterpart in RTLib, which fixes them at load): light mesh i gets
  * host_rgb[3i..3i+2], both as MeshLight::emission for NEE and as the emission of its material.
  * Every light mesh must have its own emissive material. */

@@ -88,7 +88,7 @@ struct TracerDev {
     const int32_t* mat_light;  // light mesh of an emissive material, -1 otherwise
     // learned guide: hits found ahead of shading, the mixture of every path, record appends
     MlpView ml;
-    float mlp_fraction, mlp_keep;
+    float mlp_fraction, mlp_keep, mlp_share;
     uint32_t* hit_prim;
     float4* hit_tuv;
     __half* lobes;  // 40 per path: 8 x (mu xyz, kappa, weight)
@@ -225,7 +225,9 @@ __device__ __forceinline__ bool bounce_path(const TracerDev& T, uint32_t p, bool
     uint32_t flags = 0;
     uint32_t dt = 0;
     uint32_t cell = 0xffffffffu;  // hash-grid slot of this vertex (SimpleGuide2.cu: curGridIndex)
-    if (use_tree) dt = stree_lookup(T.tree.snode, T.tree.mn, T.tree.mx, position.x, position.y, position.z);
+    // the learned guide may carry the SD-tree as its fallback (T.tree set, mlp_share < 1)
+    const bool mlp_mix = use_mlp && T.tree.snode != nullptr;
+    if (use_tree || mlp_mix) dt = stree_lookup(T.tree.snode, T.tree.mn, T.tree.mx, position.x, position.y, position.z);
     if (m.type == MAT_PHONG) {
         uint32_t gbucket = 0, prv_cell = 0xffffffffu;
         unsigned long long gkey = 0;
@@ -288,18 +290,36 @@ __device__ __forceinline__ bool bounce_path(const TracerDev& T, uint32_t p, bool
                 Lb[k].kappa = __half2float(lp[5 * k + 3]);
                 Lb[k].weight = __half2float(lp[5 * k + 4]);
             }
+            // guide density q = share * network + (1 - share) * SD-tree (the fallback)
+            uint32_t soff = 0;
+            bool tguided = false;
+            if (mlp_mix) {
+                soff = T.tree.s_off[dt];
+                tguided = dtree_mean(T.tree.s_statw[dt], T.tree.s_sum[dt]) > 0.0f;
+            }
             if (rnd1(rng) < T.mlp_fraction) {
-                const float u0 = rnd1(rng);
-                const float u1 = rnd1(rng);
-                const float u2 = rnd1(rng);
-                direction = normalize3(vmf_mixture_sample(Lb, u0, u1, u2));
+                if (!mlp_mix || rnd1(rng) < T.mlp_share) {
+                    const float u0 = rnd1(rng);
+                    const float u1 = rnd1(rng);
+                    const float u2 = rnd1(rng);
+                    direction = normalize3(vmf_mixture_sample(Lb, u0, u1, u2));
+                } else {
+                    const float2 c = dtree_sample_g(T.tree.s_nodes, soff, tguided, rng);
+                    direction = normalize3(canonical_to_dir(c.x, c.y));
+                }
                 cosine = dot3(direction, fn);
                 const float cp2 = fmaxf(cosine * kInvPi, 0.0f);
                 const float pp2 = glossy ? phong_pdf(direction, refl, m.shininess) : 0.0f;
                 bsdf_val = diffuse * kInvPi + m.specular * sf * pp2;
                 bsdf_pdf = sel * cp2 + (1.0f - sel) * pp2;
             }
-            wo_pdf = (1.0f - T.mlp_fraction) * bsdf_pdf + T.mlp_fraction * vmf_mixture_pdf(Lb, direction);
+            float q = vmf_mixture_pdf(Lb, direction);
+            if (mlp_mix) {
+                const float2 c = dir_to_canonical(direction.x, direction.y, direction.z);
+                const float qt = fmaxf(dtree_pdf_g(T.tree.s_nodes, soff, tguided, c.x, c.y), 0.0f);
+                q = T.mlp_share * q + (1.0f - T.mlp_share) * qt;
+            }
+            wo_pdf = (1.0f - T.mlp_fraction) * bsdf_pdf + T.mlp_fraction * q;
         } else if (use_grid && build && prv_cell != 0xffffffffu) {
             // the Morton quadtree of the cell (SimpleGuide2.cu:350-377)
             float dtree_pdf;
@@ -434,7 +454,7 @@ __device__ __forceinline__ bool bounce_path(const TracerDev& T, uint32_t p, bool
         const bool has_guide = use_grid ? cell != 0xffffffffu : true;
         T.v_flags[vi] = (uint8_t)((has_guide && ok_b ? 1u : 0u) | ((flags & HF_DELTA) ? 2u : 0u));
         if (use_grid) T.v_cell[vi] = cell;
-        if (use_tree) T.v_cell[vi] = dt;  // the vertex's DTree, found once here for the commit
+        if (use_tree || mlp_mix) T.v_cell[vi] = dt;  // the vertex's DTree, found once here for the commit
         if (use_mlp) {
             T.v_nrm[vi] = fn;
             T.v_wo[vi] = f3(-in_dir.x, -in_dir.y, -in_dir.z);
@@ -577,7 +597,7 @@ __global__ void __launch_bounds__(kMlpThreads) k_mlp_lobes(TracerDev T, int in) 
 }
 
 template <int G>
-__global__ void __launch_bounds__(kTB, 6) k_bounce(TracerDev T, int in) {
+__global__ void __launch_bounds__(kTB, 8) k_bounce(TracerDev T, int in) {
     const uint32_t n = T.qcount[in];
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         T.qcount[in ^ 1] = 0;
@@ -614,6 +634,8 @@ __global__ void __launch_bounds__(kTB, 6) k_bounce(TracerDev T, int in) {
 template <int G>
 __global__ void __launch_bounds__(kTB) k_finish(TracerDev T) {
     constexpr bool use_grid = G == kGuideGrid;
+    // the learned guide with the SD-tree as fallback commits to both
+    const bool tree_too = G == kGuideMlp && T.tree.snode != nullptr;
     const bool recording = (G == kGuideTree || G == kGuideGrid || G == kGuideMlp) && !(T.flags & RTPG_TRACE_FLAG_FINAL);
     for (uint32_t base = blockIdx.x * blockDim.x; base < T.npath; base += gridDim.x * blockDim.x) {
         const uint32_t p = base + threadIdx.x;
@@ -684,6 +706,8 @@ __global__ void __launch_bounds__(kTB) k_finish(TracerDev T) {
                                 T.ml.r_w[idx] = irr;
                             }
                         }
+                    }
+                    if (G == kGuideMlp && !tree_too) {
                     } else if (use_grid) {
                         // MortonTraceVertexT::Commit (OPX7UtilsMorton.h:550-585) ->
                         // MortonQuadTreeWrapperT::Record: leaf of the cell's building quadtree
@@ -705,7 +729,7 @@ __global__ void __launch_bounds__(kTB) k_finish(TracerDev T) {
                     }
                 }
             }
-            if (G == kGuideMlp) {
+            if (G == kGuideMlp && !tree_too) {
             } else if (use_grid) {
                 warp_add_u64(k_s, v_s, T.mqt.leaves);
             } else {
@@ -1125,10 +1149,14 @@ int rtpg_tracer_render_grid(rtpg_tracer* h, uint32_t spp, uint32_t flags, rtpg_h
 // One launch guided by the learned mixture (no counterpart in RTLib): every bounce runs the
 // closest-hit queries, the network on the tensor cores for the hit points (with BUILD), then
 // shading; unless FINAL, committed trace vertices become training records of the guide, each
-// kept with probability record_keep.
-int rtpg_tracer_render_mlp(rtpg_tracer* h, uint32_t spp, uint32_t flags, rtpg_mlp* mlp, float fraction,
-                           float record_keep, void* stream) {
+// kept with probability record_keep.  With a fallback SD-tree the guide density is
+// mlp_share * network + (1 - mlp_share) * SD-tree, and the vertices are committed to the tree
+// as well.
+int rtpg_tracer_render_mlp(rtpg_tracer* h, uint32_t spp, uint32_t flags, rtpg_mlp* mlp, rtpg_sdtree* fallback,
+                           float fraction, float mlp_share, float record_keep, void* stream) {
     if (!h || !mlp) return fail(RTPG_EINVAL, "rtpg_tracer_render_mlp: null argument");
+    if (fallback && !(mlp_share >= 0.0f && mlp_share <= 1.0f))
+        return fail(RTPG_EINVAL, "rtpg_tracer_render_mlp: mlp_share outside [0, 1]");
     if (!(flags & RTPG_TRACE_FLAG_USE_MLP) || (flags & (RTPG_TRACE_FLAG_USE_TREE | RTPG_TRACE_FLAG_USE_GRID)))
         return fail(RTPG_EINVAL, "rtpg_tracer_render_mlp: flags must hold USE_MLP and no other guide");
     if (!(fraction >= 0.0f && fraction <= 1.0f)) return fail(RTPG_EINVAL, "rtpg_tracer_render_mlp: fraction outside [0, 1]");
@@ -1142,12 +1170,14 @@ int rtpg_tracer_render_mlp(rtpg_tracer* h, uint32_t spp, uint32_t flags, rtpg_ml
             return r;
         RTPG_CUDA(cudaFuncSetAttribute(k_mlp_lobes, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemEval));
     }
-    memset(&T.tree, 0, sizeof(SDTreeDev));
+    if (fallback) T.tree = sdtree_device_view(fallback);
+    else memset(&T.tree, 0, sizeof(SDTreeDev));
     memset(&T.grid, 0, sizeof(HashGridDev));
     memset(&T.mqt, 0, sizeof(MqtDev));
     T.ml = mlp_view(mlp);
     T.mlp_fraction = fraction;
     T.mlp_keep = record_keep;
+    T.mlp_share = fallback ? mlp_share : 1.0f;
     return render_waves(h, spp, flags, as_stream(stream));
 }
 

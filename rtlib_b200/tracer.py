@@ -131,9 +131,10 @@ class Tracer:
         call("rtpg_tracer_render_grid_guided", self.h, grid.h, mqt.h, controller.h, int(base_flags),
              int(samples_per_launch), int(max_launches), stream_ptr(stream))
 
-    def render_mlp(self, spp, flags, mlp, fraction=0.5, record_keep=1.0, stream=None):
-        call("rtpg_tracer_render_mlp", self.h, int(spp), int(flags) | FLAG_USE_MLP, mlp.h, float(fraction),
-             float(record_keep), stream_ptr(stream))
+    def render_mlp(self, spp, flags, mlp, fraction=0.5, record_keep=1.0, fallback=None, mlp_share=0.5, stream=None):
+        call("rtpg_tracer_render_mlp", self.h, int(spp), int(flags) | FLAG_USE_MLP, mlp.h,
+             fallback.h if fallback is not None else None, float(fraction), float(mlp_share), float(record_keep),
+             stream_ptr(stream))
 
     def set_light_emission(self, rgb):
         """rgb: (num_lights, 3) host array; NEE radiance and material emission of every light."""

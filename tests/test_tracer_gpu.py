@@ -297,3 +297,35 @@ def test_config_tracers_run(cuda, name):
                                             "HashGrid.CellSize": 4096, "HashGrid.GridSize": [16, 16, 16]}})
     tr, img, spp, dt = run(cfg, scenes.cornell_box(48, 48), cuda)
     assert spp >= 15 and img.shape == (48, 48, 3) and np.isfinite(img).all() and img.mean() > 0.05
+
+
+def test_learned_guide_with_sdtree_fallback_runs(cuda):
+    """The learned guide mixed with the SD-tree (its fallback) under the SD-tree's pass
+    schedule: both guides learn from the same vertices and the render converges like the
+    plain SD-tree render of the same budget."""
+    from rtlib_b200 import metrics
+    from rtlib_b200.learned import render_learned_with_fallback
+    from rtlib_b200.mlp import MLPGuide
+    from rtlib_b200.sdtree import SDTree, SDTreeController
+    from rtlib_b200.tracer import FLAG_NEE, FLAG_RIS, Tracer
+    sc = scenes.occluded_rooms(128, 72, n_objects=60, n_lights=256, seed=5, sphere_level=1)
+    flags = FLAG_NEE | FLAG_RIS
+    aabb = ((-0.005,) * 3, (14.005, 4.005, 10.005))
+    ref_tr = Tracer(sc, cuda, max_depth=16, width=128, height=72, seed=99)
+    ref_tr.render(2048, flags)
+    ref = ref_tr.image().cpu().numpy()
+    tr = Tracer(sc, cuda, max_depth=16, width=128, height=72, seed=3)
+    g = MLPGuide((-0.1, -0.1, -0.1), (14.1, 4.1, 10.1), seed=1, record_capacity=1 << 16)
+    tree = SDTree(*aabb, fraction=0.5)
+    log = []
+    n = render_learned_with_fallback(tr, g, tree, budget_spp=63, base_flags=flags, log=log)
+    assert n == 64 and g.status() == 0 and tree.status() == 0 and log
+    assert tree.stats()["dtree_nodes"] > 4  # the fallback tree learned from the same vertices
+    e_mix = metrics.relmse(tr.image().cpu().numpy(), ref, normalize=True)
+    pt = Tracer(sc, cuda, max_depth=16, width=128, height=72, seed=3)
+    tree2 = SDTree(*aabb, fraction=0.5)
+    ctrl = SDTreeController(tree2, 63, iteration_for_built=0, ratio_for_budget=0.5, samples_per_launch=1)
+    ctrl.start()
+    pt.render_guided(tree2, ctrl, flags)
+    e_sd = metrics.relmse(pt.image().cpu().numpy(), ref, normalize=True)
+    assert e_mix < 1.5 * e_sd, (e_mix, e_sd, log)
