@@ -24,6 +24,29 @@ def relmse(img, ref, eps=1e-2, normalize=False):
     return float(np.mean(((img - ref) ** 2 / (ref ** 2 + eps))[ok]))
 
 
+def relmse_denoised(img, ref_a, ref_b, n_a, n_b, eps=1e-2, normalize=False):
+    """relMSE of img against the converged image, estimated from two independent reference
+    renders of n_a and n_b samples per pixel.  Against their weighted mean r, the error of img
+    is E[(img - t)^2] + Var(r) (t the converged image, img independent of r); with per-sample
+    variance s^2, Var(r) = s^2 / (n_a + n_b) and E[(a - b)^2] = s^2 (1/n_a + 1/n_b), so
+    Var(r) = E[(a - b)^2] * n_a n_b / (n_a + n_b)^2, which is subtracted per pixel with the
+    same denominator.  Returns (relmse vs r, the estimate with r's variance removed)."""
+    a = np.asarray(ref_a, np.float64)
+    b = np.asarray(ref_b, np.float64)
+    img = np.asarray(img, np.float64)
+    r = (n_a * a + n_b * b) / float(n_a + n_b)
+    if normalize:
+        m = float(np.mean(r[np.isfinite(r)]))
+        if m > 0:
+            img, r, a, b = img / m, r / m, a / m, b / m
+    ok = np.isfinite(img).all(axis=-1) & np.isfinite(a).all(axis=-1) & np.isfinite(b).all(axis=-1)
+    den = r ** 2 + eps
+    raw = (img - r) ** 2 / den
+    c = float(n_a) * float(n_b) / float(n_a + n_b) ** 2
+    noise = c * (a - b) ** 2 / den
+    return float(np.mean(raw[ok])), float(np.mean((raw - noise)[ok]))
+
+
 def rmae(img, ref):
     """sum |img - ref| (Euclidean RGB distance) / sum (|ref| + |img|) / 2 over pixels with ref != 0."""
     b = np.asarray(ref, np.float32).reshape(-1, 3)

@@ -22,3 +22,20 @@ def test_relmse_rmae_smape_small_cases(tmp_path):
     raw = np.fromfile(p, np.float32).reshape(-1, 3)
     assert np.array_equal(raw[0], img[0, 1]) and np.array_equal(raw[1], img[0, 0])
     assert np.array_equal(metrics.load_result_bin(p, 2, 1), img)
+
+
+def test_relmse_denoised_removes_reference_noise():
+    # truth t, image and two references with independent Gaussian noise of per-sample
+    # variance s^2: the de-noised estimate recovers the image's own error
+    rng = np.random.default_rng(0)
+    t = rng.uniform(0.5, 2.0, (256, 256, 3))
+    s, n_img, n_a, n_b = 0.5, 16, 40, 24
+    img = t + rng.normal(0, s / np.sqrt(n_img), t.shape)
+    a = t + rng.normal(0, s / np.sqrt(n_a), t.shape)
+    b = t + rng.normal(0, s / np.sqrt(n_b), t.shape)
+    raw, den = metrics.relmse_denoised(img, a, b, n_a, n_b)
+    r = (n_a * a + n_b * b) / (n_a + n_b)
+    assert abs(raw - metrics.relmse(img, r)) < 1e-12
+    truth = metrics.relmse(img, t)
+    assert raw > 1.15 * truth
+    assert abs(den - truth) < 0.03 * truth
