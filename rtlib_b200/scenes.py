@@ -141,13 +141,19 @@ def _icosphere(level):
     return np.array(v), np.array(f)
 
 
-def occluded_rooms(width=1280, height=720, n_objects=2048, n_lights=4096, seed=3, sphere_level=3):
+def occluded_rooms(width=1280, height=720, n_objects=2048, n_lights=4096, seed=3, sphere_level=3, light_margin=0.25):
     """The occluded-light scene: a 10 x 4 x 10 room filled with n_objects random icospheres and
     boxes (radii U[0.05, 0.4]); light enters only through a 1 x 2 doorway in the x = 10 wall
     from a neighbouring 4 x 4 x 10 room whose far wall (x = 14, facing the doorway) holds
     n_lights emissive triangles, each its own NEE light with radiance lognormal(0, 1.5) (grey).  With level-3 icospheres (1280
     triangles) for 807 of the objects and boxes for the rest the scene has about 2^20
-    triangles."""
+    triangles.
+
+    The emitter panel keeps a margin of `light_margin` metres from the light room's floor,
+    ceiling and side walls.  An emitter whose edge touches another surface makes the NEE
+    estimator at that surface's points next to the edge unbounded (cos * cos / d^2 with d -> 0)
+    and of infinite variance, so an image error would then be dominated by a few fireflies;
+    with the margin the geometry term of a light-room surface is at most 1 / margin^2."""
     rng = np.random.default_rng(seed)
     b = _Builder()
     mats = [_mat(diffuse=(0.7, 0.7, 0.7)), _mat(diffuse=(0.6, 0.55, 0.5)), _mat(diffuse=(0.5, 0.6, 0.7))]
@@ -194,10 +200,11 @@ def occluded_rooms(width=1280, height=720, n_objects=2048, n_lights=4096, seed=3
     rad = rng.lognormal(0.0, 1.5, 2 * gy * gz).astype(np.float32)
     light_emit, light_first = [], []
     k = 0
+    ly, lz = 4.0 - 2 * light_margin, 10.0 - 2 * light_margin
     for i in range(gy):
         for j in range(gz):
-            p = (13.99, 4 * i / gy, 10 * j / gz)
-            e1, e2 = (0, 0, 10 / gz), (0, 4 / gy, 0)
+            p = (13.99, light_margin + ly * i / gy, light_margin + lz * j / gz)
+            e1, e2 = (0, 0, lz / gz), (0, ly / gy, 0)
             # quad(p, e1, e2): normal e1 x e2 = -x
             for tri in range(2):
                 mats.append(_mat(emission=(rad[k],) * 3, type=NEE_LIGHT))
