@@ -283,12 +283,18 @@ __device__ __forceinline__ bool bounce_path(const TracerDev& T, uint32_t p, bool
         } else if (use_mlp && build) {
             // the learned mixture of this path's hit (k_mlp_lobes)
             VmfLobe Lb[kMlpLobes];
-            const __half* lp = T.lobes + size_t(p) * 40;
+            {
+                // 80 bytes per path: five 16-byte loads
+                __align__(16) __half lp[40];
+                const uint4* src = reinterpret_cast<const uint4*>(T.lobes + size_t(p) * 40);
 #pragma unroll
-            for (int k = 0; k < kMlpLobes; ++k) {
-                Lb[k].mu = f3(__half2float(lp[5 * k]), __half2float(lp[5 * k + 1]), __half2float(lp[5 * k + 2]));
-                Lb[k].kappa = __half2float(lp[5 * k + 3]);
-                Lb[k].weight = __half2float(lp[5 * k + 4]);
+                for (int k = 0; k < 5; ++k) reinterpret_cast<uint4*>(lp)[k] = src[k];
+#pragma unroll
+                for (int k = 0; k < kMlpLobes; ++k) {
+                    Lb[k].mu = f3(__half2float(lp[5 * k]), __half2float(lp[5 * k + 1]), __half2float(lp[5 * k + 2]));
+                    Lb[k].kappa = __half2float(lp[5 * k + 3]);
+                    Lb[k].weight = __half2float(lp[5 * k + 4]);
+                }
             }
             // guide density q = share * network + (1 - share) * SD-tree (the fallback)
             uint32_t soff = 0;
@@ -505,6 +511,14 @@ __device__ __forceinline__ bool bounce_path(const TracerDev& T, uint32_t p, bool
     const bool bad = any_nan3(direction) || any_nan3(cur_thr) || any_nan3(L);
     if (bad || (flags & HF_FINISH) || d >= T.max_depth - 1) return false;
     T.depth[p] = d + 1;
+    if (use_mlp) {
+        // the closest hit of the continuing ray, traced here rather than in a pass of its own,
+        // so the network of the next bounce finds it waiting (k_hit serves the first bounce)
+        const Hit nh = bvh_trace<false>(T.scene, position.x, position.y, position.z, direction.x, direction.y,
+                                        direction.z, 0.0001f, 1.0e20f);
+        T.hit_prim[p] = nh.prim;
+        T.hit_tuv[p] = make_float4(nh.t, nh.u, nh.v, 0.0f);
+    }
     return true;
 }
 
@@ -517,7 +531,8 @@ __host__ __device__ constexpr int guide_of(uint32_t flags) {
                                                  : kGuideNone;
 }
 
-// learned guide, stage 1 of a bounce: closest hits of the queue
+// learned guide, stage 1 of the first bounce: closest hits of the camera rays (later bounces
+// find theirs traced at the end of the previous k_bounce)
 __global__ void __launch_bounds__(kTB) k_hit(TracerDev T, int in) {
     const uint32_t n = T.qcount[in];
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
@@ -578,7 +593,7 @@ __global__ void __launch_bounds__(kMlpThreads) k_mlp_lobes(TracerDev T, int in) 
         if (live) {
             VmfLobe L[kMlpLobes];
             mlp_head(o, L);
-            __half* lp = T.lobes + size_t(p) * 40;
+            __align__(16) __half lp[40];
 #pragma unroll
             for (int k = 0; k < kMlpLobes; ++k) {
                 lp[5 * k] = __float2half_rn(L[k].mu.x);
@@ -587,6 +602,10 @@ __global__ void __launch_bounds__(kMlpThreads) k_mlp_lobes(TracerDev T, int in) 
                 lp[5 * k + 3] = __float2half_rn(L[k].kappa);
                 lp[5 * k + 4] = __float2half_rn(L[k].weight);
             }
+            // 80 bytes per path: five 16-byte stores
+            uint4* dst = reinterpret_cast<uint4*>(T.lobes + size_t(p) * 40);
+#pragma unroll
+            for (int k = 0; k < 5; ++k) dst[k] = reinterpret_cast<const uint4*>(lp)[k];
         }
     }
     if (!ok) atomicOr(T.status, RTPG_STATUS_TIMEOUT);
@@ -808,9 +827,10 @@ struct rtpg_tracer {
     }
 };
 
-static void launch_bounce(const TracerDev& T, int g, cudaStream_t st, int in) {
+static void launch_bounce(const TracerDev& T, int g, cudaStream_t st, uint32_t b) {
+    const int in = int(b & 1);
     if (guide_of(T.flags) == kGuideMlp) {
-        k_hit<<<g, kTB, 0, st>>>(T, in);
+        if (b == 0) k_hit<<<g, kTB, 0, st>>>(T, in);
         if (T.flags & RTPG_TRACE_FLAG_BUILD) k_mlp_lobes<<<kSMs * 4, kMlpThreads, kSmemEval, st>>>(T, in);
         k_bounce<kGuideMlp><<<g, kTB, 0, st>>>(T, in);
         return;
@@ -847,7 +867,7 @@ static int timed_wave(rtpg_tracer* h, cudaStream_t st) {
     h->t_launch[0] += 1;
     for (uint32_t b = 0; b < T.max_depth; ++b) {
         cudaEventRecord(h->ev[2], st);
-        launch_bounce(T, g, st, int(b & 1));
+        launch_bounce(T, g, st, b);
         cudaEventRecord(h->ev[3], st);
         RTPG_CUDA(cudaEventSynchronize(h->ev[3]));
         cudaEventElapsedTime(&ms, h->ev[2], h->ev[3]);
@@ -869,7 +889,7 @@ static void launch_wave(rtpg_tracer* h, cudaStream_t st) {
     TracerDev& T = h->dev;
     const int g = kSMs * 8;
     k_raygen<<<g, kTB, 0, st>>>(T);
-    for (uint32_t b = 0; b < T.max_depth; ++b) launch_bounce(T, g, st, int(b & 1));
+    for (uint32_t b = 0; b < T.max_depth; ++b) launch_bounce(T, g, st, b);
     launch_finish(T, g, st);
 }
 
