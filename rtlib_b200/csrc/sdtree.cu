@@ -452,9 +452,10 @@ __global__ void __launch_bounds__(256) k_sample_pdf(SDTreeDev t, int64_t n, cons
         uint32_t rng = seeds ? seeds[i] : (pcg1d(seed_base + (uint32_t)i) | 1u);
         const uint32_t off = t.s_off[d];
         const bool guided = dtree_mean(t.s_statw[d], t.s_sum[d]) > 0.0f;
-        const float2 uv = dtree_sample_g(t.s_nodes, off, guided, rng);
+        DSquare sq;
+        const float2 uv = dtree_sample_sq(t.s_nodes, off, guided, rng, sq);
         if (out_uv) reinterpret_cast<float2*>(out_uv)[i] = uv;
-        if (out_pdf_uv) out_pdf_uv[i] = dtree_pdf_g(t.s_nodes, off, guided, uv.x, uv.y);
+        if (out_pdf_uv) out_pdf_uv[i] = dtree_pdf_in(t.s_nodes, off, guided, sq, uv.x, uv.y);
         if (out_dir || out_pdf_dir) {
             const float3 dv = normalize3(canonical_to_dir(uv.x, uv.y));
             if (out_dir) {
@@ -464,7 +465,7 @@ __global__ void __launch_bounds__(256) k_sample_pdf(SDTreeDev t, int64_t n, cons
             }
             if (out_pdf_dir) {
                 const float2 c = dir_to_canonical(dv.x, dv.y, dv.z);
-                out_pdf_dir[i] = dtree_pdf_g(t.s_nodes, off, guided, c.x, c.y);
+                out_pdf_dir[i] = dtree_pdf_in(t.s_nodes, off, guided, sq, c.x, c.y);
             }
         }
     }

@@ -135,61 +135,6 @@ __device__ __forceinline__ float dtree_mean(float statw, float sum) {
     return __fmul_rn(factor, sum);
 }
 
-// DTreeT::Sample (PG.h:478-484) -> DTreeNodeT::Sample (PG.h:229-277), float order as written.
-// `guided` is DTreeT::GetMean() > 0 (uniform sampling of the square otherwise).
-__device__ __forceinline__ float2 dtree_sample_g(const SNode* __restrict__ nodes, uint32_t off, bool guided,
-                                                 uint32_t& rng) {
-    if (!guided) {
-        const float a = rnd1(rng);
-        const float b = rnd1(rng);
-        return make_float2(a, b);
-    }
-    uint32_t cur = 0;
-    float rx = 0.0f, ry = 0.0f, size = 1.0f;
-    for (;;) {
-        const SNode nd = nodes[off + cur];
-        const float4 s = nd.sums;
-        int idx = 0;
-        const float topLeft = s.x, topRight = s.y;
-        float partial = __fadd_rn(s.x, s.z);
-        const float total = __fadd_rn(__fadd_rn(__fadd_rn(s.x, s.y), s.z), s.w);
-        float boundary = __fdiv_rn(partial, total);
-        float ox = 0.0f, oy = 0.0f;
-        float sample = rnd1(rng);
-        if (sample < boundary) {
-            sample = __fdiv_rn(sample, boundary);
-            boundary = __fdiv_rn(topLeft, partial);
-        } else {
-            partial = __fsub_rn(total, partial);
-            ox = 0.5f;
-            sample = __fdiv_rn(__fsub_rn(sample, boundary), __fsub_rn(1.0f, boundary));
-            boundary = __fdiv_rn(topRight, partial);
-            idx |= 1;
-        }
-        if (sample >= boundary) {
-            oy = 0.5f;
-            idx |= 2;
-        }
-        rx = __fadd_rn(rx, __fmul_rn(size, ox));
-        ry = __fadd_rn(ry, __fmul_rn(size, oy));
-        size = __fmul_rn(size, 0.5f);
-        const uint32_t c = sel4(nd.child, idx);
-        if (c == 0 || sel4(s, idx) <= 0.0f) {
-            const float a = rnd1(rng);
-            const float b = rnd1(rng);
-            rx = __fadd_rn(rx, __fmul_rn(size, a));
-            ry = __fadd_rn(ry, __fmul_rn(size, b));
-            break;
-        }
-        cur = c;
-    }
-    return make_float2(fminf(fmaxf(rx, 0.0f), 1.0f), fminf(fmaxf(ry, 0.0f), 1.0f));
-}
-__device__ __forceinline__ float2 dtree_sample(const SNode* __restrict__ nodes, uint32_t off, float statw, float sum,
-                                               uint32_t& rng) {
-    return dtree_sample_g(nodes, off, dtree_mean(statw, sum) > 0.0f, rng);
-}
-
 // DTreeT::Pdf (PG.h:485-490) -> DTreeNodeT::Pdf (PG.h:279-320)
 __device__ __forceinline__ float dtree_pdf_g(const SNode* __restrict__ nodes, uint32_t off, bool guided, float u,
                                              float v) {
@@ -217,6 +162,86 @@ __device__ __forceinline__ float dtree_pdf_g(const SNode* __restrict__ nodes, ui
 __device__ __forceinline__ float dtree_pdf(const SNode* __restrict__ nodes, uint32_t off, float statw, float sum,
                                            float u, float v) {
     return dtree_pdf_g(nodes, off, dtree_mean(statw, sum) > 0.0f, u, v);
+}
+
+// The square [x, x + w) x [y, y + w) of the node where a sampling descent stopped, and the
+// pdf DTreeNodeT::Pdf gives every point inside it.
+struct DSquare {
+    float x, y, w, pdf;
+    __device__ __forceinline__ bool holds(float u, float v) const { return u >= x && u < x + w && v >= y && v < y + w; }
+};
+
+// dtree_pdf_g at (u, v) when the point lies in the square sampling stopped in, else the full
+// descent: equal to dtree_pdf_g(nodes, off, guided, u, v) bit for bit either way.
+__device__ __forceinline__ float dtree_pdf_in(const SNode* __restrict__ nodes, uint32_t off, bool guided,
+                                              const DSquare& sq, float u, float v) {
+    return sq.holds(u, v) ? sq.pdf : dtree_pdf_g(nodes, off, guided, u, v);
+}
+
+// DTreeT::Sample (PG.h:478-484) -> DTreeNodeT::Sample (PG.h:229-277), float order as written;
+// `guided` is DTreeT::GetMean() > 0 (uniform sampling of the square otherwise).  The pdf of
+// the sampled point comes out of the same descent: DTreeNodeT::Pdf walks the binary digits of
+// (u, v) (quad_child doubles exactly), so for any point inside the square of the node where
+// sampling stopped it visits exactly the nodes sampling visited, with the same quadrant sums;
+// the factors 4 s_i / total are formed in the same order here.  `sq` returns that square and
+// pdf (uniform sampling: the unit square, whose pdf is constant).
+__device__ __forceinline__ float2 dtree_sample_sq(const SNode* __restrict__ nodes, uint32_t off, bool guided,
+                                                  uint32_t& rng, DSquare& sq) {
+    if (!guided) {
+        const float a = rnd1(rng);
+        const float b = rnd1(rng);
+        sq = DSquare{0.0f, 0.0f, 1.0f, __fdiv_rn(__fmul_rn(1.0f, kInv2Pi), 2.0f)};
+        return make_float2(a, b);
+    }
+    uint32_t cur = 0;
+    float rx = 0.0f, ry = 0.0f, size = 1.0f, result = 1.0f;
+    float bx = 0.0f, by = 0.0f;  // corner of the square where the descent stopped
+    for (;;) {
+        const SNode nd = nodes[off + cur];
+        const float4 s = nd.sums;
+        int idx = 0;
+        const float topLeft = s.x, topRight = s.y;
+        float partial = __fadd_rn(s.x, s.z);
+        const float total = __fadd_rn(__fadd_rn(__fadd_rn(s.x, s.y), s.z), s.w);
+        float boundary = __fdiv_rn(partial, total);
+        float ox = 0.0f, oy = 0.0f;
+        float sample = rnd1(rng);
+        if (sample < boundary) {
+            sample = __fdiv_rn(sample, boundary);
+            boundary = __fdiv_rn(topLeft, partial);
+        } else {
+            partial = __fsub_rn(total, partial);
+            ox = 0.5f;
+            sample = __fdiv_rn(__fsub_rn(sample, boundary), __fsub_rn(1.0f, boundary));
+            boundary = __fdiv_rn(topRight, partial);
+            idx |= 1;
+        }
+        if (sample >= boundary) {
+            oy = 0.5f;
+            idx |= 2;
+        }
+        rx = __fadd_rn(rx, __fmul_rn(size, ox));
+        ry = __fadd_rn(ry, __fmul_rn(size, oy));
+        size = __fmul_rn(size, 0.5f);
+        const float si = sel4(s, idx);
+        // the pdf descent's step at this node (DTreeNodeT::Pdf, PG.h:295-300)
+        if (si <= 0.0f) result = 0.0f;
+        else result = __fmul_rn(result, __fdiv_rn(__fmul_rn(4.0f, si), total));
+        const uint32_t c = sel4(nd.child, idx);
+        if (c == 0 || si <= 0.0f) {
+            bx = rx;
+            by = ry;
+            const float a = rnd1(rng);
+            const float b = rnd1(rng);
+            rx = __fadd_rn(rx, __fmul_rn(size, a));
+            ry = __fadd_rn(ry, __fmul_rn(size, b));
+            break;
+        }
+        cur = c;
+    }
+    // bx, by and bx + size are dyadic with few bits: the comparisons of holds() are exact
+    sq = DSquare{bx, by, size, __fdiv_rn(__fmul_rn(result, kInv2Pi), 2.0f)};
+    return make_float2(fminf(fmaxf(rx, 0.0f), 1.0f), fminf(fmaxf(ry, 0.0f), 1.0f));
 }
 
 }  // namespace rtpg

@@ -89,6 +89,7 @@ struct TracerDev {
     // learned guide: hits found ahead of shading, the mixture of every path, record appends
     MlpView ml;
     float mlp_fraction, mlp_keep, mlp_share;
+    uint32_t mlp_keep_pow;  // record keep probability scaled by throughput luminance^pow (0: uniform)
     uint32_t* hit_prim;
     float4* hit_tuv;
     __half* lobes;  // 40 per path: 8 x (mu xyz, kappa, weight)
@@ -268,8 +269,11 @@ __device__ __forceinline__ bool bounce_path(const TracerDev& T, uint32_t p, bool
         if (use_tree && build) {
             const uint32_t soff = T.tree.s_off[dt];
             const bool guided = dtree_mean(T.tree.s_statw[dt], T.tree.s_sum[dt]) > 0.0f;
+            // square + pdf of a guided sample; the empty default sends the pdf of a BSDF sample
+            // through the full descent
+            DSquare sq{2.0f, 2.0f, 0.0f, 0.0f};
             if (rnd1(rng) < T.tree.fraction) {
-                const float2 c = dtree_sample_g(T.tree.s_nodes, soff, guided, rng);
+                const float2 c = dtree_sample_sq(T.tree.s_nodes, soff, guided, rng, sq);
                 direction = normalize3(canonical_to_dir(c.x, c.y));
                 cosine = dot3(direction, fn);
                 const float cp2 = fmaxf(cosine * kInvPi, 0.0f);
@@ -278,7 +282,7 @@ __device__ __forceinline__ bool bounce_path(const TracerDev& T, uint32_t p, bool
                 bsdf_pdf = sel * cp2 + (1.0f - sel) * pp2;
             }
             const float2 c = dir_to_canonical(direction.x, direction.y, direction.z);
-            const float dtree_pdf = fmaxf(dtree_pdf_g(T.tree.s_nodes, soff, guided, c.x, c.y), 0.0f);
+            const float dtree_pdf = fmaxf(dtree_pdf_in(T.tree.s_nodes, soff, guided, sq, c.x, c.y), 0.0f);
             wo_pdf = (1.0f - T.tree.fraction) * bsdf_pdf + T.tree.fraction * dtree_pdf;
         } else if (use_mlp && build) {
             // the learned mixture of this path's hit (k_mlp_lobes)
@@ -303,6 +307,7 @@ __device__ __forceinline__ bool bounce_path(const TracerDev& T, uint32_t p, bool
                 soff = T.tree.s_off[dt];
                 tguided = dtree_mean(T.tree.s_statw[dt], T.tree.s_sum[dt]) > 0.0f;
             }
+            DSquare sq{2.0f, 2.0f, 0.0f, 0.0f};  // as in the SD-tree guide above
             if (rnd1(rng) < T.mlp_fraction) {
                 if (!mlp_mix || rnd1(rng) < T.mlp_share) {
                     const float u0 = rnd1(rng);
@@ -310,7 +315,7 @@ __device__ __forceinline__ bool bounce_path(const TracerDev& T, uint32_t p, bool
                     const float u2 = rnd1(rng);
                     direction = normalize3(vmf_mixture_sample(Lb, u0, u1, u2));
                 } else {
-                    const float2 c = dtree_sample_g(T.tree.s_nodes, soff, tguided, rng);
+                    const float2 c = dtree_sample_sq(T.tree.s_nodes, soff, tguided, rng, sq);
                     direction = normalize3(canonical_to_dir(c.x, c.y));
                 }
                 cosine = dot3(direction, fn);
@@ -322,7 +327,7 @@ __device__ __forceinline__ bool bounce_path(const TracerDev& T, uint32_t p, bool
             float q = vmf_mixture_pdf(Lb, direction);
             if (mlp_mix) {
                 const float2 c = dir_to_canonical(direction.x, direction.y, direction.z);
-                const float qt = fmaxf(dtree_pdf_g(T.tree.s_nodes, soff, tguided, c.x, c.y), 0.0f);
+                const float qt = fmaxf(dtree_pdf_in(T.tree.s_nodes, soff, tguided, sq, c.x, c.y), 0.0f);
                 q = T.mlp_share * q + (1.0f - T.mlp_share) * qt;
             }
             wo_pdf = (1.0f - T.mlp_fraction) * bsdf_pdf + T.mlp_fraction * q;
@@ -709,8 +714,15 @@ __global__ void __launch_bounds__(kTB) k_finish(TracerDev T) {
                     if (G == kGuideMlp) {
                         // a training record of the learned guide: the SD-tree's record with the
                         // vertex's normal and outgoing direction, kept with probability mlp_keep
-                        if (isfinite(irr) && irr > 0.0f &&
-                            to_uniform_float(pcg1d(T.rng[p] ^ (i * 0x9E3779B9u))) < T.mlp_keep) {
+                        // optionally in proportion to the vertex's weight in the pixel estimate
+                        // (its throughput times its incident radiance), so that the network
+                        // learns most where the image depends on it most
+                        float keep = T.mlp_keep;
+                        if (T.mlp_keep_pow) {
+                            const float lt = fminf(1.0f, (th.x + th.y + th.z) * (1.0f / 3.0f));
+                            keep *= T.mlp_keep_pow == 1 ? lt : lt * lt;
+                        }
+                        if (isfinite(irr) && irr > 0.0f && to_uniform_float(pcg1d(T.rng[p] ^ (i * 0x9E3779B9u))) < keep) {
                             const uint32_t idx = atomicAdd(T.ml.r_count, 1u);
                             if (idx < T.ml.capacity) {
                                 const float3 ps = T.v_pos[vi], nm = T.v_nrm[vi], wo = T.v_wo[vi];
@@ -1199,6 +1211,15 @@ int rtpg_tracer_render_mlp(rtpg_tracer* h, uint32_t spp, uint32_t flags, rtpg_ml
     T.mlp_keep = record_keep;
     T.mlp_share = fallback ? mlp_share : 1.0f;
     return render_waves(h, spp, flags, as_stream(stream));
+}
+
+// Learned-guide training records: keep probability of a committed vertex scaled by the
+// luminance of its path throughput (clamped to 1) raised to `power` (0: every vertex alike).
+int rtpg_tracer_set_record_importance(rtpg_tracer* h, uint32_t power) {
+    if (!h) return fail(RTPG_EINVAL, "rtpg_tracer_set_record_importance: null handle");
+    if (power > 2) return fail(RTPG_EINVAL, "rtpg_tracer_set_record_importance: power must be 0, 1 or 2");
+    h->dev.mlp_keep_pow = power;
+    return RTPG_OK;
 }
 
 // Mean radiance per pixel (accumulation / samples), RGB float, row-major, y = 0 first.
