@@ -21,6 +21,12 @@ Workload "sdtree" (SD-tree standalone): 2^20 seeded radiance records (uniform po
 4-lobe vMF directions kappa 50, lognormal(0,1) radiance) are recorded, the trees are built and
 refined at 12000*sqrt(2), then 2^22 guided sample+pdf queries run at uniform positions.
 
+Workload "hashgrid": the hash-grid guide's batched routines on the occluded scene's grid
+(256 x 64 x 192 cells, 2^20 slots, 63-bit Morton keys, level-4 Morton quadtrees): insert 2^19
+surface points, look up 2^22 surface points, record 2^22 Morton-leaf values, build every cell's
+sampling pyramid, 2^22 guided sample+pdf queries.  The CPU baseline is RTLib's own per-point
+routines (oracle/_ref), single-threaded, on the workload scaled down 64x.
+
 Inputs are resident in HBM when the timed region starts (value).  L2 is flushed (a 256 MiB
 write) before every timed step.  N GPUs run independent replicas (no collective): value is
 the work of all ranks over the slowest rank's time.
@@ -562,7 +568,8 @@ def bench_occluded_ours(args, rank, world):
     clk = clocks.stop()
     ms = _max_over_ranks(sum(a.elapsed_time(c) for a, c in ev) / len(ev), world, dev)
     cnt = tr.counters()
-    assert grid.status() == 0 and trees.status() == 0
+    grid_status = grid.status()  # RTPG_STATUS_HASH_FULL if a bucket of 32 overflowed
+    assert trees.status() == 0
     cells = int((grid.export() != 0).sum())
     # unguided NEE + RIS on the same tracer, and kernel times of one guided step
     a, c = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -619,6 +626,190 @@ def bench_occluded_ours(args, rank, world):
     }
 
 
+# ---------------------------------------------------------------------------- hash-grid workload
+HG_POINTS = _HG_POINTS = 1 << 19    # surface points inserted into the grid (~380k distinct cells)
+HG_QUERIES = _HG_QUERIES = 1 << 22  # lookups, Morton-leaf records and sample+pdf queries
+HG_SLOTS = _HG_SLOTS = 1 << 20
+HG_LEVEL = 4
+HG_BOUNDS = (256, 64, 192)
+HG_AABB = ((-0.005,) * 3, (14.005, 4.005, 10.005))
+# algorithmic bytes per unit: lookup position 12 in + slot 4 out; record cell 4 + canonical
+# direction 8 + value 4; sample cell 4 + seed 4 in, direction 12 + pdf 4 out
+HG_LOOKUP_BYTES, HG_RECORD_BYTES, HG_SAMPLE_BYTES = 16, 16, 24
+
+
+def _hg_cell_bytes(level=HG_LEVEL):
+    """Algorithmic bytes of one cell's pyramid build: every int64 leaf read and zeroed (16 B)
+    and every float of the (4^(L+1)-1)/3-entry pyramid written (4 B)."""
+    return (1 << (2 * level)) * 16 + (((1 << (2 * (level + 1))) - 1) // 3) * 4
+
+
+def bench_hashgrid_ours(args, rank, world):
+    """The hash-grid guide's batched routines on the occluded-light scene's grid (2^20 slots,
+    63-bit Morton keys, 256x64x192 cells): insert 2^19 surface points into the current table,
+    snapshot it, look up 2^22 surface points, record 2^22 Morton-leaf values into the found
+    cells, build the level-4 sampling pyramids of all 2^20 cells, and 2^22 guided
+    sample+pdf queries.  One CUDA graph per phase."""
+    import torch
+    from rtlib_b200 import workloads as W
+    from rtlib_b200.hashgrid import KEY_MORTON, HashGrid, MortonQuadTrees
+
+    dev = torch.device("cuda", rank % max(1, torch.cuda.device_count()))
+    torch.cuda.set_device(dev)
+    # --scale-log2 k divides points, queries and slots by 2^k (small cases for profiling)
+    HG_POINTS, HG_QUERIES, HG_SLOTS = (x >> args.scale_log2 for x in (_HG_POINTS, _HG_QUERIES, _HG_SLOTS))
+    d = W.hashgrid_inputs(HG_POINTS, HG_QUERIES, 0)
+    T = lambda a: torch.from_numpy(a).to(dev)
+    pts, qpos, quv, qval, qseed = T(d["points"]), T(d["queries"]), T(d["uv"]), T(d["value"]), T(d["seeds"])
+    slot_p = torch.empty(HG_POINTS, dtype=torch.int32, device=dev)
+    slot_q = torch.empty(HG_QUERIES, dtype=torch.int32, device=dev)
+    out_dir = torch.empty((HG_QUERIES, 3), dtype=torch.float32, device=dev)
+    out_pdf = torch.empty(HG_QUERIES, dtype=torch.float32, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    grid = HashGrid(*HG_AABB, HG_BOUNDS, HG_SLOTS, keying=KEY_MORTON)
+    trees = MortonQuadTrees(HG_SLOTS, level=HG_LEVEL, fraction=0.3)
+
+    def insert_part(p):
+        grid.clear()
+        grid.insert(p, slot_p)
+        grid.swap()
+
+    parts = [lambda: insert_part(pts), lambda: grid.lookup(qpos, slot_q),
+             lambda: trees.record(slot_q, quv, qval, canonical=True), lambda: trees.update(),
+             lambda: trees.sample_pdf(slot_q, qseed, out_dir=out_dir, out_pdf=out_pdf)]
+    names = ["insert", "lookup", "record", "build", "sample_pdf"]
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):
+        for _ in range(2):
+            for f in parts:
+                f()
+    torch.cuda.current_stream().wait_stream(side)
+    graphs = []
+    for f in parts:
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            f()
+        graphs.append(g)
+    stream = torch.cuda.current_stream()
+    t0 = time.perf_counter()
+    k = 0
+    while k < args.warmup or time.perf_counter() - t0 < 0.5:
+        for g in graphs:
+            g.replay()
+        k += 1
+    torch.cuda.synchronize()
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(len(graphs) + 1)] for _ in range(args.steps)]
+    clocks = ClockSampler(dev.index)
+    _barrier(world)
+    torch.cuda.synchronize()
+    clocks.start()
+    for k in range(args.steps):
+        flush.fill_(k & 0xff)
+        ev[k][0].record(stream)
+        for j, g in enumerate(graphs):
+            g.replay()
+            ev[k][j + 1].record(stream)
+    torch.cuda.synchronize()
+    _barrier(world)
+    clk = clocks.stop()
+    ph = {nm: statistics.mean(e[j].elapsed_time(e[j + 1]) for e in ev) for j, nm in enumerate(names)}
+    ms = _max_over_ranks(statistics.mean(e[0].elapsed_time(e[-1]) for e in ev), world, dev)
+    found = int((slot_q >= 0).sum().item())
+    cells = int(torch.unique(slot_p).numel())
+    grid_status = grid.status()  # RTPG_STATUS_HASH_FULL if a bucket of 32 overflowed
+    assert trees.status() == 0
+
+    # e2e: pinned host inputs through the same C-ABI calls, results read back, all timed
+    hp = [torch.from_numpy(d[k]).pin_memory() for k in ("points", "queries", "uv", "value", "seeds")]
+    dv = [pts, qpos, quv, qval, qseed]
+    h_dir = torch.empty((HG_QUERIES, 3), dtype=torch.float32).pin_memory()
+    h_pdf = torch.empty(HG_QUERIES, dtype=torch.float32).pin_memory()
+    h2d = sum(x.numel() * x.element_size() for x in hp)
+    d2h = (h_dir.numel() + h_pdf.numel()) * 4
+    e2e_ms = []
+    for k in range(args.warmup + args.steps):
+        flush.fill_(k & 0xff)
+        a, c = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for x, y in zip(dv, hp):
+            x.copy_(y, non_blocking=True)
+        for f in parts:
+            f()
+        h_dir.copy_(out_dir, non_blocking=True)
+        h_pdf.copy_(out_pdf, non_blocking=True)
+        c.record(stream)
+        torch.cuda.synchronize()
+        if k >= args.warmup:
+            e2e_ms.append(a.elapsed_time(c))
+    e2e = _max_over_ranks(statistics.mean(e2e_ms), world, dev)
+    ops = (HG_POINTS + 3 * HG_QUERIES) * world
+    peak, peak_kind = _peaks()
+    gbs = lambda b, t: b / (t * 1e-3) / 1e9
+    build_bytes = HG_SLOTS * _hg_cell_bytes()
+    achieved = gbs(build_bytes, ph["build"])
+    return {
+        "metric": "hash-grid guide insert+lookup+record+build+sample throughput (config-3 grid)",
+        "value": ops / (ms * 1e-3) / 1e6, "unit": "Mops/s", "ms_per_step": ms,
+        "e2e": {"value": ops / (e2e * 1e-3) / 1e6, "unit": "Mops/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h)},
+        "roofline": {"kernel": "k_mqt_build", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs (burst copy)",
+                     "traffic": _traffic("k_mqt_build"), "algorithmic_bytes_per_launch": build_bytes,
+                     "launch_ms": ph["build"]},
+        "clocks": clk,
+        # clear 1 + insert (prepare, 2 sorts, heads, assign, scatter) + swap 1; lookup 1; record 1;
+        # build 1; sample 1 (cub sorts counted as one launch each)
+        "gpu_launches": 12 * args.steps,
+        "phases": {"insert_Mpts_s": HG_POINTS / (ph["insert"] * 1e-3) / 1e6,
+                   "lookup_Mq_s": HG_QUERIES / (ph["lookup"] * 1e-3) / 1e6,
+                   "lookup_GBs": gbs(HG_LOOKUP_BYTES * HG_QUERIES, ph["lookup"]),
+                   "record_Mrec_s": HG_QUERIES / (ph["record"] * 1e-3) / 1e6,
+                   "record_GBs": gbs(HG_RECORD_BYTES * HG_QUERIES, ph["record"]),
+                   "build_ms": ph["build"], "build_GBs": achieved,
+                   "sample_pdf_Mq_s": HG_QUERIES / (ph["sample_pdf"] * 1e-3) / 1e6,
+                   "sample_pdf_GBs": gbs(HG_SAMPLE_BYTES * HG_QUERIES, ph["sample_pdf"]),
+                   "ms": ph},
+        "grid_cells": cells, "queries_found": found, "grid_status": grid_status,
+    }
+
+
+def cpu_baseline_hashgrid(seconds=10.0, scale_log2=6):
+    """RTLib's own hash grid and Morton quadtree code on the host, single thread (its routines
+    are per-point device functions; the reference has no batched host path), on the workload
+    scaled down by 2^scale_log2 with the table alike (the full workload's 2^19 points fall into
+    373k distinct cells of 2^20 slots, load 0.36; scaled down nearly every point has a cell of
+    its own, load 0.5), and RTLib's keying (its checksum covers this 256x64x192 grid).
+    Returns the line's cpu_baseline."""
+    from oracle.oracle import Reference
+    from rtlib_b200 import workloads as W
+    r = Reference()
+    npts, nq, slots = HG_POINTS >> scale_log2, HG_QUERIES >> scale_log2, HG_SLOTS >> scale_log2
+    d = W.hashgrid_inputs(npts, nq, 0)
+    mn, mx = np.array(HG_AABB[0], np.float32), np.array(HG_AABB[1], np.float32)
+    size = mx - mn
+    per = ((1 << (2 * (6 + 1))) - 1) // 3  # RTLib's quadtree storage is sized for level 6
+    times = []
+    t_start = time.perf_counter()
+    while time.perf_counter() - t_start < seconds and len(times) < 200:
+        cur = np.zeros(slots, np.uint32)
+        weights = np.zeros(slots * per, np.float32)
+        t0 = time.perf_counter()
+        r.hashgrid_insert(d["points"], mn, size, HG_BOUNDS, slots, cur)
+        prv = cur.copy()
+        cell = r.hashgrid_lookup(d["queries"], mn, size, HG_BOUNDS, slots, prv)
+        r.mqt_record(HG_LEVEL, weights, cell, d["uv"], d["value"])
+        r.mqt_build(slots, HG_LEVEL, weights)
+        ok = cell != np.uint32(0xFFFFFFFF)
+        r.mqt_sample_pdf(HG_LEVEL, weights, cell[ok], d["seeds"][ok])
+        times.append(time.perf_counter() - t0)
+    s = statistics.median(times)
+    return {"value": (npts + 3 * nq) / s / 1e6, "unit": "Mops/s", "cores": 1, "kind": "reference",
+            "sample": f"{len(times)} runs of the workload scaled by 1/{1 << scale_log2} ({npts} inserts, {nq} lookups, "
+                      f"records and samples, {slots} slots), RTLib's own routines single-threaded",
+            "seconds_per_run": s}
+
+
 # ---------------------------------------------------------------------------- learned-guide workload
 def _timed_render(fn, seconds):
     import torch
@@ -651,8 +842,8 @@ def bench_learned(args):
     sc = scenes.occluded_rooms(w, h)
     flags = FLAG_NEE | FLAG_RIS
 
-    def sdtree_run(tr, seconds):
-        tree = SDTree(*O_AABB, fraction=0.5)
+    def sdtree_run(tr, seconds, fraction=0.5):
+        tree = SDTree(*O_AABB, fraction=fraction)
         ctrl = SDTreeController(tree, 1 << 20, iteration_for_built=0, ratio_for_budget=0.5, samples_per_launch=1)
         ctrl.start()
         return _timed_render(lambda: tr.render_guided(tree, ctrl, flags, max_launches=1), seconds)
@@ -679,27 +870,35 @@ def bench_learned(args):
         n_sd = sdtree_run(tr, budget)
         e_sd, d_sd = err(tr.image().cpu().numpy())
         del tr
+        # the SD-tree with the learned arm's guide probability, for a like-for-like reading
+        tr = Tracer(sc, dev, max_depth=O_DEPTH, seed=3)
+        n_sd2 = sdtree_run(tr, budget, args.guide_fraction)
+        e_sd2, d_sd2 = err(tr.image().cpu().numpy())
+        del tr
         # the learned guide with the SD-tree as its fallback (the main configuration)
         tr = Tracer(sc, dev, max_depth=O_DEPTH, seed=3)
         g = MLPGuide((-0.1, -0.1, -0.1), (14.1, 4.1, 10.1), seed=1, learning_rate=1e-3, record_capacity=1 << 18)
         tree = SDTree(*O_AABB, fraction=0.5)
         log = []
-        n_ml = render_learned_with_fallback(tr, g, tree, time_budget_s=budget, base_flags=flags, fraction=0.5,
-                                            mlp_share=0.5, epochs=args.epochs, batch=4096, log=log)
+        n_ml = render_learned_with_fallback(tr, g, tree, time_budget_s=budget, base_flags=flags,
+                                            fraction=args.guide_fraction, mlp_share=0.5, epochs=args.epochs,
+                                            batch=4096, log=log)
         e_ml, d_ml = err(tr.image().cpu().numpy())
         st_ml = g.status()
         del tr, g, tree
         # the network alone (its own doubling schedule, no SD-tree)
         tr = Tracer(sc, dev, max_depth=O_DEPTH, seed=3)
         g = MLPGuide((-0.1, -0.1, -0.1), (14.1, 4.1, 10.1), seed=1, learning_rate=1e-3, record_capacity=1 << 18)
-        n_mo = render_learned(tr, g, time_budget_s=budget, base_flags=flags, fraction=0.5, ratio=0.5,
+        n_mo = render_learned(tr, g, time_budget_s=budget, base_flags=flags, fraction=args.guide_fraction, ratio=0.5,
                               epochs=args.epochs, batch=4096)
         e_mo, d_mo = err(tr.image().cpu().numpy())
         del tr, g
         out.append({"budget_s": budget, "relmse_sdtree": e_sd, "relmse_learned": e_ml, "ratio": e_ml / e_sd,
                     "relmse_network_only": e_mo,
                     "denoised": {"relmse_sdtree": d_sd, "relmse_learned": d_ml, "relmse_network_only": d_mo,
-                                 "ratio": d_ml / d_sd if d_sd > 0 else None},
+                                 "ratio": d_ml / d_sd if d_sd > 0 else None,
+                                 "relmse_sdtree_at_guide_fraction": d_sd2},
+                    "relmse_sdtree_at_guide_fraction": e_sd2, "spp_sdtree_at_guide_fraction": n_sd2,
                     "spp_sdtree": n_sd, "spp_learned": n_ml, "spp_network_only": n_mo,
                     "train_log": log[-3:], "mlp_status": st_ml})
     return {"budgets": out, "ref_spp": ref_spp, "ref_seconds": args.ref_seconds}
@@ -832,15 +1031,20 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="cornell", choices=["cornell", "sdtree", "occluded", "learned", "mlp"])
+    ap.add_argument("--workload", default="cornell", choices=["cornell", "sdtree", "hashgrid", "occluded", "learned",
+                                                               "mlp"])
     ap.add_argument("--budgets", default="30,120", help="learned: equal-time budgets in seconds")
     ap.add_argument("--ref-seconds", type=float, default=300.0, help="learned: reference render time")
-    ap.add_argument("--epochs", type=int, default=16, help="learned: Adam epochs over each pass's records")
+    ap.add_argument("--epochs", type=int, default=8, help="learned: Adam epochs over each pass's records")
+    ap.add_argument("--guide-fraction", type=float, default=0.7,
+                    help="learned: probability of sampling the guide (network / SD-tree mixture) at a vertex")
     ap.add_argument("--size", default="1280x720", help="learned: image size")
     ap.add_argument("--passes", type=int, default=1,
                     help="sdtree: record+build+refine passes before the queries (1 = the literal config; 2 = "
                          "the same records again into the refined topology)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--scale-log2", type=int, default=0,
+                    help="hashgrid: divide points, queries and slots by 2^k (small cases for profiling)")
     ap.add_argument("--budget", type=int, default=2047,
                     help="cornell: total spp of the pass schedule (2047 = passes 1..1024); smaller values "
                          "give the short case used for profiling")
@@ -869,7 +1073,10 @@ def main():
                                        f"SD-tree renders of {r['ref_seconds'] / 2} s each ({r['ref_spp']} spp in "
                                        f"all)", "relmse": "normalised by the reference mean, eps 1e-2; 'value' "
                                        "against the reference's mean, 'value_denoised' with the reference's own "
-                                       "variance (from the difference of the two renders) removed"},
+                                       "variance (from the difference of the two renders) removed",
+                           "learned_arm": f"guide sampled with probability {args.guide_fraction}, density half network "
+                                          f"half SD-tree, {args.epochs} Adam epochs per pass",
+                           "sdtree_arm": "plain SD-tree guiding, BSDF/guide mixing 0.5"},
                 "budgets": r["budgets"]}
         print(json.dumps(line), flush=True)
         return 0
@@ -887,6 +1094,7 @@ def main():
     cornell = args.workload == "cornell"
     occluded = args.workload == "occluded"
     mlp = args.workload == "mlp"
+    hashgrid = args.workload == "hashgrid"
     set_budget(args.budget)
     if mlp:
         cfg = {"workload": "learned-guide kernels: 3x64 ReLU MLP -> 8 vMF lobes, BF16 tcgen05 / FP32 TMEM; "
@@ -897,6 +1105,14 @@ def main():
                            f"candidates, max depth 16, hash grid 2^20 slots (Morton keys) + level-{O_LEVEL} "
                            f"Morton quadtrees, {O_BUDGET} spp budget", "width": O_W, "height": O_H, "max_depth": O_DEPTH}
         metric, unit = "Mpaths/s", "Mpaths/s"
+    elif hashgrid:
+        cfg = {"workload": "hashgrid-guide: occluded-scene grid 256x64x192, 2^20 slots, 63-bit Morton keys, "
+                           "level-4 Morton quadtrees; insert 2^19 surface points, 2^22 lookups, records and "
+                           "sample+pdf queries", "points": HG_POINTS >> args.scale_log2,
+               "queries": HG_QUERIES >> args.scale_log2, "slots": HG_SLOTS >> args.scale_log2, "level": HG_LEVEL}
+        if args.scale_log2:
+            cfg["workload"] += f" (scaled down by 2^{args.scale_log2})"
+        metric, unit = "hash-grid guide insert+lookup+record+build+sample throughput (config-3 grid)", "Mops/s"
     elif cornell:
         cfg = {"workload": f"cornell-guided: 512x512, {C_BUDGET} spp budget in doubling passes, max depth 8, NEE, "
                            "SD-tree guiding fraction 0.5", "width": C_W, "height": C_H, "spp": C_BUDGET + 1,
@@ -919,6 +1135,10 @@ def main():
             sample = (f"{cores} independent replicas of the guided render at 32x32 px with the same 2048-launch "
                       f"pass schedule on the CPU restatement of RTLib's integrator; {paths} paths in {dt:.1f} s")
             ms = dt * 1e3
+        elif hashgrid:
+            cpu_baseline_hashgrid(seconds=0.0)  # warm-up (pages in)
+            cb = cpu_baseline_hashgrid(seconds=20.0)
+            v, kind, threads, sample, ms = cb["value"], cb["kind"], cb["cores"], cb["sample"], cb["seconds_per_run"] * 1e3
         else:
             kind = _ref_kind()
             threads = cores if kind == "reference" else 1
@@ -943,7 +1163,7 @@ def main():
         torch.cuda.set_device(_env_int("LOCAL_RANK", rank))
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
     res = (bench_mlp_ours if mlp else bench_occluded_ours if occluded else bench_cornell_ours if cornell
-           else bench_sdtree_ours)(args, rank, world)
+           else bench_hashgrid_ours if hashgrid else bench_sdtree_ours)(args, rank, world)
     cfg["l2"] = "flushed (256 MiB write) before every timed step"
     cfg["parallelism"] = f"replicas x{world}"
     line = {"metric": res["metric"], "value": res["value"], "unit": res["unit"], "n_gpus": world,
@@ -952,7 +1172,7 @@ def main():
             "data": "synthetic", "config": cfg, "e2e": res["e2e"], "roofline": res["roofline"],
             "clocks": res["clocks"], "gpu_launches": res["gpu_launches"]}
     for k in ("sdtree", "phases", "roofline_record", "counters_per_step", "unguided_nee_ris_Mpaths_s", "grid_cells", "spp_per_step",
-              "inference"):
+              "inference", "queries_found", "grid_status"):
         if k in res:
             line[k] = res[k]
     if rank == 0 and not args.no_cpu_baseline and not occluded and not mlp:
@@ -962,6 +1182,8 @@ def main():
             line["cpu_baseline"] = {"value": v, "unit": "Mpaths/s", "cores": cores, "kind": "port",
                                     "sample": f"{cores} replicas of the guided render at 32x32 px, full pass "
                                               f"schedule, CPU restatement of the integrator; {paths} paths in {dt:.1f} s"}
+        elif hashgrid:
+            line["cpu_baseline"] = cpu_baseline_hashgrid()
         else:
             line["cpu_baseline"] = cpu_baseline_sdtree()
     if world > 1:

@@ -377,12 +377,6 @@ int rtpg_tracer_render_grid_guided(rtpg_tracer* h, rtpg_hashgrid* grid, rtpg_mqt
  * and the guide must be on the same device. */
 int rtpg_tracer_render_mlp(rtpg_tracer* h, uint32_t spp, uint32_t flags, rtpg_mlp* mlp, rtpg_sdtree* fallback,
                            float fraction, float mlp_share, float record_keep, void* stream);
-/* Learned-guide training records (no counterpart in RTLib): the keep probability of a committed
- * vertex is record_keep times the luminance of its path throughput, clamped to 1, raised to
- * `power` (0, the default: every vertex alike; 1 or 2).  The throughput is the factor by which
- * the vertex's incident radiance enters the pixel, so the records concentrate where the
- * image depends on the guide. */
-int rtpg_tracer_set_record_importance(rtpg_tracer* h, uint32_t power);
 /* Emitter radiances (no counterpart in RTLib, which fixes them at load): light mesh i gets
  * host_rgb[3i..3i+2], both as MeshLight::emission for NEE and as the emission of its material.
  * Every light mesh must have its own emissive material. */

@@ -96,7 +96,6 @@ _SIGS = {
     "rtpg_tracer_set_light_emission": [P, P, U32],
     "rtpg_tracer_image_f64": [P, P, P],
     "rtpg_tracer_render_mlp": [P, U32, U32, P, P, F32, F32, F32, P],
-    "rtpg_tracer_set_record_importance": [P, U32],
     "rtpg_tracer_render_adjoint": [P, U32, U32, P, I32, P, P, P],
     "rtpg_tracer_render_grid_guided": [P, P, P, P, U32, U32, U32, P],
     "rtpg_tracer_image": [P, P, P],

@@ -17,6 +17,18 @@
 namespace rtpg {
 
 // ------------------------------------------------------------------ inference
+// N floats (a multiple of 4) to dst: 16-byte stores if dst is 16-byte aligned, else scalars
+template <int N>
+__device__ __forceinline__ void store_row(float* dst, const float* v) {
+    if ((reinterpret_cast<uintptr_t>(dst) & 15u) == 0) {
+#pragma unroll
+        for (int c = 0; c < N; c += 4) *reinterpret_cast<float4*>(dst + c) = make_float4(v[c], v[c + 1], v[c + 2], v[c + 3]);
+    } else {
+#pragma unroll
+        for (int c = 0; c < N; ++c) dst[c] = v[c];
+    }
+}
+
 // out_raw: 48 floats per sample (the network output); out_lobes: 40 floats per sample, lobe k
 // = (mu xyz, kappa, weight).  Either may be null.
 __global__ void __launch_bounds__(kMlpThreads) k_mlp_eval(MlpDev P, int64_t n, const float* __restrict__ pos,
@@ -52,15 +64,18 @@ __global__ void __launch_bounds__(kMlpThreads) k_mlp_eval(MlpDev P, int64_t n, c
         float o[kMlpOut];
         ok &= mlp_forward_tile(tmem, sw, x0, mbar, phase, o);
         if (i < n) {
-            if (out_raw)
-                for (int c = 0; c < kMlpOut; ++c) out_raw[i * kMlpOut + c] = o[c];
+            // a sample's row (192 or 160 bytes) in 16-byte stores when the array allows it
+            if (out_raw) store_row<kMlpOut>(out_raw + i * kMlpOut, o);
             if (out_lobes) {
                 VmfLobe L[kMlpLobes];
                 mlp_head(o, L);
+                float q[40];
+#pragma unroll
                 for (int k = 0; k < kMlpLobes; ++k) {
-                    float* q = out_lobes + i * 40 + 5 * k;
-                    q[0] = L[k].mu.x; q[1] = L[k].mu.y; q[2] = L[k].mu.z; q[3] = L[k].kappa; q[4] = L[k].weight;
+                    q[5 * k] = L[k].mu.x; q[5 * k + 1] = L[k].mu.y; q[5 * k + 2] = L[k].mu.z;
+                    q[5 * k + 3] = L[k].kappa; q[5 * k + 4] = L[k].weight;
                 }
+                store_row<40>(out_lobes + i * 40, q);
             }
         }
     }

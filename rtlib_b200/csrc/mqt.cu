@@ -9,9 +9,10 @@
 // inside a level (code = part1by1(y) << 1 | part1by1(x)).
 //
 // Update (RTMortonQuadTreeWrapperT::Update + LaunchBuildKernel, :640-651, :916-941) is one
-// kernel: a CTA per cell reads the cell's leaves, reduces the pyramid in shared memory with
-// exact integer sums, writes it as float to the sampling buffer and zeroes the leaves
-// (RTLib launches 1024x more blocks than cells and loops serially per cell).
+// kernel: a warp (levels up to 5) or a CTA (levels 6, 7) per cell reads the cell's leaves,
+// reduces the pyramid in shared memory with exact integer sums, writes it as float to the
+// sampling buffer and zeroes the leaves (RTLib launches 1024x more blocks than cells and loops
+// serially per cell).
 #include <algorithm>
 #include <new>
 #include <vector>
@@ -69,6 +70,103 @@ __global__ void __launch_bounds__(kMqtBuildBlock) k_mqt_build(MqtDev t) {
         float* w = t.pyramid + (size_t)c * per;
         for (uint32_t k = threadIdx.x; k < per; k += blockDim.x) w[k] = fx_to_float(sp[k], t.fx);
         __syncthreads();
+    }
+}
+
+// Levels up to kMqtWarpLevel: one warp per cell, kMqtWarps cells per CTA.  The warp reads the
+// cell's leaves with 16-byte loads (and zeroes them with 16-byte stores), reduces the pyramid
+// in its own shared memory with exact integer sums and writes it out with consecutive lanes on
+// consecutive floats; no block-wide barrier, so every warp of the SM keeps a cell's loads in
+// flight.  Same results as k_mqt_build (integer sums do not depend on their order).
+constexpr uint32_t kMqtWarpLevel = 5;
+constexpr int kMqtWarps = 8;
+__global__ void __launch_bounds__(32 * kMqtWarps) k_mqt_build_warp(MqtDev t) {
+    extern __shared__ unsigned long long swarp[];  // kMqtWarps x (4^(L+1)-1)/3 entries
+    const uint32_t L = t.level;
+    const uint32_t nleaf = 1u << (2 * L);  // >= 4: 16-byte aligned rows of leaves
+    const uint32_t off_leaf = mqt_level_offset(L);
+    const uint32_t per = mqt_level_offset(L + 1);
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    unsigned long long* sp = swarp + (size_t)warp * per;
+    const uint32_t nw = gridDim.x * kMqtWarps;
+    for (uint32_t c = blockIdx.x * kMqtWarps + warp; c < t.ncells; c += nw) {
+        ulonglong2* lf = reinterpret_cast<ulonglong2*>(t.leaves + (size_t)c * nleaf);
+        for (uint32_t k = lane; k < nleaf / 2; k += 32) {
+            const ulonglong2 v = lf[k];
+            lf[k] = make_ulonglong2(0ull, 0ull);
+            sp[off_leaf + 2 * k] = v.x;
+            sp[off_leaf + 2 * k + 1] = v.y;
+        }
+        __syncwarp();
+        for (int l = (int)L - 1; l >= 0; --l) {
+            const uint32_t o = mqt_level_offset(l), oc = mqt_level_offset(l + 1), cnt = 1u << (2 * l);
+            for (uint32_t k = lane; k < cnt; k += 32)
+                sp[o + k] = sp[oc + 4 * k] + sp[oc + 4 * k + 1] + sp[oc + 4 * k + 2] + sp[oc + 4 * k + 3];
+            __syncwarp();
+        }
+        float* w = t.pyramid + (size_t)c * per;
+        for (uint32_t k = lane; k < per; k += 32) w[k] = fx_to_float(sp[k], t.fx);
+        __syncwarp();
+    }
+}
+
+// Levels 3 to 5: the reduction in registers.  Lane l owns leaves [l P, (l + 1) P) with
+// P = 4^L / 32 (2, 8 or 32), loaded and zeroed as 16-byte vectors; the levels whose nodes span
+// at most P leaves are summed inside the lane, the three levels above them span 2, 8 and 32
+// lanes and come from butterfly shuffles.  The float pyramid is assembled in a per-warp
+// shared buffer and stored with consecutive lanes on consecutive floats.
+template <int L>
+__global__ void __launch_bounds__(32 * kMqtWarps) k_mqt_build_reg(MqtDev t) {
+    constexpr int NLEAF = 1 << (2 * L), P = NLEAF / 32, PER = ((1 << (2 * (L + 1))) - 1) / 3;
+    static_assert(L >= 3 && L <= 5, "levels 3..5");
+    __shared__ float sbuf[kMqtWarps][PER];
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    float* fb = sbuf[warp];
+    const uint32_t nw = gridDim.x * kMqtWarps;
+    for (uint32_t c = blockIdx.x * kMqtWarps + warp; c < t.ncells; c += nw) {
+        ulonglong2* lf = reinterpret_cast<ulonglong2*>(t.leaves + (size_t)c * NLEAF) + lane * (P / 2);
+        unsigned long long v[P];
+#pragma unroll
+        for (int j = 0; j < P / 2; ++j) {
+            const ulonglong2 x = lf[j];
+            v[2 * j] = x.x;
+            v[2 * j + 1] = x.y;
+        }
+#pragma unroll
+        for (int j = 0; j < P / 2; ++j) lf[j] = make_ulonglong2(0ull, 0ull);
+        // the leaf level, then the lane-local levels (each a quarter of the one below)
+#pragma unroll
+        for (int j = 0; j < P; ++j) fb[mqt_level_offset(L) + lane * P + j] = fx_to_float(v[j], t.fx);
+        int lvl = L - 1;
+        int n = P;  // values of the current level held by this lane
+#pragma unroll
+        for (int step = 0; step < 3 && n >= 4; ++step) {
+#pragma unroll
+            for (int j = 0; j < n / 4; ++j) v[j] = v[4 * j] + v[4 * j + 1] + v[4 * j + 2] + v[4 * j + 3];
+            n /= 4;
+#pragma unroll
+            for (int j = 0; j < n; ++j) fb[mqt_level_offset(lvl) + lane * n + j] = fx_to_float(v[j], t.fx);
+            --lvl;
+        }
+        // two values are left in every lane: their sum is the lane's run
+        unsigned long long s = 0;
+#pragma unroll
+        for (int j = 0; j < n; ++j) s += v[j];
+        // nodes spanning 2, 8 and 32 lanes
+        s += __shfl_xor_sync(0xffffffffu, s, 1);
+        if ((lane & 1u) == 0) fb[mqt_level_offset(lvl) + (lane >> 1)] = fx_to_float(s, t.fx);
+        --lvl;
+        s += __shfl_xor_sync(0xffffffffu, s, 2);
+        s += __shfl_xor_sync(0xffffffffu, s, 4);
+        if ((lane & 7u) == 0) fb[mqt_level_offset(lvl) + (lane >> 3)] = fx_to_float(s, t.fx);
+        --lvl;
+        s += __shfl_xor_sync(0xffffffffu, s, 8);
+        s += __shfl_xor_sync(0xffffffffu, s, 16);
+        if (lane == 0) fb[0] = fx_to_float(s, t.fx);
+        __syncwarp();
+        float* w = t.pyramid + (size_t)c * PER;
+        for (uint32_t k = lane; k < (uint32_t)PER; k += 32) w[k] = fb[k];
+        __syncwarp();
     }
 }
 
@@ -137,6 +235,7 @@ struct rtpg_mqt {
 };
 
 static int mqt_smem(uint32_t level) { return int(mqt_level_offset(level + 1) * sizeof(unsigned long long)); }
+static int mqt_smem_warp(uint32_t level) { return kMqtWarps * mqt_smem(level); }
 
 extern "C" {
 
@@ -166,6 +265,8 @@ int rtpg_mqt_create(uint32_t num_cells, uint32_t level, float fraction, int32_t 
         return fail(RTPG_ECUDA, "rtpg_mqt_create: memset failed");
     }
     cudaError_t e = cudaFuncSetAttribute(k_mqt_build, cudaFuncAttributeMaxDynamicSharedMemorySize, mqt_smem(kMqtMaxLevel));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_mqt_build_warp, cudaFuncAttributeMaxDynamicSharedMemorySize, mqt_smem_warp(kMqtWarpLevel));
     if (e != cudaSuccess) {
         delete h;
         return fail(RTPG_ECUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
@@ -206,8 +307,19 @@ int rtpg_mqt_record(rtpg_mqt* h, int64_t n, const uint32_t* cell, const float* d
 // Update + mortonBuildKernel: building leaves -> sampling pyramid, building cleared.
 int rtpg_mqt_update(rtpg_mqt* h, void* stream) {
     if (!h) return fail(RTPG_EINVAL, "rtpg_mqt_update: null handle");
-    const int g = (int)std::min<uint32_t>(h->dev.ncells, kSMs * 8);
-    k_mqt_build<<<g, kMqtBuildBlock, mqt_smem(h->dev.level), as_stream(stream)>>>(h->dev);
+    const int gw = (int)std::min<uint32_t>((h->dev.ncells + kMqtWarps - 1) / kMqtWarps, kSMs * 8);
+    if (h->dev.level == 3) {
+        k_mqt_build_reg<3><<<gw, 32 * kMqtWarps, 0, as_stream(stream)>>>(h->dev);
+    } else if (h->dev.level == 4) {
+        k_mqt_build_reg<4><<<gw, 32 * kMqtWarps, 0, as_stream(stream)>>>(h->dev);
+    } else if (h->dev.level == 5) {
+        k_mqt_build_reg<5><<<gw, 32 * kMqtWarps, 0, as_stream(stream)>>>(h->dev);
+    } else if (h->dev.level <= kMqtWarpLevel) {
+        k_mqt_build_warp<<<gw, 32 * kMqtWarps, mqt_smem_warp(h->dev.level), as_stream(stream)>>>(h->dev);
+    } else {
+        const int g = (int)std::min<uint32_t>(h->dev.ncells, kSMs * 8);
+        k_mqt_build<<<g, kMqtBuildBlock, mqt_smem(h->dev.level), as_stream(stream)>>>(h->dev);
+    }
     RTPG_LAUNCH_CHECK();
     return RTPG_OK;
 }

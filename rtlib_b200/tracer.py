@@ -136,10 +136,6 @@ class Tracer:
              fallback.h if fallback is not None else None, float(fraction), float(mlp_share), float(record_keep),
              stream_ptr(stream))
 
-    def set_record_importance(self, power):
-        """Learned-guide records kept in proportion to throughput luminance^power (0: uniform)."""
-        call("rtpg_tracer_set_record_importance", self.h, int(power))
-
     def set_light_emission(self, rgb):
         """rgb: (num_lights, 3) host array; NEE radiance and material emission of every light."""
         a = np.ascontiguousarray(rgb, np.float32).reshape(-1)

@@ -81,3 +81,36 @@ def spatial_threshold(iteration: int) -> int:
     """Spatial split threshold of the standalone workload: 12000 * sqrt(2^iter), as an
     integer sample count (RTLib compares the stat-weight with a size_t threshold)."""
     return int(12000.0 * np.sqrt(2.0 ** iteration))
+
+
+def surface_points(tri_v: np.ndarray, n: int, seed: int) -> np.ndarray:
+    """n points uniform by area on the triangles tri_v (nt, 9), float32 (n, 3)."""
+    tv = np.asarray(tri_v, np.float64).reshape(-1, 3, 3)
+    area = 0.5 * np.linalg.norm(np.cross(tv[:, 1] - tv[:, 0], tv[:, 2] - tv[:, 0]), axis=1)
+    rng = np.random.Generator(np.random.PCG64(seed))
+    idx = rng.choice(tv.shape[0], size=n, p=area / area.sum())
+    a, b = rng.random(n), rng.random(n)
+    m = a + b > 1.0
+    a[m], b[m] = 1.0 - a[m], 1.0 - b[m]
+    p = tv[idx, 0] + a[:, None] * (tv[idx, 1] - tv[idx, 0]) + b[:, None] * (tv[idx, 2] - tv[idx, 0])
+    return np.ascontiguousarray(p.astype(np.float32))
+
+
+def hashgrid_inputs(n_points: int, n_queries: int, seed: int = 0):
+    """The hash-grid guide workload on the occluded-light scene: n_points surface points to
+    insert (seed), n_queries surface points to look up (seed + 1), and for every query a
+    record direction from a 4-lobe vMF mixture (kappa 50) as canonical (u, v), a lognormal(0, 1)
+    record value and a nonzero Xorshift32 seed for sample+pdf."""
+    from .scenes import occluded_rooms
+    sc = occluded_rooms(64, 36)
+    geom = sc["tri_v"][: sc["geometry_triangles"]]
+    pts = surface_points(geom, n_points, seed)
+    qpos = surface_points(geom, n_queries, seed + 1)
+    rng = np.random.Generator(np.random.PCG64(seed + 2))
+    axes = rng.normal(size=(4, 3))
+    axes /= np.linalg.norm(axes, axis=1, keepdims=True)
+    d = sample_vmf(axes[rng.integers(0, 4, n_queries)], 50.0, rng).astype(np.float32)
+    value = rng.lognormal(0.0, 1.0, n_queries).astype(np.float32)
+    seeds = rng.integers(1, 2**32, n_queries, dtype=np.uint64).astype(np.uint32)
+    return {"points": pts, "queries": qpos, "uv": dir_to_canonical(d), "value": np.ascontiguousarray(value),
+            "seeds": np.ascontiguousarray(seeds)}

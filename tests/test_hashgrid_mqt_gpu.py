@@ -92,10 +92,13 @@ def test_hashgrid_morton_keying(cuda, oracle):
         assert oracle.L.or_morton3(int(c[i, 0]), int(c[i, 1]), int(c[i, 2])) + 1 == keys[i]
 
 
-def test_mqt_vs_oracle(cuda, oracle):
+@pytest.mark.parametrize("level", [1, 2, 3, 4, 5, 6, 7])
+def test_mqt_vs_oracle(cuda, oracle, level):
+    """Record, pyramid build (each level has its own build kernel shape), sample and pdf bit
+    for bit against the oracle."""
     import torch
     from rtlib_b200.hashgrid import MortonQuadTrees
-    level, ncells, bits = 6, 1024, 24
+    ncells, bits = 1024, 24
     rng = np.random.default_rng(8)
     n = 1 << 18
     rec = W.sdtree_records(n, 4)
