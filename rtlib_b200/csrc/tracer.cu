@@ -63,13 +63,18 @@ struct TracerDev {
     float3 *org, *dir, *thr, *col;
     uint32_t *rng, *depth, *hflags;
     uint32_t* queue[2];
-    uint32_t* qcount;  // [0], [1]
+    // queue lengths, three in rotation: bounce b reads [b % 3], appends to [(b + 1) % 3] and
+    // zeroes [(b + 2) % 3], which no block of that launch touches
+    uint32_t* qcount;
     // trace vertices, [kTV][npath]
     float3 *v_pos, *v_dir, *v_thr;
     float3* b_rad;  // radiance of bounce k of every path, [max_depth][npath] (recording only)
     float *v_wopdf, *v_cos;
     uint8_t* v_flags;  // bit0 valid (a DTree exists / a grid cell was found), bit1 delta
     uint32_t* v_cell;  // hash-grid slot (grid guide) or DTree (SD-tree guide) of the vertex
+    // where the commit adds the vertex's radiance: the building-quadtree quadrant (SD-tree) or
+    // the Morton leaf code inside the cell's tree (grid), found while the direction is at hand
+    uint32_t* v_slot;
     uint32_t* seeds;
     double* accum;  // 3 per pixel
     SDTreeDev tree;
@@ -89,7 +94,6 @@ struct TracerDev {
     // learned guide: hits found ahead of shading, the mixture of every path, record appends
     MlpView ml;
     float mlp_fraction, mlp_keep, mlp_share;
-    uint32_t mlp_keep_pow;  // record keep probability scaled by throughput luminance^pow (0: uniform)
     uint32_t* hit_prim;
     float4* hit_tuv;
     __half* lobes;  // 40 per path: 8 x (mu xyz, kappa, weight)
@@ -98,7 +102,10 @@ struct TracerDev {
 
 // ------------------------------------------------------------------ raygen (SimpleGuide.cu:48-81)
 __global__ void __launch_bounds__(kTB) k_raygen(TracerDev T) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) T.qcount[0] = T.npath;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        T.qcount[0] = T.npath;  // bounce 0 reads [0], appends to [1], zeroes [2]
+        T.qcount[1] = 0;
+    }
     for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < T.npath; p += gridDim.x * blockDim.x) {
         const uint32_t x = p % T.width, y = p / T.width;
         uint32_t rng = T.seeds[p];
@@ -226,6 +233,8 @@ __device__ __forceinline__ bool bounce_path(const TracerDev& T, uint32_t p, bool
     uint32_t flags = 0;
     uint32_t dt = 0;
     uint32_t cell = 0xffffffffu;  // hash-grid slot of this vertex (SimpleGuide2.cu: curGridIndex)
+    float2 cdir = make_float2(0.f, 0.f);  // dir_to_canonical(direction), once the guide formed it
+    bool have_c = false;
     // the learned guide may carry the SD-tree as its fallback (T.tree set, mlp_share < 1)
     const bool mlp_mix = use_mlp && T.tree.snode != nullptr;
     if (use_tree || mlp_mix) dt = stree_lookup(T.tree.snode, T.tree.mn, T.tree.mx, position.x, position.y, position.z);
@@ -282,6 +291,8 @@ __device__ __forceinline__ bool bounce_path(const TracerDev& T, uint32_t p, bool
                 bsdf_pdf = sel * cp2 + (1.0f - sel) * pp2;
             }
             const float2 c = dir_to_canonical(direction.x, direction.y, direction.z);
+            cdir = c;
+            have_c = true;
             const float dtree_pdf = fmaxf(dtree_pdf_in(T.tree.s_nodes, soff, guided, sq, c.x, c.y), 0.0f);
             wo_pdf = (1.0f - T.tree.fraction) * bsdf_pdf + T.tree.fraction * dtree_pdf;
         } else if (use_mlp && build) {
@@ -327,6 +338,8 @@ __device__ __forceinline__ bool bounce_path(const TracerDev& T, uint32_t p, bool
             float q = vmf_mixture_pdf(Lb, direction);
             if (mlp_mix) {
                 const float2 c = dir_to_canonical(direction.x, direction.y, direction.z);
+                cdir = c;
+                have_c = true;
                 const float qt = fmaxf(dtree_pdf_in(T.tree.s_nodes, soff, tguided, sq, c.x, c.y), 0.0f);
                 q = T.mlp_share * q + (1.0f - T.mlp_share) * qt;
             }
@@ -346,6 +359,8 @@ __device__ __forceinline__ bool bounce_path(const TracerDev& T, uint32_t p, bool
                 bsdf_pdf = sel * cp2 + (1.0f - sel) * pp2;
             } else {
                 const float2 c = dir_to_canonical(direction.x, direction.y, direction.z);
+                cdir = c;
+                have_c = true;
                 const float tp = mqt_pdf(T.mqt, prv_cell, c.x, c.y);
                 dtree_pdf = fmaxf((float)((double)(tp * 0.25f) * kInvPiD), 0.0f);
             }
@@ -453,8 +468,10 @@ __device__ __forceinline__ bool bounce_path(const TracerDev& T, uint32_t p, bool
     T.hflags[p] = flags;
     T.rng[p] = rng;
     if (recording && d < kTV) {
-        if (use_mlp) T.v_pos[vi] = position;
-        T.v_dir[vi] = direction;
+        if (use_mlp) {
+            T.v_pos[vi] = position;
+            T.v_dir[vi] = direction;
+        }
         T.v_thr[vi] = cur_thr;
         T.v_wopdf[vi] = wo_pdf;
         T.v_cos[vi] = cosine;
@@ -466,6 +483,13 @@ __device__ __forceinline__ bool bounce_path(const TracerDev& T, uint32_t p, bool
         T.v_flags[vi] = (uint8_t)((has_guide && ok_b ? 1u : 0u) | ((flags & HF_DELTA) ? 2u : 0u));
         if (use_grid) T.v_cell[vi] = cell;
         if (use_tree || mlp_mix) T.v_cell[vi] = dt;  // the vertex's DTree, found once here for the commit
+        if ((use_tree || mlp_mix || use_grid) && !(flags & HF_DELTA)) {
+            // canonical of the direction exactly as the commit would form it; the building
+            // tree's topology does not change within a pass
+            const float2 cr = have_c ? cdir : dir_to_canonical(direction.x, direction.y, direction.z);
+            T.v_slot[vi] = use_grid ? mqt_leaf_code(T.mqt.level, cr.x, cr.y)
+                                    : dtree_record_slot(T.tree.b_child, T.tree.b_off[dt], cr.x, cr.y);
+        }
         if (use_mlp) {
             T.v_nrm[vi] = fn;
             T.v_wo[vi] = f3(-in_dir.x, -in_dir.y, -in_dir.z);
@@ -538,8 +562,9 @@ __host__ __device__ constexpr int guide_of(uint32_t flags) {
 
 // learned guide, stage 1 of the first bounce: closest hits of the camera rays (later bounces
 // find theirs traced at the end of the previous k_bounce)
-__global__ void __launch_bounds__(kTB) k_hit(TracerDev T, int in) {
-    const uint32_t n = T.qcount[in];
+__global__ void __launch_bounds__(kTB) k_hit(TracerDev T, uint32_t bounce) {
+    const int in = int(bounce & 1);
+    const uint32_t n = T.qcount[bounce % 3];
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
         const uint32_t p = T.queue[in][q];
         const float3 o = T.org[p], d = T.dir[p];
@@ -551,7 +576,8 @@ __global__ void __launch_bounds__(kTB) k_hit(TracerDev T, int in) {
 
 // learned guide, stage 2: the mixture of every queued path that hit a Phong surface, 128
 // paths per tile on the tensor cores (features of path q in row q of the tile)
-__global__ void __launch_bounds__(kMlpThreads) k_mlp_lobes(TracerDev T, int in) {
+__global__ void __launch_bounds__(kMlpThreads) k_mlp_lobes(TracerDev T, uint32_t bounce) {
+    const int in = int(bounce & 1);
     extern __shared__ __align__(128) uint8_t sm[];
     __nv_bfloat16* ws = reinterpret_cast<__nv_bfloat16*>(sm);
     __nv_bfloat16* x0 = reinterpret_cast<__nv_bfloat16*>(sm + kSmemW);
@@ -567,7 +593,7 @@ __global__ void __launch_bounds__(kMlpThreads) k_mlp_lobes(TracerDev T, int in) 
     const uint32_t tmem = *tslot, sw = smem_u32(ws);
     uint32_t phase = 0;
     bool ok = true;
-    const uint32_t n = T.qcount[in];
+    const uint32_t n = T.qcount[bounce % 3];
     for (uint32_t base = blockIdx.x * kMlpTile; base < n; base += gridDim.x * kMlpTile) {
         const uint32_t q = base + t;
         bool live = false;
@@ -621,14 +647,17 @@ __global__ void __launch_bounds__(kMlpThreads) k_mlp_lobes(TracerDev T, int in) 
 }
 
 template <int G>
-__global__ void __launch_bounds__(kTB, 8) k_bounce(TracerDev T, int in) {
-    const uint32_t n = T.qcount[in];
+__global__ void __launch_bounds__(kTB, 8) k_bounce(TracerDev T, uint32_t bounce) {
+    const int in = int(bounce & 1);
+    uint32_t* const next_count = T.qcount + (bounce + 1) % 3;
+    const uint32_t n = T.qcount[bounce % 3];
     if (blockIdx.x == 0 && threadIdx.x == 0) {
-        T.qcount[in ^ 1] = 0;
+        T.qcount[(bounce + 2) % 3] = 0;  // the next bounce's output
         atomicAdd(T.counters, (unsigned long long)n);
     }
     const bool build = (T.flags & RTPG_TRACE_FLAG_BUILD) != 0;
     const bool recording = (G == kGuideTree || G == kGuideGrid || G == kGuideMlp) && !(T.flags & RTPG_TRACE_FLAG_FINAL);
+    const uint32_t lane = threadIdx.x & 31u;
     for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
         const uint32_t q = base + threadIdx.x;
         bool keep = false, shadow = false;
@@ -642,9 +671,8 @@ __global__ void __launch_bounds__(kTB, 8) k_bounce(TracerDev T, int in) {
         // warp-aggregated append to the next queue
         const unsigned m = __ballot_sync(0xffffffffu, keep);
         if (m) {
-            const int lane = threadIdx.x & 31;
             uint32_t base_q = 0;
-            if (lane == __ffs(m) - 1) base_q = atomicAdd(T.qcount + (in ^ 1), (uint32_t)__popc(m));
+            if (lane == __ffs(m) - 1) base_q = atomicAdd(next_count, (uint32_t)__popc(m));
             base_q = __shfl_sync(0xffffffffu, base_q, __ffs(m) - 1);
             if (keep) T.queue[in ^ 1][base_q + __popc(m & ((1u << lane) - 1u))] = p;
         }
@@ -709,23 +737,15 @@ __global__ void __launch_bounds__(kTB) k_finish(TracerDev T) {
                     if (th.z * wo > 1e-4f) lr.z = rad.z / th.z;
                     lr = lr * fabsf(T.v_cos[vi]);
                     const float lavg = (lr.x + lr.y + lr.z) / 3.0f;
-                    const float3 dr = T.v_dir[vi];
                     const float irr = __fdiv_rn(lavg, wo);
                     if (G == kGuideMlp) {
                         // a training record of the learned guide: the SD-tree's record with the
                         // vertex's normal and outgoing direction, kept with probability mlp_keep
-                        // optionally in proportion to the vertex's weight in the pixel estimate
-                        // (its throughput times its incident radiance), so that the network
-                        // learns most where the image depends on it most
-                        float keep = T.mlp_keep;
-                        if (T.mlp_keep_pow) {
-                            const float lt = fminf(1.0f, (th.x + th.y + th.z) * (1.0f / 3.0f));
-                            keep *= T.mlp_keep_pow == 1 ? lt : lt * lt;
-                        }
-                        if (isfinite(irr) && irr > 0.0f && to_uniform_float(pcg1d(T.rng[p] ^ (i * 0x9E3779B9u))) < keep) {
+                        if (isfinite(irr) && irr > 0.0f &&
+                            to_uniform_float(pcg1d(T.rng[p] ^ (i * 0x9E3779B9u))) < T.mlp_keep) {
                             const uint32_t idx = atomicAdd(T.ml.r_count, 1u);
                             if (idx < T.ml.capacity) {
-                                const float3 ps = T.v_pos[vi], nm = T.v_nrm[vi], wo = T.v_wo[vi];
+                                const float3 ps = T.v_pos[vi], nm = T.v_nrm[vi], wo = T.v_wo[vi], dr = T.v_dir[vi];
                                 float* rp = T.ml.r_pos + 3 * size_t(idx);
                                 float* rn = T.ml.r_nrm + 3 * size_t(idx);
                                 float* ro = T.ml.r_wo + 3 * size_t(idx);
@@ -744,8 +764,7 @@ __global__ void __launch_bounds__(kTB) k_finish(TracerDev T) {
                         // MortonQuadTreeWrapperT::Record: leaf of the cell's building quadtree
                         if (isfinite(irr) && irr > 0.0f) {
                             const uint32_t cell = T.v_cell[vi];
-                            const float2 c = dir_to_canonical(dr.x, dr.y, dr.z);
-                            k_s = ((unsigned long long)cell << (2 * T.mqt.level)) + mqt_leaf_code(T.mqt.level, c.x, c.y);
+                            k_s = ((unsigned long long)cell << (2 * T.mqt.level)) + T.v_slot[vi];
                             v_s = to_fx(irr, T.mqt.fx, T.mqt.status);
                         }
                     } else {
@@ -753,8 +772,7 @@ __global__ void __launch_bounds__(kTB) k_finish(TracerDev T) {
                         k_w = dt;
                         v_w = to_fx(1.0f, T.tree.fx, T.tree.status);
                         if (isfinite(irr) && irr > 0.0f) {
-                            const float2 c = dir_to_canonical(dr.x, dr.y, dr.z);
-                            k_s = dtree_record_slot(T.tree.b_child, T.tree.b_off[dt], c.x, c.y);
+                            k_s = T.v_slot[vi];
                             v_s = to_fx(irr, T.tree.fx, T.tree.status);
                         }
                     }
@@ -840,17 +858,16 @@ struct rtpg_tracer {
 };
 
 static void launch_bounce(const TracerDev& T, int g, cudaStream_t st, uint32_t b) {
-    const int in = int(b & 1);
     if (guide_of(T.flags) == kGuideMlp) {
-        if (b == 0) k_hit<<<g, kTB, 0, st>>>(T, in);
-        if (T.flags & RTPG_TRACE_FLAG_BUILD) k_mlp_lobes<<<kSMs * 4, kMlpThreads, kSmemEval, st>>>(T, in);
-        k_bounce<kGuideMlp><<<g, kTB, 0, st>>>(T, in);
+        if (b == 0) k_hit<<<g, kTB, 0, st>>>(T, b);
+        if (T.flags & RTPG_TRACE_FLAG_BUILD) k_mlp_lobes<<<kSMs * 4, kMlpThreads, kSmemEval, st>>>(T, b);
+        k_bounce<kGuideMlp><<<g, kTB, 0, st>>>(T, b);
         return;
     }
     switch (guide_of(T.flags)) {
-        case kGuideTree: k_bounce<kGuideTree><<<g, kTB, 0, st>>>(T, in); break;
-        case kGuideGrid: k_bounce<kGuideGrid><<<g, kTB, 0, st>>>(T, in); break;
-        default: k_bounce<kGuideNone><<<g, kTB, 0, st>>>(T, in); break;
+        case kGuideTree: k_bounce<kGuideTree><<<g, kTB, 0, st>>>(T, b); break;
+        case kGuideGrid: k_bounce<kGuideGrid><<<g, kTB, 0, st>>>(T, b); break;
+        default: k_bounce<kGuideNone><<<g, kTB, 0, st>>>(T, b); break;
     }
 }
 static void launch_finish(const TracerDev& T, int g, cudaStream_t st) {
@@ -949,10 +966,10 @@ int rtpg_tracer_create(rtpg_scene* scene, const float* tri_vertices, const uint3
         (r = h->alloc(&T.dir, P)) || (r = h->alloc(&T.thr, P)) || (r = h->alloc(&T.col, P)) ||
         (r = h->alloc(&T.rng, P)) || (r = h->alloc(&T.depth, P)) ||
         (r = h->alloc(&T.hflags, P)) || (r = h->alloc(&T.queue[0], P)) ||
-        (r = h->alloc(&T.queue[1], P)) || (r = h->alloc(&T.qcount, 2)) ||
+        (r = h->alloc(&T.queue[1], P)) || (r = h->alloc(&T.qcount, 3)) ||
         (r = h->alloc(&T.v_dir, P * kTV)) || (r = h->alloc(&T.v_thr, P * kTV)) || (r = h->alloc(&T.b_rad, P * std::max<uint32_t>(D.max_depth, 1))) ||
         (r = h->alloc(&T.v_wopdf, P * kTV)) ||
-        (r = h->alloc(&T.v_cos, P * kTV)) || (r = h->alloc(&T.v_flags, P * kTV)) || (r = h->alloc(&T.v_cell, P * kTV)) || (r = h->alloc(&T.seeds, P)) ||
+        (r = h->alloc(&T.v_cos, P * kTV)) || (r = h->alloc(&T.v_flags, P * kTV)) || (r = h->alloc(&T.v_cell, P * kTV)) || (r = h->alloc(&T.v_slot, P * kTV)) || (r = h->alloc(&T.seeds, P)) ||
         (r = h->alloc(&T.accum, 3 * P)) || (r = h->alloc(&T.status, 1)) || (r = h->alloc(&T.counters, 2)) || (r = h->alloc(&h->d_tex, 64)) ||
         (r = h->alloc(&h->d_tex_wh, 64))) {
         delete h;
@@ -1213,15 +1230,6 @@ int rtpg_tracer_render_mlp(rtpg_tracer* h, uint32_t spp, uint32_t flags, rtpg_ml
     return render_waves(h, spp, flags, as_stream(stream));
 }
 
-// Learned-guide training records: keep probability of a committed vertex scaled by the
-// luminance of its path throughput (clamped to 1) raised to `power` (0: every vertex alike).
-int rtpg_tracer_set_record_importance(rtpg_tracer* h, uint32_t power) {
-    if (!h) return fail(RTPG_EINVAL, "rtpg_tracer_set_record_importance: null handle");
-    if (power > 2) return fail(RTPG_EINVAL, "rtpg_tracer_set_record_importance: power must be 0, 1 or 2");
-    h->dev.mlp_keep_pow = power;
-    return RTPG_OK;
-}
-
 // Mean radiance per pixel (accumulation / samples), RGB float, row-major, y = 0 first.
 int rtpg_tracer_image(rtpg_tracer* h, float* out_rgb, void* stream) {
     if (!h || !out_rgb) return fail(RTPG_EINVAL, "rtpg_tracer_image: null argument");
@@ -1361,9 +1369,9 @@ int rtpg_tracer_render_adjoint(rtpg_tracer* h, uint32_t spp, uint32_t flags, con
     const int g = kSMs * 8;
     for (uint32_t s = 0; s < spp; ++s) {
         k_raygen<<<g, kTB, 0, st>>>(A);
-        for (uint32_t b = 0; b < A.max_depth; ++b) k_bounce<kGuideNone><<<g, kTB, 0, st>>>(A, int(b & 1));
+        for (uint32_t b = 0; b < A.max_depth; ++b) k_bounce<kGuideNone><<<g, kTB, 0, st>>>(A, b);
         k_raygen<<<g, kTB, 0, st>>>(B);
-        for (uint32_t b = 0; b < B.max_depth; ++b) k_bounce<kAdjoint><<<g, kTB, 0, st>>>(B, int(b & 1));
+        for (uint32_t b = 0; b < B.max_depth; ++b) k_bounce<kAdjoint><<<g, kTB, 0, st>>>(B, b);
         k_seed_store<<<g, kTB, 0, st>>>(B);
     }
     RTPG_LAUNCH_CHECK();
