@@ -28,6 +28,7 @@ int fail(int code, const char* fmt, ...) {
 // ---------------------------------------------------------------- scan
 __global__ void __launch_bounds__(kScanBlock) scan_tile_sums(const uint32_t* __restrict__ in, const uint32_t* n_dev,
                                                             uint32_t* __restrict__ partials) {
+    grid_dependency_wait();
     const uint32_t n = *n_dev;
     const uint32_t base = blockIdx.x * kScanTile;
     if (base >= n) return;
@@ -45,6 +46,7 @@ __global__ void __launch_bounds__(kScanBlock) scan_tile_sums(const uint32_t* __r
 }
 
 __global__ void __launch_bounds__(kScanBlock) scan_partials(uint32_t* partials, const uint32_t* n_dev, uint32_t* total_out) {
+    grid_dependency_wait();
     __shared__ uint32_t ws[kScanBlock / 32];
     const uint32_t n = *n_dev;
     const uint32_t tiles = (n + kScanTile - 1) / kScanTile;
@@ -62,6 +64,7 @@ __global__ void __launch_bounds__(kScanBlock) scan_partials(uint32_t* partials, 
 
 __global__ void __launch_bounds__(kScanBlock) scan_tiles(const uint32_t* __restrict__ in, uint32_t* __restrict__ out,
                                                         const uint32_t* n_dev, const uint32_t* __restrict__ partials) {
+    grid_dependency_wait();
     __shared__ uint32_t ws[kScanBlock / 32];
     const uint32_t n = *n_dev;
     const uint32_t base = blockIdx.x * kScanTile;
@@ -88,10 +91,10 @@ int scan_exclusive_u32(const uint32_t* in, uint32_t* out, const uint32_t* n_dev,
                        uint32_t* total_out, cudaStream_t st) {
     const uint32_t tiles = (cap + kScanTile - 1) / kScanTile;
     const uint32_t g = tiles ? tiles : 1;
-    scan_tile_sums<<<g, kScanBlock, 0, st>>>(in, n_dev, partials);
-    scan_partials<<<1, kScanBlock, 0, st>>>(partials, n_dev, total_out);
-    scan_tiles<<<g, kScanBlock, 0, st>>>(in, out, n_dev, partials);
-    RTPG_LAUNCH_CHECK();
+    // launched as dependent grids: each may be scheduled while its predecessor finishes
+    RTPG_CUDA(launch_dependent(scan_tile_sums, g, kScanBlock, 0, st, in, n_dev, partials));
+    RTPG_CUDA(launch_dependent(scan_partials, 1, kScanBlock, 0, st, partials, n_dev, total_out));
+    RTPG_CUDA(launch_dependent(scan_tiles, g, kScanBlock, 0, st, in, out, n_dev, partials));
     return RTPG_OK;
 }
 

@@ -156,4 +156,27 @@ int scan_exclusive_u32(const uint32_t* in, uint32_t* out, const uint32_t* n_dev,
                        uint32_t* total_out, cudaStream_t st);
 inline size_t scan_partials_words(uint32_t cap) { return size_t(cap + kScanTile - 1) / kScanTile + 1; }
 
+// Programmatic dependent launch.  A kernel started with launch_dependent() may be scheduled
+// while the kernel before it in the stream is still running, which hides the launch gap of
+// chains of short kernels; it must call grid_dependency_wait() before it touches memory, which
+// returns once the preceding grid has completed and its writes are visible.  For a kernel
+// launched the ordinary way the wait returns at once.
+__device__ __forceinline__ void grid_dependency_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_dependent(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                                    Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+
 }  // namespace rtpg

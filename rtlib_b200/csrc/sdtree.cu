@@ -112,6 +112,13 @@ __global__ void __launch_bounds__(kRecordBlock) k_record(SDTreeDev t, int64_t n,
     }
 }
 
+// zeroes n 64-bit counters (a kernel rather than a memset so the refine chain stays a chain of
+// dependent launches)
+__global__ void k_zero_u64(unsigned long long* p, int n) {
+    grid_dependency_wait();
+    if (threadIdx.x < n) p[threadIdx.x] = 0ull;
+}
+
 // ------------------------------------------------------------------ build
 // One CTA per DTree (grid-stride over trees).  Levels of the breadth-first building tree are
 // processed deepest first: an interior quadrant's fixed-point sum is the exact sum of its
@@ -119,6 +126,7 @@ __global__ void __launch_bounds__(kRecordBlock) k_record(SDTreeDev t, int64_t n,
 // (DTreeNodeT::GetArea, PG.h:342-355, same float order), the root sum (RTDTreeT::Build,
 // PG.h:948-957) and the sampling copy (RTDTreeWrapperT::Build, PG.h:1086-1090).
 __global__ void __launch_bounds__(kTreeBlock) k_build(SDTreeDev t) {
+    grid_dependency_wait();
     const uint32_t ndt = t.counts[1];
     for (uint32_t d = blockIdx.x; d < ndt; d += gridDim.x) {
         const uint32_t off = t.b_off[d];
@@ -183,6 +191,7 @@ __global__ void __launch_bounds__(kTreeBlock) k_build(SDTreeDev t) {
 // of the building and sampling tree of every STree node; interior nodes hold default
 // one-node trees (SubDivide resets the parent's wrapper, PG.h:1246).
 __global__ void k_footprint(SDTreeDev t, unsigned long long* fp) {
+    grid_dependency_wait();
     const uint32_t n = t.counts[0];
     unsigned long long s = 0;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -206,6 +215,7 @@ __global__ void k_footprint(SDTreeDev t, unsigned long long* fp) {
 // step checks against the capacities (the 32-bit scan totals could wrap).
 __global__ void k_refine_count(SDTreeDev t, float thf, int32_t max_mb, uint32_t kmax, unsigned long long* tot64,
                                uint32_t* cnt_s, uint32_t* cnt_d, uint32_t* ksplit) {
+    grid_dependency_wait();
     const uint32_t n = t.counts[0];
     const bool allowed = max_mb < 0 || (tot64[0] / 1000000ull) < (unsigned long long)max_mb;
     unsigned long long ss = 0, sd = 0;
@@ -254,6 +264,7 @@ __device__ __forceinline__ uint32_t owner_of(const uint32_t* off, const uint32_t
 }
 __global__ void k_refine_apply(SDTreeDev t, const uint32_t* ksplit, const uint32_t* off_s, const uint32_t* cnt_s,
                                const uint32_t* off_d, const uint32_t* cnt_d, const unsigned long long* tot64) {
+    grid_dependency_wait();
     const uint32_t n = t.counts[0], ndt = t.counts[1];
     if (n + tot64[1] > t.cap_snodes || ndt + tot64[2] > t.cap_dtrees) {
         if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(t.status, RTPG_STATUS_STREE_CAPACITY);
@@ -298,12 +309,14 @@ __global__ void k_refine_apply(SDTreeDev t, const uint32_t* ksplit, const uint32
 // the split leaves become interior nodes; runs after k_refine_apply read snode[i]
 __global__ void k_refine_link(SDTreeDev t, const uint32_t* ksplit, const uint32_t* off_s,
                               const unsigned long long* tot64) {
+    grid_dependency_wait();
     const uint32_t n = t.counts[0], ndt = t.counts[1];
     if (n + tot64[1] > t.cap_snodes || ndt + tot64[2] > t.cap_dtrees) return;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
         if (ksplit[i]) t.snode[i] = n + off_s[i];
 }
 __global__ void k_refine_commit(SDTreeDev t, const unsigned long long* tot64) {
+    grid_dependency_wait();
     const uint32_t n = t.counts[0], ndt = t.counts[1];
     if (n + tot64[1] > t.cap_snodes || ndt + tot64[2] > t.cap_dtrees) return;
     t.counts[0] = n + (uint32_t)tot64[1];
@@ -321,6 +334,7 @@ __global__ void k_refine_commit(SDTreeDev t, const unsigned long long* tot64) {
 template <bool WRITE>
 __global__ void __launch_bounds__(kTreeBlock) k_reset(SDTreeDev t, float th, uint32_t* node_count,
                                                       const uint32_t* node_off, unsigned long long* node_total) {
+    grid_dependency_wait();
     extern __shared__ uint32_t sm[];
     uint32_t* src = sm;                                              // kDTreeNodeCap
     float* vsum = reinterpret_cast<float*>(sm + kDTreeNodeCap);      // kDTreeNodeCap
@@ -427,6 +441,7 @@ __global__ void __launch_bounds__(kTreeBlock) k_reset(SDTreeDev t, float th, uin
     }
 }
 __global__ void k_reset_commit(SDTreeDev t, const unsigned long long* node_total) {
+    grid_dependency_wait();
     if (*node_total <= t.cap_nodes) t.counts[2] = (uint32_t)*node_total;
 }
 
@@ -642,8 +657,7 @@ int rtpg_sdtree_record(rtpg_sdtree* h, int64_t n, const float* pos, const float*
 
 int rtpg_sdtree_build(rtpg_sdtree* h, void* stream) {
     if (!h) return fail(RTPG_EINVAL, "rtpg_sdtree_build: null handle");
-    k_build<<<kSMs * 4, kTreeBlock, 0, as_stream(stream)>>>(h->dev);
-    RTPG_LAUNCH_CHECK();
+    RTPG_CUDA(launch_dependent(k_build, kSMs * 4, kTreeBlock, 0, as_stream(stream), h->dev));
     return RTPG_OK;
 }
 
@@ -652,32 +666,29 @@ int rtpg_sdtree_refine(rtpg_sdtree* h, uint64_t spatial_threshold, int32_t max_m
     cudaStream_t st = as_stream(stream);
     SDTreeDev& t = h->dev;
     // spatial part; fp[0] footprint, fp[1..2] new STree nodes / DTrees, fp[3] quadtree nodes
-    RTPG_CUDA(cudaMemsetAsync(h->fp, 0, 4 * sizeof(unsigned long long), st));
-    if (max_mb >= 0) {
-        k_footprint<<<kSMs * 2, 256, 0, st>>>(t, h->fp);
-        RTPG_LAUNCH_CHECK();
-    }
+    // every kernel of the refine is a dependent launch (it waits for its predecessor in-kernel)
+    RTPG_CUDA(launch_dependent(k_zero_u64, 1, 32, 0, st, h->fp, 4));
+    if (max_mb >= 0) RTPG_CUDA(launch_dependent(k_footprint, kSMs * 2, 256, 0, st, t, h->fp));
     const float thf = (float)spatial_threshold;  // the size_t threshold as the float compare sees it
     uint32_t kmax = 0;
     while (kmax < 24 && (2ull << (kmax + 1)) <= t.cap_snodes) ++kmax;
-    k_refine_count<<<grid_for(t.cap_snodes, 256, 8), 256, 0, st>>>(t, thf, max_mb, kmax, h->fp, h->cnt_s, h->cnt_d,
-                                                                   h->ksplit);
-    RTPG_LAUNCH_CHECK();
+    RTPG_CUDA(launch_dependent(k_refine_count, grid_for(t.cap_snodes, 256, 8), 256, 0, st, t, thf, max_mb, kmax, h->fp,
+                               h->cnt_s, h->cnt_d, h->ksplit));
     int r;
     if ((r = scan_exclusive_u32(h->cnt_s, h->off_s, t.counts + 0, t.cap_snodes, h->partials, h->totals + 0, st))) return r;
     if ((r = scan_exclusive_u32(h->cnt_d, h->off_d, t.counts + 0, t.cap_snodes, h->partials, h->totals + 1, st))) return r;
-    k_refine_apply<<<kSMs * 4, 256, 0, st>>>(t, h->ksplit, h->off_s, h->cnt_s, h->off_d, h->cnt_d, h->fp);
-    k_refine_link<<<grid_for(t.cap_snodes, 256, 4), 256, 0, st>>>(t, h->ksplit, h->off_s, h->fp);
-    k_refine_commit<<<1, 1, 0, st>>>(t, h->fp);
-    RTPG_LAUNCH_CHECK();
+    RTPG_CUDA(launch_dependent(k_refine_apply, kSMs * 4, 256, 0, st, t, h->ksplit, h->off_s, h->cnt_s, h->off_d,
+                               h->cnt_d, h->fp));
+    RTPG_CUDA(launch_dependent(k_refine_link, grid_for(t.cap_snodes, 256, 4), 256, 0, st, t, h->ksplit, h->off_s, h->fp));
+    RTPG_CUDA(launch_dependent(k_refine_commit, 1, 1, 0, st, t, h->fp));
     // quadtree reset of every leaf
-    k_reset<false><<<kSMs, kTreeBlock, reset_smem(), st>>>(t, dtree_subdiv_th, h->node_cnt, nullptr, h->fp + 3);
-    RTPG_LAUNCH_CHECK();
+    RTPG_CUDA(launch_dependent(k_reset<false>, kSMs, kTreeBlock, reset_smem(), st, t, dtree_subdiv_th, h->node_cnt,
+                               (const uint32_t*)nullptr, h->fp + 3));
     if ((r = scan_exclusive_u32(h->node_cnt, h->node_off, t.counts + 1, t.cap_dtrees, h->partials, h->totals + 2, st)))
         return r;
-    k_reset<true><<<kSMs, kTreeBlock, reset_smem(), st>>>(t, dtree_subdiv_th, nullptr, h->node_off, h->fp + 3);
-    k_reset_commit<<<1, 1, 0, st>>>(t, h->fp + 3);
-    RTPG_LAUNCH_CHECK();
+    RTPG_CUDA(launch_dependent(k_reset<true>, kSMs, kTreeBlock, reset_smem(), st, t, dtree_subdiv_th, (uint32_t*)nullptr,
+                               (const uint32_t*)h->node_off, h->fp + 3));
+    RTPG_CUDA(launch_dependent(k_reset_commit, 1, 1, 0, st, t, (const unsigned long long*)(h->fp + 3)));
     return RTPG_OK;
 }
 
