@@ -102,6 +102,7 @@ struct TracerDev {
 
 // ------------------------------------------------------------------ raygen (SimpleGuide.cu:48-81)
 __global__ void __launch_bounds__(kTB) k_raygen(TracerDev T) {
+    grid_dependency_wait();  // the wave's kernels are dependent launches (see launch_wave)
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         T.qcount[0] = T.npath;  // bounce 0 reads [0], appends to [1], zeroes [2]
         T.qcount[1] = 0;
@@ -563,6 +564,7 @@ __host__ __device__ constexpr int guide_of(uint32_t flags) {
 // learned guide, stage 1 of the first bounce: closest hits of the camera rays (later bounces
 // find theirs traced at the end of the previous k_bounce)
 __global__ void __launch_bounds__(kTB) k_hit(TracerDev T, uint32_t bounce) {
+    grid_dependency_wait();
     const int in = int(bounce & 1);
     const uint32_t n = T.qcount[bounce % 3];
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
@@ -577,6 +579,7 @@ __global__ void __launch_bounds__(kTB) k_hit(TracerDev T, uint32_t bounce) {
 // learned guide, stage 2: the mixture of every queued path that hit a Phong surface, 128
 // paths per tile on the tensor cores (features of path q in row q of the tile)
 __global__ void __launch_bounds__(kMlpThreads) k_mlp_lobes(TracerDev T, uint32_t bounce) {
+    grid_dependency_wait();
     const int in = int(bounce & 1);
     extern __shared__ __align__(128) uint8_t sm[];
     __nv_bfloat16* ws = reinterpret_cast<__nv_bfloat16*>(sm);
@@ -648,6 +651,7 @@ __global__ void __launch_bounds__(kMlpThreads) k_mlp_lobes(TracerDev T, uint32_t
 
 template <int G>
 __global__ void __launch_bounds__(kTB, 8) k_bounce(TracerDev T, uint32_t bounce) {
+    grid_dependency_wait();
     const int in = int(bounce & 1);
     uint32_t* const next_count = T.qcount + (bounce + 1) % 3;
     const uint32_t n = T.qcount[bounce % 3];
@@ -685,6 +689,7 @@ __global__ void __launch_bounds__(kTB, 8) k_bounce(TracerDev T, uint32_t bounce)
 // MortonTraceVertexT::Commit for the grid guide).
 template <int G>
 __global__ void __launch_bounds__(kTB) k_finish(TracerDev T) {
+    grid_dependency_wait();
     constexpr bool use_grid = G == kGuideGrid;
     // the learned guide with the SD-tree as fallback commits to both
     const bool tree_too = G == kGuideMlp && T.tree.snode != nullptr;
@@ -857,25 +862,28 @@ struct rtpg_tracer {
     }
 };
 
+// The kernels of a wave are dependent launches: each may be scheduled while its predecessor
+// drains and waits for it in-kernel (grid_dependency_wait), which hides the launch gaps of
+// the bounce chain.  Launch errors surface at graph instantiation or the next checked call.
 static void launch_bounce(const TracerDev& T, int g, cudaStream_t st, uint32_t b) {
     if (guide_of(T.flags) == kGuideMlp) {
-        if (b == 0) k_hit<<<g, kTB, 0, st>>>(T, b);
-        if (T.flags & RTPG_TRACE_FLAG_BUILD) k_mlp_lobes<<<kSMs * 4, kMlpThreads, kSmemEval, st>>>(T, b);
-        k_bounce<kGuideMlp><<<g, kTB, 0, st>>>(T, b);
+        if (b == 0) (void)launch_dependent(k_hit, g, kTB, 0, st, T, b);
+        if (T.flags & RTPG_TRACE_FLAG_BUILD) (void)launch_dependent(k_mlp_lobes, kSMs * 4, kMlpThreads, kSmemEval, st, T, b);
+        (void)launch_dependent(k_bounce<kGuideMlp>, g, kTB, 0, st, T, b);
         return;
     }
     switch (guide_of(T.flags)) {
-        case kGuideTree: k_bounce<kGuideTree><<<g, kTB, 0, st>>>(T, b); break;
-        case kGuideGrid: k_bounce<kGuideGrid><<<g, kTB, 0, st>>>(T, b); break;
-        default: k_bounce<kGuideNone><<<g, kTB, 0, st>>>(T, b); break;
+        case kGuideTree: (void)launch_dependent(k_bounce<kGuideTree>, g, kTB, 0, st, T, b); break;
+        case kGuideGrid: (void)launch_dependent(k_bounce<kGuideGrid>, g, kTB, 0, st, T, b); break;
+        default: (void)launch_dependent(k_bounce<kGuideNone>, g, kTB, 0, st, T, b); break;
     }
 }
 static void launch_finish(const TracerDev& T, int g, cudaStream_t st) {
     switch (guide_of(T.flags)) {
-        case kGuideTree: k_finish<kGuideTree><<<g, kTB, 0, st>>>(T); break;
-        case kGuideGrid: k_finish<kGuideGrid><<<g, kTB, 0, st>>>(T); break;
-        case kGuideMlp: k_finish<kGuideMlp><<<g, kTB, 0, st>>>(T); break;
-        default: k_finish<kGuideNone><<<g, kTB, 0, st>>>(T); break;
+        case kGuideTree: (void)launch_dependent(k_finish<kGuideTree>, g, kTB, 0, st, T); break;
+        case kGuideGrid: (void)launch_dependent(k_finish<kGuideGrid>, g, kTB, 0, st, T); break;
+        case kGuideMlp: (void)launch_dependent(k_finish<kGuideMlp>, g, kTB, 0, st, T); break;
+        default: (void)launch_dependent(k_finish<kGuideNone>, g, kTB, 0, st, T); break;
     }
 }
 
@@ -917,7 +925,7 @@ static int timed_wave(rtpg_tracer* h, cudaStream_t st) {
 static void launch_wave(rtpg_tracer* h, cudaStream_t st) {
     TracerDev& T = h->dev;
     const int g = kSMs * 8;
-    k_raygen<<<g, kTB, 0, st>>>(T);
+    (void)launch_dependent(k_raygen, g, kTB, 0, st, T);
     for (uint32_t b = 0; b < T.max_depth; ++b) launch_bounce(T, g, st, b);
     launch_finish(T, g, st);
 }
