@@ -791,7 +791,7 @@ def cpu_baseline_hashgrid(seconds=10.0, scale_log2=6):
     per = ((1 << (2 * (6 + 1))) - 1) // 3  # RTLib's quadtree storage is sized for level 6
     times = []
     t_start = time.perf_counter()
-    while time.perf_counter() - t_start < seconds and len(times) < 200:
+    while not times or (time.perf_counter() - t_start < seconds and len(times) < 200):
         cur = np.zeros(slots, np.uint32)
         weights = np.zeros(slots * per, np.float32)
         t0 = time.perf_counter()
