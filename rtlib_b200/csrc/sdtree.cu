@@ -646,7 +646,8 @@ int rtpg_sdtree_record(rtpg_sdtree* h, int64_t n, const float* pos, const float*
     if (!pos || !dir || !radiance) return fail(RTPG_EINVAL, "rtpg_sdtree_record: pos, dir and radiance are required");
     if ((dir_is_canonical && !aligned8(dir)) || !aligned4(pos) || !aligned4(radiance))
         return fail(RTPG_EINVAL, "rtpg_sdtree_record: misaligned array (float2 arrays need 8-byte alignment)");
-    const int g = grid_for(n, kRecordBlock, 8);
+    // one resident wave: 6 CTAs of 256 per SM (36 KB of static shared memory each)
+    const int g = grid_for(n, kRecordBlock, 6);
     if (dir_is_canonical)
         k_record<true><<<g, kRecordBlock, 0, as_stream(stream)>>>(h->dev, n, pos, dir, radiance, wo_pdf, stat_weight, is_delta);
     else
