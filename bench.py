@@ -263,7 +263,7 @@ def bench_sdtree_ours(args, rank, world):
         if k >= args.warmup:
             e2e_ms.append(a.elapsed_time(c))
     e2e = _max_over_ranks(sum(e2e_ms) / len(e2e_ms), world, dev)
-    ops = (N_REC + N_Q) * world
+    ops = (args.passes * N_REC + N_Q) * world  # every pass records the 2^20 records once
     peak, peak_kind = _peaks()
     s_ms = sum(sample_ms) / len(sample_ms)
     achieved = Q_BYTES * N_Q / (s_ms * 1e-3) / 1e9

@@ -36,12 +36,16 @@ struct Hit {
     uint32_t prim;  // 0xffffffff: miss
 };
 
-__device__ __forceinline__ bool box_hit(float lox, float loy, float loz, float hix, float hiy, float hiz, float ox,
-                                        float oy, float oz, float ix, float iy, float iz, float tmin, float tmax,
+// Slab test with the ray's origin pre-scaled (oix = ox * ix, ...): each slab distance is one
+// fused multiply-add, lo * ix - ox * ix with a single rounding.  Box tests only prune the
+// traversal (the hit itself comes from tri_hit), so this arithmetic need not follow the
+// oracle's rounding, which intersects triangles by brute force.
+__device__ __forceinline__ bool box_hit(float lox, float loy, float loz, float hix, float hiy, float hiz, float oix,
+                                        float oiy, float oiz, float ix, float iy, float iz, float tmin, float tmax,
                                         float& tnear) {
-    const float tx0 = (lox - ox) * ix, tx1 = (hix - ox) * ix;
-    const float ty0 = (loy - oy) * iy, ty1 = (hiy - oy) * iy;
-    const float tz0 = (loz - oz) * iz, tz1 = (hiz - oz) * iz;
+    const float tx0 = __fmaf_rn(lox, ix, -oix), tx1 = __fmaf_rn(hix, ix, -oix);
+    const float ty0 = __fmaf_rn(loy, iy, -oiy), ty1 = __fmaf_rn(hiy, iy, -oiy);
+    const float tz0 = __fmaf_rn(loz, iz, -oiz), tz1 = __fmaf_rn(hiz, iz, -oiz);
     const float t0 = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), tmin));
     const float t1 = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fminf(fmaxf(tz0, tz1), tmax));
     tnear = t0;
@@ -81,6 +85,7 @@ __device__ __forceinline__ Hit bvh_trace(const SceneDev& s, float ox, float oy, 
     const float iy = 1.0f / (fabsf(dy) > 1e-30f ? dy : copysignf(1e-30f, dy));
     const float iz = 1.0f / (fabsf(dz) > 1e-30f ? dz : copysignf(1e-30f, dz));
     if (s.ntris == 0) return h;
+    const float oix = ox * ix, oiy = oy * iy, oiz = oz * iz;
     uint32_t stack[kBvhStack];
     int sp = 0;
     uint32_t cur = s.ntris == 1 ? kBvhLeafBit : 0u;
@@ -100,8 +105,8 @@ __device__ __forceinline__ Hit bvh_trace(const SceneDev& s, float ox, float oy, 
         } else {
             const BvhNode nd = s.nodes[cur];
             float t0, t1;
-            const bool h0 = box_hit(nd.a.x, nd.a.y, nd.a.z, nd.a.w, nd.b.x, nd.b.y, ox, oy, oz, ix, iy, iz, tmin, h.t, t0);
-            const bool h1 = box_hit(nd.b.z, nd.b.w, nd.c.x, nd.c.y, nd.c.z, nd.c.w, ox, oy, oz, ix, iy, iz, tmin, h.t, t1);
+            const bool h0 = box_hit(nd.a.x, nd.a.y, nd.a.z, nd.a.w, nd.b.x, nd.b.y, oix, oiy, oiz, ix, iy, iz, tmin, h.t, t0);
+            const bool h1 = box_hit(nd.b.z, nd.b.w, nd.c.x, nd.c.y, nd.c.z, nd.c.w, oix, oiy, oiz, ix, iy, iz, tmin, h.t, t1);
             if (h0 && h1) {
                 const bool first0 = t0 <= t1;
                 const uint32_t near = first0 ? nd.child[0] : nd.child[1];
