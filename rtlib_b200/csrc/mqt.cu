@@ -73,12 +73,12 @@ __global__ void __launch_bounds__(kMqtBuildBlock) k_mqt_build(MqtDev t) {
     }
 }
 
-// Levels up to kMqtWarpLevel: one warp per cell, kMqtWarps cells per CTA.  The warp reads the
+// Levels 1 and 2 (up to kMqtWarpLevel): one warp per cell, kMqtWarps cells per CTA.  The warp reads the
 // cell's leaves with 16-byte loads (and zeroes them with 16-byte stores), reduces the pyramid
 // in its own shared memory with exact integer sums and writes it out with consecutive lanes on
 // consecutive floats; no block-wide barrier, so every warp of the SM keeps a cell's loads in
 // flight.  Same results as k_mqt_build (integer sums do not depend on their order).
-constexpr uint32_t kMqtWarpLevel = 5;
+constexpr uint32_t kMqtWarpLevel = 2;  // levels 3 to 5 use k_mqt_build_reg
 constexpr int kMqtWarps = 8;
 __global__ void __launch_bounds__(32 * kMqtWarps) k_mqt_build_warp(MqtDev t) {
     extern __shared__ unsigned long long swarp[];  // kMqtWarps x (4^(L+1)-1)/3 entries

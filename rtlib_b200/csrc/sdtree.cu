@@ -100,8 +100,15 @@ __global__ void __launch_bounds__(kRecordBlock) k_record(SDTreeDev t, int64_t n,
                 }
             }
         }
-        warp_add_u64(k_w, v_w, acc_w);
-        warp_add_u64(k_s, v_s, acc_q);
+        if (priv) {
+            // shared-memory sums: a warp's records spread over many quadrants, so plain
+            // 64-bit shared atomics beat aggregating them first
+            if (k_w != ~0ull) atomicAdd(acc_w + k_w, v_w);
+            if (k_s != ~0ull) atomicAdd(acc_q + k_s, v_s);
+        } else {
+            warp_add_u64(k_w, v_w, acc_w);
+            warp_add_u64(k_s, v_s, acc_q);
+        }
     }
     if (priv) {
         __syncthreads();
