@@ -30,7 +30,7 @@ __global__ void k_clear(SDTreeDev t) {
         t.snode[0] = kLeafBit | 0u;
         t.b_off[0] = 0; t.b_cnt[0] = 1; t.s_off[0] = 0; t.s_cnt[0] = 1;
         t.b_statw[0] = 0ull;
-        t.s_sum[0] = 0.0f; t.s_area[0] = 0.0f; t.s_statw[0] = 0.0f;
+        t.s_sum[0] = 0.0f; t.s_area[0] = 0.0f; t.s_statw[0] = 0.0f; t.s_guided[0] = 0;
         t.b_lvl[0] = 0; t.b_lvl[1] = 1; t.b_nlvl[0] = 1;
         for (int q = 0; q < 4; ++q) t.b_sums[q] = 0ull;
         t.b_child[0] = make_ushort4(0, 0, 0, 0);
@@ -183,9 +183,12 @@ __global__ void __launch_bounds__(kTreeBlock) k_build(SDTreeDev t) {
         }
         if (threadIdx.x == 0) {
             const float4 r = t.s_nodes[off].sums;
-            t.s_sum[d] = __fadd_rn(__fadd_rn(__fadd_rn(r.x, r.y), r.z), r.w);
+            const float sum = __fadd_rn(__fadd_rn(__fadd_rn(r.x, r.y), r.z), r.w);
+            const float statw = fx_to_float(t.b_statw[d], t.fx);
+            t.s_sum[d] = sum;
             t.s_area[d] = t.b_area[off];
-            t.s_statw[d] = fx_to_float(t.b_statw[d], t.fx);
+            t.s_statw[d] = statw;
+            t.s_guided[d] = dtree_mean(statw, sum) > 0.0f ? 1 : 0;  // read per query instead of recomputed
             t.s_off[d] = off;
             t.s_cnt[d] = cnt;
         }
@@ -311,6 +314,7 @@ __global__ void k_refine_apply(SDTreeDev t, const uint32_t* ksplit, const uint32
         t.s_sum[d] = t.s_sum[dold];
         t.s_area[d] = t.s_area[dold];
         t.s_statw[d] = t.s_statw[dold];
+        t.s_guided[d] = t.s_guided[dold];
     }
 }
 // the split leaves become interior nodes; runs after k_refine_apply read snode[i]
@@ -473,7 +477,7 @@ __global__ void __launch_bounds__(256) k_sample_pdf(SDTreeDev t, int64_t n, cons
         const uint32_t d = stree_lookup(st, t.mn, t.mx, pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]);
         uint32_t rng = seeds ? seeds[i] : (pcg1d(seed_base + (uint32_t)i) | 1u);
         const uint32_t off = t.s_off[d];
-        const bool guided = dtree_mean(t.s_statw[d], t.s_sum[d]) > 0.0f;
+        const bool guided = t.s_guided[d] != 0;
         DSquare sq;
         const float2 uv = dtree_sample_sq(t.s_nodes, off, guided, rng, sq);
         if (out_uv) reinterpret_cast<float2*>(out_uv)[i] = uv;
@@ -501,7 +505,7 @@ __global__ void __launch_bounds__(256) k_pdf(SDTreeDev t, int64_t n, const float
         float2 c;
         if (canonical) c = reinterpret_cast<const float2*>(dir)[i];
         else c = dir_to_canonical(dir[3 * i], dir[3 * i + 1], dir[3 * i + 2]);
-        out[i] = dtree_pdf(t.s_nodes, t.s_off[d], t.s_statw[d], t.s_sum[d], c.x, c.y);
+        out[i] = dtree_pdf_g(t.s_nodes, t.s_off[d], t.s_guided[d] != 0, c.x, c.y);
     }
 }
 
@@ -602,7 +606,7 @@ int rtpg_sdtree_create(const float* aabb_min, const float* aabb_max, uint32_t ma
     if ((r = h->alloc(&t.status, 1)) || (r = h->alloc(&t.counts, 4)) || (r = h->alloc(&t.snode, ns)) ||
         (r = h->alloc(&t.b_off, nd)) || (r = h->alloc(&t.b_cnt, nd)) || (r = h->alloc(&t.s_off, nd)) ||
         (r = h->alloc(&t.s_cnt, nd)) || (r = h->alloc(&t.b_statw, nd)) || (r = h->alloc(&t.s_sum, nd)) ||
-        (r = h->alloc(&t.s_area, nd)) || (r = h->alloc(&t.s_statw, nd)) ||
+        (r = h->alloc(&t.s_area, nd)) || (r = h->alloc(&t.s_statw, nd)) || (r = h->alloc(&t.s_guided, nd)) ||
         (r = h->alloc(&t.b_lvl, nd * (kMaxLevels + 1))) || (r = h->alloc(&t.b_nlvl, nd)) ||
         (r = h->alloc(&t.b_sums, nn * 4)) || (r = h->alloc(&t.b_child, nn)) || (r = h->alloc(&t.b_area, nn)) ||
         (r = h->alloc(&t.s_nodes, nn)) || (r = h->alloc(&h->cnt_s, ns)) || (r = h->alloc(&h->off_s, ns)) ||

@@ -39,6 +39,7 @@ struct SDTreeDev {
     float* s_sum;
     float* s_area;
     float* s_statw;
+    uint8_t* s_guided;  // DTreeT::GetMean() > 0 of each sampling tree, set where its sum and stat-weight are
     uint16_t* b_lvl;  // kMaxLevels + 1 per tree
     uint8_t* b_nlvl;
     unsigned long long* b_sums;  // 4 per building node
@@ -158,10 +159,6 @@ __device__ __forceinline__ float dtree_pdf_g(const SNode* __restrict__ nodes, ui
         idx = quad_child(u, v);
     }
     return __fdiv_rn(__fmul_rn(result, kInv2Pi), 2.0f);
-}
-__device__ __forceinline__ float dtree_pdf(const SNode* __restrict__ nodes, uint32_t off, float statw, float sum,
-                                           float u, float v) {
-    return dtree_pdf_g(nodes, off, dtree_mean(statw, sum) > 0.0f, u, v);
 }
 
 // The square [x, x + w) x [y, y + w) of the node where a sampling descent stopped, and the

@@ -278,7 +278,7 @@ __device__ __forceinline__ bool bounce_path(const TracerDev& T, uint32_t p, bool
         }
         if (use_tree && build) {
             const uint32_t soff = T.tree.s_off[dt];
-            const bool guided = dtree_mean(T.tree.s_statw[dt], T.tree.s_sum[dt]) > 0.0f;
+            const bool guided = T.tree.s_guided[dt] != 0;
             // square + pdf of a guided sample; the empty default sends the pdf of a BSDF sample
             // through the full descent
             DSquare sq{2.0f, 2.0f, 0.0f, 0.0f};
@@ -317,7 +317,7 @@ __device__ __forceinline__ bool bounce_path(const TracerDev& T, uint32_t p, bool
             bool tguided = false;
             if (mlp_mix) {
                 soff = T.tree.s_off[dt];
-                tguided = dtree_mean(T.tree.s_statw[dt], T.tree.s_sum[dt]) > 0.0f;
+                tguided = T.tree.s_guided[dt] != 0;
             }
             DSquare sq{2.0f, 2.0f, 0.0f, 0.0f};  // as in the SD-tree guide above
             if (rnd1(rng) < T.mlp_fraction) {
