@@ -875,7 +875,7 @@ def bench_learned(args):
         n_sd2 = sdtree_run(tr, budget, args.guide_fraction)
         e_sd2, d_sd2 = err(tr.image().cpu().numpy())
         del tr
-        # the learned guide with the SD-tree as its fallback (the main configuration)
+        # the learned guide with the SD-tree as its fallback (the configuration the line reports)
         tr = Tracer(sc, dev, max_depth=O_DEPTH, seed=3)
         g = MLPGuide((-0.1, -0.1, -0.1), (14.1, 4.1, 10.1), seed=1, learning_rate=1e-3, record_capacity=1 << 18)
         tree = SDTree(*O_AABB, fraction=0.5)
@@ -1055,7 +1055,7 @@ def main():
     if args.workload == "learned":
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "the learned guide has no counterpart in RTLib; "
-                              "its judge is the SD-tree arm of the same run"}), flush=True)
+                              "it is compared with the SD-tree arm of the same run"}), flush=True)
             return 0
         if rank != 0:
             return 0
