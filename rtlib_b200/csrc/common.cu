@@ -26,9 +26,20 @@ int fail(int code, const char* fmt, ...) {
 }
 
 // ---------------------------------------------------------------- scan
-__global__ void __launch_bounds__(kScanBlock) scan_tile_sums(const uint32_t* __restrict__ in, const uint32_t* n_dev,
-                                                            uint32_t* __restrict__ partials) {
+// Up to two arrays of the same device-side length per launch: blockIdx.y picks the array, each
+// with its own region of `partials` (ceil(cap / kScanTile) + 1 words apart).
+struct ScanPair {
+    const uint32_t* in[2];
+    uint32_t* out[2];
+    uint32_t* total[2];
+    uint32_t stride;  // words between the two partials regions
+};
+
+__global__ void __launch_bounds__(kScanBlock) scan_tile_sums(ScanPair a, const uint32_t* n_dev, uint32_t* partials) {
     grid_dependency_wait();
+    const uint32_t y = blockIdx.y;
+    const uint32_t* __restrict__ in = y ? a.in[1] : a.in[0];
+    partials += y * a.stride;
     const uint32_t n = *n_dev;
     const uint32_t base = blockIdx.x * kScanTile;
     if (base >= n) return;
@@ -45,8 +56,11 @@ __global__ void __launch_bounds__(kScanBlock) scan_tile_sums(const uint32_t* __r
     }
 }
 
-__global__ void __launch_bounds__(kScanBlock) scan_partials(uint32_t* partials, const uint32_t* n_dev, uint32_t* total_out) {
+__global__ void __launch_bounds__(kScanBlock) scan_partials(ScanPair a, const uint32_t* n_dev, uint32_t* partials) {
     grid_dependency_wait();
+    const uint32_t y = blockIdx.y;
+    uint32_t* total_out = y ? a.total[1] : a.total[0];
+    partials += y * a.stride;
     __shared__ uint32_t ws[kScanBlock / 32];
     const uint32_t n = *n_dev;
     const uint32_t tiles = (n + kScanTile - 1) / kScanTile;
@@ -62,9 +76,12 @@ __global__ void __launch_bounds__(kScanBlock) scan_partials(uint32_t* partials, 
     if (threadIdx.x == 0 && total_out) *total_out = carry;
 }
 
-__global__ void __launch_bounds__(kScanBlock) scan_tiles(const uint32_t* __restrict__ in, uint32_t* __restrict__ out,
-                                                        const uint32_t* n_dev, const uint32_t* __restrict__ partials) {
+__global__ void __launch_bounds__(kScanBlock) scan_tiles(ScanPair a, const uint32_t* n_dev, const uint32_t* partials) {
     grid_dependency_wait();
+    const uint32_t y = blockIdx.y;
+    const uint32_t* __restrict__ in = y ? a.in[1] : a.in[0];
+    uint32_t* __restrict__ out = y ? a.out[1] : a.out[0];
+    partials += y * a.stride;
     __shared__ uint32_t ws[kScanBlock / 32];
     const uint32_t n = *n_dev;
     const uint32_t base = blockIdx.x * kScanTile;
@@ -87,15 +104,27 @@ __global__ void __launch_bounds__(kScanBlock) scan_tiles(const uint32_t* __restr
     }
 }
 
+static int scan_launch(const ScanPair& a, uint32_t arrays, const uint32_t* n_dev, uint32_t cap, uint32_t* partials,
+                       cudaStream_t st) {
+    const uint32_t tiles = (cap + kScanTile - 1) / kScanTile;
+    const dim3 g(tiles ? tiles : 1, arrays);
+    // launched as dependent grids: each may be scheduled while its predecessor finishes
+    RTPG_CUDA(launch_dependent(scan_tile_sums, g, kScanBlock, 0, st, a, n_dev, partials));
+    RTPG_CUDA(launch_dependent(scan_partials, dim3(1, arrays), kScanBlock, 0, st, a, n_dev, partials));
+    RTPG_CUDA(launch_dependent(scan_tiles, g, kScanBlock, 0, st, a, n_dev, (const uint32_t*)partials));
+    return RTPG_OK;
+}
+
 int scan_exclusive_u32(const uint32_t* in, uint32_t* out, const uint32_t* n_dev, uint32_t cap, uint32_t* partials,
                        uint32_t* total_out, cudaStream_t st) {
-    const uint32_t tiles = (cap + kScanTile - 1) / kScanTile;
-    const uint32_t g = tiles ? tiles : 1;
-    // launched as dependent grids: each may be scheduled while its predecessor finishes
-    RTPG_CUDA(launch_dependent(scan_tile_sums, g, kScanBlock, 0, st, in, n_dev, partials));
-    RTPG_CUDA(launch_dependent(scan_partials, 1, kScanBlock, 0, st, partials, n_dev, total_out));
-    RTPG_CUDA(launch_dependent(scan_tiles, g, kScanBlock, 0, st, in, out, n_dev, partials));
-    return RTPG_OK;
+    const ScanPair a{{in, in}, {out, out}, {total_out, total_out}, 0};
+    return scan_launch(a, 1, n_dev, cap, partials, st);
+}
+
+int scan_exclusive_u32x2(const uint32_t* in0, uint32_t* out0, uint32_t* total0, const uint32_t* in1, uint32_t* out1,
+                         uint32_t* total1, const uint32_t* n_dev, uint32_t cap, uint32_t* partials, cudaStream_t st) {
+    const ScanPair a{{in0, in1}, {out0, out1}, {total0, total1}, (uint32_t)scan_partials_words(cap)};
+    return scan_launch(a, 2, n_dev, cap, partials, st);
 }
 
 }  // namespace rtpg

@@ -155,6 +155,10 @@ constexpr int kScanTile = kScanBlock * 4;
 int scan_exclusive_u32(const uint32_t* in, uint32_t* out, const uint32_t* n_dev, uint32_t cap, uint32_t* partials,
                        uint32_t* total_out, cudaStream_t st);
 inline size_t scan_partials_words(uint32_t cap) { return size_t(cap + kScanTile - 1) / kScanTile + 1; }
+// Two arrays of the same length n (in one pass of three launches); `partials` needs
+// 2 * scan_partials_words(cap) words.
+int scan_exclusive_u32x2(const uint32_t* in0, uint32_t* out0, uint32_t* total0, const uint32_t* in1, uint32_t* out1,
+                         uint32_t* total1, const uint32_t* n_dev, uint32_t cap, uint32_t* partials, cudaStream_t st);
 
 // Programmatic dependent launch.  A kernel started with launch_dependent() may be scheduled
 // while the kernel before it in the stream is still running, which hides the launch gap of

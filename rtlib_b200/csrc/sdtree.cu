@@ -612,7 +612,7 @@ int rtpg_sdtree_create(const float* aabb_min, const float* aabb_max, uint32_t ma
         (r = h->alloc(&t.s_nodes, nn)) || (r = h->alloc(&h->cnt_s, ns)) || (r = h->alloc(&h->off_s, ns)) ||
         (r = h->alloc(&h->cnt_d, ns)) || (r = h->alloc(&h->off_d, ns)) || (r = h->alloc(&h->ksplit, ns)) ||
         (r = h->alloc(&h->node_cnt, nd)) || (r = h->alloc(&h->node_off, nd)) ||
-        (r = h->alloc(&h->partials, scan_partials_words(std::max(c.max_stree_nodes, c.max_dtrees)))) ||
+        (r = h->alloc(&h->partials, 2 * scan_partials_words(std::max(c.max_stree_nodes, c.max_dtrees)))) ||
         (r = h->alloc(&h->totals, 4)) || (r = h->alloc(&h->fp, 4))) {
         delete h;
         return r;
@@ -687,8 +687,10 @@ int rtpg_sdtree_refine(rtpg_sdtree* h, uint64_t spatial_threshold, int32_t max_m
     RTPG_CUDA(launch_dependent(k_refine_count, grid_for(t.cap_snodes, 256, 8), 256, 0, st, t, thf, max_mb, kmax, h->fp,
                                h->cnt_s, h->cnt_d, h->ksplit));
     int r;
-    if ((r = scan_exclusive_u32(h->cnt_s, h->off_s, t.counts + 0, t.cap_snodes, h->partials, h->totals + 0, st))) return r;
-    if ((r = scan_exclusive_u32(h->cnt_d, h->off_d, t.counts + 0, t.cap_snodes, h->partials, h->totals + 1, st))) return r;
+    // new STree nodes and new DTrees per leaf: one pass over both count arrays
+    if ((r = scan_exclusive_u32x2(h->cnt_s, h->off_s, h->totals + 0, h->cnt_d, h->off_d, h->totals + 1, t.counts + 0,
+                                  t.cap_snodes, h->partials, st)))
+        return r;
     RTPG_CUDA(launch_dependent(k_refine_apply, kSMs * 4, 256, 0, st, t, h->ksplit, h->off_s, h->cnt_s, h->off_d,
                                h->cnt_d, h->fp));
     RTPG_CUDA(launch_dependent(k_refine_link, grid_for(t.cap_snodes, 256, 4), 256, 0, st, t, h->ksplit, h->off_s, h->fp));
