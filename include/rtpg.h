@@ -123,6 +123,22 @@ int rtpg_sdtree_status(rtpg_sdtree* h, uint32_t* host_status, int clear, void* s
 int rtpg_sdtree_export(rtpg_sdtree* h, int sampling, int64_t* host_sizes, uint8_t* host_stree_mask,
                        float* host_leaf_scalars, int64_t* host_leaf_counts, uint8_t* host_dnode_mask,
                        float* host_dnode_sums, void* stream);
+/* Inverse of rtpg_sdtree_export, for checkpoints and for trees built elsewhere (e.g. on the
+ * host): replaces the whole tree with the one described by the streams of two exports of it,
+ * one with sampling = 0 (building quadtrees) and one with sampling = 1 (sampling quadtrees).
+ * The STree mask (stree_nodes bytes) and the leaf scalars (4 floats per leaf) are those of
+ * either export; each quadtree stream gives per leaf its node count and, per node in pre-order,
+ * the child mask and 4 sums (building_nodes / sampling_nodes nodes in all).  Building sums and
+ * stat-weights become fixed point (round to nearest), sampling sums stay float, and every
+ * sampling tree's guided flag (DTreeT::GetMean() > 0, PG.h:447-451) is recomputed from its
+ * scalars, so an exported tree imported again exports identically and samples identically.
+ * RTLib's counterpart is RTSTreeWrapperT::Upload (PG.h:1353-1564) of the host trees that
+ * RTSTreeWrapperT::Dump (PG.h:1749-1756) writes out.  Synchronises the stream. */
+int rtpg_sdtree_import(rtpg_sdtree* h, int64_t stree_nodes, int64_t leaves, const uint8_t* host_stree_mask,
+                       const float* host_leaf_scalars, int64_t building_nodes, const int64_t* host_building_counts,
+                       const uint8_t* host_building_mask, const float* host_building_sums, int64_t sampling_nodes,
+                       const int64_t* host_sampling_counts, const uint8_t* host_sampling_mask,
+                       const float* host_sampling_sums, void* stream);
 
 /* ---------------------------------------------------------------- pass controller
  * RTSTreeControllerT (PG.h:1769-1920): the doubling pass schedule.  Host-side state only;
@@ -274,6 +290,12 @@ int rtpg_mlp_train(rtpg_mlp* h, int64_t n, const float* pos, const float* nrm, c
 int rtpg_mlp_records(rtpg_mlp* h, uint32_t* host_count, int clear, void* stream);
 int rtpg_mlp_record_arrays(rtpg_mlp* h, float** pos, float** nrm, float** wo, float** wi, float** w);
 int rtpg_mlp_status(rtpg_mlp* h, uint32_t* host_status, int clear, void* stream);
+/* Test mode of the bounded waits on the tensor cores (no counterpart in RTLib): skip_mma = 1
+ * makes this guide's kernels issue no MMA and no commit, so every completion wait runs out after
+ * poll_limit polls; the kernel then sets RTPG_STATUS_TIMEOUT, issues nothing more, frees its
+ * tensor memory and returns, leaving the context usable.  skip_mma = 0, poll_limit = 0 restore
+ * normal operation (poll limit 2^22). */
+int rtpg_mlp_set_wait_test(rtpg_mlp* h, int skip_mma, uint32_t poll_limit);
 
 /* ================================================================ scene / hit queries
  * The integrator's closest-hit and any-hit queries (RTLib: optixTrace inside TraceRadiance /

@@ -31,10 +31,17 @@ def build_oracle() -> None:
     subprocess.check_call(["make", "-s", "-C", HERE], stdout=subprocess.DEVNULL)
 
 
+def reference_tree() -> str:
+    """Location of the RTLib source tree: $RTLIB_REFERENCE, else a checkout named
+    ``reference`` beside this repository."""
+    return os.environ.get("RTLIB_REFERENCE",
+                          os.path.normpath(os.path.join(HERE, os.pardir, os.pardir, "reference")))
+
+
 def build_reference() -> bool:
     """Build oracle/_ref from the reference tree when it is present.  Returns whether the
     library exists afterwards."""
-    ref = os.environ.get("RTLIB_REFERENCE", "/root/reference")
+    ref = reference_tree()
     if os.path.isdir(ref):
         subprocess.check_call(["make", "-s", "-C", os.path.join(HERE, "ref"), f"REF={ref}"],
                               stdout=subprocess.DEVNULL)

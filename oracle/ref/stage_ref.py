@@ -29,8 +29,10 @@ import os
 import re
 import sys
 
-REF = os.environ.get("RTLIB_REFERENCE", "/root/reference")
 HERE = os.path.dirname(os.path.abspath(__file__))
+# the RTLib source tree: $RTLIB_REFERENCE, else a checkout named "reference" beside the repository
+REF = os.environ.get("RTLIB_REFERENCE", os.path.normpath(os.path.join(HERE, os.pardir, os.pardir, os.pardir,
+                                                                       "reference")))
 OUT = os.path.join(os.path.dirname(HERE), "_ref")
 UTILS = "RTLib/Src/Ext/OPX7/Include/RTLib/Ext/OPX7/Utils"
 CUDA_INC = "RTLib/Src/Ext/CUDA/Include"

@@ -41,6 +41,7 @@ _SIGS = {
     "rtpg_sdtree_memory_footprint": [P, P],
     "rtpg_sdtree_status": [P, P, C.c_int, P],
     "rtpg_sdtree_export": [P, C.c_int, P, P, P, P, P, P, P],
+    "rtpg_sdtree_import": [P, I64, I64, P, P, I64, P, P, P, I64, P, P, P, P],
     "rtpg_controller_create": [P, U32, U32, F32, U32, P],
     "rtpg_controller_destroy": [P],
     "rtpg_controller_start": [P],
@@ -93,6 +94,7 @@ _SIGS = {
     "rtpg_mlp_records": [P, P, C.c_int, P],
     "rtpg_mlp_record_arrays": [P, P, P, P, P, P],
     "rtpg_mlp_status": [P, P, C.c_int, P],
+    "rtpg_mlp_set_wait_test": [P, C.c_int, U32],
     "rtpg_tracer_set_light_emission": [P, P, U32],
     "rtpg_tracer_image_f64": [P, P, P],
     "rtpg_tracer_render_mlp": [P, U32, U32, P, P, F32, F32, F32, P],

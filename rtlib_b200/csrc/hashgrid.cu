@@ -395,7 +395,7 @@ extern "C" int rtpg_hashgrid_insert_noalloc(const float* aabb_min, const float* 
         return fail(RTPG_EINVAL, "rtpg_hashgrid_insert_noalloc: num_slots must be a positive multiple of %u", kHashBlock);
     if (keying != RTPG_HASH_KEY_REFERENCE && keying != RTPG_HASH_KEY_MORTON)
         return fail(RTPG_EINVAL, "rtpg_hashgrid_insert_noalloc: unknown keying %d", keying);
-    if (!aligned8(table) || !aligned4(pos) || !aligned4(out_slot))
+    if (!aligned8(table) || !aligned4(pos) || !aligned4(out_slot) || (status && !aligned4(status)))
         return fail(RTPG_EINVAL, "rtpg_hashgrid_insert_noalloc: misaligned array");
     for (int k = 0; k < 3; ++k) {
         if (bounds[k] == 0 || !(aabb_max[k] > aabb_min[k]))

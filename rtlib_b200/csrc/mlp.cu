@@ -62,7 +62,10 @@ __global__ void __launch_bounds__(kMlpThreads) k_mlp_eval(MlpDev P, int64_t n, c
         }
         store_features(x0, t, f);
         float o[kMlpOut];
-        ok &= mlp_forward_tile(tmem, sw, x0, mbar, phase, o);
+        if (!mlp_forward_tile(P, tmem, sw, x0, mbar, phase, o)) {
+            ok = false;  // uniform over the CTA: issue nothing more
+            break;
+        }
         if (i < n) {
             // a sample's row (192 or 160 bytes) in 16-byte stores when the array allows it
             if (out_raw) store_row<kMlpOut>(out_raw + i * kMlpOut, o);
@@ -79,7 +82,10 @@ __global__ void __launch_bounds__(kMlpThreads) k_mlp_eval(MlpDev P, int64_t n, c
             }
         }
     }
-    if (!ok) atomicOr(P.status, RTPG_STATUS_TIMEOUT);
+    if (!ok) {
+        if (t == 0) atomicOr(P.status, RTPG_STATUS_TIMEOUT);
+        mma_drain(mbar, phase, P.poll_limit);
+    }
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
@@ -151,11 +157,11 @@ __global__ void __launch_bounds__(kMlpThreads, 1) k_mlp_train(MlpDev P, int64_t 
     uint32_t phase = 0;
     bool ok = true, first = true;
     float lsum = 0.0f;
-    auto sync_mma = [&]() {
-        if (t == 0) umma_commit(mbar);
-        ok &= mbar_wait(mbar, phase);
-        phase ^= 1u;
-        tc_fence_after();
+    // commit the MMAs thread 0 issued and wait for them; false (uniform over the CTA) when the
+    // wait gave up, after which nothing more is issued
+    auto sync_mma = [&]() -> bool {
+        if (t == 0 && !P.skip_mma) umma_commit(mbar);
+        return mma_complete(mbar, phase, P.poll_limit);
     };
     for (int64_t base = int64_t(blockIdx.x) * kMlpTile; base < n; base += int64_t(gridDim.x) * kMlpTile) {
         const int64_t i = base + t;
@@ -176,14 +182,15 @@ __global__ void __launch_bounds__(kMlpThreads, 1) k_mlp_train(MlpDev P, int64_t 
         // forward, keeping H1..H3
         for (int l = 0; l < 4; ++l) {
             mma_barrier();
-            if (t == 0) {
+            if (t == 0 && !P.skip_mma) {
                 if (l == 0) issue_fwd(tmem + kColD, sx, kMlpIn, kMlpIn, sw + 2 * kW0, kMlpHidden);
                 else if (l < 3) issue_fwd(tmem + kColD, sh[l - 1], kMlpHidden, kMlpHidden, sw + 2 * (l == 1 ? kW1 : kW2), kMlpHidden);
                 else issue_fwd(tmem + kColD, sh[2], kMlpHidden, kMlpHidden, sw + 2 * kW3, kMlpOut);
             }
-            sync_mma();
+            if (!(ok = sync_mma())) break;
             if (l < 3) epilogue_relu(tmem, hs[l]);
         }
+        if (!ok) break;
         // loss gradient at the outputs -> dY [128 x 64] (columns 40..63 zero)
         {
             float o[kMlpOut], g[kMlpHidden];
@@ -198,7 +205,7 @@ __global__ void __launch_bounds__(kMlpThreads, 1) k_mlp_train(MlpDev P, int64_t 
         // backward: layer 3 .. 0
         for (int l = 3; l >= 0; --l) {
             mma_barrier();
-            if (t == 0) {
+            if (t == 0 && !P.skip_mma) {
                 const uint32_t cw = l == 3 ? kColW3 : (l == 2 ? kColW2 : (l == 1 ? kColW1 : kColW0));
                 if (l > 0) {
                     issue_dw(tmem + cw, sdy, sh[l - 1], kMlpHidden, kMlpHidden, !first);
@@ -208,7 +215,7 @@ __global__ void __launch_bounds__(kMlpThreads, 1) k_mlp_train(MlpDev P, int64_t 
                     issue_dw(tmem + cw, sdy, sx, kMlpIn, kMlpIn, !first);
                 }
             }
-            sync_mma();
+            if (!(ok = sync_mma())) break;
             if (l > 0) {
                 // dH = dX masked by ReLU' of the activation it came from, back into dY
                 const __nv_bfloat16* hl = hs[l - 1];
@@ -226,10 +233,12 @@ __global__ void __launch_bounds__(kMlpThreads, 1) k_mlp_train(MlpDev P, int64_t 
                 }
             }
         }
+        if (!ok) break;
         first = false;
     }
-    // flush dW^T (M = 64 rows in lanes 16w .. 16w+15 of warp w's quarter) into grads
-    if (!first) {
+    // flush dW^T (M = 64 rows in lanes 16w .. 16w+15 of warp w's quarter) into grads; after a
+    // wait gave up the accumulators are incomplete and nothing is flushed
+    if (!first && ok) {
         const int warp = t >> 5, lane = t & 31;
         const int row = 16 * warp + lane;  // output feature
         const uint32_t cols[4] = {kColW0, kColW1, kColW2, kColW3};
@@ -249,7 +258,10 @@ __global__ void __launch_bounds__(kMlpThreads, 1) k_mlp_train(MlpDev P, int64_t 
     // loss
     for (int o = 16; o > 0; o >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
     if ((t & 31) == 0 && lsum != 0.0f) atomicAdd(loss_sum, lsum * scale);
-    if (!ok) atomicOr(P.status, RTPG_STATUS_TIMEOUT);
+    if (!ok) {
+        if (t == 0) atomicOr(P.status, RTPG_STATUS_TIMEOUT);
+        mma_drain(mbar, phase, P.poll_limit);
+    }
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
@@ -380,6 +392,8 @@ int rtpg_mlp_create(const float* aabb_min, const float* aabb_max, uint32_t seed,
                                  1.0f / (aabb_max[2] - aabb_min[2]));
     h->dev.wq = h->wq;
     h->dev.status = h->status;
+    h->dev.skip_mma = 0;
+    h->dev.poll_limit = kMbarPollLimit;
     // He-uniform initialisation from a seeded SplitMix64 stream; output padding columns zero
     std::vector<float> w(kMlpParams, 0.0f);
     uint64_t s = 0x5DEECE66Dull ^ (uint64_t(seed) << 17);
@@ -530,6 +544,17 @@ int rtpg_mlp_record_arrays(rtpg_mlp* h, float** pos, float** nrm, float** wo, fl
     if (wo) *wo = h->r_wo;
     if (wi) *wi = h->r_wi;
     if (w) *w = h->r_w;
+    return RTPG_OK;
+}
+
+// Test mode of the bounded tensor-core waits: with skip_mma = 1 the kernels of this guide
+// issue neither MMAs nor commits, so each completion wait runs out after poll_limit polls,
+// sets RTPG_STATUS_TIMEOUT and the kernel returns with nothing in flight.  skip_mma = 0 and
+// poll_limit = 0 restore normal operation.
+int rtpg_mlp_set_wait_test(rtpg_mlp* h, int skip_mma, uint32_t poll_limit) {
+    if (!h) return fail(RTPG_EINVAL, "rtpg_mlp_set_wait_test: null handle");
+    h->dev.skip_mma = skip_mma ? 1u : 0u;
+    h->dev.poll_limit = poll_limit ? poll_limit : kMbarPollLimit;
     return RTPG_OK;
 }
 

@@ -75,11 +75,14 @@ __device__ __forceinline__ void mbar_init(uint64_t* mbar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(mbar)), "r"(count) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
-// Wait for the phase `parity` of the barrier to complete, at most ~2^22 polls; returns false
-// on a timeout (the caller records an error status and carries on, so no wait is endless).
-__device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity) {
+// polls of a bounded mbarrier wait before it gives up
+constexpr uint32_t kMbarPollLimit = 1u << 22;
+// Wait for the phase `parity` of the barrier to complete, at most `limit` polls; returns
+// false on a timeout (the caller records an error status, issues no further MMA and leaves,
+// so no wait is endless).
+__device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity, uint32_t limit = kMbarPollLimit) {
     const uint32_t a = smem_u32(mbar);
-    for (uint32_t i = 0; i < (1u << 22); ++i) {
+    for (uint32_t i = 0; i < limit; ++i) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
@@ -239,7 +242,20 @@ struct MlpDev {
     const __nv_bfloat16* wq;  // bf16 weights, each matrix in the core-matrix layout
     float3 mn, inv_ext;       // AABB of the positions
     unsigned* status;
+    // Test mode of the bounded waits (rtpg_mlp_set_wait_test): skip_mma = 1 issues neither
+    // the MMAs nor their commit, so the completion barrier never arrives and the wait runs
+    // out after poll_limit polls with nothing in flight.  Normal use: 0 and kMbarPollLimit.
+    uint32_t skip_mma;
+    uint32_t poll_limit;
 };
+
+// After a wait that gave up: one more bounded wait on the same phase, so that an MMA still in
+// flight (one that completes after the timeout) has finished before its TMEM is freed.
+// Every thread of the CTA calls it.
+__device__ __forceinline__ void mma_drain(uint64_t* mbar, uint32_t phase, uint32_t limit) {
+    (void)mbar_wait(mbar, phase, limit);
+    tc_fence_after();
+}
 
 // the learned guide as the tracer sees it: weights and the record buffer it appends to
 struct MlpView {
@@ -315,29 +331,37 @@ __device__ __forceinline__ void epilogue_relu(uint32_t tmem, __nv_bfloat16* h) {
     for (int c = 0; c < kMlpHidden; c += 8) st_bf16x8(h + blk(t, c, kMlpHidden), v + c);
 }
 
+// Completion of the MMAs thread 0 committed to `mbar`: every thread waits (bounded), and the
+// outcome is made uniform over the CTA.  On success the phase flips; on a timeout it stays,
+// so mma_drain can wait for the same phase before TMEM is freed.
+__device__ __forceinline__ bool mma_complete(uint64_t* mbar, uint32_t& phase, uint32_t limit) {
+    const bool ok = __syncthreads_and(mbar_wait(mbar, phase, limit)) != 0;
+    if (ok) phase ^= 1u;
+    tc_fence_after();
+    return ok;
+}
+
 // Forward pass of one tile: the features of sample t are in row t of x0 (which the hidden
 // activations then overwrite); returns sample t's 48 raw outputs in o.  Every thread of the
-// 128-thread CTA calls it; thread 0 issues the MMAs.  False if a wait on the tensor cores gave
-// up.
-__device__ __forceinline__ bool mlp_forward_tile(uint32_t tmem, uint32_t sw, __nv_bfloat16* x0, uint64_t* mbar,
-                                                 uint32_t& phase, float* o) {
+// 128-thread CTA calls it; thread 0 issues the MMAs.  False (uniformly over the CTA, with o
+// not written) if a wait on the tensor cores gave up: the caller then issues nothing more,
+// drains with mma_drain and frees its TMEM.
+__device__ __forceinline__ bool mlp_forward_tile(const MlpDev& P, uint32_t tmem, uint32_t sw, __nv_bfloat16* x0,
+                                                 uint64_t* mbar, uint32_t& phase, float* o) {
     const uint32_t sx = smem_u32(x0);
-    bool ok = true;
     for (int l = 0; l < 4; ++l) {
         mma_barrier();
-        if (threadIdx.x == 0) {
+        if (threadIdx.x == 0 && !P.skip_mma) {
             if (l == 0) issue_fwd(tmem + kColD, sx, kMlpIn, kMlpIn, sw + 2 * kW0, kMlpHidden);
             else if (l < 3) issue_fwd(tmem + kColD, sx, kMlpHidden, kMlpHidden, sw + 2 * (l == 1 ? kW1 : kW2), kMlpHidden);
             else issue_fwd(tmem + kColD, sx, kMlpHidden, kMlpHidden, sw + 2 * kW3, kMlpOut);
             umma_commit(mbar);
         }
-        ok &= mbar_wait(mbar, phase);
-        phase ^= 1u;
-        tc_fence_after();
+        if (!mma_complete(mbar, phase, P.poll_limit)) return false;
         if (l < 3) epilogue_relu(tmem, x0);
     }
     ld_row<kMlpOut>(tmem, kColD, o);
-    return ok;
+    return true;
 }
 
 }  // namespace rtpg

@@ -7,6 +7,8 @@
 // on device-resident arrays; counts stay in device memory so a whole pass can be captured
 // in a CUDA graph.
 #include <math.h>
+#include <cmath>
+#include <string>
 #include <vector>
 #include <algorithm>
 #include <new>
@@ -866,6 +868,267 @@ extern "C" int rtpg_sdtree_export(rtpg_sdtree* h, int sampling, int64_t* sizes, 
     if (counts) memcpy(counts, e.counts.data(), e.counts.size() * sizeof(int64_t));
     if (dmask) memcpy(dmask, e.dmask.data(), e.dmask.size());
     if (dsums) memcpy(dsums, e.dsums.data(), e.dsums.size() * sizeof(float));
+    return RTPG_OK;
+}
+
+// ------------------------------------------------------------------ import (host side)
+// The inverse of the export: the pre-order streams of the STree and of every leaf's building
+// and sampling quadtree are laid out as the kernels expect them -- STree children adjacent
+// (child 1 = child 0 + 1), quadtrees breadth first with their level starts, building sums in
+// fixed point, sampling nodes as float.  RTLib's counterpart is RTSTreeWrapperT::Upload
+// (OPX7UtilsPathGuiding.h:1353-1564), which flattens the host trees into device buffers.
+namespace {
+struct QNode {
+    uint8_t mask;
+    float sums[4];
+    uint32_t child[4];  // index into the parsed node list (valid where mask has the bit)
+};
+// Parses one quadtree of `count` pre-order nodes starting at stream position `pos`.
+bool parse_dtree(const uint8_t* mask, const float* sums, int64_t total, int64_t pos, int64_t count,
+                 std::vector<QNode>& out, std::string& err) {
+    out.clear();
+    if (count < 1 || pos < 0 || pos + count > total) {
+        err = "quadtree node range outside the stream";
+        return false;
+    }
+    // explicit stack of (node, next quadrant to visit)
+    std::vector<std::pair<uint32_t, int>> stack;
+    int64_t k = pos;
+    auto take = [&](uint32_t& idx) -> bool {
+        if (k >= pos + count) return false;
+        QNode n{};
+        n.mask = mask[k];
+        if (n.mask & ~0xFu) return false;
+        for (int q = 0; q < 4; ++q) n.sums[q] = sums[4 * k + q];
+        idx = (uint32_t)out.size();
+        out.push_back(n);
+        ++k;
+        return true;
+    };
+    uint32_t root;
+    if (!take(root)) {
+        err = "empty quadtree";
+        return false;
+    }
+    stack.push_back({root, 0});
+    while (!stack.empty()) {
+        auto& top = stack.back();
+        if (top.second >= 4) {
+            stack.pop_back();
+            continue;
+        }
+        const int q = top.second++;
+        if (!(out[top.first].mask & (1u << q))) continue;
+        uint32_t c;
+        if (!take(c)) {
+            err = "quadtree stream ends inside a tree";
+            return false;
+        }
+        out[stack.back().first].child[q] = c;
+        if (stack.size() > kMaxDTreeDepth + 1) {
+            err = "quadtree deeper than the supported maximum";
+            return false;
+        }
+        stack.push_back({c, 0});
+    }
+    if (k != pos + count) {
+        err = "quadtree node count does not match its stream";
+        return false;
+    }
+    return true;
+}
+// Breadth-first numbering of a parsed quadtree: order[j] = parsed index of node j, level
+// starts (one entry per level plus the end).
+void bfs_dtree(const std::vector<QNode>& t, std::vector<uint32_t>& order, std::vector<uint32_t>& lvl) {
+    order.assign(1, 0u);
+    lvl.assign(1, 0u);
+    size_t a = 0;
+    while (a < order.size()) {
+        const size_t b = order.size();
+        lvl.push_back((uint32_t)b);
+        for (size_t j = a; j < b; ++j)
+            for (int q = 0; q < 4; ++q)
+                if (t[order[j]].mask & (1u << q)) order.push_back(t[order[j]].child[q]);
+        a = b;
+    }
+    // lvl holds the start of every level and, last, the node count (its final level is empty)
+    if (lvl.size() >= 2 && lvl[lvl.size() - 1] == lvl[lvl.size() - 2]) lvl.pop_back();
+}
+template <class T>
+cudaError_t ul(T* dst, const std::vector<T>& v, cudaStream_t st) {
+    if (v.empty()) return cudaSuccess;
+    return cudaMemcpyAsync(dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st);
+}
+}  // namespace
+
+extern "C" int rtpg_sdtree_import(rtpg_sdtree* h, int64_t stree_nodes, int64_t leaves, const uint8_t* stree_mask,
+                                  const float* leaf_scalars, int64_t building_nodes, const int64_t* building_counts,
+                                  const uint8_t* building_mask, const float* building_sums, int64_t sampling_nodes,
+                                  const int64_t* sampling_counts, const uint8_t* sampling_mask,
+                                  const float* sampling_sums, void* stream) {
+    if (!h || !stree_mask || !leaf_scalars || !building_counts || !building_mask || !building_sums ||
+        !sampling_counts || !sampling_mask || !sampling_sums)
+        return fail(RTPG_EINVAL, "rtpg_sdtree_import: null argument");
+    SDTreeDev& t = h->dev;
+    if (stree_nodes < 1 || leaves < 1 || stree_nodes != 2 * leaves - 1)
+        return fail(RTPG_EINVAL, "rtpg_sdtree_import: %lld STree nodes cannot hold %lld leaves", (long long)stree_nodes,
+                    (long long)leaves);
+    if (stree_nodes > (int64_t)t.cap_snodes || leaves > (int64_t)t.cap_dtrees)
+        return fail(RTPG_ECAPACITY, "rtpg_sdtree_import: %lld STree nodes / %lld leaves exceed the capacities %u / %u",
+                    (long long)stree_nodes, (long long)leaves, t.cap_snodes, t.cap_dtrees);
+    if (building_nodes > (int64_t)t.cap_nodes || sampling_nodes > (int64_t)t.cap_nodes)
+        return fail(RTPG_ECAPACITY, "rtpg_sdtree_import: quadtree nodes exceed the pool capacity %u", t.cap_nodes);
+    // STree: pre-order mask -> adjacent-children layout, breadth first; leaves keep their
+    // pre-order rank as DTree index (the order of the scalars and counts)
+    struct SN { int64_t c0 = -1, c1 = -1; int64_t leaf = -1; };
+    std::vector<SN> sn;
+    sn.reserve((size_t)stree_nodes);
+    {
+        std::vector<std::pair<int64_t, int>> stack;  // (node, children attached)
+        int64_t k = 0, leaf = 0;
+        auto take = [&]() -> int64_t {
+            const uint8_t m = stree_mask[k++];
+            SN n;
+            if (m == 0) n.leaf = leaf++;
+            else if (m != 1) return -2;
+            sn.push_back(n);
+            return (int64_t)sn.size() - 1;
+        };
+        const int64_t root = take();
+        if (root < 0) return fail(RTPG_EINVAL, "rtpg_sdtree_import: STree mask values must be 0 or 1");
+        if (sn[root].leaf < 0) stack.push_back({root, 0});
+        while (!stack.empty()) {
+            auto& top = stack.back();
+            if (top.second == 2) {
+                stack.pop_back();
+                continue;
+            }
+            if (k >= stree_nodes) return fail(RTPG_EINVAL, "rtpg_sdtree_import: STree stream ends inside the tree");
+            const int which = top.second++;
+            const int64_t parent = top.first;
+            const int64_t c = take();
+            if (c < 0) return fail(RTPG_EINVAL, "rtpg_sdtree_import: STree mask values must be 0 or 1");
+            (which == 0 ? sn[parent].c0 : sn[parent].c1) = c;
+            if (sn[c].leaf < 0) stack.push_back({c, 0});
+        }
+        if (k != stree_nodes || leaf != leaves)
+            return fail(RTPG_EINVAL, "rtpg_sdtree_import: STree stream does not match its sizes");
+    }
+    std::vector<uint32_t> snode((size_t)stree_nodes);
+    {
+        std::vector<int64_t> order(1, 0);  // breadth-first: order[i] = parsed node of device node i
+        for (size_t i = 0; i < order.size(); ++i) {
+            const SN& n = sn[order[i]];
+            if (n.leaf >= 0) {
+                snode[i] = kLeafBit | (uint32_t)n.leaf;
+            } else {
+                snode[i] = (uint32_t)order.size();
+                order.push_back(n.c0);
+                order.push_back(n.c1);
+            }
+        }
+    }
+    // quadtrees
+    const size_t L = (size_t)leaves;
+    std::vector<uint32_t> b_off(L), b_cnt(L), s_off(L), s_cnt(L);
+    std::vector<unsigned long long> b_statw(L);
+    std::vector<float> s_sum(L), s_area(L), s_statw(L);
+    std::vector<uint8_t> s_guided(L), b_nlvl(L);
+    std::vector<uint16_t> b_lvl(L * (kMaxLevels + 1), 0);
+    std::vector<unsigned long long> b_sums;
+    std::vector<ushort4> b_child;
+    std::vector<SNode> s_nodes;
+    const float scale = t.fx.scale;
+    auto fx = [&](float v, unsigned long long& out) -> bool {
+        const float s = v * scale;
+        if (!std::isfinite(s) || std::fabs(s) >= 9.2233720368547758e18f) return false;
+        out = (unsigned long long)std::llrint(s);
+        return true;
+    };
+    std::vector<QNode> q;
+    std::vector<uint32_t> order, lvl;
+    std::string err;
+    int64_t bpos = 0, spos = 0;
+    for (size_t d = 0; d < L; ++d) {
+        const float* sc = leaf_scalars + 4 * d;
+        if (!fx(sc[0], b_statw[d])) return fail(RTPG_EINVAL, "rtpg_sdtree_import: leaf %zu stat-weight not representable", d);
+        s_sum[d] = sc[1];
+        s_area[d] = sc[2];
+        s_statw[d] = sc[3];
+        // DTreeT::GetMean() > 0 (PG.h:447-451), as the build sets it
+        s_guided[d] = (sc[3] > 0.0f && (float)(kInv2Pi / (2.0f * sc[3])) * sc[1] > 0.0f) ? 1 : 0;
+        // building tree
+        if (!parse_dtree(building_mask, building_sums, building_nodes, bpos, building_counts[d], q, err))
+            return fail(RTPG_EINVAL, "rtpg_sdtree_import: building tree of leaf %zu: %s", d, err.c_str());
+        bpos += building_counts[d];
+        bfs_dtree(q, order, lvl);
+        if (order.size() > kDTreeNodeCap || lvl.size() - 1 > kMaxLevels)
+            return fail(RTPG_ECAPACITY, "rtpg_sdtree_import: building tree of leaf %zu exceeds %u nodes or %u levels", d,
+                        kDTreeNodeCap, kMaxLevels);
+        std::vector<uint32_t> rank(q.size());
+        for (size_t j = 0; j < order.size(); ++j) rank[order[j]] = (uint32_t)j;
+        b_off[d] = (uint32_t)b_child.size();
+        b_cnt[d] = (uint32_t)order.size();
+        b_nlvl[d] = (uint8_t)(lvl.size() - 1);
+        for (size_t l = 0; l < lvl.size(); ++l) b_lvl[d * (kMaxLevels + 1) + l] = (uint16_t)lvl[l];
+        for (uint32_t j : order) {
+            const QNode& n = q[j];
+            uint16_t c[4];
+            for (int k = 0; k < 4; ++k) {
+                c[k] = (n.mask & (1u << k)) ? (uint16_t)rank[n.child[k]] : (uint16_t)0;
+                unsigned long long v;
+                if (!fx(n.sums[k], v))
+                    return fail(RTPG_EINVAL, "rtpg_sdtree_import: building sum of leaf %zu not representable", d);
+                b_sums.push_back(v);
+            }
+            b_child.push_back(make_ushort4(c[0], c[1], c[2], c[3]));
+        }
+        // sampling tree
+        if (!parse_dtree(sampling_mask, sampling_sums, sampling_nodes, spos, sampling_counts[d], q, err))
+            return fail(RTPG_EINVAL, "rtpg_sdtree_import: sampling tree of leaf %zu: %s", d, err.c_str());
+        spos += sampling_counts[d];
+        bfs_dtree(q, order, lvl);
+        if (order.size() > kDTreeNodeCap)
+            return fail(RTPG_ECAPACITY, "rtpg_sdtree_import: sampling tree of leaf %zu exceeds %u nodes", d, kDTreeNodeCap);
+        rank.assign(q.size(), 0);
+        for (size_t j = 0; j < order.size(); ++j) rank[order[j]] = (uint32_t)j;
+        s_off[d] = (uint32_t)s_nodes.size();
+        s_cnt[d] = (uint32_t)order.size();
+        for (uint32_t j : order) {
+            const QNode& n = q[j];
+            SNode nd;
+            nd.sums = make_float4(n.sums[0], n.sums[1], n.sums[2], n.sums[3]);
+            uint16_t c[4];
+            for (int k = 0; k < 4; ++k) c[k] = (n.mask & (1u << k)) ? (uint16_t)rank[n.child[k]] : (uint16_t)0;
+            nd.child = make_ushort4(c[0], c[1], c[2], c[3]);
+            nd.pad0 = nd.pad1 = 0;
+            s_nodes.push_back(nd);
+        }
+    }
+    if (bpos != building_nodes || spos != sampling_nodes)
+        return fail(RTPG_EINVAL, "rtpg_sdtree_import: quadtree streams hold nodes beyond the leaves' counts");
+    if (b_child.size() > t.cap_nodes || s_nodes.size() > t.cap_nodes)
+        return fail(RTPG_ECAPACITY, "rtpg_sdtree_import: quadtree nodes exceed the pool capacity %u", t.cap_nodes);
+    cudaStream_t st = as_stream(stream);
+    const uint32_t counts[3] = {(uint32_t)stree_nodes, (uint32_t)leaves, (uint32_t)b_child.size()};
+    RTPG_CUDA(cudaMemcpyAsync(t.counts, counts, sizeof(counts), cudaMemcpyHostToDevice, st));
+    RTPG_CUDA(ul(t.snode, snode, st));
+    RTPG_CUDA(ul(t.b_off, b_off, st));
+    RTPG_CUDA(ul(t.b_cnt, b_cnt, st));
+    RTPG_CUDA(ul(t.s_off, s_off, st));
+    RTPG_CUDA(ul(t.s_cnt, s_cnt, st));
+    RTPG_CUDA(ul(t.b_statw, b_statw, st));
+    RTPG_CUDA(ul(t.s_sum, s_sum, st));
+    RTPG_CUDA(ul(t.s_area, s_area, st));
+    RTPG_CUDA(ul(t.s_statw, s_statw, st));
+    RTPG_CUDA(ul(t.s_guided, s_guided, st));
+    RTPG_CUDA(ul(t.b_lvl, b_lvl, st));
+    RTPG_CUDA(ul(t.b_nlvl, b_nlvl, st));
+    RTPG_CUDA(ul(t.b_sums, b_sums, st));
+    RTPG_CUDA(ul(t.b_child, b_child, st));
+    RTPG_CUDA(ul(t.s_nodes, s_nodes, st));
+    // the host vectors must outlive the copies
+    RTPG_CUDA(cudaStreamSynchronize(st));
     return RTPG_OK;
 }
 

@@ -623,7 +623,10 @@ __global__ void __launch_bounds__(kMlpThreads) k_mlp_lobes(TracerDev T, uint32_t
             for (int k = 0; k < kMlpIn; ++k) f[k] = 0.0f;
         store_features(x0, t, f);
         float o[kMlpOut];
-        ok &= mlp_forward_tile(tmem, sw, x0, mbar, phase, o);
+        if (!mlp_forward_tile(T.ml.dev, tmem, sw, x0, mbar, phase, o)) {
+            ok = false;  // uniform over the CTA: issue nothing more
+            break;
+        }
         if (live) {
             VmfLobe L[kMlpLobes];
             mlp_head(o, L);
@@ -642,7 +645,10 @@ __global__ void __launch_bounds__(kMlpThreads) k_mlp_lobes(TracerDev T, uint32_t
             for (int k = 0; k < 5; ++k) dst[k] = reinterpret_cast<const uint4*>(lp)[k];
         }
     }
-    if (!ok) atomicOr(T.status, RTPG_STATUS_TIMEOUT);
+    if (!ok) {
+        if (t == 0) atomicOr(T.status, RTPG_STATUS_TIMEOUT);
+        mma_drain(mbar, phase, T.ml.dev.poll_limit);
+    }
     tc_fence_before();
     __syncthreads();
     tc_fence_after();

@@ -73,3 +73,8 @@ class MLPGuide:
         s = C.c_uint32()
         call("rtpg_mlp_status", self.h, C.byref(s), int(bool(clear)), stream_ptr(stream))
         return s.value
+
+    def set_wait_test(self, skip_mma, poll_limit=0):
+        """Test mode of the bounded tensor-core waits: skip_mma=True issues no MMA, so every
+        wait runs out after poll_limit polls and the kernels report RTPG_STATUS_TIMEOUT."""
+        call("rtpg_mlp_set_wait_test", self.h, int(bool(skip_mma)), int(poll_limit))

@@ -117,6 +117,19 @@ class SDTree:
              stream_ptr(stream))
         return e
 
+    def import_(self, building: Export, sampling: Export, stream=None):
+        """Replace the tree with the one two exports (building, sampling) describe."""
+        b, s = building, sampling
+        if b.smask.tobytes() != s.smask.tobytes() or b.counts.shape != s.counts.shape:
+            raise ValueError("building and sampling exports describe different spatial trees")
+        a = lambda x, t: np.ascontiguousarray(x, t)
+        smask, scal = a(s.smask, np.uint8), a(s.scalars, np.float32)
+        bc, bm, bs = a(b.counts, np.int64), a(b.dmask, np.uint8), a(b.dsums, np.float32)
+        sc, sm, ss = a(s.counts, np.int64), a(s.dmask, np.uint8), a(s.dsums, np.float32)
+        call("rtpg_sdtree_import", self.h, int(smask.shape[0]), int(sc.shape[0]), smask.ctypes.data, scal.ctypes.data,
+             int(bm.shape[0]), bc.ctypes.data, bm.ctypes.data, bs.ctypes.data, int(sm.shape[0]), sc.ctypes.data,
+             sm.ctypes.data, ss.ctypes.data, stream_ptr(stream))
+
 
 class SDTreeController:
     """RTSTreeControllerT(tree, sampleForBudget, iterationForBuilt=0, ratioForBudget=0.5,

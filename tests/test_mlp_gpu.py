@@ -96,3 +96,32 @@ def test_training_lowers_loss(cuda):
     # reaches about -1.5
     assert l0 > 1.5 and l1 < 0.0, (l0, l1)
     assert g.status() == 0
+
+
+def test_bounded_wait_times_out(cuda):
+    """A completion wait that nothing will ever satisfy gives up after its poll limit: in the
+    test mode no MMA and no commit is issued (nothing is in flight), the kernels set
+    RTPG_STATUS_TIMEOUT, free their tensor memory and return, and the context stays usable."""
+    import torch
+    from rtlib_b200.mlp import MLPGuide
+    timeout_bit = 0x40
+    rng = np.random.default_rng(12)
+    g = MLPGuide(MN, MX, seed=13)
+    n = 512
+    pos, nrm, wo = (_t(a, cuda) for a in _inputs(rng, n))
+    wi = _t(_unit(rng, n), cuda)
+    w = _t(np.ones(n, np.float32), cuda)
+    ref = g.eval(pos, nrm, wo).cpu().numpy()
+    assert g.status() == 0
+    g.set_wait_test(True, poll_limit=256)
+    g.eval(pos, nrm, wo)
+    torch.cuda.synchronize()
+    assert g.status(clear=True) & timeout_bit
+    _, grad = g.loss_grad(pos, nrm, wo, wi, w)
+    torch.cuda.synchronize()
+    assert g.status(clear=True) & timeout_bit
+    assert not grad.any().item()  # incomplete accumulators are not flushed
+    g.set_wait_test(False)
+    again = g.eval(pos, nrm, wo).cpu().numpy()
+    assert np.array_equal(again, ref)
+    assert g.status() == 0

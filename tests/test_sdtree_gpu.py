@@ -223,3 +223,95 @@ def test_controller_schedule(cuda):
     want = [(a, b) for a, b, _, _ in _schedule(100, 0, 0.5, 1)]
     assert got == want
     assert {g[1] for g in got} == set(range(max(g[1] for g in got) + 1))
+
+
+def _two_pass(g, o, rec, dev, n_refines=2):
+    P, U, R = _t(rec["pos"], dev), _t(rec["uv"], dev), _t(rec["radiance"], dev)
+    for it in range(1, n_refines + 1):
+        if g is not None:
+            g.record(P, U, R)
+            g.build()
+            g.refine(W.spatial_threshold(it) // 16)
+        if o is not None:
+            o.record(rec["pos"], rec["uv"], rec["radiance"])
+            o.build()
+            o.refine(W.spatial_threshold(it) // 16)
+    if g is not None:
+        g.record(P, U, R)
+    if o is not None:
+        o.record(rec["pos"], rec["uv"], rec["radiance"])
+
+
+def test_import_round_trip(cuda):
+    """export -> import into a fresh handle -> export gives identical building and sampling
+    streams, and the imported tree samples exactly as the original."""
+    import torch
+    from rtlib_b200.sdtree import SDTree
+    rec = W.sdtree_records(1 << 16, 21)
+    g = SDTree((0, 0, 0), (1, 1, 1))
+    _two_pass(g, None, rec, cuda)
+    g.build()  # sampling trees from the last records; building trees keep their sums
+    eb, es = g.export(sampling=False), g.export(sampling=True)
+    assert len(eb.counts) > 8 and eb.dmask.shape[0] > len(eb.counts)
+    h = SDTree((0, 0, 0), (1, 1, 1))
+    h.import_(eb, es)
+    _same_export(h.export(sampling=False), eb)
+    _same_export(h.export(sampling=True), es)
+    assert h.stats() == g.stats()
+    q = W.sdtree_queries(1 << 14, 22)
+    outs = []
+    for t in (g, h):
+        uv = torch.empty((q["pos"].shape[0], 2), dtype=torch.float32, device=cuda)
+        pdf = torch.empty(q["pos"].shape[0], dtype=torch.float32, device=cuda)
+        t.sample_pdf(_t(q["pos"], cuda), _t(q["seeds"], cuda), out_uv=uv, out_pdf_uv=pdf)
+        outs.append((uv.cpu().numpy(), pdf.cpu().numpy()))
+    np.testing.assert_array_equal(outs[0][0], outs[1][0])
+    np.testing.assert_array_equal(outs[0][1], outs[1][1])
+    assert h.status() == 0
+
+
+def test_import_oracle_tree_then_continue(cuda, oracle):
+    """A tree built by the CPU oracle, imported to the GPU, samples bit-identically; recording
+    into it, building and refining then stays bit-identical to the oracle continuing alone."""
+    from rtlib_b200.sdtree import SDTree
+    rec = W.sdtree_records(1 << 16, 31)
+    o = oracle.sdtree((0, 0, 0), (1, 1, 1))
+    _two_pass(None, o, rec, cuda)
+    o.build()
+    g = SDTree((0, 0, 0), (1, 1, 1))
+    g.import_(o.export(sampling=False), o.export(sampling=True))
+    _same_export(g.export(sampling=True), o.export(sampling=True))
+    _queries(g, o, W.sdtree_queries(1 << 14, 32), cuda)
+    # continue: refine, record a new batch, build
+    th = W.spatial_threshold(3) // 16
+    g.refine(th)
+    o.refine(th)
+    rec2 = W.sdtree_records(1 << 16, 33)
+    g.record(_t(rec2["pos"], cuda), _t(rec2["uv"], cuda), _t(rec2["radiance"], cuda))
+    o.record(rec2["pos"], rec2["uv"], rec2["radiance"])
+    g.build()
+    o.build()
+    _same_export(g.export(sampling=True), o.export(sampling=True))
+    _queries(g, o, W.sdtree_queries(1 << 14, 34), cuda)
+    assert g.status() == 0
+
+
+def test_import_rejects_inconsistent_streams(cuda):
+    from rtlib_b200._lib import RtpgError
+    from rtlib_b200.sdtree import SDTree
+    rec = W.sdtree_records(1 << 14, 41)
+    g = SDTree((0, 0, 0), (1, 1, 1))
+    _two_pass(g, None, rec, cuda, n_refines=1)
+    g.build()
+    eb, es = g.export(sampling=False), g.export(sampling=True)
+    h = SDTree((0, 0, 0), (1, 1, 1))
+    bad = type(eb)(eb.smask, eb.scalars, eb.counts.copy(), eb.dmask, eb.dsums)
+    bad.counts[0] += 1  # node counts no longer add up to the stream
+    with pytest.raises(RtpgError):
+        h.import_(bad, es)
+    small = SDTree((0, 0, 0), (1, 1, 1), max_dtrees=4)
+    with pytest.raises(RtpgError):
+        small.import_(eb, es)
+    # the failed imports left the handles usable
+    h.import_(eb, es)
+    _same_export(h.export(sampling=True), es)
