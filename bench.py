@@ -33,7 +33,9 @@ the work of all ranks over the slowest rank's time.
 
 --impl reference runs the CPU implementation of the same workload on this machine's host
 cores: RTLib's own SD-tree code (oracle/_ref) for "sdtree"; for "cornell", where RTLib's
-integrator exists only as OptiX programs, the CPU restatement of that integrator (oracle/).
+integrator exists only as OptiX programs, the CPU restatement of that integrator (oracle/)
+rendering the same 512 x 512 image into one shared SD-tree over all host threads, each step
+the pass schedule truncated at 15 spp (a bounded sample of the 2047-spp step).
 """
 from __future__ import annotations
 
@@ -246,7 +248,8 @@ def bench_sdtree_ours(args, rank, world):
     h2d = sum(x.numel() * x.element_size() for x in hp.values())
     d2h = h_dir.numel() * 4 + h_pdf.numel() * 4
     e2e_ms = []
-    for k in range(args.warmup + args.steps):
+    e2e_steps = getattr(args, "e2e_steps", None) or args.steps
+    for k in range(args.warmup + e2e_steps):
         flush.fill_(k & 0xff)
         a, c = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record(stream)
@@ -343,6 +346,29 @@ def cpu_baseline_sdtree():
                        "build_refine_ms": 1e3 * statistics.median(p[1] for p in ph),
                        "sample_pdf_Mq_s": N_Q / statistics.median(p[2] for p in ph) / 1e6,
                        "sample_pdf_1thread_Mq_s": _ref_sample_1thread(kind)}}
+
+
+# steps of the config-1 SD-tree sub-record of the default line: ~0.15 ms each, so that the
+# timed region spans a few hundred milliseconds of clock samples
+SUB_SDTREE_STEPS = 2000
+
+
+def sdtree_subrecord(args, rank, world):
+    """Config 1 (SD-tree standalone) measured inside the default workload's run: the same
+    record -> build -> refine -> sample+pdf step as --workload sdtree, with its own clocks,
+    rooflines and the host-side rate of RTLib's own SD-tree code as its CPU baseline."""
+    sub = argparse.Namespace(**vars(args))
+    sub.steps, sub.warmup, sub.passes, sub.e2e_steps = SUB_SDTREE_STEPS, 20, 1, 20
+    r = bench_sdtree_ours(sub, rank, world)
+    out = {"metric": r["metric"], "value": r["value"], "unit": r["unit"], "steps": sub.steps, "warmup": sub.warmup,
+           "ms_per_step": r["ms_per_step"],
+           "config": {"workload": "sdtree-standalone: 2^20 records, refine at 12000*sqrt(2), 2^22 sample+pdf",
+                      "records": N_REC, "queries": N_Q, "l2": "flushed (256 MiB write) before every timed step"},
+           "e2e": dict(r["e2e"], steps=sub.e2e_steps), "roofline": r["roofline"], "roofline_record": r["roofline_record"],
+           "phases": r["phases"], "clocks": r["clocks"], "gpu_launches": r["gpu_launches"], "sdtree": r["sdtree"]}
+    if rank == 0 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline_sdtree()
+    return out
 
 
 def _ref_sample_1thread(kind, n=1 << 18):
@@ -488,31 +514,37 @@ def bench_cornell_ours(args, rank, world):
     }
 
 
-def _cornell_cpu(threads, seconds, scene_px=32):
-    """Independent replicas of the guided render at scene_px^2 pixels with the same pass
-    schedule on the CPU restatement of the integrator, one per thread."""
-    import concurrent.futures as cf
+# budget of the host-side sample of the Cornell workload: passes of 1, 2, 4 and 8 spp (16
+# launches) of the same 512 x 512 render; the full 2047-spp schedule would take many minutes
+C_REF_BUDGET = 15
 
+
+def _cornell_cpu_step(threads, budget=C_REF_BUDGET):
+    """One host-side step: the guided 512 x 512 render of the pass schedule truncated at
+    `budget` spp on the CPU restatement of the integrator, every frame split into pixel bands
+    over `threads` host threads that record into one shared SD-tree (exact fixed-point merge
+    after each frame).  Returns (paths, seconds)."""
     from oracle.oracle import Oracle, OracleRenderer
     from rtlib_b200 import scenes
     o = Oracle()
-    sc = scenes.cornell_box(scene_px, scene_px)
-
-    def one(_):
-        t = o.sdtree(*C_AABB)
-        r = OracleRenderer(o, sc, max_depth=C_MAX_DEPTH, fraction=C_FRACTION, width=scene_px, height=scene_px)
-        r.render_guided(t, C_BUDGET, ratio_for_budget=1.0)
-        return r.samples * scene_px * scene_px
-
-    paths = 0
+    sc = scenes.cornell_box(C_W, C_H)
+    t = o.sdtree(*C_AABB)
+    r = OracleRenderer(o, sc, max_depth=C_MAX_DEPTH, fraction=C_FRACTION, width=C_W, height=C_H)
     t0 = time.perf_counter()
-    with cf.ThreadPoolExecutor(threads) as ex:
-        while True:
-            paths += sum(ex.map(one, range(threads)))
-            if time.perf_counter() - t0 >= seconds:
-                break
+    r.render_guided(t, budget, ratio_for_budget=1.0, threads=threads)
     dt = time.perf_counter() - t0
-    return paths / dt / 1e6, dt, paths
+    return r.samples * C_W * C_H, dt
+
+
+def _cornell_cpu(threads, seconds):
+    """Host-side Mpaths/s: repeated steps (at least one) for about `seconds`."""
+    paths, dt, n = 0, 0.0, 0
+    while n == 0 or dt < seconds:
+        p, d = _cornell_cpu_step(threads)
+        paths += p
+        dt += d
+        n += 1
+    return paths / dt / 1e6, dt, paths, n
 
 
 # ---------------------------------------------------------------------------- occluded workload
@@ -1043,6 +1075,8 @@ def main():
                     help="sdtree: record+build+refine passes before the queries (1 = the literal config; 2 = "
                          "the same records again into the refined topology)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-sdtree-subrecord", action="store_true",
+                    help="cornell: skip the config-1 SD-tree sub-record of the line")
     ap.add_argument("--scale-log2", type=int, default=0,
                     help="hashgrid: divide points, queries and slots by 2^k (small cases for profiling)")
     ap.add_argument("--budget", type=int, default=2047,
@@ -1129,12 +1163,40 @@ def main():
             return 0
         cores = os.cpu_count() or 1
         if cornell:
-            _cornell_cpu(cores, 0.0, scene_px=16)  # warm-up (builds the oracle, pages in)
-            v, dt, paths = _cornell_cpu(cores, 20.0)
+            for _ in range(args.warmup):
+                _cornell_cpu_step(cores)
+            step_s, paths = [], 0
+            for _ in range(args.steps):
+                p, d = _cornell_cpu_step(cores)
+                paths += p
+                step_s.append(d)
+            dt = sum(step_s)
+            v = paths / dt / 1e6
             kind, threads = "port", cores
-            sample = (f"{cores} independent replicas of the guided render at 32x32 px with the same 2048-launch "
-                      f"pass schedule on the CPU restatement of RTLib's integrator; {paths} paths in {dt:.1f} s")
-            ms = dt * 1e3
+            sample = (f"each step: the same 512x512 guided render (NEE, depth 8, SD-tree fraction 0.5) over the pass "
+                      f"schedule truncated at {C_REF_BUDGET} spp ({C_REF_BUDGET + 1} launches of passes 1, 2, 4, 8), "
+                      f"every frame split into pixel bands over {cores} host threads recording into one shared "
+                      f"SD-tree; CPU restatement of RTLib's integrator (its own exists only as OptiX programs); "
+                      f"{paths} paths in {dt:.1f} s over {args.steps} steps")
+            ms = dt * 1e3 / args.steps
+            # the config-1 SD-tree sub-record of the default line, on RTLib's own code
+            kind_s = _ref_kind()
+            thr_s = cores if kind_s == "reference" else 1
+            _ref_workload(kind_s, thr_s, reps=1)
+            ph = []
+            times_s = _ref_workload(kind_s, thr_s, reps=5, phases=ph)
+            sec_s = sum(times_s) / len(times_s)
+            sdtree_sub = {"metric": "SD-tree record+refine+sample throughput (config 1)",
+                          "value": (N_REC + N_Q) / sec_s / 1e6, "unit": "Mops/s", "steps": len(times_s),
+                          "ms_per_step": sec_s * 1e3,
+                          "cpu_baseline": {"value": (N_REC + N_Q) / sec_s / 1e6, "unit": "Mops/s", "cores": thr_s,
+                                           "kind": kind_s,
+                                           "sample": "full config-1 passes (2^20 records, refine, 2^22 queries); "
+                                                     "record/build/refine single-threaded as in RTLib, sample+pdf on "
+                                                     f"{thr_s} thread(s)"},
+                          "phases": {"record_Mrec_s": N_REC / statistics.median(p[0] for p in ph) / 1e6,
+                                     "build_refine_ms": 1e3 * statistics.median(p[1] for p in ph),
+                                     "sample_pdf_Mq_s": N_Q / statistics.median(p[2] for p in ph) / 1e6}}
         elif hashgrid:
             cpu_baseline_hashgrid(seconds=0.0)  # warm-up (pages in)
             cb = cpu_baseline_hashgrid(seconds=20.0)
@@ -1153,6 +1215,8 @@ def main():
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": cfg,
                 "cpu_baseline": {"value": v, "unit": unit, "cores": threads, "kind": kind, "sample": sample},
                 "e2e": {"value": v, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        if cornell and not args.no_sdtree_subrecord:
+            line["sdtree_config1"] = sdtree_sub
         print(json.dumps(line), flush=True)
         return 0
 
@@ -1175,13 +1239,18 @@ def main():
               "inference", "queries_found", "grid_status"):
         if k in res:
             line[k] = res[k]
+    if cornell and not args.no_sdtree_subrecord:
+        # the north star's SD-tree target (config 1) measured in the same run
+        line["sdtree_config1"] = sdtree_subrecord(args, rank, world)
     if rank == 0 and not args.no_cpu_baseline and not occluded and not mlp:
         if cornell:
             cores = os.cpu_count() or 1
-            v, dt, paths = _cornell_cpu(cores, 10.0)
+            v, dt, paths, n = _cornell_cpu(cores, 10.0)
             line["cpu_baseline"] = {"value": v, "unit": "Mpaths/s", "cores": cores, "kind": "port",
-                                    "sample": f"{cores} replicas of the guided render at 32x32 px, full pass "
-                                              f"schedule, CPU restatement of the integrator; {paths} paths in {dt:.1f} s"}
+                                    "sample": f"{n} x the same 512x512 guided render over the pass schedule truncated "
+                                              f"at {C_REF_BUDGET} spp, pixel bands over {cores} host threads into one "
+                                              f"shared SD-tree, CPU restatement of the integrator; {paths} paths in "
+                                              f"{dt:.1f} s"}
         elif hashgrid:
             line["cpu_baseline"] = cpu_baseline_hashgrid()
         else:

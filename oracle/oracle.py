@@ -447,11 +447,35 @@ class OracleRenderer:
         self.accum = np.zeros(3 * o.width * o.height, np.float64)
         self.samples = 0
 
-    def render(self, spp, flags, tree=None, grid=None):
-        for _ in range(spp):
-            self.L.or_render(C.byref(self.sc), int(flags), tree.h if tree is not None else None,
-                             C.byref(grid.g) if grid is not None else None, 0, self.width * self.height, self.seeds,
-                             self.accum)
+    def render(self, spp, flags, tree=None, grid=None, threads=1):
+        """spp samples per pixel.  threads > 1 splits every frame into bands of pixels rendered
+        on that many host threads; an SD-tree then receives each band's records in a private
+        shadow that is merged into it exactly after the frame (grid guides stay single-threaded)."""
+        npx = self.width * self.height
+        if threads <= 1 or grid is not None:
+            for _ in range(spp):
+                self.L.or_render(C.byref(self.sc), int(flags), tree.h if tree is not None else None,
+                                 C.byref(grid.g) if grid is not None else None, 0, npx, self.seeds, self.accum)
+            self.samples += spp
+            return
+        import concurrent.futures as cf
+        L = self.L
+        L.or_sdtree_shadow_new.argtypes = [P]
+        L.or_sdtree_shadow_new.restype = P
+        L.or_sdtree_shadow_merge.argtypes = [P, P]
+        bands = [(npx * k // threads, npx * (k + 1) // threads) for k in range(threads)]
+        with cf.ThreadPoolExecutor(threads) as ex:
+            for _ in range(spp):
+                shadows = [L.or_sdtree_shadow_new(tree.h) if tree is not None else None for _ in bands]
+
+                def one(k):
+                    a, b = bands[k]
+                    L.or_render(C.byref(self.sc), int(flags), shadows[k], None, a, b, self.seeds, self.accum)
+
+                list(ex.map(one, range(threads)))
+                if tree is not None:
+                    for sh in shadows:
+                        L.or_sdtree_shadow_merge(tree.h, sh)
         self.samples += spp
 
     def image(self):
@@ -470,7 +494,7 @@ class OracleRenderer:
         for i, c in enumerate(rgb):
             self.mats[light_material_first + i].emission[:] = [float(x) for x in c]
 
-    def render_guided(self, tree, budget, ratio_for_budget=1.0, iteration_for_built=0, base_flags=1):
+    def render_guided(self, tree, budget, ratio_for_budget=1.0, iteration_for_built=0, base_flags=1, threads=1):
         """RTSTreeControllerT::BegTrace / EndTrace (OPX7UtilsPathGuiding.h:1808-1887) with one
         sample per launch, flags by state as the application sets them."""
         remain, pas, per_all, per_tmp, it = budget, 0, 0, 0, 0
@@ -485,7 +509,7 @@ class OracleRenderer:
             flags = (base_flags & 3) | 8
             if it > iteration_for_built:
                 flags |= 16 if remain > pas else 16 | 32
-            self.render(1, flags, tree)
+            self.render(1, flags, tree, threads=threads)
             per_all += 1
             per_tmp += 1
             if per_tmp >= pas:

@@ -530,6 +530,38 @@ void or_sdtree_pdf(void* h, int64_t n, const float* pos, const float* uv, float*
 uint32_t or_sdtree_num_stree_nodes(void* h) { return ((OSDTree*)h)->nst; }
 uint32_t or_sdtree_num_dtrees(void* h) { return ((OSDTree*)h)->ndt; }
 
+/* Thread-private record target of a tree, for rendering one frame on several host threads
+ * into one shared tree: the shadow shares the tree's topology and sampling trees (read only
+ * while it exists) and has its own zeroed building sums and stat-weights, which
+ * or_sdtree_shadow_merge adds into the tree.  Fixed-point sums make the merged result the
+ * same as recording every vertex into the tree on one thread, in any order. */
+void* or_sdtree_shadow_new(void* h) {
+    const OSDTree* t = (const OSDTree*)h;
+    OSDTree* s = (OSDTree*)malloc(sizeof(OSDTree));
+    *s = *t;
+    s->status = 0;
+    s->dt = (ODTree*)malloc(sizeof(ODTree) * (t->ndt ? t->ndt : 1));
+    s->capdt = t->ndt;
+    for (uint32_t i = 0; i < t->ndt; ++i) {
+        s->dt[i] = t->dt[i];
+        s->dt[i].bsum = (int64_t*)calloc(4 * (size_t)t->dt[i].nb, sizeof(int64_t));
+        s->dt[i].bstatw = 0;
+    }
+    return s;
+}
+void or_sdtree_shadow_merge(void* h, void* shadow) {
+    OSDTree* t = (OSDTree*)h;
+    OSDTree* s = (OSDTree*)shadow;
+    for (uint32_t i = 0; i < t->ndt; ++i) {
+        for (size_t k = 0; k < 4 * (size_t)t->dt[i].nb; ++k) t->dt[i].bsum[k] += s->dt[i].bsum[k];
+        t->dt[i].bstatw += s->dt[i].bstatw;
+        free(s->dt[i].bsum);
+    }
+    t->status |= s->status;
+    free(s->dt);
+    free(s);
+}
+
 /* ------------------------------------------------------------------ hash grid */
 /* Cell coordinates as DoubleBufferedHashGrid3T::FindFromCur/Prv compute them
  * (OPX7UtilsGrid.h:189-199): uint(bounds * (p - off) / size), clamped to bounds-1; negative
