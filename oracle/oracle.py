@@ -599,3 +599,100 @@ class OracleGrid:
     @property
     def status(self):
         return self.g.status
+
+
+# ------------------------------------------------------------------ integrator known answers
+class IntegratorKAT:
+    """The integrator's building blocks one call at a time, on the C restatement (``Oracle``)
+    or on RTLib's own code run on the host (``Reference``): cosine and Phong lobe sampling,
+    random_in_unit_triangle, Reservoir::Update, MeshLightList::Sample and the whole
+    closest-hit shading of a vertex.  Xorshift32 seeds go in, end states come out."""
+
+    def __init__(self, checker, scene, max_depth=8, num_candidates=32, fraction=0.5):
+        self.ref = isinstance(checker, Reference)
+        self.L = L = checker.L
+        self.max_depth, self.num_candidates, self.fraction = max_depth, num_candidates, fraction
+        pre = "ref_kat_" if self.ref else "or_kat_"
+        self.fn = {k: getattr(L, pre + k) for k in ("cosine", "phong", "triangle", "reservoir", "light", "shade")}
+        for k in ("cosine", "triangle"):
+            self.fn[k].argtypes = [C.c_int64, _f, _u32, _f]
+        self.fn["phong"].argtypes = [C.c_int64, _f, _f, _u32, _f]
+        self.fn["reservoir"].argtypes = [C.c_int64, C.c_int32, _f, _f, np.ctypeslib.ndpointer(np.int32), _f, _u32]
+        case = [C.c_int64, _f, _f, _f, _u32, _f, _u32, _u32, _u32, _f, _u32]
+        if self.ref:
+            self.fn["light"].argtypes = [C.c_int64, _f, _u32, _f]
+            self.fn["shade"].argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, P, C.c_float] + case
+            mats = scene["materials"]
+            mf = np.array([[*m["diffuse"], *m["specular"], *m["emission"], m["shininess"], m["ref_index"]]
+                           for m in mats], np.float32)
+            mt = np.array([m["type"] for m in mats], np.int32)
+            L.ref_kat_set_scene.argtypes = [_f, C.c_uint32, _u32, _f, np.ctypeslib.ndpointer(np.int32), C.c_uint32,
+                                            _u32, _u32, _u32, _f, C.c_uint32]
+            tv = np.ascontiguousarray(scene["tri_v"], np.float32)
+            L.ref_kat_set_scene(tv, tv.shape[0], np.ascontiguousarray(scene["tri_mat"], np.uint32), mf, mt, len(mats),
+                                np.ascontiguousarray(scene["light_tris"], np.uint32),
+                                np.ascontiguousarray(scene["light_first"], np.uint32),
+                                np.ascontiguousarray(scene["light_count"], np.uint32),
+                                np.ascontiguousarray(scene["light_emission"], np.float32), len(scene["light_first"]))
+        else:
+            self.fn["light"].argtypes = [P, C.c_int64, _f, _u32, _f]
+            self.fn["shade"].argtypes = [P, C.c_uint32, P] + case
+            self.r = OracleRenderer(checker, scene, max_depth=max_depth, num_candidates=num_candidates,
+                                    fraction=fraction, width=1, height=1)
+
+    @staticmethod
+    def _a(x, t):
+        return np.ascontiguousarray(x, t)
+
+    def cosine(self, normal, seeds):
+        st = self._a(seeds, np.uint32).copy()
+        out = np.empty((st.shape[0], 3), np.float32)
+        self.fn["cosine"](st.shape[0], self._a(normal, np.float32), st, out)
+        return out, st
+
+    def phong(self, refl, shininess, seeds):
+        st = self._a(seeds, np.uint32).copy()
+        out = np.empty((st.shape[0], 3), np.float32)
+        self.fn["phong"](st.shape[0], self._a(refl, np.float32), self._a(shininess, np.float32), st, out)
+        return out, st
+
+    def triangle(self, verts, seeds):
+        st = self._a(seeds, np.uint32).copy()
+        out = np.empty((st.shape[0], 3), np.float32)
+        self.fn["triangle"](st.shape[0], self._a(verts, np.float32), st, out)
+        return out, st
+
+    def reservoir(self, w, rnd):
+        w, rnd = self._a(w, np.float32), self._a(rnd, np.float32)
+        k = w.shape[0]
+        sel, ws, m = np.empty(k, np.int32), np.empty(k, np.float32), np.empty(k, np.uint32)
+        self.fn["reservoir"](k, w.shape[1], w, rnd, sel, ws, m)
+        return sel, ws, m
+
+    def light(self, p_in, seeds):
+        st = self._a(seeds, np.uint32).copy()
+        out = np.empty((st.shape[0], 14), np.float32)
+        if self.ref:
+            self.fn["light"](st.shape[0], self._a(p_in, np.float32), st, out)
+        else:
+            self.fn["light"](C.byref(self.r.sc), st.shape[0], self._a(p_in, np.float32), st, out)
+        return out, st
+
+    def shade(self, flags, cases, tree=None):
+        """cases: org, dir (n x 3), t, prim, thr (n x 3), pflags, depth, seeds.  Returns the 17
+        floats per case (position, direction, throughput after, BSDF value, radiance added,
+        cosine, woPdf), the hit flags and the end states.  tree: a matching RefSDTree or
+        OracleSDTree for USE_TREE."""
+        c = cases
+        st = self._a(c["seeds"], np.uint32).copy()
+        n = st.shape[0]
+        out, fl = np.empty((n, 17), np.float32), np.empty(n, np.uint32)
+        args = (n, self._a(c["org"], np.float32), self._a(c["dir"], np.float32), self._a(c["t"], np.float32),
+                self._a(c["prim"], np.uint32), self._a(c["thr"], np.float32), self._a(c["pflags"], np.uint32),
+                self._a(c["depth"], np.uint32), st, out, fl)
+        th = tree.h if tree is not None else None
+        if self.ref:
+            self.fn["shade"](int(flags), self.max_depth, self.num_candidates, th, self.fraction, *args)
+        else:
+            self.fn["shade"](C.byref(self.r.sc), int(flags), th, *args)
+        return out, fl, st

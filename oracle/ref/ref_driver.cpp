@@ -374,3 +374,220 @@ void ref_mqt_sample_pdf(int64_t n, uint32_t level, uint32_t count_per_cell, cons
 uint32_t ref_morton2_code(uint32_t x, uint32_t y) { return Morton2Utils<3>::GetCodeFromPosIdx((unsigned char)x, (unsigned char)y); }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------- integrator known answers
+// RTLib's closest-hit shading (SimpleGuide.cu:287-496), its light sampling and reservoir
+// (SimpleKernel.h:26-143) and its BSDF sampling helpers (SimpleGuide.cu:28-47), staged by
+// stage_ref.py, run on the host.  What the OptiX launch would supply comes from here:
+// textures are white (tex2D returns 1), `params` holds the flags, the light list and the
+// SD-tree view, and TraceOccluded is answered by brute force over the scene's triangles.
+#include <cstdio>
+template <class T>
+inline T tex2D(cudaTextureObject_t, float, float) { return T{}; }
+template <>
+inline float4 tex2D<float4>(cudaTextureObject_t, float, float) { return make_float4(1.0f, 1.0f, 1.0f, 1.0f); }
+#include <rtlib_kat/ShadeTypes.h>
+namespace rtlib { namespace test {
+using DTreeWrapper = DTreeWrapperT<24>;
+using STree = STreeT<69, 24>;
+} }
+struct KatHitgroup { int type; };
+struct KatUserData { float3 throughPut; unsigned int depth; };
+struct KatHitRecord { unsigned int seed; unsigned int flags; KatUserData userData; };
+struct KatShadeOut {
+    float3 position, direction, currThroughput, bsdfVal, radiance;
+    float cosine, woPdf;
+    unsigned int flags, seed;
+};
+struct KatParams {
+    unsigned int flags, maxDepth, numCandidates;
+    int gasHandle;
+    MeshLightList lights;
+    rtlib::test::STree tree;
+};
+static KatParams params;  // the launch parameters the staged closest-hit body reads
+
+struct KatScene {
+    std::vector<float> tri_v;      // 9 per triangle
+    std::vector<uint32_t> tri_mat;
+    std::vector<float> mat_f;      // 11 per material: diffuse, specular, emission, shininess, refIndex
+    std::vector<int> mat_type;     // HitgroupType
+    std::vector<std::vector<float3>> lv;
+    std::vector<std::vector<uint3>> li;
+    std::vector<std::vector<float2>> lt;
+    std::vector<MeshLight> lights;
+};
+static KatScene g_kat;
+
+// TraceOccluded (SimpleKernel.h:357-366): any hit in (tmin, tmax), Moller-Trumbore
+static bool TraceOccluded(int, float3 o, float3 d, float tmin, float tmax) {
+    const size_t nt = g_kat.tri_mat.size();
+    for (size_t k = 0; k < nt; ++k) {
+        const float* q = g_kat.tri_v.data() + 9 * k;
+        const float3 v0 = make_float3(q[0], q[1], q[2]);
+        const float3 e1 = make_float3(q[3] - q[0], q[4] - q[1], q[5] - q[2]);
+        const float3 e2 = make_float3(q[6] - q[0], q[7] - q[1], q[8] - q[2]);
+        const float3 pv = M::cross(d, e2);
+        const float det = M::dot(e1, pv);
+        if (std::fabs(det) < 1e-20f) continue;
+        const float inv = 1.0f / det;
+        const float3 sv = o - v0;
+        const float u = M::dot(sv, pv) * inv;
+        if (u < 0.0f || u > 1.0f) continue;
+        const float3 qv = M::cross(sv, e1);
+        const float v = M::dot(d, qv) * inv;
+        if (v < 0.0f || u + v > 1.0f) continue;
+        const float t = M::dot(e2, qv) * inv;
+        if (t > tmin && t < tmax) return true;
+    }
+    return false;
+}
+#include <rtlib_kat/ShadeKernel.h>
+
+extern "C" {
+
+// The scene of the known answers.  mat_type holds rtlib_b200's material types (0 Phong,
+// 1 glass, 2 NEE light, 3 light outside the NEE list), mapped here to RTLib's HitgroupType
+// (SimpleKernel.h:203-210).  Every light mesh becomes a MeshLight of unshared vertices with
+// the identity transform and a white emission texture.
+void ref_kat_set_scene(const float* tri_v, uint32_t ntris, const uint32_t* tri_mat, const float* mat_f,
+                       const int32_t* mat_type, uint32_t nmats, const uint32_t* light_tris, const uint32_t* light_first,
+                       const uint32_t* light_count, const float* light_emit, uint32_t nlights) {
+    g_kat = KatScene{};
+    g_kat.tri_v.assign(tri_v, tri_v + 9 * size_t(ntris));
+    g_kat.tri_mat.assign(tri_mat, tri_mat + ntris);
+    g_kat.mat_f.assign(mat_f, mat_f + 11 * size_t(nmats));
+    static const int kType[4] = {HIT_GROUP_TYPE_PHONG, HIT_GROUP_TYPE_GLASS, HIT_GROUP_TYPE_NEE_LIGHT,
+                                 HIT_GROUP_TYPE_DEF_LIGHT};
+    for (uint32_t i = 0; i < nmats; ++i) g_kat.mat_type.push_back(kType[mat_type[i] & 3]);
+    g_kat.lv.resize(nlights);
+    g_kat.li.resize(nlights);
+    g_kat.lt.resize(nlights);
+    for (uint32_t i = 0; i < nlights; ++i) {
+        for (uint32_t k = 0; k < light_count[i]; ++k) {
+            const float* q = tri_v + 9 * size_t(light_tris[light_first[i] + k]);
+            for (int c = 0; c < 3; ++c) {
+                g_kat.lv[i].push_back(make_float3(q[3 * c], q[3 * c + 1], q[3 * c + 2]));
+                g_kat.lt[i].push_back(make_float2(0.0f, 0.0f));
+            }
+            g_kat.li[i].push_back(make_uint3(3 * k, 3 * k + 1, 3 * k + 2));
+        }
+    }
+    for (uint32_t i = 0; i < nlights; ++i) {
+        MeshLight l{};
+        l.vertices = g_kat.lv[i].data();
+        l.normals = nullptr;
+        l.texCrds = g_kat.lt[i].data();
+        l.indices = g_kat.li[i].data();
+        l.indCount = light_count[i];
+        l.emission = make_float3(light_emit[3 * i], light_emit[3 * i + 1], light_emit[3 * i + 2]);
+        l.transform = M::Matrix4x4::Identity();
+        l.emissionTex = 0;
+        g_kat.lights.push_back(l);
+    }
+}
+
+// sampleCosinePDF / samplePhongPDF (SimpleGuide.cu:28-42), random_in_unit_triangle
+// (Random.h:289-296): Xorshift32 states in/out, one per case.
+void ref_kat_cosine(int64_t n, const float* normal, uint32_t* state, float* out) {
+    for (int64_t i = 0; i < n; ++i) {
+        M::Xorshift32 rng(state[i]);
+        const float3 d = sampleCosinePDF(make_float3(normal[3 * i], normal[3 * i + 1], normal[3 * i + 2]), rng);
+        out[3 * i] = d.x; out[3 * i + 1] = d.y; out[3 * i + 2] = d.z;
+        state[i] = rng.m_seed;
+    }
+}
+void ref_kat_phong(int64_t n, const float* refl, const float* shininess, uint32_t* state, float* out) {
+    for (int64_t i = 0; i < n; ++i) {
+        M::Xorshift32 rng(state[i]);
+        const float3 d = samplePhongPDF(make_float3(refl[3 * i], refl[3 * i + 1], refl[3 * i + 2]), shininess[i], rng);
+        out[3 * i] = d.x; out[3 * i + 1] = d.y; out[3 * i + 2] = d.z;
+        state[i] = rng.m_seed;
+    }
+}
+void ref_kat_triangle(int64_t n, const float* v, uint32_t* state, float* out) {
+    for (int64_t i = 0; i < n; ++i) {
+        M::Xorshift32 rng(state[i]);
+        const float* q = v + 9 * i;
+        const float3 p = M::random_in_unit_triangle(make_float3(q[0], q[1], q[2]), make_float3(q[3], q[4], q[5]),
+                                                    make_float3(q[6], q[7], q[8]), rng);
+        out[3 * i] = p.x; out[3 * i + 1] = p.y; out[3 * i + 2] = p.z;
+        state[i] = rng.m_seed;
+    }
+}
+// Reservoir<int>::Update (SimpleKernel.h:124-143) over nseq sequences of len candidates
+void ref_kat_reservoir(int64_t nseq, int32_t len, const float* w, const float* rnd, int32_t* sel, float* wsum,
+                       uint32_t* m) {
+    for (int64_t k = 0; k < nseq; ++k) {
+        Reservoir<int> r{};
+        r.y = -1;
+        for (int32_t i = 0; i < len; ++i) r.Update(i, w[k * len + i], rnd[k * len + i]);
+        sel[k] = r.y;
+        wsum[k] = r.w_sum;
+        m[k] = r.m;
+    }
+}
+// MeshLightList::Sample (SimpleKernel.h:107-122) of the scene's lights; per case 14 floats:
+// direction, normal, emission, distance, invPdf, position
+void ref_kat_light(int64_t n, const float* p_in, uint32_t* state, float* out) {
+    MeshLightList list{(unsigned int)g_kat.lights.size(), g_kat.lights.data()};
+    for (int64_t i = 0; i < n; ++i) {
+        M::Xorshift32 rng(state[i]);
+        const LightRecord l = list.Sample(make_float3(p_in[3 * i], p_in[3 * i + 1], p_in[3 * i + 2]), rng);
+        float* o = out + 14 * i;
+        o[0] = l.direction.x; o[1] = l.direction.y; o[2] = l.direction.z;
+        o[3] = l.normal.x; o[4] = l.normal.y; o[5] = l.normal.z;
+        o[6] = l.emission.x; o[7] = l.emission.y; o[8] = l.emission.z;
+        o[9] = l.distance; o[10] = l.invPdf;
+        o[11] = l.position.x; o[12] = l.position.y; o[13] = l.position.z;
+        state[i] = rng.m_seed;
+    }
+}
+// __closesthit__radiance of n vertices: the ray (org, dir), hit distance t and triangle prim,
+// and the path's throughput, hit flags and depth before the vertex.  Per case 17 floats out
+// (position, direction, throughput after the vertex, BSDF value, radiance added, cosine,
+// woPdf) and the hit flags; states in/out.  tree: a ref_sdtree handle (USE_TREE) or NULL.
+void ref_kat_shade(uint32_t flags, uint32_t max_depth, uint32_t num_candidates, void* tree, float fraction, int64_t n,
+                   const float* org, const float* dir, const float* t, const uint32_t* prim, const float* thr,
+                   const uint32_t* pflags, const uint32_t* depth, uint32_t* state, float* out, uint32_t* out_flags) {
+    params = KatParams{};
+    params.flags = flags;
+    params.maxDepth = max_depth;
+    params.numCandidates = num_candidates;
+    params.lights = MeshLightList{(unsigned int)g_kat.lights.size(), g_kat.lights.data()};
+    if (tree) {
+        auto* rt = static_cast<RefSDTree*>(tree);
+        rt->flatten();
+        params.tree = rt->view;
+        params.tree.fraction = fraction;
+    }
+    for (int64_t i = 0; i < n; ++i) {
+        const float* q = g_kat.tri_v.data() + 9 * size_t(prim[i]);
+        const float3 p0 = make_float3(q[0], q[1], q[2]), p1 = make_float3(q[3], q[4], q[5]),
+                     p2 = make_float3(q[6], q[7], q[8]);
+        const float3 fNormal = M::normalize(M::cross(p1 - p0, p2 - p0));  // GetTriangleFNormal, identity transform
+        const float3 inDir = make_float3(dir[3 * i], dir[3 * i + 1], dir[3 * i + 2]);
+        const float3 position = make_float3(org[3 * i], org[3 * i + 1], org[3 * i + 2]) + t[i] * inDir;
+        const uint32_t mi = g_kat.tri_mat[prim[i]];
+        const float* mf = g_kat.mat_f.data() + 11 * size_t(mi);
+        KatHitgroup hg{g_kat.mat_type[mi]};
+        KatHitRecord hrec{};
+        hrec.seed = state[i];
+        hrec.flags = pflags[i];
+        hrec.userData.throughPut = make_float3(thr[3 * i], thr[3 * i + 1], thr[3 * i + 2]);
+        hrec.userData.depth = depth[i];
+        KatShadeOut so{};
+        // white textures: SampleDiffuse / SampleSpecular / SampleEmission return the factors
+        kat_closesthit(&hg, &hrec, position, inDir, fNormal, fNormal, make_float3(mf[0], mf[1], mf[2]),
+                       make_float3(mf[3], mf[4], mf[5]), make_float3(mf[6], mf[7], mf[8]), mf[10], mf[9], t[i], &so);
+        float* o = out + 17 * i;
+        const float3* vv[5] = {&so.position, &so.direction, &so.currThroughput, &so.bsdfVal, &so.radiance};
+        for (int k = 0; k < 5; ++k) { o[3 * k] = vv[k]->x; o[3 * k + 1] = vv[k]->y; o[3 * k + 2] = vv[k]->z; }
+        o[15] = so.cosine;
+        o[16] = so.woPdf;
+        out_flags[i] = so.flags;
+        state[i] = so.seed;
+    }
+}
+
+}  // extern "C"

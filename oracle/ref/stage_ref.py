@@ -23,7 +23,24 @@ and applies *mechanical* fixes that change no arithmetic:
 
 Every other header (Math, Hash, VectorFunction, OPX7UtilsGrid.h) is used in place
 from the reference tree through ``-I``; a lower-case ``math`` symlink fixes the include
-case in Hash.h:3-4.
+case in Hash.h:3-4 and an upper-case ``EXT`` one that in Matrix.h:3.
+
+For the integrator's known answers it also writes ``oracle/_ref/include/rtlib_kat/ShadeTypes.h``
+and ``ShadeKernel.h`` from text cut out of RTLib's OptiX test programs, which include optix.h and so cannot be
+compiled here as a whole:
+
+* SimpleKernel.h:26-143 (LightRecord, MeshLight, MeshLightList, Reservoir) with its two
+  ``#ifdef __CUDACC__`` guards removed, and the enums ParamFlag, HitgroupType and
+  HitRecordFlag (SimpleKernel.h:149-158, 203-210, 281-289);
+* SimpleGuide.cu:28-47 (sampleCosinePDF, samplePhongPDF, getValPhongPDF) with
+  ``static __forceinline__ __device__`` -> ``static inline``;
+* the body of __closesthit__radiance from the Xorshift32 it seeds to the emission rule
+  (SimpleGuide.cu:306-496), unchanged, inside a function whose parameters carry the values
+  the program's first lines read from OptiX (SimpleGuide.cu:288-304).
+
+The first two items go to ShadeTypes.h, the last two to ShadeKernel.h.  The names the body
+uses from the launch (``params``, ``TraceOccluded``, the hit record and hit-group data) are
+supplied by ref_driver.cpp between the two includes.
 """
 import os
 import re
@@ -105,6 +122,63 @@ def patch_random(src):
     return t
 
 
+TEST_CUDA = "RTLib/Src/Ext/OPX7/Test/cuda"
+
+
+def _cut(text, start, end, include_end=False):
+    a = text.index(start)
+    b = text.index(end, a)
+    return text[a:b + (len(end) if include_end else 0)]
+
+
+def _enum(text, head):
+    a = text.index(head)
+    b = text.index("};", a)
+    return text[a:b + 2]
+
+
+def stage_shade(ref, out_dir):
+    with open(os.path.join(ref, TEST_CUDA, "SimpleKernel.h"), encoding="latin-1") as f:
+        sk = f.read()
+    with open(os.path.join(ref, TEST_CUDA, "SimpleGuide.cu"), encoding="latin-1") as f:
+        sg = f.read()
+    lights = _cut(sk, "struct LightRecord", "struct ReservoirState")
+    n_guard = lights.count("#ifdef __CUDACC__")
+    if n_guard != 2 or lights.count("#endif") != 2:
+        raise SystemExit("stage_ref: unexpected preprocessor guards in SimpleKernel.h")
+    lights = "\n".join(l for l in lights.split("\n") if l.strip() not in ("#ifdef __CUDACC__", "#endif"))
+    enums = "\n".join(_enum(sk, h) for h in ("enum   ParamFlag", "enum   HitgroupType", "enum   HitRecordFlag"))
+    helpers = _cut(sg, "template<typename RNG>\nstatic __forceinline__ __device__ float3       sampleCosinePDF",
+                   'extern "C" __global__ void     __raygen__default')
+    if helpers.count("static __forceinline__ __device__") != 3:
+        raise SystemExit("stage_ref: unexpected helper declarations in SimpleGuide.cu")
+    helpers = helpers.replace("static __forceinline__ __device__", "static inline")
+    prog = sg[sg.index('extern "C" __global__ void     __closesthit__radiance() {'):]
+    body = _cut(prog, "    auto xor32 = RTLib::Ext::CUDA::Math::Xorshift32(hrec->seed);",
+                "    hrec->SetGlobalRayOrigin(position);")
+    head = ("// Staged by oracle/ref/stage_ref.py from RTLib's SimpleKernel.h and SimpleGuide.cu (see\n"
+            "// that script).  Test infrastructure only; not part of the product.\n#pragma once\n")
+    types = head + "#include <RTLib/Ext/CUDA/Math/Matrix.h>\n\n" + lights + "\n" + enums + "\n"
+    text = (
+        head + helpers + "\n"
+        "// __closesthit__radiance (SimpleGuide.cu:287-496) from its Xorshift32 on; the parameters\n"
+        "// are the values its first lines read through OptiX.\n"
+        "static inline void kat_closesthit(const KatHitgroup* hgData, KatHitRecord* hrec, float3 position, float3 inDir,\n"
+        "                                  float3 fNormal, float3 vNormal, float3 diffuse, float3 specular,\n"
+        "                                  float3 emission, float refIndex, float shinness, float distance,\n"
+        "                                  KatShadeOut* out) {\n"
+        + body +
+        "    out->position = position;\n    out->direction = direction;\n    out->currThroughput = currThroughput;\n"
+        "    out->bsdfVal = bsdfVal;\n    out->radiance = radiance;\n    out->cosine = cosine;\n    out->woPdf = woPdf;\n"
+        "    out->flags = currHitFlags;\n    out->seed = xor32.m_seed;\n}\n")
+    kdir = os.path.join(out_dir, "include", "rtlib_kat")
+    os.makedirs(kdir, exist_ok=True)
+    with open(os.path.join(kdir, "ShadeTypes.h"), "w", encoding="latin-1") as f:
+        f.write(types)
+    with open(os.path.join(kdir, "ShadeKernel.h"), "w", encoding="latin-1") as f:
+        f.write(text)
+
+
 def main():
     if not os.path.isdir(REF):
         print(f"stage_ref: reference tree {REF} not present; nothing staged")
@@ -137,6 +211,14 @@ def main():
     if os.path.lexists(link):
         os.remove(link)
     os.symlink(os.path.join(REF, CUDA_INC, "RTLib", "Ext", "CUDA", "Math"), link)
+    # upper-case include path used by Matrix.h:3
+    shim_up = os.path.join(OUT, "shim", "RTLib", "EXT", "CUDA")
+    os.makedirs(shim_up, exist_ok=True)
+    link = os.path.join(shim_up, "Math")
+    if os.path.lexists(link):
+        os.remove(link)
+    os.symlink(os.path.join(REF, CUDA_INC, "RTLib", "Ext", "CUDA", "Math"), link)
+    stage_shade(REF, OUT)
     print("stage_ref: staged patched headers into", OUT)
     return 0
 

@@ -861,6 +861,20 @@ static OOnb onb(V3 normal) {
     return r;
 }
 static V3 onb_local(OOnb o, V3 d) { return vadd(vadd(vs(d.x, o.t), vs(d.y, o.b)), vs(d.z, o.n)); }
+/* sampleCosinePDF (SimpleGuide.cu:28-33): ONB(normal).local(random_cosine_direction(rng))
+ * (VectorFunction.h:5666-5697, Random.h:321-334); sin / cos of 2 pi x as sinpi / cospi of 2x */
+static V3 o_sample_cosine(V3 normal, uint32_t* rng) {
+    float a = rnd1(rng), c = rnd1(rng);
+    float r = sqrtf(a), z = sqrtf(1.0f - a);
+    return onb_local(onb(normal), v3(r * cospi_f(2.0f * c), r * sinpi_f(2.0f * c), z));
+}
+/* samplePhongPDF (SimpleGuide.cu:34-42): cos theta = u^(1/(s+1)), phi = 2 pi u' around refl */
+static V3 o_sample_phong(V3 refl, float shininess, uint32_t* rng) {
+    float cosT = powf(rnd1(rng), 1.0f / (shininess + 1.0f));
+    float sinT = sqrtf(fmaxf(1.0f - cosT * cosT, 0.0f));
+    float phi = O_2PI * rnd1(rng);
+    return onb_local(onb(refl), v3(sinT * cosf(phi), sinT * sinf(phi), cosT));
+}
 static float phong_pdf_o(V3 d, V3 refl, float s) {
     float c = vdot(refl, d);
     c = c > 0.0f ? c : 0.0f;
@@ -871,17 +885,33 @@ static V3 phong_bsdf_o(V3 kd, V3 ks, float s, V3 d, V3 refl) {
     return vadd(vs((float)0.318309886183790691216444201927515678107738494873046875, kd),
                 vs(phong_pdf_o(d, refl, s), vs((s + 2.0f) / (s + 1.0f), ks)));
 }
-typedef struct { V3 dir, normal, emission; float dist, inv_pdf; } OLight;
+typedef struct { V3 dir, normal, emission, pos; float dist, inv_pdf; } OLight;
+/* random_in_unit_triangle (Random.h:289-296): a = min, b = max of two uniforms,
+ * v0 a + v1 (1 - b) + v2 (b - a).  MeshLight::Sample forms the same point through
+ * barycentrics of the unit vectors (SimpleKernel.h:81-98), bit for bit the same floats. */
+static V3 o_random_in_unit_triangle(V3 v0, V3 v1, V3 v2, uint32_t* rng) {
+    float r0 = rnd1(rng), r1 = rnd1(rng);
+    float a = fminf(r0, r1), b = fmaxf(r0, r1);
+    return vadd(vadd(vs(a, v0), vs(1.0f - b, v1)), vs(b - a, v2));
+}
+/* Reservoir::Update (SimpleKernel.h:124-143): w_sum += w_i, ++m, keep x_i iff
+ * w_i / w_sum >= rnd01.  Returns whether x_i was kept. */
+static int o_reservoir_update(float* w_sum, uint32_t* m, float w_i, float rnd01) {
+    *w_sum += w_i;
+    ++*m;
+    return (w_i / *w_sum) >= rnd01;
+}
+/* MeshLightList::Sample -> MeshLight::Sample (SimpleKernel.h:81-122) with white emission
+ * textures: mesh next() % count, triangle next() % indCount, invPdf = area * indCount * count */
 static OLight o_sample_light(const OScene* s, V3 p_in, uint32_t* rng) {
     uint32_t mi = xs32_next(rng) % s->nlights;
     uint32_t ti = s->light_tris[s->light_first[mi] + xs32_next(rng) % s->light_count[mi]];
     V3 v0 = tri_vert(s, ti, 0), v1 = tri_vert(s, ti, 1), v2 = tri_vert(s, ti, 2);
     V3 nf = vcross(vsub(v1, v0), vsub(v2, v0));
-    float r0 = rnd1(rng), r1 = rnd1(rng);
-    float a = fminf(r0, r1), b = fmaxf(r0, r1);
-    V3 p = vadd(vadd(vs(a, v0), vs(1.0f - b, v1)), vs(b - a, v2));
+    V3 p = o_random_in_unit_triangle(v0, v1, v2, rng);
     V3 d = vsub(p, p_in);
     OLight l;
+    l.pos = p;
     l.dist = vlen(d);
     l.dir = vunit(d);
     l.emission = v3(s->light_emit[3 * mi], s->light_emit[3 * mi + 1], s->light_emit[3 * mi + 2]);
@@ -985,6 +1015,201 @@ static void commit_vertex(OSDTree* t, const OVert* v) {
     or_sdtree_record(t, 1, pos, uv, &lavg, &v->wopdf, &one, NULL);
 }
 
+/* The closest-hit shading of one path vertex, as RTLib's __closesthit__radiance does it
+ * (SimpleGuide.cu:287-497; the hash-grid guide of SimpleGuide2.cu:285-523): BSDF / guide
+ * mixture sampling, NEE or RIS with its shadow ray, the glass branch, the emission rule.
+ * In: the ray (org, dir), its hit (t, prim, barycentrics hu, hv), the throughput, hit flags
+ * and depth of the path before the vertex, its Xorshift32 state.  Out: the next ray, the
+ * throughput after the vertex (zero unless a Phong or glass branch sets it, as
+ * currThroughput starts), the radiance the vertex adds (L), its hit flags and, for the grid
+ * guide, its cell. */
+typedef struct {
+    V3 position, direction, cur_thr, bsdf_val, L;
+    float cosine, wo_pdf;
+    uint32_t hflags, cell;
+} OShade;
+static void o_shade(const OScene* s, uint32_t flags, OSDTree* tree, OGrid* grid, V3 org, V3 dir, float t,
+                    uint32_t prim, float hu, float hv, V3 thr, uint32_t pflags, uint32_t depth, uint32_t* prng,
+                    OShade* out) {
+    const int use_tree = (flags & O_TREE) != 0, use_grid = (flags & O_GRID) != 0, build = (flags & O_BUILD) != 0;
+    const uint32_t mqt_per = use_grid ? mqt_off(grid->level + 1) : 0;
+    const float inv_pi = (float)0.318309886183790691216444201927515678107738494873046875;
+    uint32_t rng = *prng;
+    V3 L = v3(0, 0, 0), cur_thr = v3(0, 0, 0), direction = v3(0, 0, 0), bsdf_val = v3(0, 0, 0);
+    float cosine = 0.0f, wo_pdf = 0.0f;
+    uint32_t hflags = 0;
+    V3 position = org;
+    V3 v0 = tri_vert(s, prim, 0), v1 = tri_vert(s, prim, 1), v2 = tri_vert(s, prim, 2);
+    V3 fn = vunit(vcross(vsub(v1, v0), vsub(v2, v0)));
+    position = vadd(org, vs(t, dir));
+    const OMat* m = &s->mats[s->tri_mat[prim]];
+    V3 diffuse = v3(m->diffuse[0], m->diffuse[1], m->diffuse[2]);
+    V3 spec = v3(m->specular[0], m->specular[1], m->specular[2]);
+    V3 emis = v3(m->emission[0], m->emission[1], m->emission[2]);
+    if (m->tex >= 0 && s->tex && s->tri_uv) {
+        const float* uv = s->tri_uv + 6 * (size_t)prim;
+        float w0 = 1.0f - hu - hv;
+        float tu = w0 * uv[0] + hu * uv[2] + hv * uv[4], tv = w0 * uv[1] + hu * uv[3] + hv * uv[5];
+        float fu = tu - floorf(tu), fv = tv - floorf(tv);
+        uint32_t ix = (uint32_t)(fu * s->tex_w), iy = (uint32_t)(fv * s->tex_h);
+        if (ix > s->tex_w - 1) ix = s->tex_w - 1;
+        if (iy > s->tex_h - 1) iy = s->tex_h - 1;
+        const float* px = s->tex + 3 * ((size_t)iy * s->tex_w + ix);
+        diffuse = vmul(diffuse, v3(px[0], px[1], px[2]));
+    }
+    int count_emitted = (pflags & 8u) || m->type == 3;
+    uint32_t dt = 0, cell = UINT32_MAX;
+    if (use_tree) dt = (uint32_t)leaf_dtree(tree, &position.x);
+    if (m->type == 0) {
+        uint32_t gb = 0, prv_cell = UINT32_MAX;
+        uint64_t gk = 0;
+        if (use_grid) {
+            gk = grid_key(grid, position, &gb);
+            prv_cell = grid_find_prv(grid, gk, gb);
+        }
+        V3 refl = vunit(reflect_o(dir, fn));
+        V3 d0 = o_sample_cosine(fn, &rng);
+        V3 d1 = o_sample_phong(refl, m->shininess, &rng);
+        float c0 = vdot(d0, fn), c1 = vdot(d1, fn);
+        float cp0 = fmaxf(c0 * inv_pi, 0.0f), cp1 = fmaxf(c1 * inv_pi, 0.0f);
+        float pp0 = phong_pdf_o(d0, refl, m->shininess), pp1 = phong_pdf_o(d1, refl, m->shininess);
+        float ad = 1.0e-10f + vavg(diffuse), as = 1.0e-10f + vavg(spec);
+        float sel = ad / (ad + as);
+        float sf = (m->shininess + 2.0f) / (m->shininess + 1.0f);
+        float bsdf_pdf;
+        if (rnd1(&rng) < sel) {
+            direction = d0; cosine = c0;
+            bsdf_val = vadd(vs(inv_pi, diffuse), vs(pp0, vs(sf, spec)));
+            bsdf_pdf = sel * cp0 + (1.0f - sel) * pp0;
+        } else {
+            direction = d1; cosine = c1;
+            bsdf_val = vadd(vs(inv_pi, diffuse), vs(pp1, vs(sf, spec)));
+            bsdf_pdf = sel * cp1 + (1.0f - sel) * pp1;
+        }
+        if (use_tree && build) {
+            const ODTree* dd = &tree->dt[dt];
+            if (rnd1(&rng) < s->fraction) {
+                float uv[2];
+                dtree_sample(dd, &rng, uv);
+                float dv[3];
+                const float cosTheta = 2.0f * uv[0] - 1.0f;
+                const float sinTheta = sqrtf(fmaxf(1.0f - cosTheta * cosTheta, 0.0f));
+                dv[0] = sinTheta * cospi_f(2.0f * uv[1]);
+                dv[1] = sinTheta * sinpi_f(2.0f * uv[1]);
+                dv[2] = cosTheta;
+                float l = 1.0f / sqrtf(dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2]);
+                direction = v3(dv[0] * l, dv[1] * l, dv[2] * l);
+                cosine = vdot(direction, fn);
+                float cp2 = fmaxf(cosine * inv_pi, 0.0f);
+                float pp2 = phong_pdf_o(direction, refl, m->shininess);
+                bsdf_val = vadd(vs(inv_pi, diffuse), vs(pp2, vs(sf, spec)));
+                bsdf_pdf = sel * cp2 + (1.0f - sel) * pp2;
+            }
+            float dd3[3] = {direction.x, direction.y, direction.z}, c2[2];
+            or_dir_to_canonical(1, dd3, c2);
+            float dpdf = fmaxf(dtree_pdf(dd, c2[0], c2[1]), 0.0f);
+            wo_pdf = (1.0f - s->fraction) * bsdf_pdf + s->fraction * dpdf;
+        } else if (use_grid && build && prv_cell != UINT32_MAX) {
+            /* SimpleGuide2.cu:350-377 */
+            const float* w = grid->pyramid + (uint64_t)prv_cell * mqt_per;
+            float dpdf;
+            if (rnd1(&rng) < grid->fraction) {
+                float uv[2], tp;
+                mqt_sample_one(w, grid->level, &rng, &uv[0], &uv[1], &tp);
+                dpdf = (float)((double)tp * (0.25 * 0.318309886183790691216444201927515678107738494873046875));
+                float dv[3];
+                const float cosTheta = 2.0f * uv[0] - 1.0f;
+                const float sinTheta = sqrtf(fmaxf(1.0f - cosTheta * cosTheta, 0.0f));
+                dv[0] = sinTheta * cospi_f(2.0f * uv[1]);
+                dv[1] = sinTheta * sinpi_f(2.0f * uv[1]);
+                dv[2] = cosTheta;
+                float l = 1.0f / sqrtf(dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2]);
+                direction = v3(dv[0] * l, dv[1] * l, dv[2] * l);
+                cosine = vdot(direction, fn);
+                float cp2 = fmaxf(cosine * inv_pi, 0.0f);
+                float pp2 = phong_pdf_o(direction, refl, m->shininess);
+                bsdf_val = vadd(vs(inv_pi, diffuse), vs(pp2, vs(sf, spec)));
+                bsdf_pdf = sel * cp2 + (1.0f - sel) * pp2;
+            } else {
+                float dd3[3] = {direction.x, direction.y, direction.z}, c2[2];
+                or_dir_to_canonical(1, dd3, c2);
+                const float tp = mqt_pdf_one(w, grid->level, c2[0], c2[1]);
+                dpdf = fmaxf((float)((double)(tp * 0.25f) * 0.318309886183790691216444201927515678107738494873046875), 0.0f);
+            }
+            wo_pdf = grid->fraction * dpdf + (1.0f - grid->fraction) * bsdf_pdf;
+        } else {
+            wo_pdf = bsdf_pdf;
+        }
+        cur_thr = wo_pdf > 0.0f ? vmul(thr, vdivs(vs(fmaxf(cosine, 0.0f), bsdf_val), wo_pdf)) : v3(0, 0, 0);
+        if (flags & O_NEE) {
+            if (depth < s->max_depth - 1 && s->nlights > 0) {
+                if (flags & O_RIS) {
+                    float w_sum = 0.0f, fay = 0.0f, disty = 0.0f;
+                    uint32_t mc = 0;
+                    V3 fy = v3(0, 0, 0), ldy = v3(0, 0, 0);
+                    for (uint32_t k = 0; k < s->num_candidates; ++k) {
+                        OLight l = o_sample_light(s, position, &rng);
+                        float ndl = vdot(l.dir, fn), lndl = -vdot(l.dir, l.normal);
+                        V3 b = phong_bsdf_o(diffuse, spec, m->shininess, l.dir, refl);
+                        float g = fmaxf(ndl, 0.0f) * fmaxf(lndl, 0.0f) / (l.dist * l.dist);
+                        V3 f = vmul(vmul(b, l.emission), v3(g, g, g));
+                        float fa = vavg(f), wi = fa * l.inv_pdf;
+                        if (o_reservoir_update(&w_sum, &mc, wi, rnd1(&rng))) { fy = f; fay = fa; ldy = l.dir; disty = l.dist; }
+                    }
+                    if (w_sum > 0.0f && fay > 0.0f &&
+                        !o_trace(s, position, ldy, 0.0001f, disty - 0.0001f, 1, 0, 0, 0, 0))
+                        L = vadd(L, vs(w_sum / (fay * (float)mc), vmul(thr, fy)));
+                } else {
+                    OLight l = o_sample_light(s, position, &rng);
+                    V3 b = phong_bsdf_o(diffuse, spec, m->shininess, l.dir, refl);
+                    float g = fmaxf(-vdot(l.dir, l.normal), 0.0f) * fabsf(vdot(l.dir, fn)) / (l.dist * l.dist);
+                    if (!o_trace(s, position, l.dir, 0.0001f, l.dist - 0.0001f, 1, 0, 0, 0, 0))
+                        L = vadd(L, vs(l.inv_pdf, vs(g, vmul(vmul(thr, b), l.emission))));
+                }
+            }
+        } else {
+            hflags |= 8u;
+        }
+        if (use_grid)
+            cell = ((flags & O_LOCATE) && prv_cell == UINT32_MAX) ? grid_insert_cur(grid, gk, gb) : prv_cell;
+    } else if (m->type == 1) {
+        V3 rn;
+        float rri, ci = vdot(fn, dir);
+        if (ci < 0.0f) { rn = fn; rri = 1.0f / m->ref_index; ci = -ci; }
+        else { rn = v3(-fn.x, -fn.y, -fn.z); rri = m->ref_index; }
+        float so2 = (1.0f - ci * ci) * (rri * rri);
+        float f0 = ((1.0f - rri) / (1.0f + rri)) * ((1.0f - rri) / (1.0f + rri));
+        float om = 1.0f - ci;
+        float fres = f0 + (1.0f - f0) * (om * om * om * om * om);
+        V3 rd = vunit(reflect_o(dir, rn));
+        if (rnd1(&rng) < fres || so2 > 1.0f) {
+            position = vadd(position, vs(0.0001f, rn));
+            direction = rd; cosine = fabsf(ci); bsdf_val = spec; cur_thr = vmul(thr, spec);
+        } else {
+            position = vsub(position, vs(0.0001f, rn));
+            float si2 = fmaxf(1.0f - ci * ci, 0.0f), co = sqrtf(1.0f - so2);
+            V3 rf;
+            if (si2 > 0.0f) rf = vunit(vsub(vs(sqrtf(so2), vdivs(vadd(dir, vs(ci, rn)), sqrtf(si2))), vs(co, rn)));
+            else rf = dir;
+            direction = rf; cosine = fabsf(vdot(rf, rn)); bsdf_val = v3(1, 1, 1); cur_thr = thr;
+        }
+        wo_pdf = fabsf(cosine);
+        hflags |= 8u | 2u;
+    }
+    if (vdot(dir, fn) < 0.0f && count_emitted) L = vadd(L, vmul(thr, emis));
+    if (emis.x + emis.y + emis.z > 0.0f) hflags |= 16u;
+    out->position = position;
+    out->direction = direction;
+    out->cur_thr = cur_thr;
+    out->bsdf_val = bsdf_val;
+    out->L = L;
+    out->cosine = cosine;
+    out->wo_pdf = wo_pdf;
+    out->hflags = hflags;
+    out->cell = cell;
+    *prng = rng;
+}
+
 /* One sample per pixel for pixels [p0, p1) of the frame; accum += color (double), seeds
  * updated.  tree: an or_sdtree handle or NULL.  Returns the number of paths traced. */
 static uint32_t* g_depth_out = NULL;
@@ -999,10 +1224,8 @@ int64_t or_render(const OScene* s, uint32_t flags, void* tree_h, void* grid_h, u
                   uint32_t* seeds, double* accum) {
     OSDTree* tree = (OSDTree*)tree_h;
     OGrid* grid = (OGrid*)grid_h;
-    const int use_tree = (flags & O_TREE) != 0, use_grid = (flags & O_GRID) != 0, build = (flags & O_BUILD) != 0;
+    const int use_tree = (flags & O_TREE) != 0, use_grid = (flags & O_GRID) != 0;
     const int recording = (use_tree || use_grid) && !(flags & O_FINAL);
-    const uint32_t mqt_per = use_grid ? mqt_off(grid->level + 1) : 0;
-    const float inv_pi = (float)0.318309886183790691216444201927515678107738494873046875;
     for (uint32_t p = p0; p < p1; ++p) {
         uint32_t x = p % s->width, y = p / s->width;
         uint32_t rng = seeds[p];
@@ -1036,172 +1259,17 @@ int64_t or_render(const OScene* s, uint32_t flags, void* tree_h, void* grid_h, u
                 hflags = 16u;
                 if (recording && depth < O_KTV) verts[depth].valid = 0;
             } else {
-                V3 v0 = tri_vert(s, prim, 0), v1 = tri_vert(s, prim, 1), v2 = tri_vert(s, prim, 2);
-                V3 fn = vunit(vcross(vsub(v1, v0), vsub(v2, v0)));
-                position = vadd(org, vs(t, dir));
-                const OMat* m = &s->mats[s->tri_mat[prim]];
-                V3 diffuse = v3(m->diffuse[0], m->diffuse[1], m->diffuse[2]);
-                V3 spec = v3(m->specular[0], m->specular[1], m->specular[2]);
-                V3 emis = v3(m->emission[0], m->emission[1], m->emission[2]);
-                if (m->tex >= 0 && s->tex && s->tri_uv) {
-                    const float* uv = s->tri_uv + 6 * (size_t)prim;
-                    float w0 = 1.0f - hu - hv;
-                    float tu = w0 * uv[0] + hu * uv[2] + hv * uv[4], tv = w0 * uv[1] + hu * uv[3] + hv * uv[5];
-                    float fu = tu - floorf(tu), fv = tv - floorf(tv);
-                    uint32_t ix = (uint32_t)(fu * s->tex_w), iy = (uint32_t)(fv * s->tex_h);
-                    if (ix > s->tex_w - 1) ix = s->tex_w - 1;
-                    if (iy > s->tex_h - 1) iy = s->tex_h - 1;
-                    const float* px = s->tex + 3 * ((size_t)iy * s->tex_w + ix);
-                    diffuse = vmul(diffuse, v3(px[0], px[1], px[2]));
-                }
-                int count_emitted = (pflags & 8u) || m->type == 3;
-                uint32_t dt = 0, cell = UINT32_MAX;
-                if (use_tree) dt = (uint32_t)leaf_dtree(tree, &position.x);
-                if (m->type == 0) {
-                    uint32_t gb = 0, prv_cell = UINT32_MAX;
-                    uint64_t gk = 0;
-                    if (use_grid) {
-                        gk = grid_key(grid, position, &gb);
-                        prv_cell = grid_find_prv(grid, gk, gb);
-                    }
-                    V3 refl = vunit(reflect_o(dir, fn));
-                    float a = rnd1(&rng), c = rnd1(&rng);
-                    float r = sqrtf(a), z = sqrtf(1.0f - a);
-                    V3 d0 = onb_local(onb(fn), v3(r * cospi_f(2.0f * c), r * sinpi_f(2.0f * c), z));
-                    float cosT = powf(rnd1(&rng), 1.0f / (m->shininess + 1.0f));
-                    float sinT = sqrtf(fmaxf(1.0f - cosT * cosT, 0.0f));
-                    float phi = O_2PI * rnd1(&rng);
-                    V3 d1 = onb_local(onb(refl), v3(sinT * cosf(phi), sinT * sinf(phi), cosT));
-                    float c0 = vdot(d0, fn), c1 = vdot(d1, fn);
-                    float cp0 = fmaxf(c0 * inv_pi, 0.0f), cp1 = fmaxf(c1 * inv_pi, 0.0f);
-                    float pp0 = phong_pdf_o(d0, refl, m->shininess), pp1 = phong_pdf_o(d1, refl, m->shininess);
-                    float ad = 1.0e-10f + vavg(diffuse), as = 1.0e-10f + vavg(spec);
-                    float sel = ad / (ad + as);
-                    float sf = (m->shininess + 2.0f) / (m->shininess + 1.0f);
-                    float bsdf_pdf;
-                    if (rnd1(&rng) < sel) {
-                        direction = d0; cosine = c0;
-                        bsdf_val = vadd(vs(inv_pi, diffuse), vs(pp0, vs(sf, spec)));
-                        bsdf_pdf = sel * cp0 + (1.0f - sel) * pp0;
-                    } else {
-                        direction = d1; cosine = c1;
-                        bsdf_val = vadd(vs(inv_pi, diffuse), vs(pp1, vs(sf, spec)));
-                        bsdf_pdf = sel * cp1 + (1.0f - sel) * pp1;
-                    }
-                    if (use_tree && build) {
-                        const ODTree* dd = &tree->dt[dt];
-                        if (rnd1(&rng) < s->fraction) {
-                            float uv[2];
-                            dtree_sample(dd, &rng, uv);
-                            float dv[3];
-                            const float cosTheta = 2.0f * uv[0] - 1.0f;
-                            const float sinTheta = sqrtf(fmaxf(1.0f - cosTheta * cosTheta, 0.0f));
-                            dv[0] = sinTheta * cospi_f(2.0f * uv[1]);
-                            dv[1] = sinTheta * sinpi_f(2.0f * uv[1]);
-                            dv[2] = cosTheta;
-                            float l = 1.0f / sqrtf(dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2]);
-                            direction = v3(dv[0] * l, dv[1] * l, dv[2] * l);
-                            cosine = vdot(direction, fn);
-                            float cp2 = fmaxf(cosine * inv_pi, 0.0f);
-                            float pp2 = phong_pdf_o(direction, refl, m->shininess);
-                            bsdf_val = vadd(vs(inv_pi, diffuse), vs(pp2, vs(sf, spec)));
-                            bsdf_pdf = sel * cp2 + (1.0f - sel) * pp2;
-                        }
-                        float dd3[3] = {direction.x, direction.y, direction.z}, c2[2];
-                        or_dir_to_canonical(1, dd3, c2);
-                        float dpdf = fmaxf(dtree_pdf(dd, c2[0], c2[1]), 0.0f);
-                        wo_pdf = (1.0f - s->fraction) * bsdf_pdf + s->fraction * dpdf;
-                    } else if (use_grid && build && prv_cell != UINT32_MAX) {
-                        /* SimpleGuide2.cu:350-377 */
-                        const float* w = grid->pyramid + (uint64_t)prv_cell * mqt_per;
-                        float dpdf;
-                        if (rnd1(&rng) < grid->fraction) {
-                            float uv[2], tp;
-                            mqt_sample_one(w, grid->level, &rng, &uv[0], &uv[1], &tp);
-                            dpdf = (float)((double)tp * (0.25 * 0.318309886183790691216444201927515678107738494873046875));
-                            float dv[3];
-                            const float cosTheta = 2.0f * uv[0] - 1.0f;
-                            const float sinTheta = sqrtf(fmaxf(1.0f - cosTheta * cosTheta, 0.0f));
-                            dv[0] = sinTheta * cospi_f(2.0f * uv[1]);
-                            dv[1] = sinTheta * sinpi_f(2.0f * uv[1]);
-                            dv[2] = cosTheta;
-                            float l = 1.0f / sqrtf(dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2]);
-                            direction = v3(dv[0] * l, dv[1] * l, dv[2] * l);
-                            cosine = vdot(direction, fn);
-                            float cp2 = fmaxf(cosine * inv_pi, 0.0f);
-                            float pp2 = phong_pdf_o(direction, refl, m->shininess);
-                            bsdf_val = vadd(vs(inv_pi, diffuse), vs(pp2, vs(sf, spec)));
-                            bsdf_pdf = sel * cp2 + (1.0f - sel) * pp2;
-                        } else {
-                            float dd3[3] = {direction.x, direction.y, direction.z}, c2[2];
-                            or_dir_to_canonical(1, dd3, c2);
-                            const float tp = mqt_pdf_one(w, grid->level, c2[0], c2[1]);
-                            dpdf = fmaxf((float)((double)(tp * 0.25f) * 0.318309886183790691216444201927515678107738494873046875), 0.0f);
-                        }
-                        wo_pdf = grid->fraction * dpdf + (1.0f - grid->fraction) * bsdf_pdf;
-                    } else {
-                        wo_pdf = bsdf_pdf;
-                    }
-                    cur_thr = wo_pdf > 0.0f ? vmul(thr, vdivs(vs(fmaxf(cosine, 0.0f), bsdf_val), wo_pdf)) : v3(0, 0, 0);
-                    if (flags & O_NEE) {
-                        if (depth < s->max_depth - 1 && s->nlights > 0) {
-                            if (flags & O_RIS) {
-                                float w_sum = 0.0f, fay = 0.0f, disty = 0.0f;
-                                uint32_t mc = 0;
-                                V3 fy = v3(0, 0, 0), ldy = v3(0, 0, 0);
-                                for (uint32_t k = 0; k < s->num_candidates; ++k) {
-                                    OLight l = o_sample_light(s, position, &rng);
-                                    float ndl = vdot(l.dir, fn), lndl = -vdot(l.dir, l.normal);
-                                    V3 b = phong_bsdf_o(diffuse, spec, m->shininess, l.dir, refl);
-                                    float g = fmaxf(ndl, 0.0f) * fmaxf(lndl, 0.0f) / (l.dist * l.dist);
-                                    V3 f = vmul(vmul(b, l.emission), v3(g, g, g));
-                                    float fa = vavg(f), wi = fa * l.inv_pdf;
-                                    w_sum += wi;
-                                    ++mc;
-                                    if ((wi / w_sum) >= rnd1(&rng)) { fy = f; fay = fa; ldy = l.dir; disty = l.dist; }
-                                }
-                                if (w_sum > 0.0f && fay > 0.0f &&
-                                    !o_trace(s, position, ldy, 0.0001f, disty - 0.0001f, 1, 0, 0, 0, 0))
-                                    L = vadd(L, vs(w_sum / (fay * (float)mc), vmul(thr, fy)));
-                            } else {
-                                OLight l = o_sample_light(s, position, &rng);
-                                V3 b = phong_bsdf_o(diffuse, spec, m->shininess, l.dir, refl);
-                                float g = fmaxf(-vdot(l.dir, l.normal), 0.0f) * fabsf(vdot(l.dir, fn)) / (l.dist * l.dist);
-                                if (!o_trace(s, position, l.dir, 0.0001f, l.dist - 0.0001f, 1, 0, 0, 0, 0))
-                                    L = vadd(L, vs(l.inv_pdf, vs(g, vmul(vmul(thr, b), l.emission))));
-                            }
-                        }
-                    } else {
-                        hflags |= 8u;
-                    }
-                    if (use_grid)
-                        cell = ((flags & O_LOCATE) && prv_cell == UINT32_MAX) ? grid_insert_cur(grid, gk, gb) : prv_cell;
-                } else if (m->type == 1) {
-                    V3 rn;
-                    float rri, ci = vdot(fn, dir);
-                    if (ci < 0.0f) { rn = fn; rri = 1.0f / m->ref_index; ci = -ci; }
-                    else { rn = v3(-fn.x, -fn.y, -fn.z); rri = m->ref_index; }
-                    float so2 = (1.0f - ci * ci) * (rri * rri);
-                    float f0 = ((1.0f - rri) / (1.0f + rri)) * ((1.0f - rri) / (1.0f + rri));
-                    float om = 1.0f - ci;
-                    float fres = f0 + (1.0f - f0) * (om * om * om * om * om);
-                    V3 rd = vunit(reflect_o(dir, rn));
-                    if (rnd1(&rng) < fres || so2 > 1.0f) {
-                        position = vadd(position, vs(0.0001f, rn));
-                        direction = rd; cosine = fabsf(ci); bsdf_val = spec; cur_thr = vmul(thr, spec);
-                    } else {
-                        position = vsub(position, vs(0.0001f, rn));
-                        float si2 = fmaxf(1.0f - ci * ci, 0.0f), co = sqrtf(1.0f - so2);
-                        V3 rf;
-                        if (si2 > 0.0f) rf = vunit(vsub(vs(sqrtf(so2), vdivs(vadd(dir, vs(ci, rn)), sqrtf(si2))), vs(co, rn)));
-                        else rf = dir;
-                        direction = rf; cosine = fabsf(vdot(rf, rn)); bsdf_val = v3(1, 1, 1); cur_thr = thr;
-                    }
-                    wo_pdf = fabsf(cosine);
-                    hflags |= 8u | 2u;
-                }
-                if (vdot(dir, fn) < 0.0f && count_emitted) L = vadd(L, vmul(thr, emis));
-                if (emis.x + emis.y + emis.z > 0.0f) hflags |= 16u;
+                OShade sh;
+                o_shade(s, flags, tree, grid, org, dir, t, prim, hu, hv, thr, pflags, depth, &rng, &sh);
+                position = sh.position;
+                direction = sh.direction;
+                cur_thr = sh.cur_thr;
+                bsdf_val = sh.bsdf_val;
+                L = sh.L;
+                cosine = sh.cosine;
+                wo_pdf = sh.wo_pdf;
+                hflags = sh.hflags;
+                const uint32_t cell = sh.cell;
                 if (recording && depth < O_KTV) {
                     OVert* v = &verts[depth];
                     v->pos = position; v->dir = direction; v->thr = cur_thr; v->rad = v3(0, 0, 0);
@@ -1235,4 +1303,77 @@ int64_t or_render(const OScene* s, uint32_t flags, void* tree_h, void* grid_h, u
         seeds[p] = rng;
     }
     return (int64_t)(p1 - p0);
+}
+
+/* ------------------------------------------------------------------ known answers
+ * The integrator's building blocks one call at a time, for the known-answer tests that pin
+ * them against RTLib's own code run on the host (oracle/ref) and against the golden
+ * fixture it wrote.  Xorshift32 states are in/out (one per case). */
+void or_kat_cosine(int64_t n, const float* normal, uint32_t* state, float* out) {
+    for (int64_t i = 0; i < n; ++i) {
+        V3 d = o_sample_cosine(v3(normal[3 * i], normal[3 * i + 1], normal[3 * i + 2]), &state[i]);
+        out[3 * i] = d.x; out[3 * i + 1] = d.y; out[3 * i + 2] = d.z;
+    }
+}
+void or_kat_phong(int64_t n, const float* refl, const float* shininess, uint32_t* state, float* out) {
+    for (int64_t i = 0; i < n; ++i) {
+        V3 d = o_sample_phong(v3(refl[3 * i], refl[3 * i + 1], refl[3 * i + 2]), shininess[i], &state[i]);
+        out[3 * i] = d.x; out[3 * i + 1] = d.y; out[3 * i + 2] = d.z;
+    }
+}
+void or_kat_triangle(int64_t n, const float* v, uint32_t* state, float* out) {
+    for (int64_t i = 0; i < n; ++i) {
+        const float* q = v + 9 * i;
+        V3 p = o_random_in_unit_triangle(v3(q[0], q[1], q[2]), v3(q[3], q[4], q[5]), v3(q[6], q[7], q[8]), &state[i]);
+        out[3 * i] = p.x; out[3 * i + 1] = p.y; out[3 * i + 2] = p.z;
+    }
+}
+/* nseq sequences of len updates: weights w[nseq][len], uniforms rnd[nseq][len]; per sequence
+ * the index last kept (-1: none), w_sum and m */
+void or_kat_reservoir(int64_t nseq, int32_t len, const float* w, const float* rnd, int32_t* sel, float* wsum,
+                      uint32_t* m) {
+    for (int64_t k = 0; k < nseq; ++k) {
+        float ws = 0.0f;
+        uint32_t mm = 0;
+        int32_t y = -1;
+        for (int32_t i = 0; i < len; ++i)
+            if (o_reservoir_update(&ws, &mm, w[k * len + i], rnd[k * len + i])) y = i;
+        sel[k] = y;
+        wsum[k] = ws;
+        m[k] = mm;
+    }
+}
+/* per case 14 floats: direction, normal, emission, distance, invPdf, position */
+void or_kat_light(const OScene* s, int64_t n, const float* p_in, uint32_t* state, float* out) {
+    for (int64_t i = 0; i < n; ++i) {
+        V3 pin = v3(p_in[3 * i], p_in[3 * i + 1], p_in[3 * i + 2]);
+        OLight l = o_sample_light(s, pin, &state[i]);
+        float* o = out + 14 * i;
+        V3 pos = l.pos;
+        o[0] = l.dir.x; o[1] = l.dir.y; o[2] = l.dir.z;
+        o[3] = l.normal.x; o[4] = l.normal.y; o[5] = l.normal.z;
+        o[6] = l.emission.x; o[7] = l.emission.y; o[8] = l.emission.z;
+        o[9] = l.dist; o[10] = l.inv_pdf;
+        o[11] = pos.x; o[12] = pos.y; o[13] = pos.z;
+    }
+}
+/* o_shade of n vertices: the ray (org, dir), hit distance t and triangle prim, throughput,
+ * previous hit flags and depth of each; per case 17 floats out (position, direction,
+ * throughput after the vertex, BSDF value, radiance added, cosine, woPdf) and the hit flags.
+ * tree: an or_sdtree handle (USE_TREE) or NULL. */
+void or_kat_shade(const OScene* s, uint32_t flags, void* tree, int64_t n, const float* org, const float* dir,
+                  const float* t, const uint32_t* prim, const float* thr, const uint32_t* pflags, const uint32_t* depth,
+                  uint32_t* state, float* out, uint32_t* out_flags) {
+    for (int64_t i = 0; i < n; ++i) {
+        OShade sh;
+        o_shade(s, flags, (OSDTree*)tree, NULL, v3(org[3 * i], org[3 * i + 1], org[3 * i + 2]),
+                v3(dir[3 * i], dir[3 * i + 1], dir[3 * i + 2]), t[i], prim[i], 0.0f, 0.0f,
+                v3(thr[3 * i], thr[3 * i + 1], thr[3 * i + 2]), pflags[i], depth[i], &state[i], &sh);
+        float* o = out + 17 * i;
+        const V3* vv[5] = {&sh.position, &sh.direction, &sh.cur_thr, &sh.bsdf_val, &sh.L};
+        for (int k = 0; k < 5; ++k) { o[3 * k] = vv[k]->x; o[3 * k + 1] = vv[k]->y; o[3 * k + 2] = vv[k]->z; }
+        o[15] = sh.cosine;
+        o[16] = sh.wo_pdf;
+        out_flags[i] = sh.hflags;
+    }
 }

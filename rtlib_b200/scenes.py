@@ -75,16 +75,32 @@ def _camera(eye, look, up, vfov_deg, aspect):
             "v": (v * th).astype(np.float32), "w": w.astype(np.float32)}
 
 
-def cornell_box(width=512, height=512, light_grid=1, back_texture=False):
+def cornell_box(width=512, height=512, light_grid=1, back_texture=False, materials="lambert"):
     """Cornell-style box in [0,1]^3: five wall quads, two boxes rotated -18 / +18 degrees
     (34 triangles), and a 0.25 x 0.25 emissive quad under the ceiling, radiance (17,12,4),
     split into light_grid x light_grid quads (each its own NEE light mesh).  Albedos 0.73
     (white), (0.65,0.05,0.05) (red, left), (0.12,0.45,0.15) (green, right).  back_texture
-    gives the back wall material diffuse texture 0 (albedo 1 times the texture)."""
+    gives the back wall material diffuse texture 0 (albedo 1 times the texture).
+
+    materials="glass_phong" exercises RTLib's other two shading branches: the tall box is a
+    dielectric (index 1.5, specular (0.98, 0.98, 0.98); SimpleGuide.cu:424-491), the back wall a
+    Phong surface (diffuse 0.45, specular 0.25, shininess 40) and the short box a glossy one
+    (diffuse 0.2, specular 0.6, shininess 200), so the Phong lobe and its selection
+    probability (SimpleGuide.cu:331-377) and delta vertices enter every path."""
     b = _Builder()
-    mats = [_mat(diffuse=(0.73, 0.73, 0.73)), _mat(diffuse=(0.65, 0.05, 0.05)), _mat(diffuse=(0.12, 0.45, 0.15)),
-            _mat(diffuse=(1.0, 1.0, 1.0) if back_texture else (0.73, 0.73, 0.73), texture=0 if back_texture else -1)]
+    if materials not in ("lambert", "glass_phong"):
+        raise ValueError(f"unknown material set {materials!r}")
+    gp = materials == "glass_phong"
+    back = (_mat(diffuse=(1.0, 1.0, 1.0) if back_texture else (0.73, 0.73, 0.73), texture=0 if back_texture else -1)
+            if not gp else _mat(diffuse=(0.45, 0.45, 0.45), specular=(0.25, 0.25, 0.25), shininess=40.0))
+    mats = [_mat(diffuse=(0.73, 0.73, 0.73)), _mat(diffuse=(0.65, 0.05, 0.05)), _mat(diffuse=(0.12, 0.45, 0.15)), back]
     W, R, G, BK = 0, 1, 2, 3
+    short_box, tall_box = W, W
+    if gp:
+        mats.append(_mat(diffuse=(0.2, 0.2, 0.2), specular=(0.6, 0.6, 0.6), shininess=200.0))
+        short_box = len(mats) - 1
+        mats.append(_mat(specular=(0.98, 0.98, 0.98), ref_index=1.5, type=GLASS))
+        tall_box = len(mats) - 1
     b.quad((0, 0, 0), (0, 0, 1), (1, 0, 0), W)      # floor, normal +y
     b.quad((0, 1, 0), (1, 0, 0), (0, 0, 1), W)      # ceiling, normal -y
     b.quad((0, 0, 0), (1, 0, 0), (0, 1, 0), BK)     # back wall z=0, normal +z
@@ -92,8 +108,8 @@ def cornell_box(width=512, height=512, light_grid=1, back_texture=False):
     b.quad((1, 0, 0), (0, 0, 1), (0, 1, 0), G)      # right wall x=1, normal -x
     # the boxes stand 1 mm above the floor: a bottom face coplanar with the floor would make
     # the closest hit a tie between two triangles with opposite normals
-    b.box((0.33, 0.151, 0.62), (0.3, 0.3, 0.3), -18.0, W)
-    b.box((0.66, 0.301, 0.36), (0.3, 0.6, 0.3), 18.0, W)
+    b.box((0.33, 0.151, 0.62), (0.3, 0.3, 0.3), -18.0, short_box)
+    b.box((0.66, 0.301, 0.36), (0.3, 0.6, 0.3), 18.0, tall_box)
     n_geom = len(b.tris)
     light_first, light_count, light_emit = [], [], []
     s = 0.25 / light_grid

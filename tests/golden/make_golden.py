@@ -5,7 +5,7 @@ the host by oracle/ref) on small seeded inputs and stores inputs and outputs as 
 so the parity tests can check the CPU oracle (and the CUDA path) against the reference on
 machines where the reference tree is absent.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [kat sdtree hashgrid mqt integrator]
 """
 import os
 import sys
@@ -121,10 +121,49 @@ def mqt(r):
                         sample_uv=suv, sample_pdf=spdf, pdf_eval=pe)
 
 
+def integrator(r):
+    """The integrator's building blocks from RTLib's own code (SimpleKernel.h, SimpleGuide.cu,
+    Random.h, VectorFunction.h, staged by oracle/ref): cosine and Phong lobe samples, points
+    in triangles, reservoir sequences, light samples of the glass / Phong Cornell box (2 x 2
+    light meshes), and whole closest-hit shadings of 1024 random vertices under each flag set,
+    the SD-tree ones in the tree both sides build from tests/kat_integrator.py's records."""
+    sys.path.insert(0, os.path.dirname(OUT))
+    import kat_integrator as K
+    from oracle.oracle import IntegratorKAT
+    sc = K.scene()
+    kat_ = IntegratorKAT(r, sc, fraction=0.5)
+    rng = np.random.default_rng(17)
+    n = 2048
+    nrm = rng.normal(size=(n, 3)).astype(np.float32)
+    nrm /= np.linalg.norm(nrm, axis=1, keepdims=True)
+    seeds = rng.integers(1, 2 ** 32, n, dtype=np.uint64).astype(np.uint32)
+    shin = rng.choice(np.array([1.0, 10.0, 40.0, 200.0], np.float32), n)
+    tri = rng.uniform(-1, 1, (n, 9)).astype(np.float32)
+    pin = rng.uniform(0, 1, (n, 3)).astype(np.float32)
+    w = rng.lognormal(0.0, 1.0, (256, 32)).astype(np.float32)
+    w[::5, ::3] = 0.0
+    w[7] = 0.0
+    rnd = rng.random((256, 32)).astype(np.float32)
+    cos_d, cos_s = kat_.cosine(nrm, seeds)
+    ph_d, ph_s = kat_.phong(nrm, shin, seeds)
+    tr_p, tr_s = kat_.triangle(tri, seeds)
+    lt_o, lt_s = kat_.light(pin, seeds)
+    sel, wsum, m = kat_.reservoir(w, rnd)
+    out = dict(normal=nrm, seeds=seeds, shininess=shin, tri=tri, p_in=pin, res_w=w, res_rnd=rnd, cos_dir=cos_d,
+               cos_state=cos_s, phong_dir=ph_d, phong_state=ph_s, tri_point=tr_p, tri_state=tr_s, light=lt_o,
+               light_state=lt_s, res_sel=sel, res_wsum=wsum, res_m=m)
+    cases = K.shade_cases(sc, 1024, 23)
+    out.update({"case_" + k: v for k, v in cases.items()})
+    tree = K.build_tree(r, K.tree_records())
+    for fl in K.FLAG_SETS:
+        o, f, st = kat_.shade(fl, cases, tree if fl & 8 else None)
+        out.update({f"shade{fl}_out": o, f"shade{fl}_flags": f, f"shade{fl}_state": st})
+    np.savez_compressed(os.path.join(OUT, "kat_integrator.npz"), flag_sets=np.array(K.FLAG_SETS), **out)
+
+
 if __name__ == "__main__":
     r = Reference()
-    kat(r)
-    sdtree(r)
-    hashgrid(r)
-    mqt(r)
-    print("golden fixtures written to", OUT)
+    which = sys.argv[1:] or ["kat", "sdtree", "hashgrid", "mqt", "integrator"]
+    for name in which:
+        globals()[name](r)
+    print("golden fixtures", which, "written to", OUT)

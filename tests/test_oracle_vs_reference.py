@@ -149,3 +149,89 @@ def test_live_reference_hashgrid_random(oracle, reference):
     np.testing.assert_array_equal(oracle.hashgrid_insert(pos, off, size, bounds, nslots, a),
                                   reference.hashgrid_insert(pos, off, size, bounds, nslots, b))
     np.testing.assert_array_equal(a, b)
+
+
+# ---------------------------------------------------------------- integrator (A-6)
+# RTLib's shading code run on the host (oracle/ref stages SimpleKernel.h:26-143 and
+# SimpleGuide.cu:28-47, 287-496) against the C restatement.  Random numbers: the same
+# draws in the same order (end states equal).  Floats: bit-exact except where sin / cos
+# enter (the restatement forms cos(2 pi x) as cospi(2x), as the CUDA path does), within
+# 5e-4 of max(|value|, 1e-3).
+SHADE_RTOL = 5e-4
+
+
+def _kat_scene():
+    import kat_integrator as K
+    return K, K.scene()
+
+
+def _check_shade(mine, ref):
+    (o, f, s), (ro, rf, rs) = mine, ref
+    np.testing.assert_array_equal(f, rf)
+    np.testing.assert_array_equal(s, rs)
+    err = np.abs(o - ro) / np.maximum(np.abs(ro), 1e-3)
+    assert err.max() <= SHADE_RTOL, err.max()
+    assert (o == ro).all(1).mean() > 0.6  # the rest carry the sin / cos ulps
+
+
+def test_golden_integrator_building_blocks(oracle):
+    from oracle.oracle import IntegratorKAT
+    g = _load("kat_integrator.npz")
+    K, sc = _kat_scene()
+    k = IntegratorKAT(oracle, sc, fraction=0.5)
+    d, st = k.cosine(g["normal"], g["seeds"])
+    np.testing.assert_array_equal(st, g["cos_state"])
+    np.testing.assert_allclose(d, g["cos_dir"], rtol=0, atol=1e-6)
+    for got, want in zip(k.phong(g["normal"], g["shininess"], g["seeds"]), (g["phong_dir"], g["phong_state"])):
+        np.testing.assert_array_equal(got, want)
+    for got, want in zip(k.triangle(g["tri"], g["seeds"]), (g["tri_point"], g["tri_state"])):
+        np.testing.assert_array_equal(got, want)
+    for got, want in zip(k.light(g["p_in"], g["seeds"]), (g["light"], g["light_state"])):
+        np.testing.assert_array_equal(got, want)
+    for got, want in zip(k.reservoir(g["res_w"], g["res_rnd"]), (g["res_sel"], g["res_wsum"], g["res_m"])):
+        np.testing.assert_array_equal(got, want)
+    assert (g["res_sel"] == -1).any() and (g["res_sel"] >= 0).any()
+
+
+def test_golden_integrator_shading(oracle):
+    """Closest-hit shading of 1024 vertices on Phong (Lambertian and glossy), glass and
+    emitter triangles, front and back faces, under DEF, NEE, NEE+RIS, SD-tree recording and
+    SD-tree guiding with NEE and with RIS, against RTLib's own __closesthit__radiance."""
+    from oracle.oracle import IntegratorKAT
+    g = _load("kat_integrator.npz")
+    K, sc = _kat_scene()
+    k = IntegratorKAT(oracle, sc, fraction=0.5)
+    tree = K.build_tree(oracle, K.tree_records())
+    cases = {key[5:]: g[key] for key in g.files if key.startswith("case_")}
+    for fl in g["flag_sets"]:
+        fl = int(fl)
+        _check_shade(k.shade(fl, cases, tree if fl & 8 else None),
+                     (g[f"shade{fl}_out"], g[f"shade{fl}_flags"], g[f"shade{fl}_state"]))
+    # the fixture covers every branch: glass (delta flag), Phong with NEE, emitters (finish)
+    f = g["shade25_flags"]
+    assert (f & 2).any() and (f & 16).any() and ((f & 8) == 0).any()
+
+
+def test_live_reference_integrator(oracle, reference):
+    from oracle.oracle import IntegratorKAT
+    K, sc = _kat_scene()
+    mine, ref = IntegratorKAT(oracle, sc, fraction=0.5), IntegratorKAT(reference, sc, fraction=0.5)
+    rng = np.random.default_rng(99)
+    n = 20000
+    nrm = rng.normal(size=(n, 3)).astype(np.float32)
+    nrm /= np.linalg.norm(nrm, axis=1, keepdims=True)
+    seeds = rng.integers(1, 2 ** 32, n, dtype=np.uint64).astype(np.uint32)
+    shin = rng.uniform(0.0, 300.0, n).astype(np.float32)
+    for a, b in ((mine.phong(nrm, shin, seeds), ref.phong(nrm, shin, seeds)),
+                 (mine.light(nrm * 0.3 + 0.5, seeds), ref.light(nrm * 0.3 + 0.5, seeds))):
+        for x, y in zip(a, b):
+            np.testing.assert_array_equal(x, y)
+    (d, s), (rd, rs) = mine.cosine(nrm, seeds), ref.cosine(nrm, seeds)
+    np.testing.assert_array_equal(s, rs)
+    np.testing.assert_allclose(d, rd, rtol=0, atol=1e-6)
+    rec = K.tree_records()
+    to, tr = K.build_tree(oracle, rec), K.build_tree(reference, rec)
+    assert to.export(True).topology == tr.export(True).topology
+    cases = K.shade_cases(sc, n, 7)
+    for fl in K.FLAG_SETS:
+        _check_shade(mine.shade(fl, cases, to if fl & 8 else None), ref.shade(fl, cases, tr if fl & 8 else None))

@@ -128,6 +128,47 @@ def test_guided_render_matches_oracle(cuda, oracle):
     assert tree.status() == 0
 
 
+@pytest.mark.parametrize("flags", [0, 1, 3])
+def test_glass_phong_render_matches_oracle(cuda, oracle, flags):
+    """DEF, NEE and NEE + RIS on the Cornell box with a glass box (delta vertices, emission
+    counted after a delta bounce), a Phong back wall and a glossy Phong box (specular lobe,
+    its selection probability and pdf mixture), 64 x 64, 8 spp, against the CPU integrator
+    whose per-vertex shading is pinned to RTLib's own closest-hit code."""
+    from oracle.oracle import OracleRenderer
+    sc = scenes.cornell_box(64, 64, materials="glass_phong")
+    gimg, _ = _gpu_render(cuda, sc, 64, 64, 8, flags)
+    r = OracleRenderer(oracle, sc, width=64, height=64)
+    r.render(8, flags)
+    _compare(gimg, r.image())
+
+
+def test_glass_phong_guided_render_matches_oracle(cuda, oracle):
+    """The guided PGNEE schedule on the glass / Phong box: delta vertices are not recorded,
+    glossy vertices are, and the guide mixes with the Phong lobe's pdf."""
+    from oracle.oracle import OracleRenderer
+    from rtlib_b200.sdtree import SDTree, SDTreeController
+    from rtlib_b200.tracer import FLAG_NEE, Tracer
+    w = h = 48
+    budget = 31
+    sc = scenes.cornell_box(w, h, materials="glass_phong")
+    mn, mx = (-0.005,) * 3, (1.005,) * 3
+    tree = SDTree(mn, mx, fraction=0.5)
+    ctrl = SDTreeController(tree, budget, iteration_for_built=0, ratio_for_budget=1.0, samples_per_launch=1)
+    tr = Tracer(sc, cuda, max_depth=8, width=w, height=h)
+    ctrl.start()
+    tr.render_guided(tree, ctrl, FLAG_NEE, samples_per_launch=1)
+    gimg = tr.image().cpu().numpy()
+    ot = oracle.sdtree(mn, mx)
+    r = OracleRenderer(oracle, sc, width=w, height=h, fraction=0.5)
+    r.render_guided(ot, budget, ratio_for_budget=1.0)
+    assert tr.stats()["samples"] == r.samples
+    _compare(gimg, r.image(), rel_mse=1e-3, frac=0.97)
+    eg, eo = tree.export(True), ot.export(True)
+    assert eg.topology == eo.topology
+    np.testing.assert_allclose(eg.dsums, eo.dsums, rtol=1e-3, atol=1e-2)
+    assert tree.status() == 0
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("keying", [0, 1])
 def test_grid_guided_render_matches_oracle(cuda, oracle, keying):
