@@ -1040,6 +1040,47 @@ def _peaks_tensor():
     return 1590.0, "fallback bf16 TFLOP/s"
 
 
+# ---------------------------------------------------------------------------- adjoint workload
+def bench_adjoint(args):
+    """Config 4: path-replay gradients of an L2 image loss w.r.t. a 256 x 256 albedo texture and
+    16 emitter radiances at 512 x 512, 64 spp, against common-random-number central differences
+    (eps 1e-3) on 512 texels and all emitters.  The value is the largest relative error of the
+    checked gradients (those above 1 % of the largest, below which the difference itself is
+    float noise); the line also carries the median, the relative error of the whole vector and
+    the render rates."""
+    import torch
+    from rtlib_b200 import diff
+    dev = torch.device("cuda", 0)
+    clocks = ClockSampler(0)
+    clocks.start()
+    t0 = time.perf_counter()
+    r = diff.config4_gradients(dev)
+    wall = time.perf_counter() - t0
+    clk = clocks.stop()
+    adj = np.concatenate([r["adj_texels"], r["adj_lights"]]).astype(np.float64)
+    fd = np.concatenate([r["fd_texels"], r["fd_lights"]])
+    rel_all = []
+    for a, f in ((r["adj_texels"], r["fd_texels"]), (r["adj_lights"], r["fd_lights"])):
+        a, f = np.asarray(a, np.float64), np.asarray(f, np.float64)
+        big = np.abs(f) > 1e-2 * np.abs(f).max()
+        rel_all.append(np.abs(a[big] - f[big]) / np.abs(f[big]))
+    rel = np.concatenate(rel_all)
+    paths = r["paths_per_render"]
+    return {"metric": "adjoint-vs-FD gradient relative error (max over checked gradients)", "value": float(rel.max()),
+            "unit": "ratio", "n_gpus": 1, "steps": 1, "warmup": 0, "ms_per_step": wall * 1e3,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "config 4: Cornell box 512x512, back-wall albedo texture 256x256 RGB, ceiling light "
+                                   "as 4x4 emitters, L2 loss to a target with the texture perturbed N(0,0.05); "
+                                   "forward and adjoint 64 spp, depth 8, NEE; CRN central differences eps 1e-3 on "
+                                   "512 random texels (x3 channels) and all 16 emitters (x3)"},
+            "median_rel_err": float(np.median(rel)), "checked": int(rel.size), "gradients": int(adj.size),
+            "texel_rel_err_max": float(rel_all[0].max()), "emitter_rel_err_max": float(rel_all[1].max()),
+            "vector_rel_err": float(np.linalg.norm(adj - fd) / np.linalg.norm(fd)),
+            "forward_Mpaths_s": paths / (r["forward_ms"] * 1e-3) / 1e6,
+            "adjoint_Mpaths_s": paths / (r["adjoint_ms"] * 1e-3) / 1e6,
+            "note": "adjoint = one primal and one adjoint replay wave per sample", "clocks": clk}
+
+
 # ---------------------------------------------------------------------------- plumbing
 def _barrier(world):
     if world > 1:
@@ -1064,7 +1105,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="cornell", choices=["cornell", "sdtree", "hashgrid", "occluded", "learned",
-                                                               "mlp"])
+                                                               "mlp", "adjoint"])
     ap.add_argument("--budgets", default="30,120", help="learned: equal-time budgets in seconds")
     ap.add_argument("--ref-seconds", type=float, default=300.0, help="learned: reference render time")
     ap.add_argument("--epochs", type=int, default=8, help="learned: Adam epochs over each pass's records")
@@ -1113,6 +1154,16 @@ def main():
                            "sdtree_arm": "plain SD-tree guiding, BSDF/guide mixing 0.5"},
                 "budgets": r["budgets"]}
         print(json.dumps(line), flush=True)
+        return 0
+    if args.workload == "adjoint":
+        if args.impl == "reference":
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "unavailable": "RTLib has no adjoint / differentiable renderer"}),
+                      flush=True)
+            return 0
+        if rank != 0:
+            return 0
+        print(json.dumps(bench_adjoint(args)), flush=True)
         return 0
     if args.workload == "mlp" and args.impl == "reference":
         if rank == 0:

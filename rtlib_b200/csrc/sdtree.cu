@@ -21,7 +21,6 @@ namespace rtpg {
 constexpr int kRecordBlock = 256;
 constexpr int kTreeBlock = 256;
 constexpr uint32_t kVirtual = 0xffffffffu;
-constexpr uint32_t kStageSTree = 8192;  // STree nodes staged in shared memory by the queries
 
 // ------------------------------------------------------------------ clear
 __global__ void k_clear(SDTreeDev t) {
@@ -29,6 +28,7 @@ __global__ void k_clear(SDTreeDev t) {
         t.counts[0] = 1;
         t.counts[1] = 1;
         t.counts[2] = 1;
+        t.counts[3] = 1;
         t.snode[0] = kLeafBit | 0u;
         t.b_off[0] = 0; t.b_cnt[0] = 1; t.s_off[0] = 0; t.s_cnt[0] = 1;
         t.b_statw[0] = 0ull;
@@ -41,6 +41,7 @@ __global__ void k_clear(SDTreeDev t) {
         z.child = make_ushort4(0, 0, 0, 0);
         z.pad0 = z.pad1 = 0;
         t.s_nodes[0] = z;
+        t.s_q[0] = make_sqnode(z.sums, z.child);
     }
 }
 
@@ -85,7 +86,7 @@ __global__ void __launch_bounds__(kRecordBlock) k_record(SDTreeDev t, int64_t n,
             const float sw = stat_w ? stat_w[i] : 1.0f;
             const float irr = __fdiv_rn(radiance[i], wo);
             if (isfinite(sw) && sw > 0.0f) {
-                const uint32_t d = stree_lookup(st, t.mn, t.mx, pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]);
+                const uint32_t d = stree_lookup(st, t.mn, t.mx, pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], t.inv_size);
                 k_w = d;
                 v_w = to_fx(sw, t.fx, t.status);
                 if (isfinite(irr) && irr > 0.0f) {
@@ -180,6 +181,7 @@ __global__ void __launch_bounds__(kTreeBlock) k_build(SDTreeDev t) {
                 nd.child = c;
                 nd.pad0 = nd.pad1 = 0;
                 t.s_nodes[off + j] = nd;
+                t.s_q[off + j] = make_sqnode(nd.sums, c);
             }
             __syncthreads();
         }
@@ -196,6 +198,8 @@ __global__ void __launch_bounds__(kTreeBlock) k_build(SDTreeDev t) {
         }
         __syncthreads();
     }
+    // every building node is now a sampling node, at the same index
+    if (blockIdx.x == 0 && threadIdx.x == 0) t.counts[3] = t.counts[2];
 }
 
 // ------------------------------------------------------------------ spatial refine
@@ -463,27 +467,39 @@ __global__ void k_reset_commit(SDTreeDev t, const unsigned long long* node_total
 // DTree's GetMean test once, the guided sample, the pdf of the sampled canonical point
 // (DTreeT::Pdf) and optionally the direction and the pdf of that direction after the
 // dir -> canonical round trip the closest-hit program performs (SimpleGuide.cu:361-368).
-__global__ void __launch_bounds__(256) k_sample_pdf(SDTreeDev t, int64_t n, const float* __restrict__ pos,
-                                                    const uint32_t* __restrict__ seeds, uint32_t seed_base,
-                                                    float* __restrict__ out_uv, float* __restrict__ out_pdf_uv,
-                                                    float* __restrict__ out_dir, float* __restrict__ out_pdf_dir) {
-    __shared__ uint32_t s_st[kStageSTree];
-    const uint32_t nst = t.counts[0];
-    const bool staged = nst <= kStageSTree;
+// The descents read the 32-byte SQNode of each visited node, from shared memory when the
+// whole sampling pool fits (kStageSQ nodes), else through L1.
+constexpr uint32_t kSampleBlock = 256;
+constexpr uint32_t kStageSTreeSample = 4096;  // 16 KB
+constexpr uint32_t kStageSQ = 256;            // 8 KB
+__global__ void __launch_bounds__(kSampleBlock, 8) k_sample_pdf(SDTreeDev t, int64_t n, const float* __restrict__ pos,
+                                                            const uint32_t* __restrict__ seeds, uint32_t seed_base,
+                                                            float* __restrict__ out_uv, float* __restrict__ out_pdf_uv,
+                                                            float* __restrict__ out_dir, float* __restrict__ out_pdf_dir) {
+    __shared__ uint32_t s_st[kStageSTreeSample];
+    __shared__ SQNode s_sq[kStageSQ];
+    const uint32_t nst = t.counts[0], nsq = t.counts[3];
+    const bool staged = nst <= kStageSTreeSample, staged_q = nsq <= kStageSQ;
     if (staged)
         for (uint32_t i = threadIdx.x; i < nst; i += blockDim.x) s_st[i] = t.snode[i];
+    if (staged_q) {
+        const uint4* src = reinterpret_cast<const uint4*>(t.s_q);
+        uint4* dst = reinterpret_cast<uint4*>(s_sq);
+        for (uint32_t i = threadIdx.x; i < 2 * nsq; i += blockDim.x) dst[i] = src[i];
+    }
     __syncthreads();
     const uint32_t* st = staged ? s_st : t.snode;
+    const SQNode* sq_nodes = staged_q ? s_sq : t.s_q;
     const int64_t stride = int64_t(gridDim.x) * blockDim.x;
     for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
-        const uint32_t d = stree_lookup(st, t.mn, t.mx, pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]);
+        const uint32_t d = stree_lookup(st, t.mn, t.mx, pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], t.inv_size);
         uint32_t rng = seeds ? seeds[i] : (pcg1d(seed_base + (uint32_t)i) | 1u);
         const uint32_t off = t.s_off[d];
         const bool guided = t.s_guided[d] != 0;
         DSquare sq;
-        const float2 uv = dtree_sample_sq(t.s_nodes, off, guided, rng, sq);
+        const float2 uv = dtree_sample_sq(sq_nodes, off, guided, rng, sq);
         if (out_uv) reinterpret_cast<float2*>(out_uv)[i] = uv;
-        if (out_pdf_uv) out_pdf_uv[i] = dtree_pdf_in(t.s_nodes, off, guided, sq, uv.x, uv.y);
+        if (out_pdf_uv) out_pdf_uv[i] = dtree_pdf_in(sq_nodes, off, guided, sq, uv.x, uv.y);
         if (out_dir || out_pdf_dir) {
             const float3 dv = normalize3(canonical_to_dir(uv.x, uv.y));
             if (out_dir) {
@@ -493,7 +509,7 @@ __global__ void __launch_bounds__(256) k_sample_pdf(SDTreeDev t, int64_t n, cons
             }
             if (out_pdf_dir) {
                 const float2 c = dir_to_canonical(dv.x, dv.y, dv.z);
-                out_pdf_dir[i] = dtree_pdf_in(t.s_nodes, off, guided, sq, c.x, c.y);
+                out_pdf_dir[i] = dtree_pdf_in(sq_nodes, off, guided, sq, c.x, c.y);
             }
         }
     }
@@ -503,11 +519,11 @@ __global__ void __launch_bounds__(256) k_pdf(SDTreeDev t, int64_t n, const float
                                              const float* __restrict__ dir, int canonical, float* __restrict__ out) {
     const int64_t stride = int64_t(gridDim.x) * blockDim.x;
     for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
-        const uint32_t d = stree_lookup(t.snode, t.mn, t.mx, pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]);
+        const uint32_t d = stree_lookup(t.snode, t.mn, t.mx, pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], t.inv_size);
         float2 c;
         if (canonical) c = reinterpret_cast<const float2*>(dir)[i];
         else c = dir_to_canonical(dir[3 * i], dir[3 * i + 1], dir[3 * i + 2]);
-        out[i] = dtree_pdf_g(t.s_nodes, t.s_off[d], t.s_guided[d] != 0, c.x, c.y);
+        out[i] = dtree_pdf_g(t.s_q, t.s_off[d], t.s_guided[d] != 0, c.x, c.y);
     }
 }
 
@@ -596,6 +612,17 @@ int rtpg_sdtree_create(const float* aabb_min, const float* aabb_max, uint32_t ma
     SDTreeDev& t = h->dev;
     t.mn = make_float3(h->mn[0], h->mn[1], h->mn[2]);
     t.mx = make_float3(h->mx[0], h->mx[1], h->mx[2]);
+    {
+        // a division by a power of two equals the product with its reciprocal, bit for bit
+        float inv[3];
+        for (int k = 0; k < 3; ++k) {
+            const float d = h->mx[k] - h->mn[k];
+            int e = 0;
+            inv[k] = (d > 0.0f && std::isfinite(d) && std::frexp(d, &e) == 0.5f && e > -120 && e < 120)
+                         ? std::ldexp(1.0f, 1 - e) : 0.0f;
+        }
+        t.inv_size = make_float3(inv[0], inv[1], inv[2]);
+    }
     t.fx.scale = ldexpf(1.0f, c.fixed_point_bits);
     t.fx.inv_scale = ldexpf(1.0f, -c.fixed_point_bits);
     t.cap_snodes = c.max_stree_nodes;
@@ -611,7 +638,7 @@ int rtpg_sdtree_create(const float* aabb_min, const float* aabb_max, uint32_t ma
         (r = h->alloc(&t.s_area, nd)) || (r = h->alloc(&t.s_statw, nd)) || (r = h->alloc(&t.s_guided, nd)) ||
         (r = h->alloc(&t.b_lvl, nd * (kMaxLevels + 1))) || (r = h->alloc(&t.b_nlvl, nd)) ||
         (r = h->alloc(&t.b_sums, nn * 4)) || (r = h->alloc(&t.b_child, nn)) || (r = h->alloc(&t.b_area, nn)) ||
-        (r = h->alloc(&t.s_nodes, nn)) || (r = h->alloc(&h->cnt_s, ns)) || (r = h->alloc(&h->off_s, ns)) ||
+        (r = h->alloc(&t.s_nodes, nn)) || (r = h->alloc(&t.s_q, nn)) || (r = h->alloc(&h->cnt_s, ns)) || (r = h->alloc(&h->off_s, ns)) ||
         (r = h->alloc(&h->cnt_d, ns)) || (r = h->alloc(&h->off_d, ns)) || (r = h->alloc(&h->ksplit, ns)) ||
         (r = h->alloc(&h->node_cnt, nd)) || (r = h->alloc(&h->node_off, nd)) ||
         (r = h->alloc(&h->partials, 2 * scan_partials_words(std::max(c.max_stree_nodes, c.max_dtrees)))) ||
@@ -722,8 +749,8 @@ int rtpg_sdtree_sample_pdf(rtpg_sdtree* h, int64_t n, const float* pos, const ui
     if (n < 0 || (n > 0 && !pos)) return fail(RTPG_EINVAL, "rtpg_sdtree_sample_pdf: bad arguments");
     if (!aligned8(out_uv) || !aligned4(pos)) return fail(RTPG_EINVAL, "rtpg_sdtree_sample_pdf: misaligned array");
     if (n == 0) return RTPG_OK;
-    k_sample_pdf<<<grid_for(n, 256, 8), 256, 0, as_stream(stream)>>>(h->dev, n, pos, seeds, seed_base, out_uv,
-                                                                     out_pdf_uv, out_dir, out_pdf_dir);
+    k_sample_pdf<<<grid_for(n, kSampleBlock, 8), kSampleBlock, 0, as_stream(stream)>>>(
+        h->dev, n, pos, seeds, seed_base, out_uv, out_pdf_uv, out_dir, out_pdf_dir);
     RTPG_LAUNCH_CHECK();
     return RTPG_OK;
 }
@@ -1038,6 +1065,7 @@ extern "C" int rtpg_sdtree_import(rtpg_sdtree* h, int64_t stree_nodes, int64_t l
     std::vector<unsigned long long> b_sums;
     std::vector<ushort4> b_child;
     std::vector<SNode> s_nodes;
+    std::vector<SQNode> s_q;
     const float scale = t.fx.scale;
     auto fx = [&](float v, unsigned long long& out) -> bool {
         const float s = v * scale;
@@ -1103,6 +1131,7 @@ extern "C" int rtpg_sdtree_import(rtpg_sdtree* h, int64_t stree_nodes, int64_t l
             nd.child = make_ushort4(c[0], c[1], c[2], c[3]);
             nd.pad0 = nd.pad1 = 0;
             s_nodes.push_back(nd);
+            s_q.push_back(make_sqnode(nd.sums, nd.child));
         }
     }
     if (bpos != building_nodes || spos != sampling_nodes)
@@ -1110,7 +1139,8 @@ extern "C" int rtpg_sdtree_import(rtpg_sdtree* h, int64_t stree_nodes, int64_t l
     if (b_child.size() > t.cap_nodes || s_nodes.size() > t.cap_nodes)
         return fail(RTPG_ECAPACITY, "rtpg_sdtree_import: quadtree nodes exceed the pool capacity %u", t.cap_nodes);
     cudaStream_t st = as_stream(stream);
-    const uint32_t counts[3] = {(uint32_t)stree_nodes, (uint32_t)leaves, (uint32_t)b_child.size()};
+    const uint32_t counts[4] = {(uint32_t)stree_nodes, (uint32_t)leaves, (uint32_t)b_child.size(),
+                                (uint32_t)s_nodes.size()};
     RTPG_CUDA(cudaMemcpyAsync(t.counts, counts, sizeof(counts), cudaMemcpyHostToDevice, st));
     RTPG_CUDA(ul(t.snode, snode, st));
     RTPG_CUDA(ul(t.b_off, b_off, st));
@@ -1127,6 +1157,7 @@ extern "C" int rtpg_sdtree_import(rtpg_sdtree* h, int64_t stree_nodes, int64_t l
     RTPG_CUDA(ul(t.b_sums, b_sums, st));
     RTPG_CUDA(ul(t.b_child, b_child, st));
     RTPG_CUDA(ul(t.s_nodes, s_nodes, st));
+    RTPG_CUDA(ul(t.s_q, s_q, st));
     // the host vectors must outlive the copies
     RTPG_CUDA(cudaStreamSynchronize(st));
     return RTPG_OK;

@@ -8,7 +8,8 @@
 //           stat-weight (int64 fixed point), sampling sum / area / stat-weight (float),
 //           level starts of the breadth-first building tree.
 //   pools   building nodes: 4 x u64 fixed-point sums (32 B) + ushort4 local children;
-//           sampling nodes: SNode, 32 B = one DRAM sector: float4 sums + ushort4 children.
+//           sampling nodes: SNode, 32 B = one DRAM sector: float4 sums + ushort4 children,
+//           and beside it SQNode, the 32 B a sampling or pdf descent reads (see there).
 #pragma once
 #include "common.cuh"
 #include "limits.cuh"
@@ -25,11 +26,64 @@ struct __align__(32) SNode {
     uint32_t pad0, pad1;
 };
 
+// What a sampling or pdf descent reads of a sampling node (32 B, one sector): the quotients of
+// the quadrant sums that DTreeNodeT::Sample and ::Pdf (PG.h:229-320) divide out at every visit,
+// formed once when the node is written, with the same IEEE operations on the same operands, so
+// that a descent reads them instead of dividing (bit-identical results):
+//   bnd = partial / total, btl = topLeft / partial, btr = topRight / (total - partial)
+//         with partial = s0 + s2 and total = ((s0 + s1) + s2) + s3;
+//   fac_i = 4 s_i / total (the pdf factor of quadrant i);
+//   meta: bits 0-15 the first child, 16-19 which quadrants have a child, 20-23 which have
+//         s_i <= 0 (where DTreeNodeT::Sample / Pdf stop, PG.h:268-300).
+// The children of a node are consecutive in quadrant order (the reset numbers them so, and
+// so does the import), so child q = first + the number of children before q.
+struct __align__(32) SQNode {
+    float bnd, btl, btr;
+    uint32_t meta;
+    float fac[4];
+};
+__host__ __device__ inline float sq_div(float a, float b) {
+#ifdef __CUDA_ARCH__
+    return __fdiv_rn(a, b);
+#else
+    return a / b;
+#endif
+}
+__host__ __device__ inline SQNode make_sqnode(float4 s, ushort4 child) {
+    SQNode n;
+    const float partial = s.x + s.z;
+    const float total = ((s.x + s.y) + s.z) + s.w;
+    n.bnd = sq_div(partial, total);
+    n.btl = sq_div(s.x, partial);
+    n.btr = sq_div(s.y, total - partial);
+    n.fac[0] = sq_div(4.0f * s.x, total);
+    n.fac[1] = sq_div(4.0f * s.y, total);
+    n.fac[2] = sq_div(4.0f * s.z, total);
+    n.fac[3] = sq_div(4.0f * s.w, total);
+    const uint32_t c[4] = {child.x, child.y, child.z, child.w};
+    uint32_t first = 0, cmask = 0;
+    for (int q = 3; q >= 0; --q)
+        if (c[q]) {
+            first = c[q];
+            cmask |= 1u << q;
+        }
+    const uint32_t zmask = (s.x <= 0.0f ? 1u : 0u) | (s.y <= 0.0f ? 2u : 0u) | (s.z <= 0.0f ? 4u : 0u) |
+                           (s.w <= 0.0f ? 8u : 0u);
+    n.meta = (first & 0xffffu) | (cmask << 16) | (zmask << 20);
+    return n;
+}
+// child of quadrant idx (0 = none) of a node with the given meta word
+__device__ __forceinline__ uint32_t sq_child(uint32_t meta, int idx) {
+    const uint32_t cm = (meta >> 16) & 0xfu;
+    return ((cm >> idx) & 1u) ? (meta & 0xffffu) + (uint32_t)__popc(cm & ((1u << idx) - 1u)) : 0u;
+}
+
 struct SDTreeDev {
     float3 mn, mx;  // cubified AABB
     FixedPoint fx;
     unsigned* status;
-    uint32_t* counts;  // [0] STree nodes, [1] DTrees, [2] building nodes in use
+    uint32_t* counts;  // [0] STree nodes, [1] DTrees, [2] building nodes in use, [3] sampling nodes
+    float3 inv_size;   // 1 / (mx - mn) per axis where that size is a power of two, else 0
     uint32_t* snode;
     uint32_t* b_off;
     uint32_t* b_cnt;
@@ -46,6 +100,7 @@ struct SDTreeDev {
     ushort4* b_child;
     float* b_area;  // per building node, scratch of the build
     SNode* s_nodes;
+    SQNode* s_q;  // per sampling node, what the descents read
     uint32_t cap_snodes, cap_dtrees, cap_nodes;
     uint32_t max_depth;
     float fraction;
@@ -64,18 +119,51 @@ __device__ __forceinline__ bool stree_step(const uint32_t* __restrict__ snode, u
     code = snode[code + (uint32_t)idx];
     return (code & kLeafBit) != 0;
 }
+// (p - mn) / (mx - mn); inv: the reciprocal of that size where it is a power of two (0 else),
+// whose product is the quotient bit for bit
+__device__ __forceinline__ float stree_norm(float p, float mn, float mx, float inv) {
+    const float d = __fsub_rn(p, mn);
+    return inv != 0.0f ? __fmul_rn(d, inv) : __fdiv_rn(d, __fsub_rn(mx, mn));
+}
+// The child indices stree_step produces along one axis are the binary digits of p: doubling
+// and subtracting 1 are exact in float, so for p in [0, 1) level k of that axis yields bit k of
+// the fraction, floor(p 2^31) holds the first 31 of them, and frac(p 2^31) (exact) is the p the
+// steps would carry on with.  p >= 1 yields 1 at every level and p < 0 or NaN yields 0, with p
+// itself carried on.
+struct AxisDigits {
+    uint32_t bits;
+    float rest;
+};
+__device__ __forceinline__ AxisDigits axis_digits(float p) {
+    if (p >= 0.0f && p < 1.0f) {
+        const float s = __fmul_rn(p, 2147483648.0f);
+        const uint32_t b = __float2uint_rz(s);
+        return AxisDigits{b, __fsub_rn(s, __uint2float_rz(b))};
+    }
+    return AxisDigits{p >= 1.0f ? 0x7fffffffu : 0u, p};
+}
 __device__ __forceinline__ uint32_t stree_lookup(const uint32_t* __restrict__ snode, float3 mn, float3 mx, float px,
-                                                 float py, float pz) {
-    float x = __fdiv_rn(__fsub_rn(px, mn.x), __fsub_rn(mx.x, mn.x));
-    float y = __fdiv_rn(__fsub_rn(py, mn.y), __fsub_rn(mx.y, mn.y));
-    float z = __fdiv_rn(__fsub_rn(pz, mn.z), __fsub_rn(mx.z, mn.z));
+                                                 float py, float pz, float3 inv = float3{0.0f, 0.0f, 0.0f}) {
     uint32_t code = snode[0];
-    if (!(code & kLeafBit)) {
-        for (;;) {
-            if (stree_step(snode, code, x)) break;
-            if (stree_step(snode, code, y)) break;
-            if (stree_step(snode, code, z)) break;
-        }
+    if (code & kLeafBit) return code & ~kLeafBit;
+    const AxisDigits ax = axis_digits(stree_norm(px, mn.x, mx.x, inv.x));
+    const AxisDigits ay = axis_digits(stree_norm(py, mn.y, mx.y, inv.y));
+    const AxisDigits az = axis_digits(stree_norm(pz, mn.z, mx.z, inv.z));
+    // levels 3k, 3k+1, 3k+2 take bit 30-k of x, y, z
+    for (int sh = 30; sh >= 0; --sh) {
+        code = snode[code + ((ax.bits >> sh) & 1u)];
+        if (code & kLeafBit) return code & ~kLeafBit;
+        code = snode[code + ((ay.bits >> sh) & 1u)];
+        if (code & kLeafBit) return code & ~kLeafBit;
+        code = snode[code + ((az.bits >> sh) & 1u)];
+        if (code & kLeafBit) return code & ~kLeafBit;
+    }
+    // deeper than 93 levels: the per-level steps from where the digits end
+    float x = ax.rest, y = ay.rest, z = az.rest;
+    for (;;) {
+        if (stree_step(snode, code, x)) break;
+        if (stree_step(snode, code, y)) break;
+        if (stree_step(snode, code, z)) break;
     }
     return code & ~kLeafBit;
 }
@@ -136,29 +224,30 @@ __device__ __forceinline__ float dtree_mean(float statw, float sum) {
     return __fmul_rn(factor, sum);
 }
 
-// DTreeT::Pdf (PG.h:485-490) -> DTreeNodeT::Pdf (PG.h:279-320)
-__device__ __forceinline__ float dtree_pdf_g(const SNode* __restrict__ nodes, uint32_t off, bool guided, float u,
+// DTreeT::Pdf (PG.h:485-490) -> DTreeNodeT::Pdf (PG.h:279-320), with the factors 4 s_i / total
+// precomputed in the node (SQNode); the last division by 2 is the exact product by 0.5
+__device__ __forceinline__ float dtree_pdf_g(const SQNode* __restrict__ nodes, uint32_t off, bool guided, float u,
                                              float v) {
-    if (!guided) return __fdiv_rn(__fmul_rn(1.0f, kInv2Pi), 2.0f);
+    if (!guided) return __fmul_rn(__fmul_rn(1.0f, kInv2Pi), 0.5f);
     float result = 1.0f;
     uint32_t cur = 0;
     int idx = quad_child(u, v);
     for (;;) {
-        const SNode nd = nodes[off + cur];
-        const float4 s = nd.sums;
-        const float total = __fadd_rn(__fadd_rn(__fadd_rn(s.x, s.y), s.z), s.w);
-        const float si = sel4(s, idx);
-        if (si <= 0.0f) {
+        // both halves of the node in two independent 16-byte loads
+        const float4* np = reinterpret_cast<const float4*>(nodes + off + cur);
+        const float4 w = np[0], f = np[1];
+        const uint32_t meta = __float_as_uint(w.w);
+        if ((meta >> (20 + idx)) & 1u) {  // s_idx <= 0
             result = 0.0f;
             break;
         }
-        result = __fmul_rn(result, __fdiv_rn(__fmul_rn(4.0f, si), total));
-        const uint32_t c = sel4(nd.child, idx);
+        result = __fmul_rn(result, sel4(f, idx));
+        const uint32_t c = sq_child(meta, idx);
         if (!c) break;
         cur = c;
         idx = quad_child(u, v);
     }
-    return __fdiv_rn(__fmul_rn(result, kInv2Pi), 2.0f);
+    return __fmul_rn(__fmul_rn(result, kInv2Pi), 0.5f);
 }
 
 // The square [x, x + w) x [y, y + w) of the node where a sampling descent stopped, and the
@@ -170,7 +259,7 @@ struct DSquare {
 
 // dtree_pdf_g at (u, v) when the point lies in the square sampling stopped in, else the full
 // descent: equal to dtree_pdf_g(nodes, off, guided, u, v) bit for bit either way.
-__device__ __forceinline__ float dtree_pdf_in(const SNode* __restrict__ nodes, uint32_t off, bool guided,
+__device__ __forceinline__ float dtree_pdf_in(const SQNode* __restrict__ nodes, uint32_t off, bool guided,
                                               const DSquare& sq, float u, float v) {
     return sq.holds(u, v) ? sq.pdf : dtree_pdf_g(nodes, off, guided, u, v);
 }
@@ -179,38 +268,37 @@ __device__ __forceinline__ float dtree_pdf_in(const SNode* __restrict__ nodes, u
 // `guided` is DTreeT::GetMean() > 0 (uniform sampling of the square otherwise).  The pdf of
 // the sampled point comes out of the same descent: DTreeNodeT::Pdf walks the binary digits of
 // (u, v) (quad_child doubles exactly), so for any point inside the square of the node where
-// sampling stopped it visits exactly the nodes sampling visited, with the same quadrant sums;
-// the factors 4 s_i / total are formed in the same order here.  `sq` returns that square and
+// sampling stopped it visits exactly the nodes sampling visited, with the same quadrant sums
+// and so the same precomputed factors 4 s_i / total.  `sq` returns that square and
 // pdf (uniform sampling: the unit square, whose pdf is constant).
-__device__ __forceinline__ float2 dtree_sample_sq(const SNode* __restrict__ nodes, uint32_t off, bool guided,
+__device__ __forceinline__ float2 dtree_sample_sq(const SQNode* __restrict__ nodes, uint32_t off, bool guided,
                                                   uint32_t& rng, DSquare& sq) {
     if (!guided) {
         const float a = rnd1(rng);
         const float b = rnd1(rng);
-        sq = DSquare{0.0f, 0.0f, 1.0f, __fdiv_rn(__fmul_rn(1.0f, kInv2Pi), 2.0f)};
+        sq = DSquare{0.0f, 0.0f, 1.0f, __fmul_rn(__fmul_rn(1.0f, kInv2Pi), 0.5f)};
         return make_float2(a, b);
     }
     uint32_t cur = 0;
     float rx = 0.0f, ry = 0.0f, size = 1.0f, result = 1.0f;
     float bx = 0.0f, by = 0.0f;  // corner of the square where the descent stopped
     for (;;) {
-        const SNode nd = nodes[off + cur];
-        const float4 s = nd.sums;
+        // boundaries and meta word, and the pdf factors: two independent 16-byte loads, so that
+        // no load waits for the quadrant choice
+        const float4* np = reinterpret_cast<const float4*>(nodes + off + cur);
+        const float4 w = np[0], f = np[1];
+        const float bnd = w.x;
+        const uint32_t meta = __float_as_uint(w.w);
         int idx = 0;
-        const float topLeft = s.x, topRight = s.y;
-        float partial = __fadd_rn(s.x, s.z);
-        const float total = __fadd_rn(__fadd_rn(__fadd_rn(s.x, s.y), s.z), s.w);
-        float boundary = __fdiv_rn(partial, total);
-        float ox = 0.0f, oy = 0.0f;
+        float ox = 0.0f, oy = 0.0f, boundary;
         float sample = rnd1(rng);
-        if (sample < boundary) {
-            sample = __fdiv_rn(sample, boundary);
-            boundary = __fdiv_rn(topLeft, partial);
+        if (sample < bnd) {
+            sample = __fdiv_rn(sample, bnd);
+            boundary = w.y;  // topLeft / partial
         } else {
-            partial = __fsub_rn(total, partial);
             ox = 0.5f;
-            sample = __fdiv_rn(__fsub_rn(sample, boundary), __fsub_rn(1.0f, boundary));
-            boundary = __fdiv_rn(topRight, partial);
+            sample = __fdiv_rn(__fsub_rn(sample, bnd), __fsub_rn(1.0f, bnd));
+            boundary = w.z;  // topRight / (total - partial)
             idx |= 1;
         }
         if (sample >= boundary) {
@@ -220,12 +308,12 @@ __device__ __forceinline__ float2 dtree_sample_sq(const SNode* __restrict__ node
         rx = __fadd_rn(rx, __fmul_rn(size, ox));
         ry = __fadd_rn(ry, __fmul_rn(size, oy));
         size = __fmul_rn(size, 0.5f);
-        const float si = sel4(s, idx);
         // the pdf descent's step at this node (DTreeNodeT::Pdf, PG.h:295-300)
-        if (si <= 0.0f) result = 0.0f;
-        else result = __fmul_rn(result, __fdiv_rn(__fmul_rn(4.0f, si), total));
-        const uint32_t c = sel4(nd.child, idx);
-        if (c == 0 || si <= 0.0f) {
+        const bool zero = ((meta >> (20 + idx)) & 1u) != 0;  // s_idx <= 0
+        if (zero) result = 0.0f;
+        else result = __fmul_rn(result, sel4(f, idx));
+        const uint32_t c = sq_child(meta, idx);
+        if (c == 0 || zero) {
             bx = rx;
             by = ry;
             const float a = rnd1(rng);
@@ -237,7 +325,7 @@ __device__ __forceinline__ float2 dtree_sample_sq(const SNode* __restrict__ node
         cur = c;
     }
     // bx, by and bx + size are dyadic with few bits: the comparisons of holds() are exact
-    sq = DSquare{bx, by, size, __fdiv_rn(__fmul_rn(result, kInv2Pi), 2.0f)};
+    sq = DSquare{bx, by, size, __fmul_rn(__fmul_rn(result, kInv2Pi), 0.5f)};
     return make_float2(fminf(fmaxf(rx, 0.0f), 1.0f), fminf(fmaxf(ry, 0.0f), 1.0f));
 }
 
