@@ -467,39 +467,26 @@ __global__ void k_reset_commit(SDTreeDev t, const unsigned long long* node_total
 // DTree's GetMean test once, the guided sample, the pdf of the sampled canonical point
 // (DTreeT::Pdf) and optionally the direction and the pdf of that direction after the
 // dir -> canonical round trip the closest-hit program performs (SimpleGuide.cu:361-368).
-// The descents read the 32-byte SQNode of each visited node, from shared memory when the
-// whole sampling pool fits (kStageSQ nodes), else through L1.
+// The descents read the 32-byte SQNode of each visited node and the STree through L1.  Staging
+// them in shared memory measured slower on B200 (config 1 / its 2-pass variant: 64.8 / 23.7 G
+// queries/s with the STree and the whole pool staged, 63.4 / 28.4 with every tree's root
+// level staged, 65.5 / 31.1 with no staging): the shared memory comes out of the same 256 KB
+// per SM as L1, which then no longer holds the deeper levels.
 constexpr uint32_t kSampleBlock = 256;
-constexpr uint32_t kStageSTreeSample = 4096;  // 16 KB
-constexpr uint32_t kStageSQ = 256;            // 8 KB
 __global__ void __launch_bounds__(kSampleBlock, 8) k_sample_pdf(SDTreeDev t, int64_t n, const float* __restrict__ pos,
-                                                            const uint32_t* __restrict__ seeds, uint32_t seed_base,
-                                                            float* __restrict__ out_uv, float* __restrict__ out_pdf_uv,
-                                                            float* __restrict__ out_dir, float* __restrict__ out_pdf_dir) {
-    __shared__ uint32_t s_st[kStageSTreeSample];
-    __shared__ SQNode s_sq[kStageSQ];
-    const uint32_t nst = t.counts[0], nsq = t.counts[3];
-    const bool staged = nst <= kStageSTreeSample, staged_q = nsq <= kStageSQ;
-    if (staged)
-        for (uint32_t i = threadIdx.x; i < nst; i += blockDim.x) s_st[i] = t.snode[i];
-    if (staged_q) {
-        const uint4* src = reinterpret_cast<const uint4*>(t.s_q);
-        uint4* dst = reinterpret_cast<uint4*>(s_sq);
-        for (uint32_t i = threadIdx.x; i < 2 * nsq; i += blockDim.x) dst[i] = src[i];
-    }
-    __syncthreads();
-    const uint32_t* st = staged ? s_st : t.snode;
-    const SQNode* sq_nodes = staged_q ? s_sq : t.s_q;
+                                                               const uint32_t* __restrict__ seeds, uint32_t seed_base,
+                                                               float* __restrict__ out_uv, float* __restrict__ out_pdf_uv,
+                                                               float* __restrict__ out_dir, float* __restrict__ out_pdf_dir) {
     const int64_t stride = int64_t(gridDim.x) * blockDim.x;
     for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
-        const uint32_t d = stree_lookup(st, t.mn, t.mx, pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], t.inv_size);
+        const uint32_t d = stree_lookup(t.snode, t.mn, t.mx, pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], t.inv_size);
         uint32_t rng = seeds ? seeds[i] : (pcg1d(seed_base + (uint32_t)i) | 1u);
         const uint32_t off = t.s_off[d];
         const bool guided = t.s_guided[d] != 0;
         DSquare sq;
-        const float2 uv = dtree_sample_sq(sq_nodes, off, guided, rng, sq);
+        const float2 uv = dtree_sample_sq(t.s_q, off, guided, rng, sq);
         if (out_uv) reinterpret_cast<float2*>(out_uv)[i] = uv;
-        if (out_pdf_uv) out_pdf_uv[i] = dtree_pdf_in(sq_nodes, off, guided, sq, uv.x, uv.y);
+        if (out_pdf_uv) out_pdf_uv[i] = dtree_pdf_in(t.s_q, off, guided, sq, uv.x, uv.y);
         if (out_dir || out_pdf_dir) {
             const float3 dv = normalize3(canonical_to_dir(uv.x, uv.y));
             if (out_dir) {
@@ -509,7 +496,7 @@ __global__ void __launch_bounds__(kSampleBlock, 8) k_sample_pdf(SDTreeDev t, int
             }
             if (out_pdf_dir) {
                 const float2 c = dir_to_canonical(dv.x, dv.y, dv.z);
-                out_pdf_dir[i] = dtree_pdf_in(sq_nodes, off, guided, sq, c.x, c.y);
+                out_pdf_dir[i] = dtree_pdf_in(t.s_q, off, guided, sq, c.x, c.y);
             }
         }
     }
@@ -749,6 +736,7 @@ int rtpg_sdtree_sample_pdf(rtpg_sdtree* h, int64_t n, const float* pos, const ui
     if (n < 0 || (n > 0 && !pos)) return fail(RTPG_EINVAL, "rtpg_sdtree_sample_pdf: bad arguments");
     if (!aligned8(out_uv) || !aligned4(pos)) return fail(RTPG_EINVAL, "rtpg_sdtree_sample_pdf: misaligned array");
     if (n == 0) return RTPG_OK;
+    // one resident wave: 8 CTAs of 256 per SM (32 registers a thread)
     k_sample_pdf<<<grid_for(n, kSampleBlock, 8), kSampleBlock, 0, as_stream(stream)>>>(
         h->dev, n, pos, seeds, seed_base, out_uv, out_pdf_uv, out_dir, out_pdf_dir);
     RTPG_LAUNCH_CHECK();
