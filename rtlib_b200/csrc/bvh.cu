@@ -123,6 +123,12 @@ __global__ void k_scene_leaves(const float* __restrict__ v, const uint32_t* __re
     }
 }
 
+// the leaves back in scene order (the original index is in v0.w), for small scenes
+__global__ void k_scene_flat(const BvhTri* __restrict__ tris, uint32_t nt, BvhTri* __restrict__ flat) {
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nt; k += gridDim.x * blockDim.x)
+        flat[__float_as_uint(tris[k].v0.w)] = tris[k];
+}
+
 __device__ __forceinline__ void tri_box(const BvhTri& t, float* lo, float* hi) {
     const float v0[3] = {t.v0.x, t.v0.y, t.v0.z};
     const float e1[3] = {t.e1.x, t.e1.y, t.e1.z};
@@ -193,6 +199,7 @@ struct rtpg_scene {
     SceneDev dev{};
     BvhNode* nodes = nullptr;
     BvhTri* tris = nullptr;
+    BvhTri* flat = nullptr;
     std::vector<void*> allocs;
     size_t bytes = 0;
     template <class T>
@@ -238,12 +245,14 @@ int rtpg_scene_create(const float* vertices, uint32_t num_vertices, const uint32
     size_t tb = 0;
     cub::DoubleBuffer<unsigned long long> dk(nullptr, nullptr);
     cub::DoubleBuffer<uint32_t> dv(nullptr, nullptr);
-    if ((r = s->alloc(&s->nodes, n > 1 ? n - 1 : 1)) || (r = s->alloc(&s->tris, n))) {
+    if ((r = s->alloc(&s->nodes, n > 1 ? n - 1 : 1)) || (r = s->alloc(&s->tris, n)) ||
+        (n > 0 && n <= kFlatTris && (r = s->alloc(&s->flat, n)))) {
         delete s;
         return r;
     }
     s->dev.nodes = s->nodes;
     s->dev.tris = s->tris;
+    s->dev.flat = s->flat;
     s->dev.ntris = n;
     if (n == 0) {
         *out = s;
@@ -277,6 +286,7 @@ int rtpg_scene_create(const float* vertices, uint32_t num_vertices, const uint32
         if ((e = talloc(tb, &temp))) break;
         if ((e = cub::DeviceRadixSort::SortPairs(temp, tb, dk, dv, (int)n, 0, 63, st))) break;
         k_scene_leaves<<<g, 256, 0, st>>>(vertices, indices, n, dv.Current(), s->tris);
+        if (s->flat) k_scene_flat<<<1, 64, 0, st>>>(s->tris, n, s->flat);
         if (n > 1) {
             k_scene_hierarchy<<<g, 256, 0, st>>>(dk.Current(), (int)n, s->nodes, pi, pl);
             if ((e = cudaMemsetAsync(flags, 0, 4ull * n, st))) break;

@@ -25,9 +25,16 @@ struct __align__(16) BvhTri {
     float4 e2;  // v2 - v0
 };
 
+// Scenes of at most kFlatTris triangles are also kept as a flat list in their own order and
+// traced by testing every triangle: all lanes of a warp then run the same loop over the same
+// triangle (one broadcast load per triangle), where the BVH walk leaves most lanes idle, and the
+// lowest index wins a tie of equal distances, as in a brute-force test.
+constexpr uint32_t kFlatTris = 64;
+
 struct SceneDev {
     const BvhNode* nodes;  // n - 1 interior nodes (root 0); n == 1: no interior node
     const BvhTri* tris;    // n triangles in leaf order
+    const BvhTri* flat;    // n <= kFlatTris: the triangles in scene order, else null
     uint32_t ntris;
 };
 
@@ -73,10 +80,35 @@ __device__ __forceinline__ float tri_hit(const BvhTri& tr, float ox, float oy, f
     return (t > tmin && t < tmax) ? t : -1.0f;
 }
 
+// closest hit (ANY = false) or any hit (ANY = true) in (tmin, tmax) by testing every triangle
+// of a small scene, in scene order
+template <bool ANY>
+__device__ __forceinline__ Hit flat_trace(const SceneDev& s, float ox, float oy, float oz, float dx, float dy, float dz,
+                                          float tmin, float tmax) {
+    Hit h;
+    h.t = tmax;
+    h.prim = 0xffffffffu;
+    h.u = h.v = 0.0f;
+    for (uint32_t k = 0; k < s.ntris; ++k) {
+        const BvhTri tr = s.flat[k];
+        float u, v;
+        const float t = tri_hit(tr, ox, oy, oz, dx, dy, dz, tmin, h.t, u, v);
+        if (t > 0.0f) {
+            h.t = t;
+            h.u = u;
+            h.v = v;
+            h.prim = k;
+            if (ANY) return h;
+        }
+    }
+    return h;
+}
+
 // closest hit (ANY = false) or any hit (ANY = true) in (tmin, tmax)
 template <bool ANY>
 __device__ __forceinline__ Hit bvh_trace(const SceneDev& s, float ox, float oy, float oz, float dx, float dy, float dz,
                                          float tmin, float tmax) {
+    if (s.flat) return flat_trace<ANY>(s, ox, oy, oz, dx, dy, dz, tmin, tmax);
     Hit h;
     h.t = tmax;
     h.prim = 0xffffffffu;

@@ -71,6 +71,35 @@ def test_bvh_closest_and_any_hit(cuda):
     assert ((bt < 1.5) == ga).mean() > 0.999
 
 
+def test_flat_scene_closest_and_any_hit(cuda):
+    """A scene of at most 64 triangles (the Cornell box) is traced by testing every triangle in
+    scene order: hits equal brute force, ties going to the lower index."""
+    import torch
+    from rtlib_b200.tracer import Scene
+    tri = np.ascontiguousarray(scenes.cornell_box(8, 8, materials="glass_phong")["tri_v"])
+    assert tri.shape[0] <= 64
+    sc = Scene(_t(tri, cuda))
+    rng = np.random.default_rng(1)
+    n = 4096
+    o = rng.uniform(0.02, 0.98, (n, 3)).astype(np.float32)
+    d = rng.normal(size=(n, 3)).astype(np.float32)
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    t = torch.empty(n, device=cuda)
+    pr = torch.empty(n, dtype=torch.int32, device=cuda)
+    sc.intersect(_t(o, cuda), _t(d, cuda), out_t=t, out_prim=pr)
+    anyh = torch.empty(n, dtype=torch.int32, device=cuda)
+    sc.intersect(_t(o, cuda), _t(d, cuda), tmax=_t(np.full(n, 0.3, np.float32), cuda), any_hit=True, out_prim=anyh)
+    torch.cuda.synchronize()
+    bt, bp = _mt(tri, o, d, 0.0, 1e20)
+    gp = pr.cpu().numpy().view(np.uint32)
+    assert (gp == bp).mean() > 0.999
+    hit = (gp == bp) & (bp != 0xFFFFFFFF)
+    assert hit.mean() > 0.5  # the box is open at the front: the rest escape
+    np.testing.assert_allclose(t.cpu().numpy()[hit], bt[hit], rtol=1e-5)
+    ga = anyh.cpu().numpy().view(np.uint32) != 0xFFFFFFFF
+    assert ((bt < 0.3) == ga).mean() > 0.999
+
+
 def _gpu_render(dev, sc, w, h, spp, flags, seed=1, tree=None, max_depth=8):
     from rtlib_b200.tracer import Tracer
     tr = Tracer(sc, dev, max_depth=max_depth, seed=seed, width=w, height=h)
