@@ -36,9 +36,15 @@ def test_forward_matches_oracle(cuda):
     o, _ = M.forward(g.params(), M.features(pos, nrm, wo, MN, MX))
     scale = np.abs(o).max()
     assert scale > 0.05
+    # the restatement rounds features, weights and activations to bf16 exactly as the kernel
+    # does; what remains is the fp32 accumulation order of the tensor cores, which now and then
+    # moves a hidden activation across a bf16 rounding boundary (one bf16 ulp, 2^-8 relative).
+    # Measured on B200: 79% of outputs bit-identical, 99.9% within 1.2e-7 of the scale, the
+    # largest difference 1.4e-3 of the scale.
     err = np.abs(raw - o)
-    assert err.max() < 3e-2 * scale, err.max()
-    assert err.mean() < 2e-3 * scale, err.mean()
+    assert (err == 0).mean() > 0.5, (err == 0).mean()
+    assert np.quantile(err, 0.999) < 1e-6 * scale, np.quantile(err, 0.999) / scale
+    assert err.max() < 5e-3 * scale, err.max() / scale
     assert g.status() == 0
 
 

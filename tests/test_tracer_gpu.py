@@ -340,12 +340,14 @@ def test_learned_guide_lowers_error(cuda):
 
 
 def test_convergence_4096_spp_within_one_percent(cuda):
-    """Guided (SD-tree schedule) and unguided renders of the Cornell box at 4096 spp against a
-    65536-spp FP64-accumulated image of the same integrator: relMSE < 1%."""
+    """Config 2's check at its size: guided (SD-tree schedule) and unguided renders of the
+    Cornell box at 512 x 512 and 4096 spp against a 65536-spp FP64-accumulated image of the same
+    integrator (another seed): relMSE < 1%.  The integrator itself is tied to RTLib's by the
+    parity tests above and the known-answer tests of its shading."""
     from rtlib_b200 import metrics
     from rtlib_b200.sdtree import SDTree, SDTreeController
     from rtlib_b200.tracer import FLAG_NEE, Tracer
-    w = h = 96
+    w = h = 512
     sc = scenes.cornell_box(w, h)
     ref_tr = Tracer(sc, cuda, max_depth=8, width=w, height=h, seed=1234)
     ref_tr.render(65536, FLAG_NEE)
