@@ -401,6 +401,26 @@ C_AABB = ((-0.005,) * 3, (1.005,) * 3)  # world AABB padded by 0.005 as the appl
 BOUNCE_BYTES = 128
 
 
+def _recording_launches(budget, iteration_for_built=0):
+    """Launches of the SD-tree pass schedule (RTSTreeControllerT::BegTrace / EndTrace, one
+    sample per launch) that record, i.e. whose waves end with the trace-vertex commit."""
+    remain, pas, per_all, per_tmp, it, rec = budget, 0, 0, 0, 0, 0
+    while True:
+        if per_tmp == 0:
+            remain -= pas
+            pas = min(remain, 1 << it)
+            if remain - pas < 2 * pas or per_all >= budget:
+                pas = remain
+        rec += 0 if (it > iteration_for_built and remain <= pas) else 1
+        per_all += 1
+        per_tmp += 1
+        if per_tmp >= pas:
+            it += 1
+            per_tmp = 0
+        if per_all > budget:
+            return rec
+
+
 def set_budget(b):
     global C_BUDGET
     C_BUDGET = int(b)
@@ -508,7 +528,9 @@ def bench_cornell_ours(args, rank, world):
                      "note": "bounce = BVH closest hit + shading + shadow ray; its bound is instruction "
                              "issue and traversal latency, the HBM figure is the SoA state traffic"},
         "clocks": clk,
-        "gpu_launches": (1 + C_MAX_DEPTH + 1) * (C_BUDGET + 1) * args.steps,
+        # raygen, max_depth bounces and the accumulation per launch, plus the commit of every
+        # recording launch
+        "gpu_launches": ((1 + C_MAX_DEPTH + 1) * (C_BUDGET + 1) + _recording_launches(C_BUDGET)) * args.steps,
         "counters_per_step": cnt,
         "sdtree": st,
     }
@@ -651,7 +673,7 @@ def bench_occluded_ours(args, rank, world):
                      "note": "bounce = BVH closest hit over 1M triangles + shading + RIS over 32 light samples + "
                              "one shadow ray; bound by traversal latency and issue"},
         "clocks": clk,
-        "gpu_launches": (1 + O_DEPTH + 1) * samples * args.steps,
+        "gpu_launches": ((1 + O_DEPTH + 1) * samples + _recording_launches(O_BUDGET, 1)) * args.steps,
         "counters_per_step": cnt,
         "unguided_nee_ris_Mpaths_s": O_W * O_H * samples / (plain_ms * 1e-3) / 1e6,
         "grid_cells": cells, "spp_per_step": samples,

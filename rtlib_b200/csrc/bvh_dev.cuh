@@ -67,7 +67,7 @@ __device__ __forceinline__ float tri_hit(const BvhTri& tr, float ox, float oy, f
     const float pz = dx * tr.e2.y - dy * tr.e2.x;
     const float det = tr.e1.x * px + tr.e1.y * py + tr.e1.z * pz;
     if (fabsf(det) < 1e-20f) return -1.0f;
-    const float inv = 1.0f / det;
+    const float inv = __frcp_rn(det);  // the correctly rounded 1 / det, without a full division
     const float sx = ox - tr.v0.x, sy = oy - tr.v0.y, sz = oz - tr.v0.z;
     u = (sx * px + sy * py + sz * pz) * inv;
     if (u < 0.0f || u > 1.0f) return -1.0f;
@@ -89,6 +89,9 @@ __device__ __forceinline__ Hit flat_trace(const SceneDev& s, float ox, float oy,
     h.t = tmax;
     h.prim = 0xffffffffu;
     h.u = h.v = 0.0f;
+    // unrolled so that the next triangles' loads issue while this one is tested; the hit is
+    // still updated in scene order
+#pragma unroll 4
     for (uint32_t k = 0; k < s.ntris; ++k) {
         const BvhTri tr = s.flat[k];
         float u, v;

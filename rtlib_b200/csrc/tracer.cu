@@ -169,7 +169,7 @@ __device__ __forceinline__ LightSample sample_light(const TracerDev& T, float3 p
 // One bounce of every active path: closest hit + shading (__closesthit__radiance /
 // __miss__radiance, SimpleGuide.cu:202-520), the NEE/RIS shadow ray traced right away as the
 // closest-hit program does, then the raygen bookkeeping (SimpleGuide.cu:85-114): bounce
-// radiance into the color (and, recording, into the per-bounce store from which k_finish forms
+// radiance into the color (and, recording, into the per-bounce store from which k_commit forms
 // the trace-vertex radiance), termination, compaction of the survivors into the next queue.
 // Returns whether the path continues; *shadow tells whether a shadow ray was traced.
 constexpr int kGuideNone = 0, kGuideTree = 1, kGuideGrid = 2, kAdjoint = 3, kGuideMlp = 4;
@@ -690,113 +690,141 @@ __global__ void __launch_bounds__(kTB, 8) k_bounce(TracerDev T, uint32_t bounce)
 }
 
 // ------------------------------------------------------------------ finish
-// Accumulate, write the seed back, commit trace vertices (TraceVertexT::Commit,
-// OPX7UtilsPathGuiding.h:830-866 -> DTreeWrapperT::Record :514-520 with stat-weight 1, or
-// MortonTraceVertexT::Commit for the grid guide).
-template <int G>
+// Per path: FP64 accumulation and the seed write-back.
 __global__ void __launch_bounds__(kTB) k_finish(TracerDev T) {
     grid_dependency_wait();
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < T.npath; p += gridDim.x * blockDim.x) {
+        const float3 c = T.col[p];
+        double* a = T.accum + 3 * size_t(p);
+        a[0] += (double)c.x;
+        a[1] += (double)c.y;
+        a[2] += (double)c.z;
+        T.seeds[p] = T.rng[p];
+    }
+}
+
+// The commit of the trace vertices of recording waves (TraceVertexT::Commit,
+// OPX7UtilsPathGuiding.h:830-866 -> DTreeWrapperT::Record :514-520 with stat-weight 1, or
+// MortonTraceVertexT::Commit for the grid guide), one thread per vertex: block row
+// blockIdx.y is the vertex index i, so a warp holds vertex i of 32 consecutive paths and
+// lanes whose path is shorter leave at once.  The radiance of vertex i is
+// L_{i+1} + L_{i+2} + ... added in bounce order, exactly the float sums RTLib's raygen loop
+// accumulates into traceVertices[i].radiance (SimpleGuide.cu:98-100).
+// SD-tree commits go to shared-memory sums of the CTA while the whole building tree is small (the
+// first passes, when every vertex lands in a handful of quadrants), else straight to the tree
+// with 64-bit integer atomics: keys spread over thousands of nodes gain nothing from warp
+// aggregation, whose 64-bit match costs more than the atomic.
+constexpr uint32_t kFinPrivQuads = 2048;
+constexpr uint32_t kFinPrivTrees = 512;
+template <int G>
+__global__ void __launch_bounds__(kTB) k_commit(TracerDev T) {
+    grid_dependency_wait();
+    __shared__ unsigned long long s_q[kFinPrivQuads];
+    __shared__ unsigned long long s_w[kFinPrivTrees];
     constexpr bool use_grid = G == kGuideGrid;
     // the learned guide with the SD-tree as fallback commits to both
     const bool tree_too = G == kGuideMlp && T.tree.snode != nullptr;
-    const bool recording = (G == kGuideTree || G == kGuideGrid || G == kGuideMlp) && !(T.flags & RTPG_TRACE_FLAG_FINAL);
+    const bool tree_commit = !use_grid && (G != kGuideMlp || tree_too);
+    uint32_t nq = 0, ndt = 0;
+    if (tree_commit) {
+        nq = T.tree.counts[2] * 4u;
+        ndt = T.tree.counts[1];
+    }
+    const bool priv = tree_commit && nq <= kFinPrivQuads && ndt <= kFinPrivTrees;
+    if (priv) {
+        for (uint32_t j = threadIdx.x; j < nq; j += blockDim.x) s_q[j] = 0ull;
+        for (uint32_t j = threadIdx.x; j < ndt; j += blockDim.x) s_w[j] = 0ull;
+        __syncthreads();
+    }
+    const uint32_t i = blockIdx.y;  // vertex index
+    // warp-uniform loop (the grid guide's aggregated atomics need the whole warp)
     for (uint32_t base = blockIdx.x * blockDim.x; base < T.npath; base += gridDim.x * blockDim.x) {
         const uint32_t p = base + threadIdx.x;
-        uint32_t nv = 0;
-        if (p < T.npath) {
-            const float3 c = T.col[p];
-            double* a = T.accum + 3 * size_t(p);
-            a[0] += (double)c.x;
-            a[1] += (double)c.y;
-            a[2] += (double)c.z;
-            T.seeds[p] = T.rng[p];
-            const uint32_t d = T.depth[p];
-            nv = recording ? (d < kTV ? d : kTV) : 0;
-        }
-        // radiance of vertex i = L_{i+1} + L_{i+2} + ... added in bounce order, exactly the
-        // float sums RTLib's raygen loop accumulates into traceVertices[i].radiance; each
-        // bounce radiance is read once and added to every earlier vertex in registers
-        const uint32_t dfin = nv ? T.depth[p] : 0u;
-        float3 acc[kTV];
+        unsigned long long k_w = ~0ull, k_s = ~0ull, v_w = 0, v_s = 0;
+        const uint32_t d = p < T.npath ? T.depth[p] : 0u;
+        const size_t vi = size_t(i) * T.npath + p;
+        const uint8_t vf = i < d ? T.v_flags[vi] : 0;
+        if ((vf & 1) && !(vf & 2)) {
+            // the vertex's data and the later bounces' radiances do not depend on one another:
+            // all loads are issued before the first add (in-order issue would otherwise wait a
+            // memory latency per bounce), then the radiances are added in bounce order
+            const float wo_v = T.v_wopdf[vi];
+            const float3 th = T.v_thr[vi];
+            float3 rad = f3(0.f, 0.f, 0.f);
+            for (uint32_t k0 = i + 1; k0 <= d; k0 += 8) {
+                float3 Lk[8];
 #pragma unroll
-        for (int i = 0; i < kTV; ++i) acc[i] = f3(0.f, 0.f, 0.f);
-        for (uint32_t k = 1; k <= dfin; ++k) {
-            const float3 L = T.b_rad[size_t(k) * T.npath + p];
+                for (uint32_t j = 0; j < 8; ++j)
+                    Lk[j] = (k0 + j <= d) ? T.b_rad[size_t(k0 + j) * T.npath + p] : f3(0.f, 0.f, 0.f);
 #pragma unroll
-            for (uint32_t i = 0; i < kTV; ++i)
-                if (i < k) acc[i] = acc[i] + L;
-        }
-        // warp-uniform loop (the aggregated atomics need the whole warp) up to the warp's deepest path
-        const uint32_t nv_warp = __reduce_max_sync(0xffffffffu, nv);
-        for (uint32_t i = 0; i < nv_warp; ++i) {
-            unsigned long long k_w = ~0ull, k_s = ~0ull, v_w = 0, v_s = 0;
-            if (i < nv) {
-                const size_t vi = size_t(i) * T.npath + p;
-                const uint8_t vf = T.v_flags[vi];
-                float3 rad = acc[0];
-#pragma unroll
-                for (uint32_t j = 1; j < kTV; ++j)
-                    if (j == i) rad = acc[j];
-                const bool ok_r = isfinite(rad.x) && rad.x >= 0.f && isfinite(rad.y) && rad.y >= 0.f &&
-                                  isfinite(rad.z) && rad.z >= 0.f;
-                const float wo = (vf & 1) && !(vf & 2) && ok_r ? T.v_wopdf[vi] : 0.0f;
-                if (wo > 0.0f) {
-                    const float3 th = T.v_thr[vi];
-                    float3 lr = f3(0.f, 0.f, 0.f);
-                    if (th.x * wo > 1e-4f) lr.x = rad.x / th.x;
-                    if (th.y * wo > 1e-4f) lr.y = rad.y / th.y;
-                    if (th.z * wo > 1e-4f) lr.z = rad.z / th.z;
-                    lr = lr * fabsf(T.v_cos[vi]);
-                    const float lavg = (lr.x + lr.y + lr.z) / 3.0f;
-                    const float irr = __fdiv_rn(lavg, wo);
-                    if (G == kGuideMlp) {
-                        // a training record of the learned guide: the SD-tree's record with the
-                        // vertex's normal and outgoing direction, kept with probability mlp_keep
-                        if (isfinite(irr) && irr > 0.0f &&
-                            to_uniform_float(pcg1d(T.rng[p] ^ (i * 0x9E3779B9u))) < T.mlp_keep) {
-                            const uint32_t idx = atomicAdd(T.ml.r_count, 1u);
-                            if (idx < T.ml.capacity) {
-                                const float3 ps = T.v_pos[vi], nm = T.v_nrm[vi], wo = T.v_wo[vi], dr = T.v_dir[vi];
-                                float* rp = T.ml.r_pos + 3 * size_t(idx);
-                                float* rn = T.ml.r_nrm + 3 * size_t(idx);
-                                float* ro = T.ml.r_wo + 3 * size_t(idx);
-                                float* ri = T.ml.r_wi + 3 * size_t(idx);
-                                rp[0] = ps.x; rp[1] = ps.y; rp[2] = ps.z;
-                                rn[0] = nm.x; rn[1] = nm.y; rn[2] = nm.z;
-                                ro[0] = wo.x; ro[1] = wo.y; ro[2] = wo.z;
-                                ri[0] = dr.x; ri[1] = dr.y; ri[2] = dr.z;
-                                T.ml.r_w[idx] = irr;
-                            }
-                        }
-                    }
-                    if (G == kGuideMlp && !tree_too) {
-                    } else if (use_grid) {
-                        // MortonTraceVertexT::Commit (OPX7UtilsMorton.h:550-585) ->
-                        // MortonQuadTreeWrapperT::Record: leaf of the cell's building quadtree
-                        if (isfinite(irr) && irr > 0.0f) {
-                            const uint32_t cell = T.v_cell[vi];
-                            k_s = ((unsigned long long)cell << (2 * T.mqt.level)) + T.v_slot[vi];
-                            v_s = to_fx(irr, T.mqt.fx, T.mqt.status);
-                        }
-                    } else {
-                        const uint32_t dt = T.v_cell[vi];  // stree_lookup of the vertex, from k_bounce
-                        k_w = dt;
-                        v_w = to_fx(1.0f, T.tree.fx, T.tree.status);
-                        if (isfinite(irr) && irr > 0.0f) {
-                            k_s = T.v_slot[vi];
-                            v_s = to_fx(irr, T.tree.fx, T.tree.status);
+                for (uint32_t j = 0; j < 8; ++j)
+                    if (k0 + j <= d) rad = rad + Lk[j];
+            }
+            const bool ok_r = isfinite(rad.x) && rad.x >= 0.f && isfinite(rad.y) && rad.y >= 0.f &&
+                              isfinite(rad.z) && rad.z >= 0.f;
+            const float wo = ok_r ? wo_v : 0.0f;
+            if (wo > 0.0f) {
+                float3 lr = f3(0.f, 0.f, 0.f);
+                if (th.x * wo > 1e-4f) lr.x = rad.x / th.x;
+                if (th.y * wo > 1e-4f) lr.y = rad.y / th.y;
+                if (th.z * wo > 1e-4f) lr.z = rad.z / th.z;
+                lr = lr * fabsf(T.v_cos[vi]);
+                const float lavg = (lr.x + lr.y + lr.z) / 3.0f;
+                const float irr = __fdiv_rn(lavg, wo);
+                if (G == kGuideMlp) {
+                    // a training record of the learned guide: the SD-tree's record with the
+                    // vertex's normal and outgoing direction, kept with probability mlp_keep
+                    if (isfinite(irr) && irr > 0.0f &&
+                        to_uniform_float(pcg1d(T.rng[p] ^ (i * 0x9E3779B9u))) < T.mlp_keep) {
+                        const uint32_t idx = atomicAdd(T.ml.r_count, 1u);
+                        if (idx < T.ml.capacity) {
+                            const float3 ps = T.v_pos[vi], nm = T.v_nrm[vi], wv = T.v_wo[vi], dr = T.v_dir[vi];
+                            float* rp = T.ml.r_pos + 3 * size_t(idx);
+                            float* rn = T.ml.r_nrm + 3 * size_t(idx);
+                            float* ro = T.ml.r_wo + 3 * size_t(idx);
+                            float* ri = T.ml.r_wi + 3 * size_t(idx);
+                            rp[0] = ps.x; rp[1] = ps.y; rp[2] = ps.z;
+                            rn[0] = nm.x; rn[1] = nm.y; rn[2] = nm.z;
+                            ro[0] = wv.x; ro[1] = wv.y; ro[2] = wv.z;
+                            ri[0] = dr.x; ri[1] = dr.y; ri[2] = dr.z;
+                            T.ml.r_w[idx] = irr;
                         }
                     }
                 }
-            }
-            if (G == kGuideMlp && !tree_too) {
-            } else if (use_grid) {
-                warp_add_u64(k_s, v_s, T.mqt.leaves);
-            } else {
-                warp_add_u64(k_w, v_w, T.tree.b_statw);
-                warp_add_u64(k_s, v_s, T.tree.b_sums);
+                if (G == kGuideMlp && !tree_too) {
+                } else if (use_grid) {
+                    // MortonTraceVertexT::Commit (OPX7UtilsMorton.h:550-585) ->
+                    // MortonQuadTreeWrapperT::Record: leaf of the cell's building quadtree
+                    if (isfinite(irr) && irr > 0.0f) {
+                        const uint32_t cell = T.v_cell[vi];
+                        k_s = ((unsigned long long)cell << (2 * T.mqt.level)) + T.v_slot[vi];
+                        v_s = to_fx(irr, T.mqt.fx, T.mqt.status);
+                    }
+                } else {
+                    const uint32_t dt = T.v_cell[vi];  // stree_lookup of the vertex, from k_bounce
+                    k_w = dt;
+                    v_w = to_fx(1.0f, T.tree.fx, T.tree.status);
+                    if (isfinite(irr) && irr > 0.0f) {
+                        k_s = T.v_slot[vi];
+                        v_s = to_fx(irr, T.tree.fx, T.tree.status);
+                    }
+                }
             }
         }
+        if (G == kGuideMlp && !tree_too) {
+        } else if (use_grid) {
+            warp_add_u64(k_s, v_s, T.mqt.leaves);
+        } else {
+            if (k_w != ~0ull) atomicAdd(priv ? s_w + k_w : T.tree.b_statw + k_w, v_w);
+            if (k_s != ~0ull) atomicAdd(priv ? s_q + k_s : T.tree.b_sums + k_s, v_s);
+        }
+    }
+    if (priv) {
+        __syncthreads();
+        for (uint32_t j = threadIdx.x; j < nq; j += blockDim.x)
+            if (s_q[j]) atomicAdd(T.tree.b_sums + j, s_q[j]);
+        for (uint32_t j = threadIdx.x; j < ndt; j += blockDim.x)
+            if (s_w[j]) atomicAdd(T.tree.b_statw + j, s_w[j]);
     }
 }
 
@@ -884,12 +912,17 @@ static void launch_bounce(const TracerDev& T, int g, cudaStream_t st, uint32_t b
         default: (void)launch_dependent(k_bounce<kGuideNone>, g, kTB, 0, st, T, b); break;
     }
 }
+// accumulation, then (recording waves of a guide) the commit of the trace vertices, one block
+// row per vertex index
 static void launch_finish(const TracerDev& T, int g, cudaStream_t st) {
+    (void)launch_dependent(k_finish, g, kTB, 0, st, T);
+    if (T.flags & RTPG_TRACE_FLAG_FINAL) return;
+    const dim3 gc(kSMs * 2, kTV);
     switch (guide_of(T.flags)) {
-        case kGuideTree: (void)launch_dependent(k_finish<kGuideTree>, g, kTB, 0, st, T); break;
-        case kGuideGrid: (void)launch_dependent(k_finish<kGuideGrid>, g, kTB, 0, st, T); break;
-        case kGuideMlp: (void)launch_dependent(k_finish<kGuideMlp>, g, kTB, 0, st, T); break;
-        default: (void)launch_dependent(k_finish<kGuideNone>, g, kTB, 0, st, T); break;
+        case kGuideTree: (void)launch_dependent(k_commit<kGuideTree>, gc, kTB, 0, st, T); break;
+        case kGuideGrid: (void)launch_dependent(k_commit<kGuideGrid>, gc, kTB, 0, st, T); break;
+        case kGuideMlp: (void)launch_dependent(k_commit<kGuideMlp>, gc, kTB, 0, st, T); break;
+        default: break;
     }
 }
 
