@@ -47,6 +47,7 @@ constexpr int kTB = 128;
 struct TracerDev {
     SceneDev scene;
     const float* tri_v;     // 9 floats per triangle (original order)
+    const TriFrame* tri_frame;  // per triangle: face normal, half area, the normal's ONB
     const float* tri_uv;    // 6 floats per triangle or null
     const uint32_t* tri_mat;
     const Material* mats;
@@ -148,7 +149,7 @@ __device__ __forceinline__ LightSample sample_light(const TracerDev& T, float3 p
     const uint32_t ti = min(T.light_tris[mesh.x + xs32_next(rng) % mesh.y], T.scene.ntris - 1);
     const float* tv = T.tri_v + 9 * size_t(ti);
     const float3 v0 = f3(tv[0], tv[1], tv[2]), v1 = f3(tv[3], tv[4], tv[5]), v2 = f3(tv[6], tv[7], tv[8]);
-    const float3 nf = cross3(v1 - v0, v2 - v0);
+    const float4 f0 = T.tri_frame[ti].fr[0];  // unit3(cross(v1 - v0, v2 - v0)), half its length
     const float r0 = rnd1(rng);
     const float r1 = rnd1(rng);
     const float a = fminf(r0, r1), b = fmaxf(r0, r1);
@@ -159,8 +160,8 @@ __device__ __forceinline__ LightSample sample_light(const TracerDev& T, float3 p
     l.dist = len3(d);
     l.dir = unit3(d);
     l.emission = T.light_emit[mi];
-    l.normal = unit3(nf);
-    l.inv_pdf = len3(nf) / 2.0f * (float)mesh.y * (float)T.light_count;
+    l.normal = xyz(f0);
+    l.inv_pdf = f0.w * (float)mesh.y * (float)T.light_count;
     l.mesh = mi;
     return l;
 }
@@ -211,9 +212,8 @@ __device__ __forceinline__ bool bounce_path(const TracerDev& T, uint32_t p, bool
         return false;
     }
     uint32_t rng = T.rng[p];
-    const float* tv = T.tri_v + 9 * size_t(h.prim);
-    const float3 v0 = f3(tv[0], tv[1], tv[2]), v1 = f3(tv[3], tv[4], tv[5]), v2 = f3(tv[6], tv[7], tv[8]);
-    const float3 fn = unit3(cross3(v1 - v0, v2 - v0));
+    const TriFrame& tf = T.tri_frame[h.prim];
+    const float3 fn = xyz(tf.fr[0]);
     float3 position = org + h.t * in_dir;
     const uint32_t mi = T.tri_mat[h.prim];
     const Material m = T.mats[mi < T.num_materials ? mi : T.num_materials - 1];
@@ -254,7 +254,7 @@ __device__ __forceinline__ bool bounce_path(const TracerDev& T, uint32_t p, bool
         // (sel == 1 as well: then the lobe choice and the pdf mixture never use it either)
         const bool glossy = m.specular.x != 0.0f || m.specular.y != 0.0f || m.specular.z != 0.0f || sel != 1.0f;
         const float3 refl = unit3(reflect3(in_dir, fn));
-        const float3 d0 = sample_cosine(fn, rng);
+        const float3 d0 = sample_cosine(Onb(xyz(tf.fr[2]), xyz(tf.fr[3]), xyz(tf.fr[1])), rng);
         float3 d1 = d0;
         if (glossy) {
             d1 = sample_phong(refl, m.shininess, rng);
@@ -612,9 +612,7 @@ __global__ void __launch_bounds__(kMlpThreads) k_mlp_lobes(TracerDev T, uint32_t
             if (live) {
                 const float4 tuv = T.hit_tuv[p];
                 const float3 o = T.org[p], d = T.dir[p];
-                const float* tv = T.tri_v + 9 * size_t(prim);
-                const float3 v0 = f3(tv[0], tv[1], tv[2]), v1 = f3(tv[3], tv[4], tv[5]), v2 = f3(tv[6], tv[7], tv[8]);
-                const float3 fn = unit3(cross3(v1 - v0, v2 - v0));
+                const float3 fn = xyz(T.tri_frame[prim].fr[0]);
                 mlp_features(o + tuv.x * d, fn, f3(-d.x, -d.y, -d.z), T.ml.dev.mn, T.ml.dev.inv_ext, f);
             }
         }
@@ -825,6 +823,13 @@ __global__ void __launch_bounds__(kTB) k_commit(TracerDev T) {
             if (s_q[j]) atomicAdd(T.tree.b_sums + j, s_q[j]);
         for (uint32_t j = threadIdx.x; j < ndt; j += blockDim.x)
             if (s_w[j]) atomicAdd(T.tree.b_statw + j, s_w[j]);
+    }
+}
+
+__global__ void k_tri_frames(const float* __restrict__ tri_v, uint32_t n, TriFrame* __restrict__ out) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float* tv = tri_v + 9 * size_t(i);
+        out[i] = make_tri_frame(f3(tv[0], tv[1], tv[2]), f3(tv[3], tv[4], tv[5]), f3(tv[6], tv[7], tv[8]));
     }
 }
 
@@ -1108,6 +1113,19 @@ int rtpg_tracer_create(rtpg_scene* scene, const float* tri_vertices, const uint3
     }
     T.tex = h->d_tex;
     T.tex_wh = h->d_tex_wh;
+    {
+        TriFrame* fr = nullptr;
+        if ((r = h->alloc(&fr, std::max(T.scene.ntris, 1u)))) {
+            delete h;
+            return r;
+        }
+        k_tri_frames<<<grid_for(T.scene.ntris, 256, 8), 256>>>(tri_vertices, T.scene.ntris, fr);
+        if ((e = cudaGetLastError()) != cudaSuccess || (e = cudaStreamSynchronize(nullptr)) != cudaSuccess) {
+            delete h;
+            return fail(RTPG_ECUDA, "rtpg_tracer_create: %s", cudaGetErrorString(e));
+        }
+        T.tri_frame = fr;
+    }
     *out = h;
     return rtpg_tracer_clear(h, nullptr);
 }

@@ -48,18 +48,41 @@ struct Onb {
         b = unit3(b);
         t = unit3(cross3(n, b));
     }
+    __device__ __forceinline__ Onb(float3 t_, float3 b_, float3 n_) : t(t_), b(b_), n(n_) {}
     __device__ __forceinline__ float3 local(float3 d) const { return d.x * t + d.y * b + d.z * n; }
 };
 
+// What shading needs of a triangle that does not depend on the ray, formed once per triangle
+// with the same operations the per-hit code would perform (so bit-identical):
+//   fr[0] = face normal unit3(cross(v1 - v0, v2 - v0)) and half its cross length (the area
+//           MeshLight::Sample weighs by, SimpleKernel.h:96);
+//   fr[1..3] = the ONB of that normal (its n, t, b), as sampleCosinePDF builds it.
+struct TriFrame {
+    float4 fr[4];
+};
+__device__ __forceinline__ TriFrame make_tri_frame(float3 v0, float3 v1, float3 v2) {
+    const float3 nf = cross3(v1 - v0, v2 - v0);
+    const float3 fn = unit3(nf);
+    const Onb o(fn);
+    TriFrame f;
+    f.fr[0] = make_float4(fn.x, fn.y, fn.z, len3(nf) / 2.0f);
+    f.fr[1] = make_float4(o.n.x, o.n.y, o.n.z, 0.0f);
+    f.fr[2] = make_float4(o.t.x, o.t.y, o.t.z, 0.0f);
+    f.fr[3] = make_float4(o.b.x, o.b.y, o.b.z, 0.0f);
+    return f;
+}
+__device__ __forceinline__ float3 xyz(float4 v) { return make_float3(v.x, v.y, v.z); }
+
 // random_cosine_direction (Random.h:321-334); draws x then y
-__device__ __forceinline__ float3 sample_cosine(float3 normal, uint32_t& rng) {
+__device__ __forceinline__ float3 sample_cosine(const Onb& onb, uint32_t& rng) {
     const float a = rnd1(rng);
     const float c = rnd1(rng);
     const float r = sqrtf(a), z = sqrtf(1.0f - a);
     float sp, cp;
     sincospif(2.0f * c, &sp, &cp);
-    return Onb(normal).local(f3(r * cp, r * sp, z));
+    return onb.local(f3(r * cp, r * sp, z));
 }
+__device__ __forceinline__ float3 sample_cosine(float3 normal, uint32_t& rng) { return sample_cosine(Onb(normal), rng); }
 // samplePhongPDF (SimpleGuide.cu:34-41)
 __device__ __forceinline__ float3 sample_phong(float3 refl, float s, uint32_t& rng) {
     const float cosT = powf(rnd1(rng), 1.0f / (s + 1.0f));
