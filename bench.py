@@ -401,6 +401,23 @@ C_AABB = ((-0.005,) * 3, (1.005,) * 3)  # world AABB padded by 0.005 as the appl
 BOUNCE_BYTES = 128
 
 
+def _issue_roofline(path_bounces, bounce_ms, clk):
+    """k_bounce against the issue limit: its warp-instructions per path-bounce (ncu, see
+    profiles/traffic.json) times the step's path-bounces over its CUDA-event time, against one
+    warp-instruction per cycle on each of the 4 schedulers of the 148 SMs at the sampled clock."""
+    ipb = _traffic("k_bounce_warp_inst_per_path_bounce")
+    if ipb is None:
+        return None
+    mhz = clk.get("sm_mhz") or 1965.0
+    achieved = ipb * path_bounces / (bounce_ms * 1e-3) / 1e9
+    peak = 4 * 148 * mhz * 1e6 / 1e9
+    return {"kernel": "k_bounce", "bound": "issue", "achieved": achieved, "peak": peak,
+            "unit": "G warp-instructions/s", "frac": achieved / peak,
+            "warp_inst_per_path_bounce": ipb, "thread_inst_per_inst": _traffic("k_bounce_thread_inst_per_inst"),
+            "peak_source": f"4 schedulers x 148 SMs x {mhz:.0f} MHz (sampled SM clock)",
+            "note": "instructions per path-bounce from ncu on the 7-spp case (profiles/k_bounce_commit_cornell_512.md)"}
+
+
 def _recording_launches(budget, iteration_for_built=0):
     """Launches of the SD-tree pass schedule (RTSTreeControllerT::BegTrace / EndTrace, one
     sample per launch) that record, i.e. whose waves end with the trace-vertex commit."""
@@ -527,6 +544,7 @@ def bench_cornell_ours(args, rank, world):
                      "kernel_ms_per_step": {kk: v[0] for kk, v in tk.items()},
                      "note": "bounce = BVH closest hit + shading + shadow ray; its bound is instruction "
                              "issue and traversal latency, the HBM figure is the SoA state traffic"},
+        "roofline_issue": _issue_roofline(cnt["path_bounces"], ext_ms, clk),
         "clocks": clk,
         # raygen, max_depth bounces and the accumulation per launch, plus the commit of every
         # recording launch
@@ -1308,7 +1326,7 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": ("bf16" if mlp else "f32"),
             "data": "synthetic", "config": cfg, "e2e": res["e2e"], "roofline": res["roofline"],
             "clocks": res["clocks"], "gpu_launches": res["gpu_launches"]}
-    for k in ("sdtree", "phases", "roofline_record", "counters_per_step", "unguided_nee_ris_Mpaths_s", "grid_cells", "spp_per_step",
+    for k in ("roofline_issue", "sdtree", "phases", "roofline_record", "counters_per_step", "unguided_nee_ris_Mpaths_s", "grid_cells", "spp_per_step",
               "inference", "queries_found", "grid_status"):
         if k in res:
             line[k] = res[k]
