@@ -951,10 +951,10 @@ def bench_learned(args):
         tr = Tracer(sc, dev, max_depth=O_DEPTH, seed=3)
         g = MLPGuide((-0.1, -0.1, -0.1), (14.1, 4.1, 10.1), seed=1, learning_rate=1e-3, record_capacity=1 << 18)
         tree = SDTree(*O_AABB, fraction=0.5)
-        log = []
+        log, crit = [], []
         n_ml = render_learned_with_fallback(tr, g, tree, time_budget_s=budget, base_flags=flags,
                                             fraction=args.guide_fraction, mlp_share=0.5, epochs=args.epochs,
-                                            batch=4096, log=log)
+                                            batch=4096, log=log, criteria=crit)
         e_ml, d_ml = err(tr.image().cpu().numpy())
         st_ml = g.status()
         del tr, g, tree
@@ -972,7 +972,10 @@ def bench_learned(args):
                                  "relmse_sdtree_at_guide_fraction": d_sd2},
                     "relmse_sdtree_at_guide_fraction": e_sd2, "spp_sdtree_at_guide_fraction": n_sd2,
                     "spp_sdtree": n_sd, "spp_learned": n_ml, "spp_network_only": n_mo,
-                    "train_log": log[-3:], "mlp_status": st_ml})
+                    "train_log": log[-3:], "mlp_status": st_ml,
+                    # per recording pass, on that pass's records before either guide is fitted to
+                    # them: second moment of f / p with p = (1 - f_g) cos/pi + f_g q for each guide q
+                    "second_moment_per_pass": crit})
     return {"budgets": out, "ref_spp": ref_spp, "ref_seconds": args.ref_seconds}
 
 

@@ -289,6 +289,9 @@ int rtpg_mlp_train(rtpg_mlp* h, int64_t n, const float* pos, const float* nrm, c
 /* records written so far (may exceed the capacity: the excess was dropped); clear = 1 empties */
 int rtpg_mlp_records(rtpg_mlp* h, uint32_t* host_count, int clear, void* stream);
 int rtpg_mlp_record_arrays(rtpg_mlp* h, float** pos, float** nrm, float** wo, float** wi, float** w);
+/* device pointer of the records' sampling densities (1 float per record): the woPdf the tracer
+ * sampled the record's direction with, so that the integrand value of a record is w * pdf */
+int rtpg_mlp_record_pdfs(rtpg_mlp* h, float** wo_pdf);
 int rtpg_mlp_status(rtpg_mlp* h, uint32_t* host_status, int clear, void* stream);
 /* Test mode of the bounded waits on the tensor cores (no counterpart in RTLib): skip_mma = 1
  * makes this guide's kernels issue no MMA and no commit, so every completion wait runs out after

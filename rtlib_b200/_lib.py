@@ -93,6 +93,7 @@ _SIGS = {
     "rtpg_mlp_train": [P, I64, P, P, P, P, P, U32, U32, P, P],
     "rtpg_mlp_records": [P, P, C.c_int, P],
     "rtpg_mlp_record_arrays": [P, P, P, P, P, P],
+    "rtpg_mlp_record_pdfs": [P, P],
     "rtpg_mlp_status": [P, P, C.c_int, P],
     "rtpg_mlp_set_wait_test": [P, C.c_int, U32],
     "rtpg_tracer_set_light_emission": [P, P, U32],

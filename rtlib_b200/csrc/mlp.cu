@@ -317,7 +317,7 @@ struct rtpg_mlp {
     float mn[3], mx[3];
     // record buffer (filled by the tracer or rtpg_mlp_add_records)
     uint32_t capacity = 0;
-    float *r_pos = nullptr, *r_nrm = nullptr, *r_wo = nullptr, *r_wi = nullptr, *r_w = nullptr;
+    float *r_pos = nullptr, *r_nrm = nullptr, *r_wo = nullptr, *r_wi = nullptr, *r_w = nullptr, *r_pdf = nullptr;
     uint32_t* r_count = nullptr;
     unsigned* status = nullptr;
     std::vector<void*> allocs;
@@ -340,7 +340,7 @@ struct rtpg_mlp {
 
 namespace rtpg {
 MlpView mlp_view(const rtpg_mlp* h) {
-    return MlpView{h->dev, h->r_pos, h->r_nrm, h->r_wo, h->r_wi, h->r_w, h->r_count, h->capacity};
+    return MlpView{h->dev, h->r_pos, h->r_nrm, h->r_wo, h->r_wi, h->r_w, h->r_pdf, h->r_count, h->capacity};
 }
 size_t mlp_eval_smem() { return kSmemEval; }
 }
@@ -378,7 +378,8 @@ int rtpg_mlp_create(const float* aabb_min, const float* aabb_max, uint32_t seed,
     if ((r = h->alloc(&h->w, kMlpParams)) || (r = h->alloc(&h->g, kMlpParams)) || (r = h->alloc(&h->m, kMlpParams)) ||
         (r = h->alloc(&h->v, kMlpParams)) || (r = h->alloc(&h->wq, kMlpParams)) || (r = h->alloc(&h->scratch, 4)) ||
         (r = h->alloc(&h->r_pos, 3 * C)) || (r = h->alloc(&h->r_nrm, 3 * C)) || (r = h->alloc(&h->r_wo, 3 * C)) ||
-        (r = h->alloc(&h->r_wi, 3 * C)) || (r = h->alloc(&h->r_w, C)) || (r = h->alloc(&h->r_count, 1)) ||
+        (r = h->alloc(&h->r_wi, 3 * C)) || (r = h->alloc(&h->r_w, C)) || (r = h->alloc(&h->r_pdf, C)) ||
+        (r = h->alloc(&h->r_count, 1)) ||
         (r = h->alloc(&h->status, 1))) {
         delete h;
         return r;
@@ -555,6 +556,14 @@ int rtpg_mlp_set_wait_test(rtpg_mlp* h, int skip_mma, uint32_t poll_limit) {
     if (!h) return fail(RTPG_EINVAL, "rtpg_mlp_set_wait_test: null handle");
     h->dev.skip_mma = skip_mma ? 1u : 0u;
     h->dev.poll_limit = poll_limit ? poll_limit : kMbarPollLimit;
+    return RTPG_OK;
+}
+
+// Device pointer of the records' sampling densities (1 float per record): the woPdf with which
+// the tracer sampled the record's direction, so that a record's integrand value is w * pdf.
+int rtpg_mlp_record_pdfs(rtpg_mlp* h, float** wo_pdf) {
+    if (!h || !wo_pdf) return fail(RTPG_EINVAL, "rtpg_mlp_record_pdfs: null argument");
+    *wo_pdf = h->r_pdf;
     return RTPG_OK;
 }
 

@@ -261,6 +261,7 @@ __device__ __forceinline__ void mma_drain(uint64_t* mbar, uint32_t phase, uint32
 struct MlpView {
     MlpDev dev;
     float *r_pos, *r_nrm, *r_wo, *r_wi, *r_w;
+    float* r_pdf;  // the density the record's direction was sampled with (the vertex's woPdf)
     uint32_t* r_count;
     uint32_t capacity;
 };

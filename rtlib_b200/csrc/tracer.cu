@@ -786,6 +786,7 @@ __global__ void __launch_bounds__(kTB) k_commit(TracerDev T) {
                             ro[0] = wv.x; ro[1] = wv.y; ro[2] = wv.z;
                             ri[0] = dr.x; ri[1] = dr.y; ri[2] = dr.z;
                             T.ml.r_w[idx] = irr;
+                            T.ml.r_pdf[idx] = wo;
                         }
                     }
                 }

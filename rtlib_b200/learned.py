@@ -68,13 +68,19 @@ def render_learned(tracer, mlp, budget_spp=None, time_budget_s=None, base_flags=
 
 
 def render_learned_with_fallback(tracer, mlp, tree, budget_spp=None, time_budget_s=None, base_flags=1, fraction=0.5,
-                                 mlp_share=0.5, ratio=0.5, epochs=32, batch=4096, sync=None, log=None):
+                                 mlp_share=0.5, ratio=0.5, epochs=32, batch=4096, sync=None, log=None,
+                                 criteria=None):
     """The learned guide with the SD-tree as its fallback: RTSTreeControllerT's pass schedule
     (one sample per launch; build and refine of the tree between passes as in plain SD-tree
     guiding), every launch guided by q = mlp_share * network + (1 - mlp_share) * SD-tree with
     both learning from the same trace vertices, and the network trained after every recording
     pass.  With a time budget the controller's sample budget is unbounded and the launches stop
-    when the time is spent.  Returns the number of samples rendered."""
+    when the time is spent.  Returns the number of samples rendered.
+
+    criteria (a list, optional) receives per recording pass, once the network has been trained,
+    guide_second_moments of that pass's records, taken after its last launch and before the
+    controller builds the SD-tree from them: both guides are judged on records they have not
+    been fitted to.  Its cost is inside the time budget."""
     import torch
 
     from .sdtree import TRACE_RECORD_AND_SAMPLE, TRACE_SAMPLE, SDTreeController
@@ -88,6 +94,8 @@ def render_learned_with_fallback(tracer, mlp, tree, budget_spp=None, time_budget
     done, keep, last_it, pass_spp = 0, 1.0, 0, 0
     mlp.records(clear=True)
     trained = False
+    # the controller's pass sizes (RTSTreeControllerT::BegTrace), to know a pass's last launch
+    remain, pas, per_all, it_m = budget, 0, 0, 0
     while True:
         if time_budget_s is not None and time.perf_counter() - t0 >= time_budget_s:
             break
@@ -101,13 +109,26 @@ def render_learned_with_fallback(tracer, mlp, tree, budget_spp=None, time_budget
         elif st["state"] == TRACE_SAMPLE:
             flags |= FLAG_BUILD | FLAG_FINAL
         # before the network has been trained the SD-tree alone guides
+        if pass_spp == 0:
+            remain -= pas
+            pas = min(remain, 1 << it_m)
+            if remain - pas < 2 * pas or per_all >= ratio * budget:
+                pas = remain
         tracer.render_mlp(1, flags, mlp, fraction, keep, fallback=tree, mlp_share=mlp_share if trained else 0.0)
+        per_all += 1
+        if (criteria is not None and trained and pass_spp + 1 == pas and not (flags & FLAG_FINAL)
+                and mlp.records() > 0):
+            c = guide_second_moments(mlp, tree, fraction, mlp_share)
+            if c is not None:
+                c["pass"] = it_m
+                criteria.append(c)
         ctrl.end()
         done += 1
         pass_spp += 1
         st2 = ctrl.get()
         if st2["iteration"] != last_it:  # a pass ended: train on its records
             last_it = st2["iteration"]
+            it_m += 1
             n = mlp.records()
             if n > 0 and not (flags & FLAG_FINAL):
                 loss = mlp.train(batch=batch, epochs=epochs)
@@ -122,3 +143,44 @@ def render_learned_with_fallback(tracer, mlp, tree, budget_spp=None, time_budget
             sync()
     sync()
     return done
+
+
+def _vmf_mixture_pdf(lobes, wi):
+    """Density of the 8-lobe mixture (n x 40: mu xyz, kappa, weight per lobe) at wi (n x 3),
+    the formula of the tracer's vmf_mixture_pdf."""
+    import torch
+    L = lobes.view(-1, 8, 5).double()
+    mu, k, wgt = L[..., :3], L[..., 3], L[..., 4]
+    c = (mu * wi.double()[:, None, :]).sum(-1)
+    return (wgt * k / (2 * torch.pi * (1 - torch.exp(-2 * k))) * torch.exp(k * (c - 1))).sum(-1)
+
+
+def guide_second_moments(mlp, tree, fraction, mlp_share):
+    """Per-vertex variance criterion of the guides on the records now in the guide's buffer: for
+    a sampling density p, E[f^2 / (q_rec p)] over the records estimates the second moment
+    integral of f^2 / p of the one-sample estimator f / p at a vertex (f = w * q_rec, the record's
+    luminance of incident radiance times |cos|, q_rec the density it was sampled with).  Returns
+    it for the densities the tracer would use with each guide, p = (1 - fraction) cos/pi +
+    fraction * q, q the network, the SD-tree, or share * network + (1 - share) * SD-tree, and for
+    cosine (BSDF) sampling alone; all surfaces of the scenes it is used on are Lambertian."""
+    import torch
+    pos, nrm, wo, wi, w, pdf = mlp.record_views()
+    n = pos.shape[0]
+    if n == 0:
+        return None
+    lobes = mlp.eval(pos, nrm, wo, raw=False)
+    q_net = _vmf_mixture_pdf(lobes, wi)
+    q_tree = torch.empty(n, dtype=torch.float32, device=pos.device)
+    tree.pdf(pos.contiguous(), wi.contiguous(), q_tree, canonical=False)
+    q_tree = q_tree.double()
+    bsdf = torch.clamp((nrm.double() * wi.double()).sum(-1), min=0.0) / torch.pi
+    f = w.double() * pdf.double()
+    ok = (pdf > 0) & (f > 0)
+
+    def moment(p):
+        p = p[ok]
+        return float((f[ok] ** 2 / (pdf.double()[ok] * p)).mean()) if bool((p > 0).all()) else float("inf")
+
+    mix = lambda q: (1 - fraction) * bsdf + fraction * q
+    return {"records": int(ok.sum()), "network": moment(mix(q_net)), "sdtree": moment(mix(q_tree)),
+            "mixture": moment(mix(mlp_share * q_net + (1 - mlp_share) * q_tree)), "bsdf": moment(bsdf)}

@@ -78,3 +78,25 @@ class MLPGuide:
         """Test mode of the bounded tensor-core waits: skip_mma=True issues no MMA, so every
         wait runs out after poll_limit polls and the kernels report RTPG_STATUS_TIMEOUT."""
         call("rtpg_mlp_set_wait_test", self.h, int(bool(skip_mma)), int(poll_limit))
+
+    def record_views(self, n=None):
+        """The first n records (default: all written, up to the capacity) as torch tensors that
+        view the guide's record buffer: pos, nrm, wo, wi (n x 3), w and pdf (n), where pdf is the
+        density the tracer sampled the record's direction with."""
+        import torch
+        n = min(self.records(), self.capacity) if n is None else int(n)
+        ptrs = [C.c_void_p() for _ in range(6)]
+        call("rtpg_mlp_record_arrays", self.h, *[C.byref(p) for p in ptrs[:5]])
+        call("rtpg_mlp_record_pdfs", self.h, C.byref(ptrs[5]))
+
+        class _View:
+            def __init__(self, ptr, shape):
+                self.__cuda_array_interface__ = {"shape": shape, "typestr": "<f4", "data": (ptr, False),
+                                                 "version": 3, "strides": None}
+
+        out = []
+        for p, k in zip(ptrs, (3, 3, 3, 3, 1, 1)):
+            shape = (n, 3) if k == 3 else (n,)
+            out.append(torch.as_tensor(_View(p.value, shape), device="cuda") if n > 0 else
+                       torch.empty(shape, dtype=torch.float32, device="cuda"))
+        return tuple(out)

@@ -406,3 +406,27 @@ def test_learned_guide_with_sdtree_fallback_runs(cuda):
     pt.render_guided(tree2, ctrl, flags)
     e_sd = metrics.relmse(pt.image().cpu().numpy(), ref, normalize=True)
     assert e_mix < 1.5 * e_sd, (e_mix, e_sd, log)
+
+
+def test_guide_second_moments_per_pass(cuda):
+    """The per-pass variance criterion of the learned guide's records: finite and positive for
+    every guide and for cosine sampling, recorded for the passes after the network was first
+    trained.  (Which guide wins depends on the case: on this small one the young SD-tree can
+    still lose to cosine sampling.)"""
+    from rtlib_b200.learned import render_learned_with_fallback
+    from rtlib_b200.mlp import MLPGuide
+    from rtlib_b200.sdtree import SDTree
+    from rtlib_b200.tracer import Tracer
+    sc = scenes.cornell_box(64, 64)
+    tr = Tracer(sc, cuda, max_depth=8, width=64, height=64)
+    g = MLPGuide((-0.1,) * 3, (1.1,) * 3, seed=2, record_capacity=1 << 16)
+    tree = SDTree((-0.005,) * 3, (1.005,) * 3, fraction=0.5)
+    crit = []
+    render_learned_with_fallback(tr, g, tree, budget_spp=63, base_flags=1, fraction=0.5, epochs=4, batch=2048,
+                                 criteria=crit)
+    assert len(crit) >= 2, crit
+    for c in crit:
+        assert c["records"] > 0
+        for k in ("network", "sdtree", "mixture", "bsdf"):
+            assert np.isfinite(c[k]) and c[k] > 0, c
+        assert max(c["network"], c["sdtree"], c["mixture"]) < 10 * c["bsdf"], c
