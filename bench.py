@@ -61,7 +61,7 @@ N_Q = 1 << 22
 Q_BYTES = 28
 # algorithmic bytes of one record: position 12 B, canonical direction 8 B, radiance 4 B
 REC_BYTES = 24
-LAUNCHES_PER_STEP = 21  # clear 1, record 1, build 1, refine 17, sample 1 (three CUDA graphs)
+LAUNCHES_PER_STEP = 23  # clear 2, record 1, build 1, refine 18, sample 1 (three CUDA graphs)
 
 
 def _env_int(k, d):
@@ -282,7 +282,7 @@ def bench_sdtree_ours(args, rank, world):
                      "traffic": _traffic("k_sample_pdf"), "algorithmic_bytes_per_launch": Q_BYTES * N_Q,
                      "launch_ms": s_ms},
         "clocks": clk,
-        "gpu_launches": (LAUNCHES_PER_STEP + (args.passes - 1) * 20) * args.steps,
+        "gpu_launches": (LAUNCHES_PER_STEP + (args.passes - 1) * 21) * args.steps,
         "sdtree": st,
         "roofline_record": {"kernel": "k_record (with clear)", "bound": "L2 atomics", "unit": "GB/s",
                             "achieved": REC_BYTES * N_REC / (statistics.mean(record_ms) * 1e-3) / 1e9,

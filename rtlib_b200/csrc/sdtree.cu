@@ -45,6 +45,21 @@ __global__ void k_clear(SDTreeDev t) {
     }
 }
 
+// The STree's top table (SDTreeDev::stop): entry c holds the node the first kTopLevels steps
+// reach for digits x = c >> 6, y = (c >> 3) & 7, z = c & 7 (three per axis, most significant
+// first), or the leaf where the walk stops earlier -- exactly what stree_lookup's per-level
+// steps give for those digits.
+__global__ void k_stree_top(SDTreeDev t) {
+    grid_dependency_wait();
+    for (uint32_t c = threadIdx.x; c < kTopCells; c += blockDim.x) {
+        const uint32_t d[3] = {c >> 6, (c >> 3) & 7u, c & 7u};
+        uint32_t code = t.snode[0];
+        for (int l = 0; l < kTopLevels && !(code & kLeafBit); ++l)
+            code = t.snode[code + ((d[l % 3] >> (2 - l / 3)) & 1u)];
+        t.stop[c] = code;
+    }
+}
+
 // ------------------------------------------------------------------ record
 // One thread per record (grid-stride, warp-uniform trip count so that the warp-aggregated
 // atomics run converged).  Two 64-bit fixed-point atomics per record: the DTree's stat-weight
@@ -86,7 +101,8 @@ __global__ void __launch_bounds__(kRecordBlock) k_record(SDTreeDev t, int64_t n,
             const float sw = stat_w ? stat_w[i] : 1.0f;
             const float irr = __fdiv_rn(radiance[i], wo);
             if (isfinite(sw) && sw > 0.0f) {
-                const uint32_t d = stree_lookup(st, t.mn, t.mx, pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], t.inv_size);
+                const uint32_t d = stree_lookup(st, t.mn, t.mx, pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], t.inv_size,
+                                                staged ? nullptr : t.stop);
                 k_w = d;
                 v_w = to_fx(sw, t.fx, t.status);
                 if (isfinite(irr) && irr > 0.0f) {
@@ -479,7 +495,7 @@ __global__ void __launch_bounds__(kSampleBlock, 8) k_sample_pdf(SDTreeDev t, int
                                                                float* __restrict__ out_dir, float* __restrict__ out_pdf_dir) {
     const int64_t stride = int64_t(gridDim.x) * blockDim.x;
     for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
-        const uint32_t d = stree_lookup(t.snode, t.mn, t.mx, pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], t.inv_size);
+        const uint32_t d = stree_lookup(t.snode, t.mn, t.mx, pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], t.inv_size, t.stop);
         uint32_t rng = seeds ? seeds[i] : (pcg1d(seed_base + (uint32_t)i) | 1u);
         const uint32_t off = t.s_off[d];
         const bool guided = t.s_guided[d] != 0;
@@ -506,7 +522,7 @@ __global__ void __launch_bounds__(256) k_pdf(SDTreeDev t, int64_t n, const float
                                              const float* __restrict__ dir, int canonical, float* __restrict__ out) {
     const int64_t stride = int64_t(gridDim.x) * blockDim.x;
     for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
-        const uint32_t d = stree_lookup(t.snode, t.mn, t.mx, pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], t.inv_size);
+        const uint32_t d = stree_lookup(t.snode, t.mn, t.mx, pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], t.inv_size, t.stop);
         float2 c;
         if (canonical) c = reinterpret_cast<const float2*>(dir)[i];
         else c = dir_to_canonical(dir[3 * i], dir[3 * i + 1], dir[3 * i + 2]);
@@ -557,6 +573,7 @@ SDTreeDev sdtree_device_view(const rtpg_sdtree* t) { return t->dev; }
 static int sdtree_clear(rtpg_sdtree* h, cudaStream_t st) {
     RTPG_CUDA(cudaMemsetAsync(h->dev.status, 0, sizeof(unsigned), st));
     k_clear<<<1, 32, 0, st>>>(h->dev);
+    k_stree_top<<<1, kTopCells, 0, st>>>(h->dev);
     RTPG_LAUNCH_CHECK();
     return RTPG_OK;
 }
@@ -620,6 +637,7 @@ int rtpg_sdtree_create(const float* aabb_min, const float* aabb_max, uint32_t ma
     int r = RTPG_OK;
     const size_t nd = c.max_dtrees, nn = c.max_dtree_nodes_total, ns = c.max_stree_nodes;
     if ((r = h->alloc(&t.status, 1)) || (r = h->alloc(&t.counts, 4)) || (r = h->alloc(&t.snode, ns)) ||
+        (r = h->alloc(&t.stop, kTopCells)) ||
         (r = h->alloc(&t.b_off, nd)) || (r = h->alloc(&t.b_cnt, nd)) || (r = h->alloc(&t.s_off, nd)) ||
         (r = h->alloc(&t.s_cnt, nd)) || (r = h->alloc(&t.b_statw, nd)) || (r = h->alloc(&t.s_sum, nd)) ||
         (r = h->alloc(&t.s_area, nd)) || (r = h->alloc(&t.s_statw, nd)) || (r = h->alloc(&t.s_guided, nd)) ||
@@ -711,6 +729,7 @@ int rtpg_sdtree_refine(rtpg_sdtree* h, uint64_t spatial_threshold, int32_t max_m
                                h->cnt_d, h->fp));
     RTPG_CUDA(launch_dependent(k_refine_link, grid_for(t.cap_snodes, 256, 4), 256, 0, st, t, h->ksplit, h->off_s, h->fp));
     RTPG_CUDA(launch_dependent(k_refine_commit, 1, 1, 0, st, t, h->fp));
+    RTPG_CUDA(launch_dependent(k_stree_top, 1, kTopCells, 0, st, t));
     // quadtree reset of every leaf
     RTPG_CUDA(launch_dependent(k_reset<false>, kSMs, kTreeBlock, reset_smem(), st, t, dtree_subdiv_th, h->node_cnt,
                                (const uint32_t*)nullptr, h->fp + 3));
@@ -1146,6 +1165,8 @@ extern "C" int rtpg_sdtree_import(rtpg_sdtree* h, int64_t stree_nodes, int64_t l
     RTPG_CUDA(ul(t.b_child, b_child, st));
     RTPG_CUDA(ul(t.s_nodes, s_nodes, st));
     RTPG_CUDA(ul(t.s_q, s_q, st));
+    k_stree_top<<<1, kTopCells, 0, st>>>(t);
+    RTPG_LAUNCH_CHECK();
     // the host vectors must outlive the copies
     RTPG_CUDA(cudaStreamSynchronize(st));
     return RTPG_OK;

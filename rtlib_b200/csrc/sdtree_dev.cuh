@@ -85,6 +85,9 @@ struct SDTreeDev {
     uint32_t* counts;  // [0] STree nodes, [1] DTrees, [2] building nodes in use, [3] sampling nodes
     float3 inv_size;   // 1 / (mx - mn) per axis where that size is a power of two, else 0
     uint32_t* snode;
+    // the node reached after the first kTopLevels levels (or the leaf above them) for every
+    // combination of the first three binary digits of x, y and z; rebuilt whenever the STree changes
+    uint32_t* stop;
     uint32_t* b_off;
     uint32_t* b_cnt;
     uint32_t* s_off;
@@ -142,15 +145,30 @@ __device__ __forceinline__ AxisDigits axis_digits(float p) {
     }
     return AxisDigits{p >= 1.0f ? 0x7fffffffu : 0u, p};
 }
+constexpr int kTopLevels = 9;  // 3 digits per axis
+constexpr uint32_t kTopCells = 1u << kTopLevels;
+// top-table index of the first three digits of each axis (bits 30..28)
+__device__ __forceinline__ uint32_t top_cell(uint32_t bx, uint32_t by, uint32_t bz) {
+    return (((bx >> 28) & 7u) << 6) | (((by >> 28) & 7u) << 3) | ((bz >> 28) & 7u);
+}
+// `top` (optional): the table of the first kTopLevels levels (SDTreeDev::stop); the walk then
+// starts from the entry and continues with the fourth digit of each axis
 __device__ __forceinline__ uint32_t stree_lookup(const uint32_t* __restrict__ snode, float3 mn, float3 mx, float px,
-                                                 float py, float pz, float3 inv = float3{0.0f, 0.0f, 0.0f}) {
+                                                 float py, float pz, float3 inv = float3{0.0f, 0.0f, 0.0f},
+                                                 const uint32_t* __restrict__ top = nullptr) {
     uint32_t code = snode[0];
     if (code & kLeafBit) return code & ~kLeafBit;
     const AxisDigits ax = axis_digits(stree_norm(px, mn.x, mx.x, inv.x));
     const AxisDigits ay = axis_digits(stree_norm(py, mn.y, mx.y, inv.y));
     const AxisDigits az = axis_digits(stree_norm(pz, mn.z, mx.z, inv.z));
+    int sh0 = 30;
+    if (top) {
+        code = top[top_cell(ax.bits, ay.bits, az.bits)];
+        if (code & kLeafBit) return code & ~kLeafBit;
+        sh0 = 30 - kTopLevels / 3;
+    }
     // levels 3k, 3k+1, 3k+2 take bit 30-k of x, y, z
-    for (int sh = 30; sh >= 0; --sh) {
+    for (int sh = sh0; sh >= 0; --sh) {
         code = snode[code + ((ax.bits >> sh) & 1u)];
         if (code & kLeafBit) return code & ~kLeafBit;
         code = snode[code + ((ay.bits >> sh) & 1u)];

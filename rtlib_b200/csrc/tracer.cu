@@ -238,7 +238,8 @@ __device__ __forceinline__ bool bounce_path(const TracerDev& T, uint32_t p, bool
     bool have_c = false;
     // the learned guide may carry the SD-tree as its fallback (T.tree set, mlp_share < 1)
     const bool mlp_mix = use_mlp && T.tree.snode != nullptr;
-    if (use_tree || mlp_mix) dt = stree_lookup(T.tree.snode, T.tree.mn, T.tree.mx, position.x, position.y, position.z, T.tree.inv_size);
+    if (use_tree || mlp_mix) dt = stree_lookup(T.tree.snode, T.tree.mn, T.tree.mx, position.x, position.y, position.z, T.tree.inv_size,
+                                                 T.tree.stop);
     if (m.type == MAT_PHONG) {
         uint32_t gbucket = 0, prv_cell = 0xffffffffu;
         unsigned long long gkey = 0;
