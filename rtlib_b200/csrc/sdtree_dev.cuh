@@ -30,15 +30,21 @@ struct __align__(32) SNode {
 // the quadrant sums that DTreeNodeT::Sample and ::Pdf (PG.h:229-320) divide out at every visit,
 // formed once when the node is written, with the same IEEE operations on the same operands, so
 // that a descent reads them instead of dividing (bit-identical results):
-//   bnd = partial / total, btl = topLeft / partial, btr = topRight / (total - partial)
-//         with partial = s0 + s2 and total = ((s0 + s1) + s2) + s3;
+//   bnd = partial / total with partial = s0 + s2 and total = ((s0 + s1) + s2) + s3;
+//   tl, tr: the second choice as a threshold on the drawn sample itself.  Sample divides the
+//         draw s out (s / bnd left of bnd, (s - bnd) / (1 - bnd) right of it) and takes
+//         quadrant 2 (3) when the quotient is >= topLeft / partial (topRight / (total - partial)).
+//         Both quotients are non-decreasing in s wherever that side can be reached, so the
+//         choice is s >= t for the smallest draw t that makes it (+inf when none does); the
+//         draws are the 2^23 values k 2^-23 (rnd1), and t is found by bisecting them with the
+//         same divisions, so the descent decides exactly as the divisions would;
 //   fac_i = 4 s_i / total (the pdf factor of quadrant i);
 //   meta: bits 0-15 the first child, 16-19 which quadrants have a child, 20-23 which have
 //         s_i <= 0 (where DTreeNodeT::Sample / Pdf stop, PG.h:268-300).
 // The children of a node are consecutive in quadrant order (the reset numbers them so, and
 // so does the import), so child q = first + the number of children before q.
 struct __align__(32) SQNode {
-    float bnd, btl, btr;
+    float bnd, tl, tr;
     uint32_t meta;
     float fac[4];
 };
@@ -49,13 +55,39 @@ __host__ __device__ inline float sq_div(float a, float b) {
     return a / b;
 #endif
 }
+__host__ __device__ inline float sq_sub(float a, float b) {
+#ifdef __CUDA_ARCH__
+    return __fsub_rn(a, b);
+#else
+    return a - b;
+#endif
+}
+constexpr uint32_t kDrawSteps = 1u << 23;  // rnd1 draws k 2^-23, k < 2^23
+__host__ __device__ inline float draw_value(uint32_t k) { return (float)k * 0x1p-23f; }
+// the vertical choice of Sample on the left (side 0) or right (side 1) of bnd for draw s
+__host__ __device__ inline bool sq_lower(int side, float s, float bnd, float b) {
+    const float q = side == 0 ? sq_div(s, bnd) : sq_div(sq_sub(s, bnd), sq_sub(1.0f, bnd));
+    return q >= b;
+}
+// the smallest draw for which sq_lower holds, +inf when none does (bisection over the draws;
+// sq_lower is non-decreasing in s where that side is reachable)
+__host__ __device__ inline float sq_threshold(int side, float bnd, float b) {
+    uint32_t lo = 0, hi = kDrawSteps - 1;
+    if (!sq_lower(side, draw_value(hi), bnd, b)) return INFINITY;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (sq_lower(side, draw_value(mid), bnd, b)) hi = mid;
+        else lo = mid + 1;
+    }
+    return draw_value(lo);
+}
 __host__ __device__ inline SQNode make_sqnode(float4 s, ushort4 child) {
     SQNode n;
     const float partial = s.x + s.z;
     const float total = ((s.x + s.y) + s.z) + s.w;
     n.bnd = sq_div(partial, total);
-    n.btl = sq_div(s.x, partial);
-    n.btr = sq_div(s.y, total - partial);
+    n.tl = sq_threshold(0, n.bnd, sq_div(s.x, partial));
+    n.tr = sq_threshold(1, n.bnd, sq_div(s.y, total - partial));
     n.fac[0] = sq_div(4.0f * s.x, total);
     n.fac[1] = sq_div(4.0f * s.y, total);
     n.fac[2] = sq_div(4.0f * s.z, total);
@@ -135,15 +167,17 @@ __device__ __forceinline__ float stree_norm(float p, float mn, float mx, float i
 // itself carried on.
 struct AxisDigits {
     uint32_t bits;
-    float rest;
+    float s;  // p 2^31 inside [0, 1), p outside
+    bool in;
+    // the p the steps carry on with after the 31 digits (only walks deeper than 93 levels)
+    __device__ __forceinline__ float rest() const { return in ? __fsub_rn(s, __uint2float_rz(bits)) : s; }
 };
 __device__ __forceinline__ AxisDigits axis_digits(float p) {
     if (p >= 0.0f && p < 1.0f) {
         const float s = __fmul_rn(p, 2147483648.0f);
-        const uint32_t b = __float2uint_rz(s);
-        return AxisDigits{b, __fsub_rn(s, __uint2float_rz(b))};
+        return AxisDigits{__float2uint_rz(s), s, true};
     }
-    return AxisDigits{p >= 1.0f ? 0x7fffffffu : 0u, p};
+    return AxisDigits{p >= 1.0f ? 0x7fffffffu : 0u, p, false};
 }
 constexpr int kTopLevels = 9;  // 3 digits per axis
 constexpr uint32_t kTopCells = 1u << kTopLevels;
@@ -177,7 +211,7 @@ __device__ __forceinline__ uint32_t stree_lookup(const uint32_t* __restrict__ sn
         if (code & kLeafBit) return code & ~kLeafBit;
     }
     // deeper than 93 levels: the per-level steps from where the digits end
-    float x = ax.rest, y = ay.rest, z = az.rest;
+    float x = ax.rest(), y = ay.rest(), z = az.rest();
     for (;;) {
         if (stree_step(snode, code, x)) break;
         if (stree_step(snode, code, y)) break;
@@ -308,18 +342,16 @@ __device__ __forceinline__ float2 dtree_sample_sq(const SQNode* __restrict__ nod
         const float bnd = w.x;
         const uint32_t meta = __float_as_uint(w.w);
         int idx = 0;
-        float ox = 0.0f, oy = 0.0f, boundary;
-        float sample = rnd1(rng);
+        float ox = 0.0f, oy = 0.0f, threshold;
+        const float sample = rnd1(rng);
         if (sample < bnd) {
-            sample = __fdiv_rn(sample, bnd);
-            boundary = w.y;  // topLeft / partial
+            threshold = w.y;  // tl
         } else {
             ox = 0.5f;
-            sample = __fdiv_rn(__fsub_rn(sample, bnd), __fsub_rn(1.0f, bnd));
-            boundary = w.z;  // topRight / (total - partial)
+            threshold = w.z;  // tr
             idx |= 1;
         }
-        if (sample >= boundary) {
+        if (sample >= threshold) {
             oy = 0.5f;
             idx |= 2;
         }
