@@ -489,12 +489,16 @@ __global__ void k_reset_commit(SDTreeDev t, const unsigned long long* node_total
 // level staged, 65.5 / 31.1 with no staging): the shared memory comes out of the same 256 KB
 // per SM as L1, which then no longer holds the deeper levels.
 constexpr uint32_t kSampleBlock = 256;
-__global__ void __launch_bounds__(kSampleBlock, 8) k_sample_pdf(SDTreeDev t, int64_t n, const float* __restrict__ pos,
+// largest query count whose 3 n element offsets (plus a grid stride) stay inside int32
+constexpr int64_t kMaxIndex32 = (int64_t(1) << 31) / 4;
+// I: the query index type (32-bit while 3 n fits, which saves the 64-bit address arithmetic)
+template <class I>
+__global__ void __launch_bounds__(kSampleBlock, 8) k_sample_pdf(SDTreeDev t, I n, const float* __restrict__ pos,
                                                                const uint32_t* __restrict__ seeds, uint32_t seed_base,
                                                                float* __restrict__ out_uv, float* __restrict__ out_pdf_uv,
                                                                float* __restrict__ out_dir, float* __restrict__ out_pdf_dir) {
-    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
-    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const I stride = I(gridDim.x) * I(blockDim.x);
+    for (I i = I(blockIdx.x) * I(blockDim.x) + I(threadIdx.x); i < n; i += stride) {
         const uint32_t d = stree_lookup(t.snode, t.mn, t.mx, pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], t.inv_size, t.stop);
         uint32_t rng = seeds ? seeds[i] : (pcg1d(seed_base + (uint32_t)i) | 1u);
         const uint32_t off = t.s_off[d];
@@ -756,8 +760,12 @@ int rtpg_sdtree_sample_pdf(rtpg_sdtree* h, int64_t n, const float* pos, const ui
     if (!aligned8(out_uv) || !aligned4(pos)) return fail(RTPG_EINVAL, "rtpg_sdtree_sample_pdf: misaligned array");
     if (n == 0) return RTPG_OK;
     // one resident wave: 8 CTAs of 256 per SM (32 registers a thread)
-    k_sample_pdf<<<grid_for(n, kSampleBlock, 8), kSampleBlock, 0, as_stream(stream)>>>(
-        h->dev, n, pos, seeds, seed_base, out_uv, out_pdf_uv, out_dir, out_pdf_dir);
+    if (n <= kMaxIndex32)
+        k_sample_pdf<int32_t><<<grid_for(n, kSampleBlock, 8), kSampleBlock, 0, as_stream(stream)>>>(
+            h->dev, (int32_t)n, pos, seeds, seed_base, out_uv, out_pdf_uv, out_dir, out_pdf_dir);
+    else
+        k_sample_pdf<int64_t><<<grid_for(n, kSampleBlock, 8), kSampleBlock, 0, as_stream(stream)>>>(
+            h->dev, n, pos, seeds, seed_base, out_uv, out_pdf_uv, out_dir, out_pdf_dir);
     RTPG_LAUNCH_CHECK();
     return RTPG_OK;
 }

@@ -38,11 +38,13 @@ struct __align__(32) SNode {
 //         choice is s >= t for the smallest draw t that makes it (+inf when none does); the
 //         draws are the 2^23 values k 2^-23 (rnd1), and t is found by bisecting them with the
 //         same divisions, so the descent decides exactly as the divisions would;
-//   fac_i = 4 s_i / total (the pdf factor of quadrant i);
-//   meta: bits 0-15 the first child, 16-19 which quadrants have a child, 20-23 which have
-//         s_i <= 0 (where DTreeNodeT::Sample / Pdf stop, PG.h:268-300).
+//   fac_i = 4 s_i / total (the pdf factor of quadrant i), 0 where s_i <= 0: there
+//         DTreeNodeT::Sample / Pdf stop with pdf 0 (PG.h:268-300), which the product by 0 gives;
+//   meta: bits 0-15 the first child; bits 16 + 4 i .. 19 + 4 i quadrant i's nibble: bit 0 set
+//         where the descent stops in quadrant i (no child, or s_i <= 0), bits 1-2 the number of
+//         children before quadrant i.
 // The children of a node are consecutive in quadrant order (the reset numbers them so, and
-// so does the import), so child q = first + the number of children before q.
+// so does the import), so child i = first + the number of children before i.
 struct __align__(32) SQNode {
     float bnd, tl, tr;
     uint32_t meta;
@@ -88,27 +90,22 @@ __host__ __device__ inline SQNode make_sqnode(float4 s, ushort4 child) {
     n.bnd = sq_div(partial, total);
     n.tl = sq_threshold(0, n.bnd, sq_div(s.x, partial));
     n.tr = sq_threshold(1, n.bnd, sq_div(s.y, total - partial));
-    n.fac[0] = sq_div(4.0f * s.x, total);
-    n.fac[1] = sq_div(4.0f * s.y, total);
-    n.fac[2] = sq_div(4.0f * s.z, total);
-    n.fac[3] = sq_div(4.0f * s.w, total);
+    const float sq[4] = {s.x, s.y, s.z, s.w};
     const uint32_t c[4] = {child.x, child.y, child.z, child.w};
-    uint32_t first = 0, cmask = 0;
-    for (int q = 3; q >= 0; --q)
-        if (c[q]) {
-            first = c[q];
-            cmask |= 1u << q;
-        }
-    const uint32_t zmask = (s.x <= 0.0f ? 1u : 0u) | (s.y <= 0.0f ? 2u : 0u) | (s.z <= 0.0f ? 4u : 0u) |
-                           (s.w <= 0.0f ? 8u : 0u);
-    n.meta = (first & 0xffffu) | (cmask << 16) | (zmask << 20);
+    uint32_t first = 0, before = 0, nib = 0;
+    for (int q = 0; q < 4; ++q) {
+        n.fac[q] = sq[q] <= 0.0f ? 0.0f : sq_div(4.0f * sq[q], total);
+        if (c[q] && !first) first = c[q];
+        nib |= ((!c[q] || sq[q] <= 0.0f ? 1u : 0u) | (before << 1)) << (4 * q);
+        if (c[q]) ++before;
+    }
+    n.meta = (first & 0xffffu) | (nib << 16);
     return n;
 }
-// child of quadrant idx (0 = none) of a node with the given meta word
-__device__ __forceinline__ uint32_t sq_child(uint32_t meta, int idx) {
-    const uint32_t cm = (meta >> 16) & 0xfu;
-    return ((cm >> idx) & 1u) ? (meta & 0xffffu) + (uint32_t)__popc(cm & ((1u << idx) - 1u)) : 0u;
-}
+// quadrant idx's nibble of a meta word (in its low 4 bits; the bits above are not cleared)
+__device__ __forceinline__ uint32_t sq_nibble(uint32_t meta, uint32_t idx) { return meta >> (16 + 4 * idx); }
+__device__ __forceinline__ bool sq_stops(uint32_t nib) { return (nib & 1u) != 0; }
+__device__ __forceinline__ uint32_t sq_child(uint32_t meta, uint32_t nib) { return (meta & 0xffffu) + ((nib >> 1) & 3u); }
 
 struct SDTreeDev {
     float3 mn, mx;  // cubified AABB
@@ -289,14 +286,10 @@ __device__ __forceinline__ float dtree_pdf_g(const SQNode* __restrict__ nodes, u
         const float4* np = reinterpret_cast<const float4*>(nodes + off + cur);
         const float4 w = np[0], f = np[1];
         const uint32_t meta = __float_as_uint(w.w);
-        if ((meta >> (20 + idx)) & 1u) {  // s_idx <= 0
-            result = 0.0f;
-            break;
-        }
-        result = __fmul_rn(result, sel4(f, idx));
-        const uint32_t c = sq_child(meta, idx);
-        if (!c) break;
-        cur = c;
+        result = __fmul_rn(result, sel4(f, idx));  // 0 where s_idx <= 0
+        const uint32_t nib = sq_nibble(meta, (uint32_t)idx);
+        if (sq_stops(nib)) break;
+        cur = sq_child(meta, nib);
         idx = quad_child(u, v);
     }
     return __fmul_rn(__fmul_rn(result, kInv2Pi), 0.5f);
@@ -339,31 +332,19 @@ __device__ __forceinline__ float2 dtree_sample_sq(const SQNode* __restrict__ nod
         // no load waits for the quadrant choice
         const float4* np = reinterpret_cast<const float4*>(nodes + off + cur);
         const float4 w = np[0], f = np[1];
-        const float bnd = w.x;
         const uint32_t meta = __float_as_uint(w.w);
-        int idx = 0;
-        float ox = 0.0f, oy = 0.0f, threshold;
         const float sample = rnd1(rng);
-        if (sample < bnd) {
-            threshold = w.y;  // tl
-        } else {
-            ox = 0.5f;
-            threshold = w.z;  // tr
-            idx |= 1;
-        }
-        if (sample >= threshold) {
-            oy = 0.5f;
-            idx |= 2;
-        }
-        rx = __fadd_rn(rx, __fmul_rn(size, ox));
-        ry = __fadd_rn(ry, __fmul_rn(size, oy));
-        size = __fmul_rn(size, 0.5f);
-        // the pdf descent's step at this node (DTreeNodeT::Pdf, PG.h:295-300)
-        const bool zero = ((meta >> (20 + idx)) & 1u) != 0;  // s_idx <= 0
-        if (zero) result = 0.0f;
-        else result = __fmul_rn(result, sel4(f, idx));
-        const uint32_t c = sq_child(meta, idx);
-        if (c == 0 || zero) {
+        const bool right = !(sample < w.x);          // quadrant 1 or 3 (bnd)
+        const bool low = sample >= (right ? w.z : w.y);  // quadrant 2 or 3 (tr, tl)
+        // rx + size * ox with ox in {0, 0.5}: size * 0.5 is exact and adding size * 0 keeps rx
+        const float hs = __fmul_rn(size, 0.5f);
+        if (right) rx = __fadd_rn(rx, hs);
+        if (low) ry = __fadd_rn(ry, hs);
+        size = hs;
+        // the pdf descent's step at this node (DTreeNodeT::Pdf, PG.h:295-300): 0 where s <= 0
+        result = __fmul_rn(result, low ? (right ? f.w : f.z) : (right ? f.y : f.x));
+        const uint32_t nib = sq_nibble(meta, (right ? 1u : 0u) | (low ? 2u : 0u));
+        if (sq_stops(nib)) {
             bx = rx;
             by = ry;
             const float a = rnd1(rng);
@@ -372,7 +353,7 @@ __device__ __forceinline__ float2 dtree_sample_sq(const SQNode* __restrict__ nod
             ry = __fadd_rn(ry, __fmul_rn(size, b));
             break;
         }
-        cur = c;
+        cur = sq_child(meta, nib);
     }
     // bx, by and bx + size are dyadic with few bits: the comparisons of holds() are exact
     sq = DSquare{bx, by, size, __fmul_rn(__fmul_rn(result, kInv2Pi), 0.5f)};
