@@ -29,15 +29,15 @@ struct __align__(32) SNode {
 // What a sampling or pdf descent reads of a sampling node (32 B, one sector): the quotients of
 // the quadrant sums that DTreeNodeT::Sample and ::Pdf (PG.h:229-320) divide out at every visit,
 // formed once when the node is written, with the same IEEE operations on the same operands, so
-// that a descent reads them instead of dividing (bit-identical results):
-//   bnd = partial / total with partial = s0 + s2 and total = ((s0 + s1) + s2) + s3;
-//   tl, tr: the second choice as a threshold on the drawn sample itself.  Sample divides the
-//         draw s out (s / bnd left of bnd, (s - bnd) / (1 - bnd) right of it) and takes
-//         quadrant 2 (3) when the quotient is >= topLeft / partial (topRight / (total - partial)).
-//         Both quotients are non-decreasing in s wherever that side can be reached, so the
-//         choice is s >= t for the smallest draw t that makes it (+inf when none does); the
-//         draws are the 2^23 values k 2^-23 (rnd1), and t is found by bisecting them with the
-//         same divisions, so the descent decides exactly as the divisions would;
+// that a descent reads them instead of dividing (bit-identical results).  A draw of rnd1 is
+// s = k 2^-23 for the integer k = (next state) >> 9 < 2^23, and both choices of Sample are
+// non-decreasing in s where they can be reached, so each is k >= K for the smallest K that
+// makes it (kNever when none does), found by bisecting the 2^23 draws with the divisions
+// themselves; the descent compares integers and decides exactly as the divisions would:
+//   kb:       s >= bnd, bnd = partial / total, partial = s0 + s2, total = ((s0 + s1) + s2) + s3
+//             (quadrant 1 or 3);
+//   ktl, ktr: left of bnd, s / bnd >= topLeft / partial; right of it,
+//             (s - bnd) / (1 - bnd) >= topRight / (total - partial) (quadrant 2 or 3);
 //   fac_i = 4 s_i / total (the pdf factor of quadrant i), 0 where s_i <= 0: there
 //         DTreeNodeT::Sample / Pdf stop with pdf 0 (PG.h:268-300), which the product by 0 gives;
 //   meta: bits 0-15 the first child; bits 16 + 4 i .. 19 + 4 i quadrant i's nibble: bit 0 set
@@ -46,7 +46,7 @@ struct __align__(32) SNode {
 // The children of a node are consecutive in quadrant order (the reset numbers them so, and
 // so does the import), so child i = first + the number of children before i.
 struct __align__(32) SQNode {
-    float bnd, tl, tr;
+    uint32_t kb, ktl, ktr;
     uint32_t meta;
     float fac[4];
 };
@@ -65,31 +65,35 @@ __host__ __device__ inline float sq_sub(float a, float b) {
 #endif
 }
 constexpr uint32_t kDrawSteps = 1u << 23;  // rnd1 draws k 2^-23, k < 2^23
+constexpr uint32_t kNever = kDrawSteps;      // a threshold no draw reaches
 __host__ __device__ inline float draw_value(uint32_t k) { return (float)k * 0x1p-23f; }
-// the vertical choice of Sample on the left (side 0) or right (side 1) of bnd for draw s
-__host__ __device__ inline bool sq_lower(int side, float s, float bnd, float b) {
-    const float q = side == 0 ? sq_div(s, bnd) : sq_div(sq_sub(s, bnd), sq_sub(1.0f, bnd));
+// Sample's choices for draw s: side 0 the first (s >= bnd), side 1 (2) the second left (right)
+// of bnd against b = topLeft / partial (topRight / (total - partial))
+__host__ __device__ inline bool sq_choice(int side, float s, float bnd, float b) {
+    if (side == 0) return !(s < bnd);
+    const float q = side == 1 ? sq_div(s, bnd) : sq_div(sq_sub(s, bnd), sq_sub(1.0f, bnd));
     return q >= b;
 }
-// the smallest draw for which sq_lower holds, +inf when none does (bisection over the draws;
-// sq_lower is non-decreasing in s where that side is reachable)
-__host__ __device__ inline float sq_threshold(int side, float bnd, float b) {
+// the smallest k for which sq_choice holds at draw k 2^-23, kNever when none does (bisection
+// over the draws; sq_choice is non-decreasing in s where that side is reachable)
+__host__ __device__ inline uint32_t sq_threshold(int side, float bnd, float b) {
     uint32_t lo = 0, hi = kDrawSteps - 1;
-    if (!sq_lower(side, draw_value(hi), bnd, b)) return INFINITY;
+    if (!sq_choice(side, draw_value(hi), bnd, b)) return kNever;
     while (lo < hi) {
         const uint32_t mid = (lo + hi) >> 1;
-        if (sq_lower(side, draw_value(mid), bnd, b)) hi = mid;
+        if (sq_choice(side, draw_value(mid), bnd, b)) hi = mid;
         else lo = mid + 1;
     }
-    return draw_value(lo);
+    return lo;
 }
 __host__ __device__ inline SQNode make_sqnode(float4 s, ushort4 child) {
     SQNode n;
     const float partial = s.x + s.z;
     const float total = ((s.x + s.y) + s.z) + s.w;
-    n.bnd = sq_div(partial, total);
-    n.tl = sq_threshold(0, n.bnd, sq_div(s.x, partial));
-    n.tr = sq_threshold(1, n.bnd, sq_div(s.y, total - partial));
+    const float bnd = sq_div(partial, total);
+    n.kb = sq_threshold(0, bnd, 0.0f);
+    n.ktl = sq_threshold(1, bnd, sq_div(s.x, partial));
+    n.ktr = sq_threshold(2, bnd, sq_div(s.y, total - partial));
     const float sq[4] = {s.x, s.y, s.z, s.w};
     const uint32_t c[4] = {child.x, child.y, child.z, child.w};
     uint32_t first = 0, before = 0, nib = 0;
@@ -330,12 +334,12 @@ __device__ __forceinline__ float2 dtree_sample_sq(const SQNode* __restrict__ nod
     for (;;) {
         // boundaries and meta word, and the pdf factors: two independent 16-byte loads, so that
         // no load waits for the quadrant choice
-        const float4* np = reinterpret_cast<const float4*>(nodes + off + cur);
-        const float4 w = np[0], f = np[1];
-        const uint32_t meta = __float_as_uint(w.w);
-        const float sample = rnd1(rng);
-        const bool right = !(sample < w.x);          // quadrant 1 or 3 (bnd)
-        const bool low = sample >= (right ? w.z : w.y);  // quadrant 2 or 3 (tr, tl)
+        const uint4 w = reinterpret_cast<const uint4*>(nodes + off + cur)[0];
+        const float4 f = reinterpret_cast<const float4*>(nodes + off + cur)[1];
+        const uint32_t meta = w.w;
+        const uint32_t k = xs32_next(rng) >> 9;     // rnd1's draw, k 2^-23
+        const bool right = k >= w.x;                // quadrant 1 or 3 (kb)
+        const bool low = k >= (right ? w.z : w.y);  // quadrant 2 or 3 (ktr, ktl)
         // rx + size * ox with ox in {0, 0.5}: size * 0.5 is exact and adding size * 0 keeps rx
         const float hs = __fmul_rn(size, 0.5f);
         if (right) rx = __fadd_rn(rx, hs);
