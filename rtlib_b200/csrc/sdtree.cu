@@ -41,7 +41,7 @@ __global__ void k_clear(SDTreeDev t) {
         z.child = make_ushort4(0, 0, 0, 0);
         z.pad0 = z.pad1 = 0;
         t.s_nodes[0] = z;
-        t.s_q[0] = make_sqnode(z.sums, z.child);
+        t.s_q[0] = make_sqnode(z.sums, z.child, t.s_fac[0]);
     }
 }
 
@@ -197,7 +197,7 @@ __global__ void __launch_bounds__(kTreeBlock) k_build(SDTreeDev t) {
                 nd.child = c;
                 nd.pad0 = nd.pad1 = 0;
                 t.s_nodes[off + j] = nd;
-                t.s_q[off + j] = make_sqnode(nd.sums, c);
+                t.s_q[off + j] = make_sqnode(nd.sums, c, t.s_fac[off + j]);
             }
             __syncthreads();
         }
@@ -504,9 +504,9 @@ __global__ void __launch_bounds__(kSampleBlock, 8) k_sample_pdf(SDTreeDev t, I n
         const uint32_t off = t.s_off[d];
         const bool guided = t.s_guided[d] != 0;
         DSquare sq;
-        const float2 uv = dtree_sample_sq(t.s_q, off, guided, rng, sq);
+        const float2 uv = dtree_sample_sq(t.s_q, t.s_fac, off, guided, rng, sq);
         if (out_uv) reinterpret_cast<float2*>(out_uv)[i] = uv;
-        if (out_pdf_uv) out_pdf_uv[i] = dtree_pdf_in(t.s_q, off, guided, sq, uv.x, uv.y);
+        if (out_pdf_uv) out_pdf_uv[i] = dtree_pdf_in(t.s_q, t.s_fac, off, guided, sq, uv.x, uv.y);
         if (out_dir || out_pdf_dir) {
             const float3 dv = normalize3(canonical_to_dir(uv.x, uv.y));
             if (out_dir) {
@@ -516,7 +516,7 @@ __global__ void __launch_bounds__(kSampleBlock, 8) k_sample_pdf(SDTreeDev t, I n
             }
             if (out_pdf_dir) {
                 const float2 c = dir_to_canonical(dv.x, dv.y, dv.z);
-                out_pdf_dir[i] = dtree_pdf_in(t.s_q, off, guided, sq, c.x, c.y);
+                out_pdf_dir[i] = dtree_pdf_in(t.s_q, t.s_fac, off, guided, sq, c.x, c.y);
             }
         }
     }
@@ -530,7 +530,7 @@ __global__ void __launch_bounds__(256) k_pdf(SDTreeDev t, int64_t n, const float
         float2 c;
         if (canonical) c = reinterpret_cast<const float2*>(dir)[i];
         else c = dir_to_canonical(dir[3 * i], dir[3 * i + 1], dir[3 * i + 2]);
-        out[i] = dtree_pdf_g(t.s_q, t.s_off[d], t.s_guided[d] != 0, c.x, c.y);
+        out[i] = dtree_pdf_g(t.s_q, t.s_fac, t.s_off[d], t.s_guided[d] != 0, c.x, c.y);
     }
 }
 
@@ -647,7 +647,7 @@ int rtpg_sdtree_create(const float* aabb_min, const float* aabb_max, uint32_t ma
         (r = h->alloc(&t.s_area, nd)) || (r = h->alloc(&t.s_statw, nd)) || (r = h->alloc(&t.s_guided, nd)) ||
         (r = h->alloc(&t.b_lvl, nd * (kMaxLevels + 1))) || (r = h->alloc(&t.b_nlvl, nd)) ||
         (r = h->alloc(&t.b_sums, nn * 4)) || (r = h->alloc(&t.b_child, nn)) || (r = h->alloc(&t.b_area, nn)) ||
-        (r = h->alloc(&t.s_nodes, nn)) || (r = h->alloc(&t.s_q, nn)) || (r = h->alloc(&h->cnt_s, ns)) || (r = h->alloc(&h->off_s, ns)) ||
+        (r = h->alloc(&t.s_nodes, nn)) || (r = h->alloc(&t.s_q, nn)) || (r = h->alloc(&t.s_fac, nn)) || (r = h->alloc(&h->cnt_s, ns)) || (r = h->alloc(&h->off_s, ns)) ||
         (r = h->alloc(&h->cnt_d, ns)) || (r = h->alloc(&h->off_d, ns)) || (r = h->alloc(&h->ksplit, ns)) ||
         (r = h->alloc(&h->node_cnt, nd)) || (r = h->alloc(&h->node_off, nd)) ||
         (r = h->alloc(&h->partials, 2 * scan_partials_words(std::max(c.max_stree_nodes, c.max_dtrees)))) ||
@@ -1081,6 +1081,7 @@ extern "C" int rtpg_sdtree_import(rtpg_sdtree* h, int64_t stree_nodes, int64_t l
     std::vector<ushort4> b_child;
     std::vector<SNode> s_nodes;
     std::vector<SQNode> s_q;
+    std::vector<float4> s_fac;
     const float scale = t.fx.scale;
     auto fx = [&](float v, unsigned long long& out) -> bool {
         const float s = v * scale;
@@ -1146,7 +1147,9 @@ extern "C" int rtpg_sdtree_import(rtpg_sdtree* h, int64_t stree_nodes, int64_t l
             nd.child = make_ushort4(c[0], c[1], c[2], c[3]);
             nd.pad0 = nd.pad1 = 0;
             s_nodes.push_back(nd);
-            s_q.push_back(make_sqnode(nd.sums, nd.child));
+            float4 fac;
+            s_q.push_back(make_sqnode(nd.sums, nd.child, fac));
+            s_fac.push_back(fac);
         }
     }
     if (bpos != building_nodes || spos != sampling_nodes)
@@ -1173,6 +1176,7 @@ extern "C" int rtpg_sdtree_import(rtpg_sdtree* h, int64_t stree_nodes, int64_t l
     RTPG_CUDA(ul(t.b_child, b_child, st));
     RTPG_CUDA(ul(t.s_nodes, s_nodes, st));
     RTPG_CUDA(ul(t.s_q, s_q, st));
+    RTPG_CUDA(ul(t.s_fac, s_fac, st));
     k_stree_top<<<1, kTopCells, 0, st>>>(t);
     RTPG_LAUNCH_CHECK();
     // the host vectors must outlive the copies

@@ -26,7 +26,7 @@ struct __align__(32) SNode {
     uint32_t pad0, pad1;
 };
 
-// What a sampling or pdf descent reads of a sampling node (32 B, one sector): the quotients of
+// What a sampling or pdf descent reads of a sampling node: the quotients of
 // the quadrant sums that DTreeNodeT::Sample and ::Pdf (PG.h:229-320) divide out at every visit,
 // formed once when the node is written, with the same IEEE operations on the same operands, so
 // that a descent reads them instead of dividing (bit-identical results).  A draw of rnd1 is
@@ -39,16 +39,18 @@ struct __align__(32) SNode {
 //   ktl, ktr: left of bnd, s / bnd >= topLeft / partial; right of it,
 //             (s - bnd) / (1 - bnd) >= topRight / (total - partial) (quadrant 2 or 3);
 //   fac_i = 4 s_i / total (the pdf factor of quadrant i), 0 where s_i <= 0: there
-//         DTreeNodeT::Sample / Pdf stop with pdf 0 (PG.h:268-300), which the product by 0 gives;
+//         DTreeNodeT::Sample / Pdf stop with pdf 0 (PG.h:268-300), which the product by 0 gives.
+//         The factors sit in an array of their own (one float4 per node): the dependent chain
+//         of a descent (node -> choice -> child) reads only the 16-byte SQNode, half the
+//         footprint in L1, and the factor it multiplies is a load off that chain;
 //   meta: bits 0-15 the first child; bits 16 + 4 i .. 19 + 4 i quadrant i's nibble: bit 0 set
 //         where the descent stops in quadrant i (no child, or s_i <= 0), bits 1-2 the number of
 //         children before quadrant i.
 // The children of a node are consecutive in quadrant order (the reset numbers them so, and
 // so does the import), so child i = first + the number of children before i.
-struct __align__(32) SQNode {
+struct __align__(16) SQNode {
     uint32_t kb, ktl, ktr;
     uint32_t meta;
-    float fac[4];
 };
 __host__ __device__ inline float sq_div(float a, float b) {
 #ifdef __CUDA_ARCH__
@@ -86,7 +88,7 @@ __host__ __device__ inline uint32_t sq_threshold(int side, float bnd, float b) {
     }
     return lo;
 }
-__host__ __device__ inline SQNode make_sqnode(float4 s, ushort4 child) {
+__host__ __device__ inline SQNode make_sqnode(float4 s, ushort4 child, float4& fac) {
     SQNode n;
     const float partial = s.x + s.z;
     const float total = ((s.x + s.y) + s.z) + s.w;
@@ -98,7 +100,7 @@ __host__ __device__ inline SQNode make_sqnode(float4 s, ushort4 child) {
     const uint32_t c[4] = {child.x, child.y, child.z, child.w};
     uint32_t first = 0, before = 0, nib = 0;
     for (int q = 0; q < 4; ++q) {
-        n.fac[q] = sq[q] <= 0.0f ? 0.0f : sq_div(4.0f * sq[q], total);
+        (&fac.x)[q] = sq[q] <= 0.0f ? 0.0f : sq_div(4.0f * sq[q], total);
         if (c[q] && !first) first = c[q];
         nib |= ((!c[q] || sq[q] <= 0.0f ? 1u : 0u) | (before << 1)) << (4 * q);
         if (c[q]) ++before;
@@ -136,7 +138,8 @@ struct SDTreeDev {
     ushort4* b_child;
     float* b_area;  // per building node, scratch of the build
     SNode* s_nodes;
-    SQNode* s_q;  // per sampling node, what the descents read
+    SQNode* s_q;    // per sampling node, what the descents read
+    float4* s_fac;  // per sampling node, the pdf factors of its quadrants
     uint32_t cap_snodes, cap_dtrees, cap_nodes;
     uint32_t max_depth;
     float fraction;
@@ -278,19 +281,16 @@ __device__ __forceinline__ float dtree_mean(float statw, float sum) {
 }
 
 // DTreeT::Pdf (PG.h:485-490) -> DTreeNodeT::Pdf (PG.h:279-320), with the factors 4 s_i / total
-// precomputed in the node (SQNode); the last division by 2 is the exact product by 0.5
-__device__ __forceinline__ float dtree_pdf_g(const SQNode* __restrict__ nodes, uint32_t off, bool guided, float u,
-                                             float v) {
+// precomputed per node; the last division by 2 is the exact product by 0.5
+__device__ __forceinline__ float dtree_pdf_g(const SQNode* __restrict__ nodes, const float4* __restrict__ facs,
+                                             uint32_t off, bool guided, float u, float v) {
     if (!guided) return __fmul_rn(__fmul_rn(1.0f, kInv2Pi), 0.5f);
     float result = 1.0f;
     uint32_t cur = 0;
     int idx = quad_child(u, v);
     for (;;) {
-        // both halves of the node in two independent 16-byte loads
-        const float4* np = reinterpret_cast<const float4*>(nodes + off + cur);
-        const float4 w = np[0], f = np[1];
-        const uint32_t meta = __float_as_uint(w.w);
-        result = __fmul_rn(result, sel4(f, idx));  // 0 where s_idx <= 0
+        const uint32_t meta = nodes[off + cur].meta;
+        result = __fmul_rn(result, (&facs[off + cur].x)[idx]);  // 0 where s_idx <= 0
         const uint32_t nib = sq_nibble(meta, (uint32_t)idx);
         if (sq_stops(nib)) break;
         cur = sq_child(meta, nib);
@@ -308,9 +308,9 @@ struct DSquare {
 
 // dtree_pdf_g at (u, v) when the point lies in the square sampling stopped in, else the full
 // descent: equal to dtree_pdf_g(nodes, off, guided, u, v) bit for bit either way.
-__device__ __forceinline__ float dtree_pdf_in(const SQNode* __restrict__ nodes, uint32_t off, bool guided,
-                                              const DSquare& sq, float u, float v) {
-    return sq.holds(u, v) ? sq.pdf : dtree_pdf_g(nodes, off, guided, u, v);
+__device__ __forceinline__ float dtree_pdf_in(const SQNode* __restrict__ nodes, const float4* __restrict__ facs,
+                                              uint32_t off, bool guided, const DSquare& sq, float u, float v) {
+    return sq.holds(u, v) ? sq.pdf : dtree_pdf_g(nodes, facs, off, guided, u, v);
 }
 
 // DTreeT::Sample (PG.h:478-484) -> DTreeNodeT::Sample (PG.h:229-277), float order as written;
@@ -320,8 +320,8 @@ __device__ __forceinline__ float dtree_pdf_in(const SQNode* __restrict__ nodes, 
 // sampling stopped it visits exactly the nodes sampling visited, with the same quadrant sums
 // and so the same precomputed factors 4 s_i / total.  `sq` returns that square and
 // pdf (uniform sampling: the unit square, whose pdf is constant).
-__device__ __forceinline__ float2 dtree_sample_sq(const SQNode* __restrict__ nodes, uint32_t off, bool guided,
-                                                  uint32_t& rng, DSquare& sq) {
+__device__ __forceinline__ float2 dtree_sample_sq(const SQNode* __restrict__ nodes, const float4* __restrict__ facs,
+                                                  uint32_t off, bool guided, uint32_t& rng, DSquare& sq) {
     if (!guided) {
         const float a = rnd1(rng);
         const float b = rnd1(rng);
@@ -332,10 +332,9 @@ __device__ __forceinline__ float2 dtree_sample_sq(const SQNode* __restrict__ nod
     float rx = 0.0f, ry = 0.0f, size = 1.0f, result = 1.0f;
     float bx = 0.0f, by = 0.0f;  // corner of the square where the descent stopped
     for (;;) {
-        // boundaries and meta word, and the pdf factors: two independent 16-byte loads, so that
-        // no load waits for the quadrant choice
-        const uint4 w = reinterpret_cast<const uint4*>(nodes + off + cur)[0];
-        const float4 f = reinterpret_cast<const float4*>(nodes + off + cur)[1];
+        // thresholds and meta word in one 16-byte load; the factors load beside it, off the chain
+        const uint4 w = *reinterpret_cast<const uint4*>(nodes + off + cur);
+        const float4 f = facs[off + cur];
         const uint32_t meta = w.w;
         const uint32_t k = xs32_next(rng) >> 9;     // rnd1's draw, k 2^-23
         const bool right = k >= w.x;                // quadrant 1 or 3 (kb)

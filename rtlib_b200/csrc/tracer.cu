@@ -284,7 +284,7 @@ __device__ __forceinline__ bool bounce_path(const TracerDev& T, uint32_t p, bool
             // through the full descent
             DSquare sq{2.0f, 2.0f, 0.0f, 0.0f};
             if (rnd1(rng) < T.tree.fraction) {
-                const float2 c = dtree_sample_sq(T.tree.s_q, soff, guided, rng, sq);
+                const float2 c = dtree_sample_sq(T.tree.s_q, T.tree.s_fac, soff, guided, rng, sq);
                 direction = normalize3(canonical_to_dir(c.x, c.y));
                 cosine = dot3(direction, fn);
                 const float cp2 = fmaxf(cosine * kInvPi, 0.0f);
@@ -295,7 +295,7 @@ __device__ __forceinline__ bool bounce_path(const TracerDev& T, uint32_t p, bool
             const float2 c = dir_to_canonical(direction.x, direction.y, direction.z);
             cdir = c;
             have_c = true;
-            const float dtree_pdf = fmaxf(dtree_pdf_in(T.tree.s_q, soff, guided, sq, c.x, c.y), 0.0f);
+            const float dtree_pdf = fmaxf(dtree_pdf_in(T.tree.s_q, T.tree.s_fac, soff, guided, sq, c.x, c.y), 0.0f);
             wo_pdf = (1.0f - T.tree.fraction) * bsdf_pdf + T.tree.fraction * dtree_pdf;
         } else if (use_mlp && build) {
             // the learned mixture of this path's hit (k_mlp_lobes)
@@ -328,7 +328,7 @@ __device__ __forceinline__ bool bounce_path(const TracerDev& T, uint32_t p, bool
                     const float u2 = rnd1(rng);
                     direction = normalize3(vmf_mixture_sample(Lb, u0, u1, u2));
                 } else {
-                    const float2 c = dtree_sample_sq(T.tree.s_q, soff, tguided, rng, sq);
+                    const float2 c = dtree_sample_sq(T.tree.s_q, T.tree.s_fac, soff, tguided, rng, sq);
                     direction = normalize3(canonical_to_dir(c.x, c.y));
                 }
                 cosine = dot3(direction, fn);
@@ -342,7 +342,7 @@ __device__ __forceinline__ bool bounce_path(const TracerDev& T, uint32_t p, bool
                 const float2 c = dir_to_canonical(direction.x, direction.y, direction.z);
                 cdir = c;
                 have_c = true;
-                const float qt = fmaxf(dtree_pdf_in(T.tree.s_q, soff, tguided, sq, c.x, c.y), 0.0f);
+                const float qt = fmaxf(dtree_pdf_in(T.tree.s_q, T.tree.s_fac, soff, tguided, sq, c.x, c.y), 0.0f);
                 q = T.mlp_share * q + (1.0f - T.mlp_share) * qt;
             }
             wo_pdf = (1.0f - T.mlp_fraction) * bsdf_pdf + T.mlp_fraction * q;
