@@ -284,6 +284,7 @@ def bench_sdtree_ours(args, rank, world):
         "clocks": clk,
         "gpu_launches": (LAUNCHES_PER_STEP + (args.passes - 1) * 21) * args.steps,
         "sdtree": st,
+        "roofline_issue": _issue_roofline_sample(s_ms, clk),
         "roofline_record": {"kernel": "k_record (with clear)", "bound": "L2 atomics", "unit": "GB/s",
                             "achieved": REC_BYTES * N_REC / (statistics.mean(record_ms) * 1e-3) / 1e9,
                             "peak": peak, "frac": REC_BYTES * N_REC / (statistics.mean(record_ms) * 1e-3) / 1e9 / peak,
@@ -364,7 +365,8 @@ def sdtree_subrecord(args, rank, world):
            "ms_per_step": r["ms_per_step"],
            "config": {"workload": "sdtree-standalone: 2^20 records, refine at 12000*sqrt(2), 2^22 sample+pdf",
                       "records": N_REC, "queries": N_Q, "l2": "flushed (256 MiB write) before every timed step"},
-           "e2e": dict(r["e2e"], steps=sub.e2e_steps), "roofline": r["roofline"], "roofline_record": r["roofline_record"],
+           "e2e": dict(r["e2e"], steps=sub.e2e_steps), "roofline": r["roofline"], "roofline_issue": r["roofline_issue"],
+           "roofline_record": r["roofline_record"],
            "phases": r["phases"], "clocks": r["clocks"], "gpu_launches": r["gpu_launches"], "sdtree": r["sdtree"]}
     if rank == 0 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline_sdtree()
@@ -416,6 +418,21 @@ def _issue_roofline(path_bounces, bounce_ms, clk):
             "warp_inst_per_path_bounce": ipb, "thread_inst_per_inst": _traffic("k_bounce_thread_inst_per_inst"),
             "peak_source": f"4 schedulers x 148 SMs x {mhz:.0f} MHz (sampled SM clock)",
             "note": "instructions per path-bounce from ncu on the 7-spp case (profiles/k_bounce_commit_cornell_512.md)"}
+
+
+def _issue_roofline_sample(launch_ms, clk):
+    """k_sample_pdf against the issue limit: its warp-instructions per query (ncu, see
+    profiles/traffic.json) times the 2^22 queries over the launch's CUDA-event time."""
+    ipq = _traffic("k_sample_pdf_warp_inst_per_query")
+    if ipq is None:
+        return None
+    mhz = clk.get("sm_mhz") or 1965.0
+    achieved = ipq * N_Q / (launch_ms * 1e-3) / 1e9
+    peak = 4 * 148 * mhz * 1e6 / 1e9
+    return {"kernel": "k_sample_pdf", "bound": "issue", "achieved": achieved, "peak": peak,
+            "unit": "G warp-instructions/s", "frac": achieved / peak, "warp_inst_per_query": ipq,
+            "peak_source": f"4 schedulers x 148 SMs x {mhz:.0f} MHz (sampled SM clock)",
+            "note": "instructions per query from ncu (profiles/k_sample_pdf_record_sdtree_cfg1.md)"}
 
 
 def _recording_launches(budget, iteration_for_built=0):

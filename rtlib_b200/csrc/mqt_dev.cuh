@@ -71,20 +71,16 @@ __device__ __forceinline__ float2 mqt_sample_and_pdf(const MqtDev& t, uint32_t c
         // level offsets (4^l-1)/3 are odd, so the four children are read one by one
         const float* qp = w + offset + (code << 2);
         const float4 q = make_float4(qp[0], qp[1], qp[2], qp[3]);
-        uint32_t cl = 0;
-        float partial = __fadd_rn(q.x, q.z);
-        float boundary = __fdiv_rn(partial, total);
-        float sample = rnd1(rng);
-        if (sample < boundary) {
-            sample = __fdiv_rn(sample, boundary);
-            boundary = __fdiv_rn(q.x, partial);
-        } else {
-            partial = __fadd_rn(q.y, q.w);
-            sample = __fdiv_rn(__fsub_rn(sample, boundary), __fsub_rn(1.0f, boundary));
-            boundary = __fdiv_rn(q.y, partial);
-            cl |= 1;
-        }
-        if (sample >= boundary) cl |= 2;
+        // both sides of the first choice as selects of their operands (the same divisions of
+        // the same values, without the two divergent branches)
+        const float partial_l = __fadd_rn(q.x, q.z);
+        const float boundary = __fdiv_rn(partial_l, total);
+        const float draw = rnd1(rng);
+        const bool right = !(draw < boundary);
+        const float partial = right ? __fadd_rn(q.y, q.w) : partial_l;
+        const float sample = __fdiv_rn(right ? __fsub_rn(draw, boundary) : draw,
+                                       right ? __fsub_rn(1.0f, boundary) : boundary);
+        const uint32_t cl = (right ? 1u : 0u) | (sample >= __fdiv_rn(right ? q.y : q.x, partial) ? 2u : 0u);
         total = cl == 0 ? q.x : (cl == 1 ? q.y : (cl == 2 ? q.z : q.w));
         code = (code << 2) + cl;
         offset += size;
