@@ -126,6 +126,18 @@ class Oracle:
                                   np.asarray(bounds, np.uint32), nslots, prv, out)
         return out
 
+    # ---- hit queries
+    def intersect(self, tri_v, org, dir, tmin=0.0, tmax=1e20, any_hit=False):
+        """Brute-force closest (or any) hit of each ray over every triangle, in scene order:
+        (t, prim), t = -1 and prim = 0xffffffff for a miss."""
+        tri_v = np.ascontiguousarray(tri_v, np.float32)
+        org, dir = np.ascontiguousarray(org, np.float32), np.ascontiguousarray(dir, np.float32)
+        n = org.shape[0]
+        t, prim = np.empty(n, np.float32), np.empty(n, np.uint32)
+        self.L.or_intersect.argtypes = [_f, C.c_uint32, C.c_int64, _f, _f, C.c_float, C.c_float, C.c_int, _f, _u32]
+        self.L.or_intersect(tri_v, tri_v.reshape(-1, 9).shape[0], n, org, dir, tmin, tmax, int(any_hit), t, prim)
+        return t, prim
+
     def mhash_insert(self, pos, off, size, bounds, nslots, cur):
         pos = np.ascontiguousarray(pos, np.float32)
         out = np.empty(pos.shape[0], np.uint32)
@@ -391,7 +403,7 @@ class _OScene(C.Structure):
                 ("tex_w", C.c_uint32), ("tex_h", C.c_uint32), ("eye", C.c_float * 3), ("cu", C.c_float * 3),
                 ("cv", C.c_float * 3), ("cw", C.c_float * 3), ("bg", C.c_float * 3), ("width", C.c_uint32),
                 ("height", C.c_uint32), ("max_depth", C.c_uint32), ("num_candidates", C.c_uint32),
-                ("fraction", C.c_float)]
+                ("fraction", C.c_float), ("tri_xf", P)]
 
 
 def tracer_seeds(width, height, seed):
@@ -430,6 +442,11 @@ class OracleRenderer:
         k = self.keep
         o.tri_v, o.tri_mat, o.tri_uv = k["tri_v"].ctypes.data, k["tri_mat"].ctypes.data, k["tri_uv"].ctypes.data
         o.ntris = k["tri_v"].shape[0]
+        # the triangles' world -> triangle-frame rows the hit test uses (or_tri_transforms)
+        L.or_tri_transforms.argtypes = [P, C.c_uint32, P]
+        xf = self.keep["tri_xf"] = np.empty((max(o.ntris, 1), 12), np.float32)
+        L.or_tri_transforms(o.tri_v, o.ntris, xf.ctypes.data)
+        o.tri_xf = xf.ctypes.data
         o.mats = C.cast(mats, P)
         o.light_tris, o.light_first = k["light_tris"].ctypes.data, k["light_first"].ctypes.data
         o.light_count, o.light_emit = k["light_count"].ctypes.data, k["light_emission"].ctypes.data

@@ -815,31 +815,57 @@ typedef struct {
     float eye[3], cu[3], cv[3], cw[3], bg[3];
     uint32_t width, height, max_depth, num_candidates;
     float fraction; /* guide/BSDF mixing fraction of the SD-tree (STreeT::fraction) */
+    const float* tri_xf; /* 12 floats per triangle: the rows of or_tri_transforms */
 } OScene;
 
 static V3 tri_vert(const OScene* s, uint32_t t, int k) {
     const float* p = s->tri_v + 9 * (size_t)t + 3 * k;
     return v3(p[0], p[1], p[2]);
 }
-/* Moller-Trumbore, the same operation order as the device test */
+/* The rows of the world -> triangle-frame map of every triangle (Baldwin and Weber, "Fast
+ * Ray-Triangle Intersections by Coordinate Transformation", JCGT 5(3), 2016), as the device's
+ * tri_transform forms them: with e1 = v1 - v0, e2 = v2 - v0, n = e1 x e2, the rows of the
+ * inverse of [e1 e2 n] are (e2 x n, n x e1, n) / |n|^2, translated by -v0; all in double
+ * (rounded as written), then rounded to float.  Row 0 gives u, row 1 v, row 2 the offset along
+ * the normal. */
+void or_tri_transforms(const float* tri_v, uint32_t n, float* out) {
+    for (uint32_t t = 0; t < n; ++t) {
+        const float* v = tri_v + 9 * (size_t)t;
+        const double ax = v[0], ay = v[1], az = v[2];
+        const double e1x = (double)v[3] - ax, e1y = (double)v[4] - ay, e1z = (double)v[5] - az;
+        const double e2x = (double)v[6] - ax, e2y = (double)v[7] - ay, e2z = (double)v[8] - az;
+        const double nx = e1y * e2z - e1z * e2y, ny = e1z * e2x - e1x * e2z, nz = e1x * e2y - e1y * e2x;
+        const double nn = nx * nx + ny * ny + nz * nz;
+        const double m[3][3] = {{e2y * nz - e2z * ny, e2z * nx - e2x * nz, e2x * ny - e2y * nx},
+                                {ny * e1z - nz * e1y, nz * e1x - nx * e1z, nx * e1y - ny * e1x},
+                                {nx, ny, nz}};
+        float* r = out + 12 * (size_t)t;
+        for (int k = 0; k < 3; ++k) {
+            const double w = -(m[k][0] * ax + m[k][1] * ay + m[k][2] * az);
+            r[4 * k] = (float)(m[k][0] / nn);
+            r[4 * k + 1] = (float)(m[k][1] / nn);
+            r[4 * k + 2] = (float)(m[k][2] / nn);
+            r[4 * k + 3] = (float)(w / nn);
+        }
+    }
+}
+/* row . d (no offset) and row . o + offset, as chains of fused multiply-adds */
+static float xf_dir(const float* r, V3 d) { return fmaf(r[0], d.x, fmaf(r[1], d.y, r[2] * d.z)); }
+static float xf_pt(const float* r, V3 o) { return fmaf(r[0], o.x, fmaf(r[1], o.y, fmaf(r[2], o.z, r[3]))); }
+/* Closest (any = 0) or any (any = 1) hit in (tmin, tmax) over every triangle in scene order,
+ * the device's tri_hit: t = -(r2 . o + w2) / (r2 . d) with the correctly rounded reciprocal,
+ * u and v as the point's coordinates plus t times the direction's; the lowest index wins a tie. */
 static int o_trace(const OScene* s, V3 o, V3 d, float tmin, float tmax, int any, float* th, uint32_t* prim, float* hu,
                    float* hv) {
     int hit = 0;
     float best = tmax;
     for (uint32_t t = 0; t < s->ntris; ++t) {
-        V3 v0 = tri_vert(s, t, 0), e1 = vsub(tri_vert(s, t, 1), v0), e2 = vsub(tri_vert(s, t, 2), v0);
-        float px = d.y * e2.z - d.z * e2.y, py = d.z * e2.x - d.x * e2.z, pz = d.x * e2.y - d.y * e2.x;
-        float det = e1.x * px + e1.y * py + e1.z * pz;
-        if (fabsf(det) < 1e-20f) continue;
-        float inv = 1.0f / det;
-        float sx = o.x - v0.x, sy = o.y - v0.y, sz = o.z - v0.z;
-        float u = (sx * px + sy * py + sz * pz) * inv;
-        if (u < 0.0f || u > 1.0f) continue;
-        float qx = sy * e1.z - sz * e1.y, qy = sz * e1.x - sx * e1.z, qz = sx * e1.y - sy * e1.x;
-        float v = (d.x * qx + d.y * qy + d.z * qz) * inv;
-        if (v < 0.0f || u + v > 1.0f) continue;
-        float tt = (e2.x * qx + e2.y * qy + e2.z * qz) * inv;
-        if (tt > tmin && tt < best) {
+        const float* r = s->tri_xf + 12 * (size_t)t;
+        const float den = xf_dir(r + 8, d), num = xf_pt(r + 8, o);
+        const float tt = -num * (1.0f / den);
+        const float u = fmaf(tt, xf_dir(r, d), xf_pt(r, o));
+        const float v = fmaf(tt, xf_dir(r + 4, d), xf_pt(r + 4, o));
+        if (tt > tmin && tt < best && u >= 0.0f && v >= 0.0f && u + v <= 1.0f) {
             best = tt; hit = 1;
             if (th) *th = tt;
             if (prim) *prim = t;
@@ -849,6 +875,26 @@ static int o_trace(const OScene* s, V3 o, V3 d, float tmin, float tmax, int any,
         }
     }
     return hit;
+}
+/* Batched o_trace over a triangle list (the brute-force check of the device hit queries). */
+void or_intersect(const float* tri_v, uint32_t ntris, int64_t n, const float* org, const float* dir, float tmin,
+                  float tmax, int any, float* out_t, uint32_t* out_prim) {
+    OScene s;
+    memset(&s, 0, sizeof(s));
+    float* xf = (float*)malloc(12 * sizeof(float) * (ntris ? ntris : 1));
+    or_tri_transforms(tri_v, ntris, xf);
+    s.tri_v = tri_v;
+    s.ntris = ntris;
+    s.tri_xf = xf;
+    for (int64_t i = 0; i < n; ++i) {
+        float t = -1.0f;
+        uint32_t p = 0xffffffffu;
+        V3 o = v3(org[3 * i], org[3 * i + 1], org[3 * i + 2]), d = v3(dir[3 * i], dir[3 * i + 1], dir[3 * i + 2]);
+        if (!o_trace(&s, o, d, tmin, tmax, any, &t, &p, 0, 0)) { t = -1.0f; p = 0xffffffffu; }
+        out_t[i] = t;
+        out_prim[i] = p;
+    }
+    free(xf);
 }
 typedef struct { V3 t, b, n; } OOnb;
 static OOnb onb(V3 normal) {

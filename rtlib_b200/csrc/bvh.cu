@@ -108,44 +108,42 @@ __global__ void k_scene_hierarchy(const unsigned long long* __restrict__ keys, i
 }
 
 __global__ void k_scene_leaves(const float* __restrict__ v, const uint32_t* __restrict__ idx, uint32_t nt,
-                               const uint32_t* __restrict__ order, BvhTri* __restrict__ tris) {
+                               const uint32_t* __restrict__ order, BvhTri* __restrict__ tris, uint32_t* __restrict__ prim) {
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nt; k += gridDim.x * blockDim.x) {
         const uint32_t p = order[k];
         const uint32_t a = idx[3 * p], b = idx[3 * p + 1], c = idx[3 * p + 2];
-        const float3 v0 = make_float3(v[3 * a], v[3 * a + 1], v[3 * a + 2]);
-        const float3 v1 = make_float3(v[3 * b], v[3 * b + 1], v[3 * b + 2]);
-        const float3 v2 = make_float3(v[3 * c], v[3 * c + 1], v[3 * c + 2]);
-        BvhTri t;
-        t.v0 = make_float4(v0.x, v0.y, v0.z, __uint_as_float(p));
-        t.e1 = make_float4(v1.x - v0.x, v1.y - v0.y, v1.z - v0.z, 0.0f);
-        t.e2 = make_float4(v2.x - v0.x, v2.y - v0.y, v2.z - v0.z, 0.0f);
-        tris[k] = t;
+        float4 r[3];
+        tri_transform(v[3 * a], v[3 * a + 1], v[3 * a + 2], v[3 * b], v[3 * b + 1], v[3 * b + 2], v[3 * c], v[3 * c + 1],
+                      v[3 * c + 2], r);
+        tris[k] = BvhTri{r[0], r[1], r[2]};
+        prim[k] = p;
     }
 }
 
-// the leaves back in scene order (the original index is in v0.w), for small scenes
-__global__ void k_scene_flat(const BvhTri* __restrict__ tris, uint32_t nt, BvhTri* __restrict__ flat) {
-    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nt; k += gridDim.x * blockDim.x)
-        flat[__float_as_uint(tris[k].v0.w)] = tris[k];
+// the leaves back in scene order, for small scenes
+__global__ void k_scene_flat(const BvhTri* __restrict__ tris, const uint32_t* __restrict__ prim, uint32_t nt,
+                             BvhTri* __restrict__ flat) {
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nt; k += gridDim.x * blockDim.x) flat[prim[k]] = tris[k];
 }
 
-__device__ __forceinline__ void tri_box(const BvhTri& t, float* lo, float* hi) {
-    const float v0[3] = {t.v0.x, t.v0.y, t.v0.z};
-    const float e1[3] = {t.e1.x, t.e1.y, t.e1.z};
-    const float e2[3] = {t.e2.x, t.e2.y, t.e2.z};
-    for (int a = 0; a < 3; ++a) {
-        const float p1 = v0[a] + e1[a], p2 = v0[a] + e2[a];
-        // widen by one ulp-ish margin so the box contains the triangle as the hit test sees it
-        lo[a] = fminf(v0[a], fminf(p1, p2));
-        hi[a] = fmaxf(v0[a], fmaxf(p1, p2));
-        const float m = 1e-6f * fmaxf(fabsf(lo[a]), fabsf(hi[a])) + 1e-12f;
-        lo[a] -= m;
-        hi[a] += m;
+// the box of scene triangle p, widened by a relative margin so that it contains the triangle
+// as the hit test sees it
+__device__ __forceinline__ void tri_box(const float* __restrict__ v, const uint32_t* __restrict__ idx, uint32_t p,
+                                        float* lo, float* hi) {
+    const uint32_t a = idx[3 * p], b = idx[3 * p + 1], c = idx[3 * p + 2];
+    for (int k = 0; k < 3; ++k) {
+        const float x0 = v[3 * a + k], x1 = v[3 * b + k], x2 = v[3 * c + k];
+        lo[k] = fminf(x0, fminf(x1, x2));
+        hi[k] = fmaxf(x0, fmaxf(x1, x2));
+        const float m = 1e-6f * fmaxf(fabsf(lo[k]), fabsf(hi[k])) + 1e-12f;
+        lo[k] -= m;
+        hi[k] += m;
     }
 }
 
 // bottom-up boxes: the second thread to reach an interior node merges its children
-__global__ void k_scene_boxes(const BvhTri* __restrict__ tris, uint32_t nt, BvhNode* nodes, const uint32_t* parent_i,
+__global__ void k_scene_boxes(const float* __restrict__ v, const uint32_t* __restrict__ idx,
+                              const uint32_t* __restrict__ prim, uint32_t nt, BvhNode* nodes, const uint32_t* parent_i,
                               const uint32_t* parent_l, float4* ibox, unsigned* flags) {
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nt; k += gridDim.x * blockDim.x) {
         uint32_t node = parent_l[k];
@@ -157,7 +155,7 @@ __global__ void k_scene_boxes(const BvhTri* __restrict__ tris, uint32_t nt, BvhN
             for (int c = 0; c < 2; ++c) {
                 const uint32_t ch = nodes[node].child[c];
                 if (ch & kBvhLeafBit) {
-                    tri_box(tris[ch & ~kBvhLeafBit], lo[c], hi[c]);
+                    tri_box(v, idx, prim[ch & ~kBvhLeafBit], lo[c], hi[c]);
                 } else {
                     const float4 a = __ldcg(ibox + 2 * ch), b = __ldcg(ibox + 2 * ch + 1);
                     lo[c][0] = a.x; lo[c][1] = a.y; lo[c][2] = a.z;
@@ -199,6 +197,7 @@ struct rtpg_scene {
     SceneDev dev{};
     BvhNode* nodes = nullptr;
     BvhTri* tris = nullptr;
+    uint32_t* prim = nullptr;
     BvhTri* flat = nullptr;
     std::vector<void*> allocs;
     size_t bytes = 0;
@@ -245,13 +244,14 @@ int rtpg_scene_create(const float* vertices, uint32_t num_vertices, const uint32
     size_t tb = 0;
     cub::DoubleBuffer<unsigned long long> dk(nullptr, nullptr);
     cub::DoubleBuffer<uint32_t> dv(nullptr, nullptr);
-    if ((r = s->alloc(&s->nodes, n > 1 ? n - 1 : 1)) || (r = s->alloc(&s->tris, n)) ||
+    if ((r = s->alloc(&s->nodes, n > 1 ? n - 1 : 1)) || (r = s->alloc(&s->tris, n)) || (r = s->alloc(&s->prim, n)) ||
         (n > 0 && n <= kFlatTris && (r = s->alloc(&s->flat, n)))) {
         delete s;
         return r;
     }
     s->dev.nodes = s->nodes;
     s->dev.tris = s->tris;
+    s->dev.prim = s->prim;
     s->dev.flat = s->flat;
     s->dev.ntris = n;
     if (n == 0) {
@@ -285,12 +285,12 @@ int rtpg_scene_create(const float* vertices, uint32_t num_vertices, const uint32
         if ((e = cub::DeviceRadixSort::SortPairs(nullptr, tb, dk, dv, (int)n, 0, 63, st))) break;
         if ((e = talloc(tb, &temp))) break;
         if ((e = cub::DeviceRadixSort::SortPairs(temp, tb, dk, dv, (int)n, 0, 63, st))) break;
-        k_scene_leaves<<<g, 256, 0, st>>>(vertices, indices, n, dv.Current(), s->tris);
-        if (s->flat) k_scene_flat<<<1, 64, 0, st>>>(s->tris, n, s->flat);
+        k_scene_leaves<<<g, 256, 0, st>>>(vertices, indices, n, dv.Current(), s->tris, s->prim);
+        if (s->flat) k_scene_flat<<<1, 64, 0, st>>>(s->tris, s->prim, n, s->flat);
         if (n > 1) {
             k_scene_hierarchy<<<g, 256, 0, st>>>(dk.Current(), (int)n, s->nodes, pi, pl);
             if ((e = cudaMemsetAsync(flags, 0, 4ull * n, st))) break;
-            k_scene_boxes<<<g, 256, 0, st>>>(s->tris, n, s->nodes, pi, pl, ibox, flags);
+            k_scene_boxes<<<g, 256, 0, st>>>(vertices, indices, s->prim, n, s->nodes, pi, pl, ibox, flags);
         }
         if ((e = cudaGetLastError())) break;
         if ((e = cudaStreamSynchronize(st))) break;

@@ -19,11 +19,34 @@ struct __align__(16) BvhNode {
     uint32_t pad[2];
 };
 
+// A triangle as the affine map of world space onto its own frame (Baldwin and Weber, "Fast
+// Ray-Triangle Intersections by Coordinate Transformation", JCGT 5(3), 2016): a point x has
+// barycentric coordinates u = dot(r0.xyz, x) + r0.w and v = dot(r1.xyz, x) + r1.w, and
+// dot(r2.xyz, x) + r2.w is its offset along the face normal in units of the normal's length.
+// tri_transform forms the rows in double precision from the vertices, once per scene.
 struct __align__(16) BvhTri {
-    float4 v0;  // xyz + original primitive index (as bits) in w
-    float4 e1;  // v1 - v0
-    float4 e2;  // v2 - v0
+    float4 r0, r1, r2;
 };
+
+// The rows of triangle (a, b, c): with e1 = b - a, e2 = c - a, n = e1 x e2, the inverse of the
+// matrix [e1 e2 n] is [e2 x n; n x e1; n] / |n|^2, translated by -a.  Every operation is a
+// double operation rounded as written (the file is built without contraction), then the rows
+// are rounded to float: the CPU restatement forms them the same way, bit for bit.
+__host__ __device__ inline void tri_transform(float ax_, float ay_, float az_, float bx_, float by_, float bz_, float cx_,
+                                              float cy_, float cz_, float4* r) {
+    const double ax = ax_, ay = ay_, az = az_;
+    const double e1x = (double)bx_ - ax, e1y = (double)by_ - ay, e1z = (double)bz_ - az;
+    const double e2x = (double)cx_ - ax, e2y = (double)cy_ - ay, e2z = (double)cz_ - az;
+    const double nx = e1y * e2z - e1z * e2y, ny = e1z * e2x - e1x * e2z, nz = e1x * e2y - e1y * e2x;
+    const double nn = nx * nx + ny * ny + nz * nz;
+    const double m[3][3] = {{e2y * nz - e2z * ny, e2z * nx - e2x * nz, e2x * ny - e2y * nx},
+                            {ny * e1z - nz * e1y, nz * e1x - nx * e1z, nx * e1y - ny * e1x},
+                            {nx, ny, nz}};
+    for (int k = 0; k < 3; ++k) {
+        const double w = -(m[k][0] * ax + m[k][1] * ay + m[k][2] * az);
+        r[k] = make_float4((float)(m[k][0] / nn), (float)(m[k][1] / nn), (float)(m[k][2] / nn), (float)(w / nn));
+    }
+}
 
 // Scenes of at most kFlatTris triangles are also kept as a flat list in their own order and
 // traced by testing every triangle: all lanes of a warp then run the same loop over the same
@@ -34,6 +57,7 @@ constexpr uint32_t kFlatTris = 64;
 struct SceneDev {
     const BvhNode* nodes;  // n - 1 interior nodes (root 0); n == 1: no interior node
     const BvhTri* tris;    // n triangles in leaf order
+    const uint32_t* prim;  // scene index of each leaf
     const BvhTri* flat;    // n <= kFlatTris: the triangles in scene order, else null
     uint32_t ntris;
 };
@@ -59,25 +83,26 @@ __device__ __forceinline__ bool box_hit(float lox, float loy, float loz, float h
     return t0 <= t1;
 }
 
-// Moller-Trumbore; returns t in (tmin, tmax) or a negative value
+// The hit of ray o + t d on triangle tr: the ray meets the triangle's plane at
+// t = -(dot(r2.xyz, o) + r2.w) / dot(r2.xyz, d), where u and v follow as o's coordinates plus
+// t times d's.  Each dot product is a chain of fused multiply-adds and 1 / den the correctly
+// rounded reciprocal, so the CPU restatement (fmaf, 1.0f / den) reproduces every value; the
+// test runs without a branch, as every lane of a warp tests the same triangle.  Returns t in
+// (tmin, tmax) or a negative value (also for a ray parallel to the plane: t is then infinite
+// or NaN).
 __device__ __forceinline__ float tri_hit(const BvhTri& tr, float ox, float oy, float oz, float dx, float dy, float dz,
                                          float tmin, float tmax, float& u, float& v) {
-    const float px = dy * tr.e2.z - dz * tr.e2.y;
-    const float py = dz * tr.e2.x - dx * tr.e2.z;
-    const float pz = dx * tr.e2.y - dy * tr.e2.x;
-    const float det = tr.e1.x * px + tr.e1.y * py + tr.e1.z * pz;
-    if (fabsf(det) < 1e-20f) return -1.0f;
-    const float inv = __frcp_rn(det);  // the correctly rounded 1 / det, without a full division
-    const float sx = ox - tr.v0.x, sy = oy - tr.v0.y, sz = oz - tr.v0.z;
-    u = (sx * px + sy * py + sz * pz) * inv;
-    if (u < 0.0f || u > 1.0f) return -1.0f;
-    const float qx = sy * tr.e1.z - sz * tr.e1.y;
-    const float qy = sz * tr.e1.x - sx * tr.e1.z;
-    const float qz = sx * tr.e1.y - sy * tr.e1.x;
-    v = (dx * qx + dy * qy + dz * qz) * inv;
-    if (v < 0.0f || u + v > 1.0f) return -1.0f;
-    const float t = (tr.e2.x * qx + tr.e2.y * qy + tr.e2.z * qz) * inv;
-    return (t > tmin && t < tmax) ? t : -1.0f;
+    const float den = __fmaf_rn(tr.r2.x, dx, __fmaf_rn(tr.r2.y, dy, __fmul_rn(tr.r2.z, dz)));
+    const float num = __fmaf_rn(tr.r2.x, ox, __fmaf_rn(tr.r2.y, oy, __fmaf_rn(tr.r2.z, oz, tr.r2.w)));
+    const float t = __fmul_rn(-num, __frcp_rn(den));
+    const float ud = __fmaf_rn(tr.r0.x, dx, __fmaf_rn(tr.r0.y, dy, __fmul_rn(tr.r0.z, dz)));
+    const float uo = __fmaf_rn(tr.r0.x, ox, __fmaf_rn(tr.r0.y, oy, __fmaf_rn(tr.r0.z, oz, tr.r0.w)));
+    const float vd = __fmaf_rn(tr.r1.x, dx, __fmaf_rn(tr.r1.y, dy, __fmul_rn(tr.r1.z, dz)));
+    const float vo = __fmaf_rn(tr.r1.x, ox, __fmaf_rn(tr.r1.y, oy, __fmaf_rn(tr.r1.z, oz, tr.r1.w)));
+    u = __fmaf_rn(t, ud, uo);
+    v = __fmaf_rn(t, vd, vo);
+    const bool hit = (t > tmin) & (t < tmax) & (u >= 0.0f) & (v >= 0.0f) & (__fadd_rn(u, v) <= 1.0f);
+    return hit ? t : -1.0f;
 }
 
 // closest hit (ANY = false) or any hit (ANY = true) in (tmin, tmax) by testing every triangle
@@ -134,8 +159,8 @@ __device__ __forceinline__ Hit bvh_trace(const SceneDev& s, float ox, float oy, 
                 h.t = t;
                 h.u = u;
                 h.v = v;
-                h.prim = __float_as_uint(tr.v0.w);
-                if (ANY) return h;
+                h.prim = li;  // the leaf; its scene index is looked up once, at the end
+                if (ANY) break;
             }
         } else {
             const BvhNode nd = s.nodes[cur];
@@ -156,6 +181,7 @@ __device__ __forceinline__ Hit bvh_trace(const SceneDev& s, float ox, float oy, 
         if (sp == 0) break;
         cur = stack[--sp];
     }
+    if (h.prim != 0xffffffffu) h.prim = s.prim[h.prim];
     return h;
 }
 
