@@ -106,10 +106,10 @@ __device__ __forceinline__ float tri_hit(const BvhTri& tr, float ox, float oy, f
 }
 
 // closest hit (ANY = false) or any hit (ANY = true) in (tmin, tmax) by testing every triangle
-// of a small scene, in scene order
+// of a small scene (tris[0, n), in scene order)
 template <bool ANY>
-__device__ __forceinline__ Hit flat_trace(const SceneDev& s, float ox, float oy, float oz, float dx, float dy, float dz,
-                                          float tmin, float tmax) {
+__device__ __forceinline__ Hit flat_trace(const BvhTri* tris, uint32_t n, float ox, float oy, float oz, float dx,
+                                          float dy, float dz, float tmin, float tmax) {
     Hit h;
     h.t = tmax;
     h.prim = 0xffffffffu;
@@ -117,8 +117,8 @@ __device__ __forceinline__ Hit flat_trace(const SceneDev& s, float ox, float oy,
     // unrolled so that the next triangles' loads issue while this one is tested; the hit is
     // still updated in scene order
 #pragma unroll 4
-    for (uint32_t k = 0; k < s.ntris; ++k) {
-        const BvhTri tr = s.flat[k];
+    for (uint32_t k = 0; k < n; ++k) {
+        const BvhTri tr = tris[k];
         float u, v;
         const float t = tri_hit(tr, ox, oy, oz, dx, dy, dz, tmin, h.t, u, v);
         if (t > 0.0f) {
@@ -136,7 +136,7 @@ __device__ __forceinline__ Hit flat_trace(const SceneDev& s, float ox, float oy,
 template <bool ANY>
 __device__ __forceinline__ Hit bvh_trace(const SceneDev& s, float ox, float oy, float oz, float dx, float dy, float dz,
                                          float tmin, float tmax) {
-    if (s.flat) return flat_trace<ANY>(s, ox, oy, oz, dx, dy, dz, tmin, tmax);
+    if (s.flat) return flat_trace<ANY>(s.flat, s.ntris, ox, oy, oz, dx, dy, dz, tmin, tmax);
     Hit h;
     h.t = tmax;
     h.prim = 0xffffffffu;

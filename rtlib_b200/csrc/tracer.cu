@@ -99,7 +99,21 @@ struct TracerDev {
     float4* hit_tuv;
     __half* lobes;  // 40 per path: 8 x (mu xyz, kappa, weight)
     float3 *v_nrm, *v_wo;
+    // A scene of at most kFlatTris triangles travels inside the kernel parameters: every lane
+    // tests the same triangle at the same time, so its rows are read from the constant bank
+    // with no load instruction, no load latency and no vector registers holding them.
+    uint32_t nflat;  // 0: trace through the BVH
+    BvhTri ftri[kFlatTris];
 };
+
+// closest hit (ANY = false) or any hit (ANY = true) in (tmin, tmax): the scene's triangles from
+// the kernel parameters when it is small, else the BVH
+template <bool ANY>
+__device__ __forceinline__ Hit trace(const TracerDev& T, float ox, float oy, float oz, float dx, float dy, float dz,
+                                     float tmin, float tmax) {
+    if (T.nflat) return flat_trace<ANY>(T.ftri, T.nflat, ox, oy, oz, dx, dy, dz, tmin, tmax);
+    return bvh_trace<ANY>(T.scene, ox, oy, oz, dx, dy, dz, tmin, tmax);
+}
 
 // ------------------------------------------------------------------ raygen (SimpleGuide.cu:48-81)
 __global__ void __launch_bounds__(kTB) k_raygen(TracerDev T) {
@@ -195,7 +209,7 @@ __device__ __forceinline__ bool bounce_path(const TracerDev& T, uint32_t p, bool
         h.u = tuv.y;
         h.v = tuv.z;
     } else {
-        h = bvh_trace<false>(T.scene, org.x, org.y, org.z, in_dir.x, in_dir.y, in_dir.z, 0.0001f, 1.0e20f);
+        h = trace<false>(T, org.x, org.y, org.z, in_dir.x, in_dir.y, in_dir.z, 0.0001f, 1.0e20f);
     }
     const size_t vi = size_t(d < kTV ? d : 0) * T.npath + p;
     bool pend = false;
@@ -501,7 +515,7 @@ __device__ __forceinline__ bool bounce_path(const TracerDev& T, uint32_t p, bool
     bool lit = false;
     if (pend) {
         shadow = true;
-        const Hit sh = bvh_trace<true>(T.scene, position.x, position.y, position.z, sdir.x, sdir.y, sdir.z, 0.0001f, sdist);
+        const Hit sh = trace<true>(T, position.x, position.y, position.z, sdir.x, sdir.y, sdir.z, 0.0001f, sdist);
         if (sh.prim == 0xffffffffu) {
             L = L + scontrib;
             lit = true;
@@ -545,7 +559,7 @@ __device__ __forceinline__ bool bounce_path(const TracerDev& T, uint32_t p, bool
     if (use_mlp) {
         // the closest hit of the continuing ray, traced here rather than in a pass of its own,
         // so the network of the next bounce finds it waiting (k_hit serves the first bounce)
-        const Hit nh = bvh_trace<false>(T.scene, position.x, position.y, position.z, direction.x, direction.y,
+        const Hit nh = trace<false>(T, position.x, position.y, position.z, direction.x, direction.y,
                                         direction.z, 0.0001f, 1.0e20f);
         T.hit_prim[p] = nh.prim;
         T.hit_tuv[p] = make_float4(nh.t, nh.u, nh.v, 0.0f);
@@ -571,7 +585,7 @@ __global__ void __launch_bounds__(kTB) k_hit(TracerDev T, uint32_t bounce) {
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
         const uint32_t p = T.queue[in][q];
         const float3 o = T.org[p], d = T.dir[p];
-        const Hit h = bvh_trace<false>(T.scene, o.x, o.y, o.z, d.x, d.y, d.z, 0.0001f, 1.0e20f);
+        const Hit h = trace<false>(T, o.x, o.y, o.z, d.x, d.y, d.z, 0.0001f, 1.0e20f);
         T.hit_prim[p] = h.prim;
         T.hit_tuv[p] = make_float4(h.t, h.u, h.v, 0.0f);
     }
@@ -995,6 +1009,16 @@ int rtpg_tracer_create(rtpg_scene* scene, const float* tri_vertices, const uint3
     h->scene = scene;
     TracerDev& T = h->dev;
     T.scene = scene_device_view(scene);
+    T.nflat = 0;
+    if (T.scene.flat && T.scene.ntris <= kFlatTris) {
+        // the scene's triangles (scene order) into the kernel parameters
+        const cudaError_t e = cudaMemcpy(T.ftri, T.scene.flat, sizeof(BvhTri) * T.scene.ntris, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) {
+            delete h;
+            return fail(RTPG_ECUDA, "rtpg_tracer_create: %s", cudaGetErrorString(e));
+        }
+        T.nflat = T.scene.ntris;
+    }
     T.tri_v = tri_vertices;
     T.tri_mat = tri_material;
     T.tri_uv = tri_uv;
