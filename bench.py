@@ -523,7 +523,7 @@ def bench_cornell_ours(args, rank, world):
     achieved = cnt["path_bounces"] * BOUNCE_BYTES / (ext_ms * 1e-3) / 1e9
 
     # e2e: scene from host memory through the C ABI, image back to host
-    e2e_ms = []
+    e2e_ms, e2e_setup_ms = [], []
     h_img = torch.empty((C_H, C_W, 3), dtype=torch.float32).pin_memory()
     h2d = sum(np.asarray(sc[k]).nbytes for k in ("tri_v", "tri_mat", "tri_uv", "light_tris"))
     # one untimed run first; the objects of each run are released (and collected) outside the
@@ -537,12 +537,15 @@ def bench_cornell_ours(args, rank, world):
         tree2 = SDTree(*C_AABB, fraction=C_FRACTION)
         ctrl2 = SDTreeController(tree2, C_BUDGET, iteration_for_built=0, ratio_for_budget=1.0, samples_per_launch=1)
         ctrl2.start()
+        b = torch.cuda.Event(enable_timing=True)
+        b.record(stream)
         tr2.render_guided(tree2, ctrl2, FLAG_NEE, samples_per_launch=1)
         h_img.copy_(tr2.image(), non_blocking=True)
         c.record(stream)
         torch.cuda.synchronize()
         if k > 0:
             e2e_ms.append(a.elapsed_time(c))
+            e2e_setup_ms.append(a.elapsed_time(b))
         del tr2, tree2, ctrl2
         gc.collect()
         torch.cuda.synchronize()
@@ -554,7 +557,10 @@ def bench_cornell_ours(args, rank, world):
         "unit": "Mpaths/s",
         "ms_per_step": ms,
         "e2e": {"value": paths / (e2e * 1e-3) / 1e6, "unit": "Mpaths/s", "h2d_bytes_per_step": int(h2d),
-                "d2h_bytes_per_step": int(h_img.numel() * 4)},
+                "d2h_bytes_per_step": int(h_img.numel() * 4), "ms_per_step": e2e,
+                "setup_ms": sum(e2e_setup_ms) / len(e2e_setup_ms),
+                "note": "setup = scene upload, BVH build, tracer and SD-tree creation; the rest is the render "
+                        "and the image read-back"},
         "roofline": {"kernel": "k_bounce", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs (burst copy)",
                      "traffic": (None if _traffic("k_bounce_bytes_per_path_bounce") is None else
@@ -705,7 +711,10 @@ def bench_occluded_ours(args, rank, world):
     return {
         "metric": "Mpaths/s", "value": paths / (ms * 1e-3) / 1e6, "unit": "Mpaths/s", "ms_per_step": ms,
         "e2e": {"value": paths / (e2e * 1e-3) / 1e6, "unit": "Mpaths/s", "h2d_bytes_per_step": int(h2d),
-                "d2h_bytes_per_step": int(h_img.numel() * 4)},
+                "d2h_bytes_per_step": int(h_img.numel() * 4), "ms_per_step": e2e,
+                "setup_ms": sum(e2e_setup_ms) / len(e2e_setup_ms),
+                "note": "setup = scene upload, BVH build, tracer and SD-tree creation; the rest is the render "
+                        "and the image read-back"},
         "roofline": {"kernel": "k_bounce", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs (burst copy)",
                      "traffic": None if bpb is None else bpb * cnt["path_bounces"] / max(1, O_DEPTH * samples),

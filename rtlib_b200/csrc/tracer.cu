@@ -268,7 +268,9 @@ __device__ __forceinline__ bool bounce_path(const TracerDev& T, uint32_t p, bool
         const float sel = ad / (ad + as);
         // (sel == 1 as well: then the lobe choice and the pdf mixture never use it either)
         const bool glossy = m.specular.x != 0.0f || m.specular.y != 0.0f || m.specular.z != 0.0f || sel != 1.0f;
-        const float3 refl = unit3(reflect3(in_dir, fn));
+        // the mirror direction only enters glossy shading (its normalisation is a square root
+        // and three divisions)
+        const float3 refl = glossy ? unit3(reflect3(in_dir, fn)) : f3(0.f, 0.f, 1.f);
         const float3 d0 = sample_cosine(Onb(xyz(tf.fr[2]), xyz(tf.fr[3]), xyz(tf.fr[1])), rng);
         float3 d1 = d0;
         if (glossy) {
