@@ -720,19 +720,23 @@ __global__ void __launch_bounds__(kTB) k_finish(TracerDev T) {
 
 // The commit of the trace vertices of recording waves (TraceVertexT::Commit,
 // OPX7UtilsPathGuiding.h:830-866 -> DTreeWrapperT::Record :514-520 with stat-weight 1, or
-// MortonTraceVertexT::Commit for the grid guide), one thread per vertex: block row
-// blockIdx.y is the vertex index i, so a warp holds vertex i of 32 consecutive paths and
-// lanes whose path is shorter leave at once.  The radiance of vertex i is
+// MortonTraceVertexT::Commit for the grid guide), one thread per vertex: each CTA walks the
+// vertex rows i = 0 .. kTV-1 over its share of the paths, so a warp holds vertex i of 32
+// consecutive paths and lanes whose path is shorter leave at once.  The radiance of vertex i is
 // L_{i+1} + L_{i+2} + ... added in bounce order, exactly the float sums RTLib's raygen loop
 // accumulates into traceVertices[i].radiance (SimpleGuide.cu:98-100).
-// SD-tree commits go to shared-memory sums of the CTA while the whole building tree is small (the
-// first passes, when every vertex lands in a handful of quadrants), else straight to the tree
-// with 64-bit integer atomics: keys spread over thousands of nodes gain nothing from warp
-// aggregation, whose 64-bit match costs more than the atomic.
+// Every committed vertex adds the same stat-weight to its DTree, a few hundred counters that
+// millions of vertices hit: those adds go to a copy of the counters in the CTA's shared memory
+// (up to kFinPrivTrees DTrees), flushed once per CTA; with kSMs * 2 CTAs of kCommitThreads the
+// flush is a few hundred adds per counter instead of thousands of contended ones.  The
+// quadrant sums go to shared memory too while the whole building tree is small (the first
+// passes), else straight to the tree with 64-bit integer atomics: keys spread over thousands
+// of nodes gain nothing from aggregation.
 constexpr uint32_t kFinPrivQuads = 2048;
-constexpr uint32_t kFinPrivTrees = 512;
+constexpr uint32_t kFinPrivTrees = 2048;
+constexpr int kCommitThreads = 512;
 template <int G>
-__global__ void __launch_bounds__(kTB) k_commit(TracerDev T) {
+__global__ void __launch_bounds__(kCommitThreads) k_commit(TracerDev T) {
     grid_dependency_wait();
     __shared__ unsigned long long s_q[kFinPrivQuads];
     __shared__ unsigned long long s_w[kFinPrivTrees];
@@ -745,13 +749,15 @@ __global__ void __launch_bounds__(kTB) k_commit(TracerDev T) {
         nq = T.tree.counts[2] * 4u;
         ndt = T.tree.counts[1];
     }
-    const bool priv = tree_commit && nq <= kFinPrivQuads && ndt <= kFinPrivTrees;
-    if (priv) {
-        for (uint32_t j = threadIdx.x; j < nq; j += blockDim.x) s_q[j] = 0ull;
+    const bool priv_w = tree_commit && ndt <= kFinPrivTrees;
+    const bool priv = priv_w && nq <= kFinPrivQuads;
+    if (priv_w) {
+        if (priv)
+            for (uint32_t j = threadIdx.x; j < nq; j += blockDim.x) s_q[j] = 0ull;
         for (uint32_t j = threadIdx.x; j < ndt; j += blockDim.x) s_w[j] = 0ull;
         __syncthreads();
     }
-    const uint32_t i = blockIdx.y;  // vertex index
+    for (uint32_t i = 0; i < (uint32_t)kTV; ++i)  // vertex index
     // warp-uniform loop (the grid guide's aggregated atomics need the whole warp)
     for (uint32_t base = blockIdx.x * blockDim.x; base < T.npath; base += gridDim.x * blockDim.x) {
         const uint32_t p = base + threadIdx.x;
@@ -831,14 +837,15 @@ __global__ void __launch_bounds__(kTB) k_commit(TracerDev T) {
         } else if (use_grid) {
             warp_add_u64(k_s, v_s, T.mqt.leaves);
         } else {
-            if (k_w != ~0ull) atomicAdd(priv ? s_w + k_w : T.tree.b_statw + k_w, v_w);
+            if (k_w != ~0ull) atomicAdd(priv_w ? s_w + k_w : T.tree.b_statw + k_w, v_w);
             if (k_s != ~0ull) atomicAdd(priv ? s_q + k_s : T.tree.b_sums + k_s, v_s);
         }
     }
-    if (priv) {
+    if (priv_w) {
         __syncthreads();
-        for (uint32_t j = threadIdx.x; j < nq; j += blockDim.x)
-            if (s_q[j]) atomicAdd(T.tree.b_sums + j, s_q[j]);
+        if (priv)
+            for (uint32_t j = threadIdx.x; j < nq; j += blockDim.x)
+                if (s_q[j]) atomicAdd(T.tree.b_sums + j, s_q[j]);
         for (uint32_t j = threadIdx.x; j < ndt; j += blockDim.x)
             if (s_w[j]) atomicAdd(T.tree.b_statw + j, s_w[j]);
     }
@@ -944,11 +951,11 @@ static void launch_bounce(const TracerDev& T, int g, cudaStream_t st, uint32_t b
 static void launch_finish(const TracerDev& T, int g, cudaStream_t st) {
     (void)launch_dependent(k_finish, g, kTB, 0, st, T);
     if (T.flags & RTPG_TRACE_FLAG_FINAL) return;
-    const dim3 gc(kSMs * 2, kTV);
+    const int gc = kSMs * 2;
     switch (guide_of(T.flags)) {
-        case kGuideTree: (void)launch_dependent(k_commit<kGuideTree>, gc, kTB, 0, st, T); break;
-        case kGuideGrid: (void)launch_dependent(k_commit<kGuideGrid>, gc, kTB, 0, st, T); break;
-        case kGuideMlp: (void)launch_dependent(k_commit<kGuideMlp>, gc, kTB, 0, st, T); break;
+        case kGuideTree: (void)launch_dependent(k_commit<kGuideTree>, gc, kCommitThreads, 0, st, T); break;
+        case kGuideGrid: (void)launch_dependent(k_commit<kGuideGrid>, gc, kCommitThreads, 0, st, T); break;
+        case kGuideMlp: (void)launch_dependent(k_commit<kGuideMlp>, gc, kCommitThreads, 0, st, T); break;
         default: break;
     }
 }
