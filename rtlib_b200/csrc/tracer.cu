@@ -757,8 +757,9 @@ __global__ void __launch_bounds__(kCommitThreads) k_commit(TracerDev T) {
         for (uint32_t j = threadIdx.x; j < ndt; j += blockDim.x) s_w[j] = 0ull;
         __syncthreads();
     }
-    for (uint32_t i = 0; i < (uint32_t)kTV; ++i)  // vertex index
-    // warp-uniform loop (the grid guide's aggregated atomics need the whole warp)
+    // vertex rows outside, paths inside: a warp-uniform loop (the grid guide's aggregated
+    // atomics need the whole warp) over coalesced rows
+    for (uint32_t i = 0; i < (uint32_t)kTV; ++i) {
     for (uint32_t base = blockIdx.x * blockDim.x; base < T.npath; base += gridDim.x * blockDim.x) {
         const uint32_t p = base + threadIdx.x;
         unsigned long long k_w = ~0ull, k_s = ~0ull, v_w = 0, v_s = 0;
@@ -840,6 +841,7 @@ __global__ void __launch_bounds__(kCommitThreads) k_commit(TracerDev T) {
             if (k_w != ~0ull) atomicAdd(priv_w ? s_w + k_w : T.tree.b_statw + k_w, v_w);
             if (k_s != ~0ull) atomicAdd(priv ? s_q + k_s : T.tree.b_sums + k_s, v_s);
         }
+    }
     }
     if (priv_w) {
         __syncthreads();
