@@ -948,8 +948,8 @@ static void launch_bounce(const TracerDev& T, int g, cudaStream_t st, uint32_t b
         default: (void)launch_dependent(k_bounce<kGuideNone>, g, kTB, 0, st, T, b); break;
     }
 }
-// accumulation, then (recording waves of a guide) the commit of the trace vertices, one block
-// row per vertex index
+// accumulation, then (recording waves of a guide) the commit of the trace vertices: two CTAs
+// of kCommitThreads per SM, each walking every vertex row over its share of the paths
 static void launch_finish(const TracerDev& T, int g, cudaStream_t st) {
     (void)launch_dependent(k_finish, g, kTB, 0, st, T);
     if (T.flags & RTPG_TRACE_FLAG_FINAL) return;
