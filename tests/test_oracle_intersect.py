@@ -79,3 +79,26 @@ def test_grazing_and_parallel_rays():
     low = o.copy()
     low[:, 2] = 0.01
     assert _check(tri, low, graze, agree=1.0) > 0.3
+
+
+def test_transform_rows_map_the_vertices():
+    """Rows of or_tri_transforms: v0 -> (u, v) = (0, 0), v1 -> (1, 0), v2 -> (0, 1), every vertex at
+    normal offset 0, and v0 + n at offset 1 (n = e1 x e2)."""
+    import ctypes as C
+    rng = np.random.default_rng(6)
+    tri = rng.normal(size=(64, 3, 3)).astype(np.float32)
+    o = Oracle()
+    xf = np.empty((64, 12), np.float32)
+    o.L.or_tri_transforms.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p]
+    o.L.or_tri_transforms(tri.ctypes.data, 64, xf.ctypes.data)
+    r = xf.reshape(64, 3, 4).astype(np.float64)
+
+    def coords(x):
+        return np.einsum("tkj,tj->tk", r[:, :, :3], x) + r[:, :, 3]
+
+    v0, v1, v2 = (tri[:, k].astype(np.float64) for k in range(3))
+    n = np.cross(v1 - v0, v2 - v0)
+    np.testing.assert_allclose(coords(v0), np.zeros((64, 3)), atol=1e-5)
+    np.testing.assert_allclose(coords(v1), np.tile([1.0, 0.0, 0.0], (64, 1)), atol=1e-5)
+    np.testing.assert_allclose(coords(v2), np.tile([0.0, 1.0, 0.0], (64, 1)), atol=1e-5)
+    np.testing.assert_allclose(coords(v0 + n), np.tile([0.0, 0.0, 1.0], (64, 1)), atol=1e-5)
